@@ -1,0 +1,86 @@
+/*
+ * hacapk_hgen.h -- H-matrix generator and writer (C ABI).
+ *
+ * Builds an H-matrix with HACApK's construction rules for the point kernel
+ * K(i,j) = 1/(4*pi*|p_i - p_j|) (K(i,i) = 1.0) on seeded point clouds, and
+ * writes it in the reference's hmatrix_1.bin / hmatrix_2.bin formats.  It
+ * stands in for the reference's Fortran construction + dump path, which needs
+ * MPI and a Fortran compiler:
+ *
+ *   hgen_build         HACApK_generate (src_hdump/m_HACApK_use.f90:62-166):
+ *                        cluster tree   HACApK_generate_cbitree  (src_hdump/m_HACApK_base.f90:994-1054)
+ *                        bounding boxes HACApK_bndbox            (src_hdump/m_HACApK_base.f90:953-991)
+ *                        block tree     HACApK_generate_leafmtx  (src_hdump/m_HACApK_base.f90:845-891)
+ *                        leaf order     qsort_row/qsort_col      (src_hdump/m_HACApK_base.f90:245-255,893-935)
+ *                        ACA            HACApK_aca               (src_hdump/m_HACApK_base.f90:494-577)
+ *                        leaf fill      HACApK_fill_leafmtx_hyp  (src_hdump/m_HACApK_base.f90:580-662)
+ *   hgen_write_bin1    HACApK_hdump_dump_leafmtx  (src_hdump/m_HACApK_hdump.f90:84-108)
+ *   hgen_write_bin2    HACApK_hdump_dump_leafmtx2 (src_hdump/m_HACApK_hdump.f90:114-180)
+ *
+ * All functions return 0 on success and a negative HGEN_E* code on failure;
+ * none of them exits the process.
+ */
+#ifndef HACAPK_HGEN_H
+#define HACAPK_HGEN_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HGEN_OK 0
+#define HGEN_EINVAL -1
+#define HGEN_ENOMEM -2
+#define HGEN_EIO -3
+#define HGEN_ERANGE -4 /* a count does not fit the file format's int32 fields */
+
+enum hgen_geometry {
+  HGEN_SPHERE = 0,       /* uniform on the unit sphere */
+  HGEN_CUBE_SURFACE = 1, /* uniform on the surface of the unit cube [0,1]^3 */
+  HGEN_PLATE_2X1 = 2     /* uniform on the flat plate [0,2]x[0,1]x{0} */
+};
+
+typedef struct hgen_params {
+  int64_t n;              /* number of points (= matrix order nd) */
+  int32_t geometry;       /* enum hgen_geometry */
+  int32_t leaf_size;      /* param(21): a cluster with <= leaf_size points is a leaf */
+  double eta;             /* param(51): admissibility parameter */
+  double eps;             /* param(71): ACA tolerance */
+  double aca_eps_factor;  /* param(72): ACA_EPS = aca_eps_factor * eps (HACApK default 1e-3) */
+  int32_t kmax;           /* param(63): rank cap per leaf (HACApK default 1000) */
+  int32_t nthreads;       /* <= 0: OpenMP default */
+  uint64_t seed;          /* point-cloud seed */
+} hgen_params;
+
+/* The generated matrix: the SoA view of src_hmvm/src_cpp/hacapk.h:23-36 with
+ * 64-bit element offsets (a1/a2/len), plus the construction by-products. */
+typedef struct hgen_hmatrix {
+  int32_t nd, nlf, ktmax, _pad0;
+  int64_t len;
+  int32_t *ltmtx, *kt, *ndl, *ndt, *nstrtl, *nstrtt; /* [nlf]; nstrtl/nstrtt are 1-based */
+  int64_t *a1, *a2;                                  /* [nlf] element offsets into rowmat */
+  double *rowmat;                                    /* [len] leaf data, file order */
+  int32_t *lod;       /* [nd] permutation: position (0-based) -> original point (1-based) */
+  double *coords;     /* [nd*3] original points, xyz interleaved */
+  int64_t n_lowrank, n_dense;
+  int64_t aca_incomplete; /* leaves where HACApK would have stopped (m_HACApK_base.f90:565-575) */
+} hgen_hmatrix;
+
+void hgen_default_params(hgen_params* p);
+int hgen_build(const hgen_params* p, hgen_hmatrix** out);
+void hgen_free(hgen_hmatrix* m);
+
+/* Writers.  bin2's int32 `len` header field is written saturated at INT32_MAX
+ * when the element count does not fit. */
+int hgen_write_bin1(const hgen_hmatrix* m, const char* fname);
+int hgen_write_bin2(const hgen_hmatrix* m, const char* fname);
+
+/* Exact entry of the permuted matrix, row/col 1-based positions (for tests). */
+double hgen_entry(const hgen_hmatrix* m, int32_t ill, int32_t itt);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HACAPK_HGEN_H */
