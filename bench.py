@@ -1,0 +1,407 @@
+#!/usr/bin/env python
+"""Benchmark: plain single-vector HMVM y = H x on one B200 (per rank).
+
+Workload (the GPU configuration of the reference's HMVM path): a synthetic
+H-matrix built with HACApK's rules -- N=262,144 points uniform on the unit
+sphere (seeded), kernel 1/(4*pi*|x-y|) with self-term 1.0, bisection cluster
+tree with leaf size 32, admissibility eta=2.0, ACA eps=1e-4 -- and x uniform in
+[-1,1] from the seed.  A step is one HMVM over the whole matrix (5 GB in FP64,
+far larger than the 126 MB L2, so no L2 flush is needed between steps).
+
+Arms
+  (default)          the B200 library: device-resident x/y (value) and, through
+                     the C ABI with pinned host buffers, H2D x + HMVM + D2H y
+                     per step (e2e).
+  --impl reference   the reference's own CPU HMVM (hmvm_omp_2<double,0>,
+                     compiled from its sources into oracle/_ref; falls back to
+                     the C restatement in oracle/) on all host cores.
+
+Multi-GPU: the HMVM does not shard in the reference (one process, one
+device); N ranks run N independent replicas ("replicas only"), value is the
+total HMVM/s of all ranks, timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libhmvm_ref.so")
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--n", type=int, default=262144)
+    ap.add_argument("--geometry", default="sphere")
+    ap.add_argument("--eps", type=float, default=1e-4)
+    ap.add_argument("--eta", type=float, default=2.0)
+    ap.add_argument("--leaf", type=int, default=32)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bound on the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--stage1-cfg", type=int, default=-1)
+    ap.add_argument("--stage2-cfg", type=int, default=-1)
+    ap.add_argument("--ctas-per-sm", type=int, default=0)
+    return ap.parse_args()
+
+
+# ---- the reference's CPU HMVM (CPU baseline / reference arm) ---------------
+class CpuReference:
+    """hmvm_omp_2<double,0> from the reference build (kind "reference"), else
+    the oracle's restatement of it (kind "port")."""
+
+    def __init__(self, hm):
+        P = C.c_void_p
+        self.nd = hm.nd
+        self._i32 = [np.ascontiguousarray(getattr(hm, n), dtype=np.int32)
+                     for n in ("ltmtx", "kt", "ndl", "ndt", "nstrtl", "nstrtt", "a1", "a2")]
+        self._rm = hm.rowmat
+        if os.path.exists(REF_SO):
+            self.kind = "reference"
+            lib = C.CDLL(REF_SO)
+            lib.ref_wrap2.restype = C.c_void_p
+            lib.ref_wrap2.argtypes = [C.c_int] * 4 + [P] * 9
+            lib.ref_omp2_d.argtypes = [C.c_void_p, P, P, C.c_int]
+            lib.ref_max_threads.restype = C.c_int
+            self.lib = lib
+            self.h = lib.ref_wrap2(hm.nd, hm.nlf, hm.ktmax, hm.len,
+                                   *[a.ctypes.data_as(P) for a in self._i32], hm.rowmat.ctypes.data_as(P))
+            self.threads = int(lib.ref_max_threads())
+        else:
+            self.kind = "port"
+            lib = C.CDLL(ORACLE_SO)
+            lib.orc_omp2_d.argtypes = [C.c_int32, C.c_int32, C.c_int32] + [P] * 11 + [C.c_int]
+            lib.orc_max_threads.restype = C.c_int
+            self.lib = lib
+            self._i64 = [self._i32[k] for k in range(6)] + [np.ascontiguousarray(hm.a1, np.int64),
+                                                             np.ascontiguousarray(hm.a2, np.int64)]
+            self.hm = hm
+            self.threads = int(lib.orc_max_threads())
+
+    def run(self, x, y):
+        P = C.c_void_p
+        if self.kind == "reference":
+            self.lib.ref_omp2_d(self.h, x.ctypes.data_as(P), y.ctypes.data_as(P), 0)
+        else:
+            hm = self.hm
+            self.lib.orc_omp2_d(hm.nd, hm.nlf, hm.ktmax, *[a.ctypes.data_as(P) for a in self._i64],
+                                hm.rowmat.ctypes.data_as(P), x.ctypes.data_as(P), y.ctypes.data_as(P), 0)
+
+    def time_sample(self, x, max_seconds):
+        """The reference's own loop shape (hmvm_omp.cpp:992-1021): L runs, the
+        first 5 discarded; L bounded so the sample stays near max_seconds."""
+        y = np.empty(self.nd)
+        t0 = time.perf_counter()
+        self.run(x, y)
+        one = max(time.perf_counter() - t0, 1e-6)
+        L = int(min(10, max(6, max_seconds / one)))
+        ts = []
+        for _ in range(L):
+            t0 = time.perf_counter()
+            self.run(x, y)
+            ts.append(time.perf_counter() - t0)
+        kept = ts[5:]
+        return y, dict(runs=L, kept=len(kept), min=min(kept), avg=sum(kept) / len(kept), max=max(kept))
+
+
+# ---- clocks -----------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = []
+        maxes = []
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                maxes.append(float(r[1]))
+            except (ValueError, IndexError):
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 4 + k and r[4 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(maxes), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_gbs():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def build_matrix(a):
+    from hacapk_hmvm_b200 import HMatrix
+
+    return HMatrix.generate(a.n, a.geometry, eta=a.eta, eps=a.eps, leaf_size=a.leaf, seed=a.seed)
+
+
+def workload_config(a, hm):
+    return {
+        "workload": f"{a.geometry} N={a.n} leaf={a.leaf} eta={a.eta} ACA eps={a.eps:g}, single-vector HMVM, "
+                    f"{a.precision.upper()}",
+        "n": a.n, "geometry": a.geometry, "leaf_size": a.leaf, "eta": a.eta, "aca_eps": a.eps,
+        "nlf": hm.nlf, "n_lowrank": int((hm.ltmtx == 1).sum()), "n_dense": int((hm.ltmtx == 2).sum()),
+        "stored_elements": hm.stored_elements(), "precision": a.precision,
+        "l2": "inputs larger than L2 (the matrix streamed each step is far above 126 MB)",
+        "parallelism": f"replicas x{a.gpus}",
+    }
+
+
+def run_reference(a, rank):
+    if rank != 0:
+        return
+    hm = build_matrix(a)
+    x = np.random.default_rng(a.seed).uniform(-1.0, 1.0, hm.nd)
+    cpu = CpuReference(hm)
+    y = np.empty(hm.nd)
+    for _ in range(max(a.warmup, 1)):
+        cpu.run(x, y)
+    # Each step is one full HMVM; cap the number of steps so the arm stays within a few minutes.
+    t0 = time.perf_counter()
+    cpu.run(x, y)
+    one = time.perf_counter() - t0
+    steps = int(max(1, min(a.steps, 120.0 / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        cpu.run(x, y)
+    dt = time.perf_counter() - t0
+    value = steps / dt
+    sample = f"{steps} full HMVMs (hmvm_omp_2<double,0>) over the whole matrix"
+    line = {
+        "impl": "reference", "metric": "HMVM/s", "value": value, "unit": "HMVM/s", "n_gpus": a.gpus,
+        "steps": steps, "warmup": a.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded HACApK-rule H-matrix; x uniform[-1,1])",
+        "config": workload_config(a, hm),
+        "gbytes_per_s": hm.algorithmic_bytes(8) / (dt / steps) / 1e9,
+        "cpu_baseline": {"value": value, "unit": "HMVM/s", "cores": cpu.threads, "kind": cpu.kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "HMVM/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(a, rank, world, local_rank):
+    import torch
+
+    from hacapk_hmvm_b200 import Plan
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+    hm = build_matrix(a)
+    rng = np.random.default_rng(a.seed)
+    x = rng.uniform(-1.0, 1.0, hm.nd)
+    t0 = time.perf_counter()
+    plan = Plan(hm, a.precision, device=local_rank, stage1_cfg=a.stage1_cfg, stage2_cfg=a.stage2_cfg,
+                ctas_per_sm=a.ctas_per_sm)
+    setup_s = time.perf_counter() - t0
+    info = plan.info()
+    tdt = torch.float64 if a.precision == "fp64" else torch.float32
+    ndt = np.float64 if a.precision == "fp64" else np.float32
+    elem = 8 if a.precision == "fp64" else 4
+    xd = torch.from_numpy(x.astype(ndt)).to(dev)
+    yd = torch.empty(hm.nd, dtype=tdt, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    for _ in range(a.warmup):
+        plan.apply(xd, yd, stream)
+    torch.cuda.synchronize(dev)
+
+    # ---- timed region: K device-resident HMVMs ----
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    clocks = ClockSampler(vis.split(",")[local_rank].strip() if vis else str(local_rank))
+    clocks.start()
+    time.sleep(0.3)
+    plan.profile(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        plan.apply(xd, yd, stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    ms_total = e0.elapsed_time(e1)
+    stage_ms, napplies = plan.profile_read()
+    plan.profile(False)
+    clk = clocks.stop()
+    if dist:
+        tt = torch.tensor([ms_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_total = float(tt.item())
+    ms_step = ms_total / a.steps
+    y_gpu = yd.cpu().numpy().astype(np.float64)
+
+    # ---- e2e: the C-ABI host-buffer call, pinned buffers, copies inside ----
+    xh = torch.from_numpy(x.astype(ndt)).pin_memory()
+    yh = torch.empty(hm.nd, dtype=tdt).pin_memory()
+    xh_np, yh_np = xh.numpy(), yh.numpy()
+    for _ in range(3):
+        plan.apply_host(xh_np, yh_np, stream)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(a.e2e_steps):
+        plan.apply_host(xh_np, yh_np, stream)
+    f1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = f0.elapsed_time(f1)
+    if dist:
+        tt = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e_step = e2e_ms / a.e2e_steps
+
+    # ---- CPU baseline (rank 0, N=1 only) and parity of this run ----
+    cpu_line = None
+    rel = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = CpuReference(hm)
+        y_cpu, st = cpu.time_sample(x, a.cpu_seconds)
+        rel = float(np.linalg.norm(y_gpu - y_cpu) / np.linalg.norm(y_cpu))
+        cpu_line = {"value": 1.0 / st["min"], "unit": "HMVM/s", "cores": cpu.threads, "kind": cpu.kind,
+                    "sample": f"hmvm_omp_2<double,0> on the full matrix, {st['runs']} runs, first 5 discarded, "
+                              f"min of {st['kept']} (avg {st['avg'] * 1e3:.2f} ms)",
+                    "relerr_gpu_vs_cpu": rel}
+    if dist:
+        dist.barrier()
+
+    # ---- roofline of the dominant kernel ----
+    peak, peak_kind = measured_peak_gbs()
+    stage_bytes = [info["stage1_bytes"], 0, info["stage2_bytes"]]
+    dom = int(np.argmax(stage_ms))
+    dom_avg_s = stage_ms[dom] / max(napplies, 1) * 1e-3
+    achieved = stage_bytes[dom] / dom_avg_s / 1e9 if dom_avg_s > 0 else 0.0
+    alg_bytes = info["algorithmic_bytes"]
+    roof = {
+        "bound": "hbm", "kernel": ["hmvm_tile_kernel (V stage)", "hmvm_reduce_kernel", "hmvm_tile_kernel (row stage)"][dom],
+        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+        "traffic": None,
+        "whole_hmvm_gbs": alg_bytes / (ms_step * 1e-3) / 1e9,
+        "whole_hmvm_frac": alg_bytes / (ms_step * 1e-3) / 1e9 / peak,
+        "stage_ms_avg": [s / max(napplies, 1) for s in stage_ms],
+        "stage_bytes": stage_bytes,
+    }
+
+    if rank == 0:
+        value = world * 1e3 / ms_step
+        cfg = workload_config(a, hm)
+        cfg.update({"stage1_cfg": info["stage1_cfg"], "stage2_cfg": info["stage2_cfg"],
+                    "device_bytes": info["device_bytes"], "plan_setup_s": setup_s})
+        line = {
+            "metric": "HMVM/s", "value": value, "unit": "HMVM/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f32",
+            "data": "synthetic (seeded HACApK-rule H-matrix; x uniform[-1,1])",
+            "config": cfg,
+            "gbytes_per_s": alg_bytes / (ms_step * 1e-3) / 1e9,
+            "algorithmic_bytes_per_step": alg_bytes,
+            "relerr_vs_fp64_cpu_reference": rel, "aca_eps": a.eps,
+            "roofline": roof,
+            "cpu_baseline": cpu_line,
+            "e2e": {"value": world * 1e3 / e2e_step, "unit": "HMVM/s", "h2d_bytes_per_step": hm.nd * elem,
+                    "d2h_bytes_per_step": hm.nd * elem, "ms_per_step": e2e_step},
+            "clocks": clk,
+            "gpu_launches": a.steps * plan.kernel_count(),
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        run_reference(a, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_b200(a, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

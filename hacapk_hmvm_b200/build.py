@@ -1,0 +1,101 @@
+"""In-tree build of the native libraries.
+
+    libhmvm_b200.so  the HMVM library: host planner + sm_100a kernels + C ABI
+                     (nvcc -gencode arch=compute_100a,code=sm_100a)
+    libhgen.so       the H-matrix generator / writer (host C++, OpenMP)
+
+Run ``python -m hacapk_hmvm_b200.build`` (or ``__graft_entry__.build()``).  The
+built files sit next to this module so they travel with the source tree.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+
+LIB_HMVM = os.path.join(PKG, "libhmvm_b200.so")
+LIB_HGEN = os.path.join(PKG, "libhgen.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+    cand = os.environ.get("NVCC") or shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    return cand
+
+
+def _hostcxx() -> str:
+    # The image's CC/CXX wrappers lack the OpenMP spec files; use the system compiler.
+    for c in ("/usr/bin/g++", shutil.which("g++") or "g++"):
+        if os.path.exists(c):
+            return c
+    return "g++"
+
+
+def _run(cmd: list[str], verbose: bool) -> None:
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+
+
+def _stale(target: str, sources: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources)
+
+
+def hmvm_sources() -> list[str]:
+    return [os.path.join(CSRC, f) for f in ("hmvm_b200.cu", "layout.cpp", "loader.cpp")]
+
+
+def hmvm_deps() -> list[str]:
+    deps = hmvm_sources() + [os.path.join(CSRC, f) for f in ("kernels.cuh", "layout.hpp")]
+    deps.append(os.path.join(INCLUDE, "hmvm_b200.h"))
+    return deps
+
+
+def build_hmvm(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
+    if not force and not _stale(LIB_HMVM, hmvm_deps()):
+        return LIB_HMVM
+    tmp = LIB_HMVM + ".tmp"
+    cmd = [
+        _nvcc(), "-O3", "-std=c++17", "-lineinfo", *ARCH,
+        "-ccbin", _hostcxx(),
+        "-Xcompiler", "-fPIC,-fopenmp,-O3",
+        "-Xptxas", "-warn-spills",
+        "-I", INCLUDE, "-I", CSRC,
+        "-shared", "-o", tmp, *hmvm_sources(), "-lgomp",
+    ]
+    if extra:
+        cmd[1:1] = extra
+    _run(cmd, verbose)
+    os.replace(tmp, LIB_HMVM)
+    return LIB_HMVM
+
+
+def build_hgen(force: bool = False, verbose: bool = False) -> str:
+    src = os.path.join(CSRC, "hgen.cpp")
+    deps = [src, os.path.join(INCLUDE, "hacapk_hgen.h")]
+    if not force and not _stale(LIB_HGEN, deps):
+        return LIB_HGEN
+    tmp = LIB_HGEN + ".tmp"
+    _run([_hostcxx(), "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-Wall",
+          "-I", INCLUDE, "-o", tmp, src], verbose)
+    os.replace(tmp, LIB_HGEN)
+    return LIB_HGEN
+
+
+def build_all(force: bool = False, verbose: bool = False) -> None:
+    build_hgen(force, verbose)
+    build_hmvm(force, verbose)
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv, verbose=True)

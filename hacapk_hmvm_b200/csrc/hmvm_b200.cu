@@ -1,0 +1,638 @@
+// C-ABI of the B200 HMVM library: plan creation (host planner + upload),
+// kernel dispatch, host-buffer apply and the one-shot reference-shaped call.
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "hmvm_b200.h"
+#include "kernels.cuh"
+#include "layout.hpp"
+
+namespace hmvm {
+
+thread_local std::string g_last_error;
+
+int set_error(int status, const std::string& msg) {
+  g_last_error = msg;
+  return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  return set_error(e == cudaErrorMemoryAllocation ? HMVM_ENOMEM : HMVM_ECUDA, m);
+}
+
+#define HMVM_CUDA_TRY(call, what)          \
+  do {                                     \
+    cudaError_t e_ = (call);               \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+// Makes `dev` current for the scope and restores the caller's device after.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) return;
+    ok = (prev == dev) || (cudaSetDevice(dev) == cudaSuccess);
+  }
+  ~DeviceGuard() {
+    int cur;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+using TileKernelFn = void (*)(TileArgs);
+
+template <typename T>
+TileKernelFn tile_kernel_for(int cfg) {
+  switch (cfg) {
+    case 0: return hmvm_tile_kernel<T, 1, 8>;
+    case 1: return hmvm_tile_kernel<T, 2, 4>;
+    case 2: return hmvm_tile_kernel<T, 4, 2>;
+    case 3: return hmvm_tile_kernel<T, 8, 1>;
+    case 4: return hmvm_tile_kernel<T, 2, 8>;
+    case 5: return hmvm_tile_kernel<T, 4, 4>;
+    case 6: return hmvm_tile_kernel<T, 8, 2>;
+    default: return hmvm_tile_kernel<T, 16, 1>;
+  }
+}
+
+}  // namespace hmvm
+
+using namespace hmvm;
+
+struct hmvm_plan {
+  int device = 0;
+  int precision = HMVM_FP64;
+  int elem = 8;
+  int32_t nd = 0, nlf = 0, n_lowrank = 0, n_dense = 0;
+  int num_sms = 0, ctas_per_sm = 2, stage1_cfg = 0, stage2_cfg = 0;
+  int32_t stage1_tiles = 0, stage2_tiles = 0, stage1_teams = 0, stage2_teams = 0, n_red = 0;
+  int64_t stored_elems = 0, device_bytes = 0, t_len = 0, p_len = 0;
+  // device buffers
+  void* d_data = nullptr;
+  hmvm_tile_desc* d_tiles = nullptr;
+  hmvm_seg_desc* d_segs = nullptr;
+  int32_t* d_tb1 = nullptr;
+  int32_t* d_tb2 = nullptr;
+  int32_t* d_out_idx = nullptr;
+  int4* d_red = nullptr;
+  void* d_t = nullptr;
+  void* d_p = nullptr;
+  void* d_x = nullptr;  // staging for apply_host
+  void* d_y = nullptr;
+  int64_t stage1_bytes = 0, stage2_bytes = 0;
+  // profiling: 4 events per recorded apply (before stage 1, reduce, stage 2, after)
+  bool profiling = false;
+  std::vector<cudaEvent_t> prof_events;
+  int prof_count = 0;
+};
+
+struct hmvm_layout {
+  HostLayout L;
+};
+
+namespace {
+
+constexpr int kMaxProfiled = 4096;
+
+void free_plan_buffers(hmvm_plan* p) {
+  for (cudaEvent_t e : p->prof_events) cudaEventDestroy(e);
+  p->prof_events.clear();
+  void* bufs[] = {p->d_data, p->d_tiles, p->d_segs, p->d_tb1, p->d_tb2, p->d_out_idx,
+                  p->d_red,  p->d_t,     p->d_p,    p->d_x,   p->d_y};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+}
+
+int check_device(int want, int* dev_out, int* sms_out) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return set_error(HMVM_ENODEV, std::string("no CUDA device available: ") + cudaGetErrorString(e));
+  }
+  int dev = want;
+  if (dev < 0) {
+    if (cudaGetDevice(&dev) != cudaSuccess) return set_error(HMVM_ENODEV, "cudaGetDevice failed");
+  }
+  if (dev >= n) return set_error(HMVM_EINVAL, "device ordinal out of range");
+  cudaDeviceProp prop;
+  HMVM_CUDA_TRY(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
+  if (prop.major < 10) {
+    return set_error(HMVM_ENODEV, std::string("device ") + prop.name +
+                                      " is not sm_100-class; this library is built for sm_100a only");
+  }
+  *dev_out = dev;
+  *sms_out = prop.multiProcessorCount;
+  return HMVM_OK;
+}
+
+template <typename Buf>
+int upload(Buf** dst, const void* src, size_t bytes, int64_t* total) {
+  size_t nb = bytes > 0 ? bytes : 16;
+  HMVM_CUDA_TRY(cudaMalloc((void**)dst, nb), "cudaMalloc");
+  if (bytes) HMVM_CUDA_TRY(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+  if (total) *total += (int64_t)bytes;
+  return HMVM_OK;
+}
+
+int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** out) {
+  if (!out) return set_error(HMVM_EINVAL, "plan output pointer is NULL");
+  *out = nullptr;
+  hmvm_plan_opts opts;
+  hmvm_b200_default_opts(&opts);
+  if (opts_in) opts = *opts_in;
+  int dev = 0, sms = 0;
+  int rc = check_device(opts.device, &dev, &sms);
+  if (rc) return rc;
+  HostLayout* L = new (std::nothrow) HostLayout();
+  if (!L) return set_error(HMVM_ENOMEM, "host allocation failed");
+  std::string msg;
+  rc = build_layout(lt, opts, sms, *L, msg);
+  if (rc) {
+    delete L;
+    return set_error(rc, msg);
+  }
+  hmvm_plan* p = new (std::nothrow) hmvm_plan();
+  if (!p) {
+    delete L;
+    return set_error(HMVM_ENOMEM, "host allocation failed");
+  }
+  p->device = dev;
+  p->precision = L->precision;
+  p->elem = L->elem_size;
+  p->nd = L->nd;
+  p->nlf = L->nlf;
+  p->n_lowrank = L->n_lowrank;
+  p->n_dense = L->n_dense;
+  p->num_sms = sms;
+  p->ctas_per_sm = L->ctas_per_sm;
+  p->stage1_cfg = L->stage1_cfg;
+  p->stage2_cfg = L->stage2_cfg;
+  p->stage1_tiles = L->stage1_tiles;
+  p->stage2_tiles = L->stage2_tiles;
+  p->stage1_teams = L->stage1_teams;
+  p->stage2_teams = L->stage2_teams;
+  p->n_red = (int32_t)(L->red.size() / 4);
+  p->stored_elems = L->stored_elems;
+  p->t_len = L->t_len;
+  p->p_len = L->p_len;
+  {
+    // Algorithmic bytes per stage: stored elements of the stage once, plus the
+    // vectors it reads/writes once (the intermediate t is not counted).
+    int64_t v_elems = 0;
+    for (int32_t i = 0; i < lt.nlf; i++)
+      if (lt.ltmtx[i] == 1) v_elems += (int64_t)lt.kt[i] * lt.ndt[i];
+    p->stage1_bytes = (v_elems + (int64_t)lt.nd) * L->elem_size;
+    p->stage2_bytes = (L->stored_elems - v_elems + 2 * (int64_t)lt.nd) * L->elem_size;
+  }
+  {
+    DeviceGuard g(dev);
+    if (!g.ok) rc = set_error(HMVM_ECUDA, "cannot select the plan's device");
+    int64_t dbytes = 0;
+    if (!rc) rc = upload(&p->d_data, L->data.data(), L->data.size() * sizeof(Vec16), &dbytes);
+    p->device_bytes = dbytes;
+    if (!rc) rc = upload(&p->d_tiles, L->tiles.data(), L->tiles.size() * sizeof(hmvm_tile_desc), nullptr);
+    if (!rc) rc = upload(&p->d_segs, L->segs.data(), L->segs.size() * sizeof(hmvm_seg_desc), nullptr);
+    if (!rc) rc = upload(&p->d_tb1, L->team_begin1.data(), L->team_begin1.size() * 4, nullptr);
+    if (!rc) rc = upload(&p->d_tb2, L->team_begin2.data(), L->team_begin2.size() * 4, nullptr);
+    if (!rc) rc = upload(&p->d_out_idx, L->out_idx.data(), L->out_idx.size() * 4, nullptr);
+    if (!rc) rc = upload(&p->d_red, L->red.data(), L->red.size() * 4, nullptr);
+    // t: the padding slots of every row group must read as zero; stage 1 only
+    // ever writes real slots, so one clear at creation keeps them zero.
+    size_t tbytes = (size_t)(L->t_len + 16) * L->elem_size;
+    if (!rc) {
+      cudaError_t e = cudaMalloc(&p->d_t, tbytes);
+      if (e == cudaSuccess) e = cudaMemset(p->d_t, 0, tbytes);
+      if (e != cudaSuccess) rc = cuda_fail(e, "t buffer");
+    }
+    if (!rc) {
+      cudaError_t e = cudaMalloc(&p->d_p, (size_t)(L->p_len + 16) * L->elem_size);
+      if (e != cudaSuccess) rc = cuda_fail(e, "partial buffer");
+    }
+    if (!rc) {
+      cudaError_t e = cudaDeviceSynchronize();
+      if (e != cudaSuccess) rc = cuda_fail(e, "plan upload");
+    }
+    if (rc) free_plan_buffers(p);
+  }
+  delete L;
+  if (rc) {
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return HMVM_OK;
+}
+
+template <typename T>
+int launch_apply(hmvm_plan* p, const void* x, void* y, cudaStream_t st) {
+  TileArgs a;
+  a.tiles = p->d_tiles;
+  a.segs = p->d_segs;
+  a.data = p->d_data;
+  a.x = x;
+  a.t = p->d_t;
+  a.y = y;
+  a.p = p->d_p;
+  a.out_idx = p->d_out_idx;
+  const int ctas = p->num_sms * p->ctas_per_sm;
+  cudaEvent_t* ev = nullptr;
+  if (p->profiling && p->prof_count < kMaxProfiled) {
+    ev = &p->prof_events[4 * (size_t)p->prof_count];
+    p->prof_count++;
+  }
+  if (ev) cudaEventRecord(ev[0], st);
+  if (p->stage1_tiles > 0) {
+    const KernelCfg c = kCfgs[p->stage1_cfg];
+    a.team_begin = p->d_tb1;
+    a.nteams = p->stage1_teams;
+    tile_kernel_for<T>(p->stage1_cfg)<<<ctas, 32 * c.wg * c.tpc, 0, st>>>(a);
+    HMVM_CUDA_TRY(cudaGetLastError(), "stage-1 launch");
+  }
+  if (ev) cudaEventRecord(ev[1], st);
+  if (p->n_red > 0) {
+    int blocks = (p->n_red + 255) / 256;
+    hmvm_reduce_kernel<T><<<blocks, 256, 0, st>>>(p->d_red, p->n_red, static_cast<const T*>(p->d_p),
+                                                  static_cast<T*>(p->d_t));
+    HMVM_CUDA_TRY(cudaGetLastError(), "reduction launch");
+  }
+  if (ev) cudaEventRecord(ev[2], st);
+  {
+    const KernelCfg c = kCfgs[p->stage2_cfg];
+    a.team_begin = p->d_tb2;
+    a.nteams = p->stage2_teams;
+    tile_kernel_for<T>(p->stage2_cfg)<<<ctas, 32 * c.wg * c.tpc, 0, st>>>(a);
+    HMVM_CUDA_TRY(cudaGetLastError(), "stage-2 launch");
+  }
+  if (ev) cudaEventRecord(ev[3], st);
+  return HMVM_OK;
+}
+
+int apply_impl(hmvm_plan* p, const void* x, void* y, cudaStream_t st) {
+  if (p->nd == 0) return HMVM_OK;
+  if (p->precision == HMVM_FP64) return launch_apply<double>(p, x, y, st);
+  return launch_apply<float>(p, x, y, st);
+}
+
+int make_table_from_matrix2(int nd, int nlf, int ktmax, int len, const int* ltmtx, const int* kt, const int* ndl,
+                            const int* ndt, const int* nstrtl, const int* nstrtt, const int* a1, const int* a2,
+                            const void* rowmat, bool is_float, LeafTable& lt) {
+  lt.nd = nd;
+  lt.nlf = nlf;
+  lt.ktmax = ktmax;
+  lt.len = len;
+  lt.ltmtx = ltmtx;
+  lt.kt = kt;
+  lt.ndl = ndl;
+  lt.ndt = ndt;
+  lt.nstrtl = nstrtl;
+  lt.nstrtt = nstrtt;
+  lt.a1_32 = a1;
+  lt.a2_32 = a2;
+  lt.rowmat = rowmat;
+  lt.rowmat_is_float = is_float;
+  return HMVM_OK;
+}
+
+void table_from_leaves64(const hmvm_leaves64* lv, bool is_float, LeafTable& lt) {
+  lt.nd = lv->nd;
+  lt.nlf = lv->nlf;
+  lt.ktmax = lv->ktmax;
+  lt.len = lv->len;
+  lt.ltmtx = lv->ltmtx;
+  lt.kt = lv->kt;
+  lt.ndl = lv->ndl;
+  lt.ndt = lv->ndt;
+  lt.nstrtl = lv->nstrtl;
+  lt.nstrtt = lv->nstrtt;
+  lt.a1_64 = lv->a1;
+  lt.a2_64 = lv->a2;
+  lt.rowmat = lv->rowmat;
+  lt.rowmat_is_float = is_float;
+}
+
+}  // namespace
+
+extern "C" {
+
+void hmvm_b200_default_opts(hmvm_plan_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->precision = HMVM_FP64;
+  o->device = -1;
+  o->max_tile_rows = 32;
+  o->split_cols = 0;
+  o->stage1_cfg = -1;
+  o->stage2_cfg = -1;
+  o->ctas_per_sm = 0;
+}
+
+int hmvm_b200_plan_create_d(const hmvm_matrix2_d* m, const hmvm_plan_opts* opts, hmvm_plan** plan) {
+  if (!m) return set_error(HMVM_EINVAL, "matrix is NULL");
+  LeafTable lt;
+  make_table_from_matrix2(m->nd, m->nlf, m->ktmax, m->len, m->ltmtx, m->kt, m->ndl, m->ndt, m->nstrtl, m->nstrtt,
+                          m->a1, m->a2, m->rowmat, false, lt);
+  return create_plan(lt, opts, plan);
+}
+
+int hmvm_b200_plan_create_f(const hmvm_matrix2_f* m, const hmvm_plan_opts* opts, hmvm_plan** plan) {
+  if (!m) return set_error(HMVM_EINVAL, "matrix is NULL");
+  hmvm_plan_opts o;
+  hmvm_b200_default_opts(&o);
+  if (opts) o = *opts;
+  o.precision = HMVM_FP32;
+  LeafTable lt;
+  make_table_from_matrix2(m->nd, m->nlf, m->ktmax, m->len, m->ltmtx, m->kt, m->ndl, m->ndt, m->nstrtl, m->nstrtt,
+                          m->a1, m->a2, m->rowmat, true, lt);
+  return create_plan(lt, &o, plan);
+}
+
+int hmvm_b200_plan_create64_d(const hmvm_leaves64* lv, const hmvm_plan_opts* opts, hmvm_plan** plan) {
+  if (!lv) return set_error(HMVM_EINVAL, "leaf table is NULL");
+  LeafTable lt;
+  table_from_leaves64(lv, false, lt);
+  return create_plan(lt, opts, plan);
+}
+
+int hmvm_b200_plan_create64_f(const hmvm_leaves64* lv, const hmvm_plan_opts* opts, hmvm_plan** plan) {
+  if (!lv) return set_error(HMVM_EINVAL, "leaf table is NULL");
+  hmvm_plan_opts o;
+  hmvm_b200_default_opts(&o);
+  if (opts) o = *opts;
+  o.precision = HMVM_FP32;
+  LeafTable lt;
+  table_from_leaves64(lv, true, lt);
+  return create_plan(lt, &o, plan);
+}
+
+void hmvm_b200_plan_destroy(hmvm_plan* p) {
+  if (!p) return;
+  {
+    DeviceGuard g(p->device);
+    free_plan_buffers(p);
+  }
+  delete p;
+}
+
+int hmvm_b200_plan_get_info(const hmvm_plan* p, hmvm_plan_info* info) {
+  if (!p || !info) return set_error(HMVM_EINVAL, "NULL argument");
+  std::memset(info, 0, sizeof(*info));
+  info->nd = p->nd;
+  info->nlf = p->nlf;
+  info->n_lowrank = p->n_lowrank;
+  info->n_dense = p->n_dense;
+  info->precision = p->precision;
+  info->device = p->device;
+  info->num_sms = p->num_sms;
+  info->algorithmic_bytes = (p->stored_elems + 2 * (int64_t)p->nd) * p->elem;
+  info->device_bytes = p->device_bytes;
+  info->t_len = p->t_len;
+  info->stage1_tiles = p->stage1_tiles;
+  info->stage2_tiles = p->stage2_tiles;
+  info->stage1_teams = p->stage1_teams;
+  info->stage2_teams = p->stage2_teams;
+  info->split_rows = p->n_red;
+  info->kernels_per_apply = hmvm_b200_plan_kernel_count(p);
+  info->stage1_cfg = p->stage1_cfg;
+  info->stage2_cfg = p->stage2_cfg;
+  info->flops = 2 * p->stored_elems;
+  info->stage1_bytes = p->stage1_bytes;
+  info->stage2_bytes = p->stage2_bytes;
+  return HMVM_OK;
+}
+
+int hmvm_b200_plan_profile(hmvm_plan* p, int enable) {
+  if (!p) return set_error(HMVM_EINVAL, "plan is NULL");
+  DeviceGuard g(p->device);
+  if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
+  if (enable && p->prof_events.empty()) {
+    p->prof_events.resize(4 * (size_t)kMaxProfiled);
+    for (auto& e : p->prof_events) HMVM_CUDA_TRY(cudaEventCreate(&e), "cudaEventCreate");
+  }
+  p->profiling = enable != 0;
+  p->prof_count = 0;
+  return HMVM_OK;
+}
+
+int hmvm_b200_plan_profile_read(hmvm_plan* p, double* ms3, int32_t* napplies) {
+  if (!p || !ms3) return set_error(HMVM_EINVAL, "NULL argument");
+  DeviceGuard g(p->device);
+  ms3[0] = ms3[1] = ms3[2] = 0.0;
+  int n = p->prof_count;
+  if (n > 0) HMVM_CUDA_TRY(cudaEventSynchronize(p->prof_events[4 * (size_t)(n - 1) + 3]), "event sync");
+  for (int k = 0; k < n; k++) {
+    for (int s = 0; s < 3; s++) {
+      float ms = 0.f;
+      HMVM_CUDA_TRY(cudaEventElapsedTime(&ms, p->prof_events[4 * (size_t)k + s], p->prof_events[4 * (size_t)k + s + 1]),
+                    "cudaEventElapsedTime");
+      ms3[s] += ms;
+    }
+  }
+  if (napplies) *napplies = n;
+  p->prof_count = 0;
+  return HMVM_OK;
+}
+
+int hmvm_b200_plan_kernel_count(const hmvm_plan* p) {
+  if (!p || p->nd == 0) return 0;
+  return (p->stage1_tiles > 0) + (p->n_red > 0) + 1;
+}
+
+int hmvm_b200_apply(hmvm_plan* p, const void* x, void* y, void* stream) {
+  if (!p) return set_error(HMVM_EINVAL, "plan is NULL");
+  if (p->nd > 0 && (!x || !y)) return set_error(HMVM_EINVAL, "x or y is NULL");
+  const char* xb = static_cast<const char*>(x);
+  const char* yb = static_cast<const char*>(y);
+  size_t nb = (size_t)p->nd * p->elem;
+  if (p->nd > 0 && xb < yb + nb && yb < xb + nb) return set_error(HMVM_EINVAL, "x and y overlap");
+  DeviceGuard g(p->device);
+  if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
+  return apply_impl(p, x, y, static_cast<cudaStream_t>(stream));
+}
+
+int hmvm_b200_apply_host(hmvm_plan* p, const void* x_host, void* y_host, void* stream) {
+  if (!p) return set_error(HMVM_EINVAL, "plan is NULL");
+  if (p->nd > 0 && (!x_host || !y_host)) return set_error(HMVM_EINVAL, "x or y is NULL");
+  if (p->nd == 0) return HMVM_OK;
+  DeviceGuard g(p->device);
+  if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
+  size_t nb = (size_t)p->nd * p->elem;
+  if (!p->d_x) HMVM_CUDA_TRY(cudaMalloc(&p->d_x, nb), "cudaMalloc x staging");
+  if (!p->d_y) HMVM_CUDA_TRY(cudaMalloc(&p->d_y, nb), "cudaMalloc y staging");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  HMVM_CUDA_TRY(cudaMemcpyAsync(p->d_x, x_host, nb, cudaMemcpyHostToDevice, st), "copy x to device");
+  int rc = apply_impl(p, p->d_x, p->d_y, st);
+  if (rc) return rc;
+  HMVM_CUDA_TRY(cudaMemcpyAsync(y_host, p->d_y, nb, cudaMemcpyDeviceToHost, st), "copy y to host");
+  HMVM_CUDA_TRY(cudaStreamSynchronize(st), "stream synchronize");
+  return HMVM_OK;
+}
+
+static int one_shot(hmvm_plan* plan, const void* x, void* y, hmvm_stats* stats, double setup_s) {
+  cudaEvent_t e0, e1;
+  HMVM_CUDA_TRY(cudaEventCreate(&e0), "cudaEventCreate");
+  HMVM_CUDA_TRY(cudaEventCreate(&e1), "cudaEventCreate");
+  size_t nb = (size_t)plan->nd * plan->elem;
+  int rc = HMVM_OK;
+  if (plan->nd > 0) {
+    if (!plan->d_x && cudaMalloc(&plan->d_x, nb) != cudaSuccess) rc = set_error(HMVM_ENOMEM, "x staging");
+    if (!rc && !plan->d_y && cudaMalloc(&plan->d_y, nb) != cudaSuccess) rc = set_error(HMVM_ENOMEM, "y staging");
+    if (!rc && cudaMemcpy(plan->d_x, x, nb, cudaMemcpyHostToDevice) != cudaSuccess) rc = set_error(HMVM_ECUDA, "copy x");
+    if (!rc) {
+      cudaEventRecord(e0, 0);
+      rc = apply_impl(plan, plan->d_x, plan->d_y, 0);
+      cudaEventRecord(e1, 0);
+    }
+    if (!rc) {
+      cudaError_t e = cudaMemcpy(y, plan->d_y, nb, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) rc = cuda_fail(e, "copy y");
+    }
+  }
+  float ms = 0.f;
+  if (!rc && plan->nd > 0) cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!rc && stats) {
+    stats->seconds_setup = setup_s;
+    stats->seconds_apply = ms * 1e-3;
+    stats->algorithmic_bytes = (plan->stored_elems + 2 * (int64_t)plan->nd) * plan->elem;
+    stats->gbytes_per_s = ms > 0 ? stats->algorithmic_bytes / (ms * 1e-3) / 1e9 : 0.0;
+  }
+  return rc;
+}
+
+int hmvm_cuda_d(const hmvm_matrix2_d* mat2, const double* x, double* y, int mode, hmvm_stats* stats) {
+  hmvm_plan_opts o;
+  hmvm_b200_default_opts(&o);
+  o.precision = HMVM_FP64;
+  (void)mode;
+  auto t0 = std::chrono::steady_clock::now();
+  hmvm_plan* plan = nullptr;
+  int rc = hmvm_b200_plan_create_d(mat2, &o, &plan);
+  if (rc) return rc;
+  double setup = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  {
+    DeviceGuard g(plan->device);
+    rc = one_shot(plan, x, y, stats, setup);
+  }
+  hmvm_b200_plan_destroy(plan);
+  return rc;
+}
+
+int hmvm_cuda_f(const hmvm_matrix2_f* mat2, const float* x, float* y, int mode, hmvm_stats* stats) {
+  (void)mode;
+  auto t0 = std::chrono::steady_clock::now();
+  hmvm_plan* plan = nullptr;
+  int rc = hmvm_b200_plan_create_f(mat2, nullptr, &plan);
+  if (rc) return rc;
+  double setup = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  {
+    DeviceGuard g(plan->device);
+    rc = one_shot(plan, x, y, stats, setup);
+  }
+  hmvm_b200_plan_destroy(plan);
+  return rc;
+}
+
+// ---- inspection --------------------------------------------------------
+int hmvm_b200_layout_build_d(const hmvm_matrix2_d* m, const hmvm_plan_opts* opts, int32_t num_sms,
+                             hmvm_layout** out) {
+  if (!m || !out) return set_error(HMVM_EINVAL, "NULL argument");
+  *out = nullptr;
+  hmvm_plan_opts o;
+  hmvm_b200_default_opts(&o);
+  if (opts) o = *opts;
+  LeafTable lt;
+  make_table_from_matrix2(m->nd, m->nlf, m->ktmax, m->len, m->ltmtx, m->kt, m->ndl, m->ndt, m->nstrtl, m->nstrtt,
+                          m->a1, m->a2, m->rowmat, false, lt);
+  hmvm_layout* h = new (std::nothrow) hmvm_layout();
+  if (!h) return set_error(HMVM_ENOMEM, "host allocation failed");
+  std::string msg;
+  int rc = build_layout(lt, o, num_sms, h->L, msg);
+  if (rc) {
+    delete h;
+    return set_error(rc, msg);
+  }
+  *out = h;
+  return HMVM_OK;
+}
+
+int hmvm_b200_layout_build64(const hmvm_leaves64* lv, int32_t rowmat_is_float, const hmvm_plan_opts* opts,
+                             int32_t num_sms, hmvm_layout** out) {
+  if (!lv || !out) return set_error(HMVM_EINVAL, "NULL argument");
+  *out = nullptr;
+  hmvm_plan_opts o;
+  hmvm_b200_default_opts(&o);
+  if (opts) o = *opts;
+  LeafTable lt;
+  table_from_leaves64(lv, rowmat_is_float != 0, lt);
+  hmvm_layout* h = new (std::nothrow) hmvm_layout();
+  if (!h) return set_error(HMVM_ENOMEM, "host allocation failed");
+  std::string msg;
+  int rc = build_layout(lt, o, num_sms, h->L, msg);
+  if (rc) {
+    delete h;
+    return set_error(rc, msg);
+  }
+  *out = h;
+  return HMVM_OK;
+}
+
+int hmvm_b200_layout_view(const hmvm_layout* h, hmvm_layout_view* v) {
+  if (!h || !v) return set_error(HMVM_EINVAL, "NULL argument");
+  const HostLayout& L = h->L;
+  std::memset(v, 0, sizeof(*v));
+  v->precision = L.precision;
+  v->vec = L.vec;
+  v->n_tiles = (int32_t)L.tiles.size();
+  v->n_segs = (int32_t)L.segs.size();
+  v->stage1_tiles = L.stage1_tiles;
+  v->stage2_tiles = L.stage2_tiles;
+  v->stage1_teams = L.stage1_teams;
+  v->stage2_teams = L.stage2_teams;
+  v->n_red = (int32_t)(L.red.size() / 4);
+  v->nd = L.nd;
+  v->data_vectors = (int64_t)L.data.size();
+  v->t_len = L.t_len;
+  v->p_len = L.p_len;
+  v->tiles = L.tiles.data();
+  v->segs = L.segs.data();
+  v->team_begin1 = L.team_begin1.data();
+  v->team_begin2 = L.team_begin2.data();
+  v->out_idx = L.out_idx.data();
+  v->red = L.red.data();
+  v->data = L.data.data();
+  return HMVM_OK;
+}
+
+void hmvm_b200_layout_destroy(hmvm_layout* h) { delete h; }
+
+const char* hmvm_b200_strerror(int s) {
+  switch (s) {
+    case HMVM_OK: return "success";
+    case HMVM_EINVAL: return "invalid argument or leaf table";
+    case HMVM_ENOMEM: return "out of memory";
+    case HMVM_ECUDA: return "CUDA runtime error";
+    case HMVM_EIO: return "file could not be opened or read";
+    case HMVM_EFORMAT: return "malformed H-matrix file";
+    case HMVM_ERANGE: return "count exceeds the structure or format";
+    case HMVM_ENODEV: return "no usable CUDA device";
+    case HMVM_EDEVICE: return "kernel reported an error";
+    default: return "unknown status";
+  }
+}
+
+const char* hmvm_b200_last_error(void) { return g_last_error.c_str(); }
+
+int hmvm_b200_version(void) { return 1; }
+
+}  // extern "C"

@@ -1,0 +1,477 @@
+// Host planner: leaf list -> row-owned, vector-packed tiles (see layout.hpp).
+
+#include "layout.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <new>
+#include <queue>
+#include <unordered_map>
+#include <utility>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace hmvm {
+
+namespace {
+
+constexpr int32_t kTFlag = (int32_t)0x80000000u;
+
+inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
+
+inline uint64_t key2(int32_t a, int32_t b) { return ((uint64_t)(uint32_t)a << 32) | (uint32_t)b; }
+
+// One part of a stage-2 segment's column list.
+struct Part {
+  int32_t leaf;   // dense leaf, or -1 for a low-rank row group
+  int32_t group;  // row group index when leaf < 0
+  int32_t ncols;
+};
+
+struct TileBuild {
+  int32_t row0 = 0, nrows = 0;       // stage 2
+  int32_t stage = 2;
+  // stage 1 panel chunk
+  int32_t cgroup = -1, panel_row0 = 0, col0 = 0;
+  int32_t mode = 0, out_base = 0;
+  // segments: [seg_first, seg_first+nseg) in the temp segment list
+  int32_t seg_first = 0, nseg = 0, nvec = 0;
+  int64_t cost = 0;
+};
+
+struct SegBuild {
+  int32_t src, ncols;
+  int32_t part_first, nparts;  // into parts (stage 2)
+};
+
+template <class S>
+inline double rd(const void *base, int64_t i) {
+  return (double)static_cast<const S *>(base)[i];
+}
+
+}  // namespace
+
+int validate_leaves(const LeafTable &lt, std::string &msg) {
+  auto fail = [&](int32_t i, const char *what) {
+    char buf[256];
+    snprintf(buf, sizeof buf, "leaf %d: %s (ltmtx=%d kt=%d ndl=%d ndt=%d nstrtl=%d nstrtt=%d)", i, what,
+             lt.ltmtx[i], lt.kt[i], lt.ndl[i], lt.ndt[i], lt.nstrtl[i], lt.nstrtt[i]);
+    msg = buf;
+    return HMVM_EINVAL;
+  };
+  if (lt.nd < 0 || lt.nlf < 0 || lt.len < 0) {
+    msg = "negative nd, nlf or len";
+    return HMVM_EINVAL;
+  }
+  if (lt.nlf > 0 && (!lt.ltmtx || !lt.kt || !lt.ndl || !lt.ndt || !lt.nstrtl || !lt.nstrtt ||
+                     (!lt.a1_32 && !lt.a1_64) || (!lt.a2_32 && !lt.a2_64))) {
+    msg = "missing leaf array";
+    return HMVM_EINVAL;
+  }
+  if (lt.len > 0 && !lt.rowmat) {
+    msg = "missing rowmat";
+    return HMVM_EINVAL;
+  }
+  for (int32_t i = 0; i < lt.nlf; i++) {
+    int32_t ty = lt.ltmtx[i], kt = lt.kt[i], ndl = lt.ndl[i], ndt = lt.ndt[i];
+    int32_t sl = lt.nstrtl[i], st = lt.nstrtt[i];
+    if (ty != 1 && ty != 2) return fail(i, "ltmtx must be 1 (low-rank) or 2 (dense)");
+    if (ndl < 0 || ndt < 0) return fail(i, "negative ndl/ndt");
+    if (ndl > 0 && (sl < 1 || (int64_t)sl - 1 + ndl > lt.nd)) return fail(i, "row range outside 1..nd");
+    if (ndt > 0 && (st < 1 || (int64_t)st - 1 + ndt > lt.nd)) return fail(i, "column range outside 1..nd");
+    int64_t a1 = lt.a1(i);
+    if (ty == 1) {
+      if (kt < 0) return fail(i, "negative kt");
+      if (kt > lt.ktmax) return fail(i, "kt > ktmax");
+      int64_t a2 = lt.a2(i);
+      int64_t n1 = (int64_t)kt * ndt, n2 = (int64_t)kt * ndl;
+      if (n1 > 0 && (a1 < 0 || a1 + n1 > lt.len)) return fail(i, "a1 range outside rowmat");
+      if (n2 > 0 && (a2 < 0 || a2 + n2 > lt.len)) return fail(i, "a2 range outside rowmat");
+    } else {
+      int64_t n1 = (int64_t)ndl * ndt;
+      if (n1 > 0 && (a1 < 0 || a1 + n1 > lt.len)) return fail(i, "a1 range outside rowmat");
+    }
+  }
+  return HMVM_OK;
+}
+
+int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, HostLayout &L,
+                 std::string &msg) {
+  int rc = validate_leaves(lt, msg);
+  if (rc) return rc;
+  if (opts.precision != HMVM_FP64 && opts.precision != HMVM_FP32) {
+    msg = "unsupported precision";
+    return HMVM_EINVAL;
+  }
+  try {
+    L = HostLayout();
+    L.precision = opts.precision;
+    L.elem_size = opts.precision == HMVM_FP64 ? 8 : 4;
+    L.vec = 16 / L.elem_size;
+    L.nd = lt.nd;
+    L.nlf = lt.nlf;
+    L.num_sms = num_sms > 0 ? num_sms : 148;
+    L.stage1_cfg = (opts.stage1_cfg >= 0 && opts.stage1_cfg < kNumCfgs) ? opts.stage1_cfg : kDefaultStage1Cfg;
+    L.stage2_cfg = (opts.stage2_cfg >= 0 && opts.stage2_cfg < kNumCfgs) ? opts.stage2_cfg : kDefaultStage2Cfg;
+    L.ctas_per_sm = opts.ctas_per_sm > 0 ? opts.ctas_per_sm : kDefaultCtasPerSm;
+    const int VEC = L.vec;
+    const int RMAX = (opts.max_tile_rows >= 1 && opts.max_tile_rows <= kMaxRows) ? opts.max_tile_rows : kMaxRows;
+    const int32_t nd = lt.nd, nlf = lt.nlf;
+
+    // ---- leaf classes ---------------------------------------------------
+    std::vector<uint8_t> live_lr(nlf, 0);
+    for (int32_t i = 0; i < nlf; i++) {
+      if (lt.ltmtx[i] == 1) {
+        L.n_lowrank++;
+        L.stored_elems += (int64_t)lt.kt[i] * (lt.ndl[i] + (int64_t)lt.ndt[i]);
+        live_lr[i] = lt.kt[i] > 0 && lt.ndl[i] > 0 && lt.ndt[i] > 0;
+      } else {
+        L.n_dense++;
+        L.stored_elems += (int64_t)lt.ndl[i] * lt.ndt[i];
+      }
+    }
+
+    // ---- row tiles: intervals between leaf row boundaries, <= RMAX rows ----
+    std::vector<int32_t> bnd;
+    bnd.reserve(2 * (size_t)nlf + 2);
+    bnd.push_back(0);
+    bnd.push_back(nd);
+    for (int32_t i = 0; i < nlf; i++) {
+      if (lt.ndl[i] <= 0) continue;
+      bnd.push_back(lt.nstrtl[i] - 1);
+      bnd.push_back(lt.nstrtl[i] - 1 + lt.ndl[i]);
+    }
+    std::sort(bnd.begin(), bnd.end());
+    bnd.erase(std::unique(bnd.begin(), bnd.end()), bnd.end());
+    std::vector<int32_t> trow0, tnrows;  // stage-2 row tiles in row order
+    for (size_t b = 0; b + 1 < bnd.size(); b++) {
+      int32_t a = bnd[b], e = bnd[b + 1], n = e - a;
+      int32_t pieces = (n + RMAX - 1) / RMAX;
+      for (int32_t p = 0; p < pieces; p++) {
+        int32_t s0 = a + (int32_t)((int64_t)n * p / pieces), s1 = a + (int32_t)((int64_t)n * (p + 1) / pieces);
+        trow0.push_back(s0);
+        tnrows.push_back(s1 - s0);
+      }
+    }
+    const int32_t nrt = (int32_t)trow0.size();
+    std::vector<int32_t> row_tile(nd > 0 ? nd : 1);
+    for (int32_t ti = 0; ti < nrt; ti++)
+      for (int32_t r = trow0[ti]; r < trow0[ti] + tnrows[ti]; r++) row_tile[r] = ti;
+
+    // ---- low-rank row groups and t slots ---------------------------------
+    std::unordered_map<uint64_t, int32_t> rgmap, cgmap;
+    std::vector<int32_t> rg_of(nlf, -1), cg_of(nlf, -1);
+    std::vector<std::vector<int32_t>> rg_members, cg_members;
+    for (int32_t i = 0; i < nlf; i++) {
+      if (!live_lr[i]) continue;
+      uint64_t kr = key2(lt.nstrtl[i], lt.ndl[i]);
+      auto it = rgmap.find(kr);
+      int32_t g;
+      if (it == rgmap.end()) {
+        g = (int32_t)rg_members.size();
+        rgmap.emplace(kr, g);
+        rg_members.emplace_back();
+      } else {
+        g = it->second;
+      }
+      rg_of[i] = g;
+      rg_members[g].push_back(i);
+      uint64_t kc = key2(lt.nstrtt[i], lt.ndt[i]);
+      auto jt = cgmap.find(kc);
+      int32_t c;
+      if (jt == cgmap.end()) {
+        c = (int32_t)cg_members.size();
+        cgmap.emplace(kc, c);
+        cg_members.emplace_back();
+      } else {
+        c = jt->second;
+      }
+      cg_of[i] = c;
+      cg_members[c].push_back(i);
+    }
+    const int32_t nrg = (int32_t)rg_members.size();
+    std::vector<int64_t> slot_of_leaf(nlf, -1);  // slot of (leaf, k=0)
+    std::vector<int32_t> rg_slot(nrg), rg_k(nrg);
+    int64_t t_len = 0;
+    for (int32_t g = 0; g < nrg; g++) {
+      rg_slot[g] = (int32_t)t_len;
+      int32_t k = 0;
+      for (int32_t i : rg_members[g]) {
+        slot_of_leaf[i] = t_len + k;
+        k += lt.kt[i];
+      }
+      rg_k[g] = k;
+      t_len += round_up(k, VEC);
+      if (t_len > INT32_MAX / 2) {
+        msg = "intermediate vector too long";
+        return HMVM_ERANGE;
+      }
+    }
+    L.t_len = t_len;
+
+    // ---- stage 1: column panels ------------------------------------------
+    const int32_t split = opts.split_cols > 0 ? std::max<int32_t>(opts.split_cols, VEC) : 4096;
+    std::vector<TileBuild> tb;
+    std::vector<SegBuild> sb;
+    std::vector<Part> parts;
+    std::vector<std::pair<int32_t, int32_t>> panel_rows;  // (leaf, k) per out_idx entry
+    int64_t p_len = 0;
+    for (int32_t c = 0; c < (int32_t)cg_members.size(); c++) {
+      const auto &mem = cg_members[c];
+      int32_t ndt = lt.ndt[mem[0]], st = lt.nstrtt[mem[0]];
+      std::vector<std::pair<int32_t, int32_t>> rows;
+      for (int32_t i : mem)
+        for (int32_t k = 0; k < lt.kt[i]; k++) rows.emplace_back(i, k);
+      // Column chunks of width w (a multiple of VEC) when the panel is wider than `split`.
+      const int32_t w = ndt > split ? std::max<int32_t>(VEC, split / VEC * VEC) : (int32_t)round_up(ndt, VEC);
+      const int32_t nchunks = ndt > split ? (ndt + w - 1) / w : 1;
+      for (size_t p0 = 0; p0 < rows.size(); p0 += kMaxRows) {
+        int32_t R = (int32_t)std::min<size_t>(kMaxRows, rows.size() - p0);
+        int32_t ob = (int32_t)L.out_idx.size();
+        for (int32_t r = 0; r < R; r++) {
+          auto lk = rows[p0 + r];
+          L.out_idx.push_back((int32_t)(slot_of_leaf[lk.first] + lk.second));
+          panel_rows.push_back(lk);
+        }
+        int64_t pb = p_len;
+        if (nchunks > 1) {
+          p_len += (int64_t)nchunks * kMaxRows;
+          for (int32_t r = 0; r < R; r++) {
+            L.red.push_back(L.out_idx[ob + r]);
+            L.red.push_back((int32_t)(pb + r));
+            L.red.push_back(nchunks);
+            L.red.push_back(0);
+          }
+          L.split_rows += R;
+        }
+        for (int32_t ch = 0; ch < nchunks; ch++) {
+          int32_t c0 = ch * w, c1 = std::min(ndt, c0 + w);
+          TileBuild t;
+          t.stage = 1;
+          t.cgroup = c;
+          t.nrows = R;
+          t.panel_row0 = ob;  // index into panel_rows / out_idx
+          t.col0 = c0;
+          t.mode = nchunks > 1 ? 2 : 1;
+          t.out_base = nchunks > 1 ? (int32_t)(pb + (int64_t)ch * kMaxRows) : ob;
+          t.seg_first = (int32_t)sb.size();
+          t.nseg = 1;
+          int32_t ncols = c1 - c0;
+          sb.push_back(SegBuild{st - 1 + c0, ncols, -1, 0});
+          t.nvec = (ncols + VEC - 1) / VEC;
+          t.cost = (int64_t)t.nvec * R * 16 + 1024;
+          tb.push_back(t);
+        }
+      }
+    }
+    if (p_len > INT32_MAX / 2) {
+      msg = "partial-sum buffer too long";
+      return HMVM_ERANGE;
+    }
+    L.p_len = p_len;
+    const int32_t n1 = (int32_t)tb.size();
+
+    // ---- stage 2: row tiles ---------------------------------------------
+    // Per tile: dense leaves (file order) and row groups touching it.
+    std::vector<int32_t> dcount(nrt + 1, 0), gcount(nrt + 1, 0);
+    for (int32_t i = 0; i < nlf; i++) {
+      if (lt.ltmtx[i] != 2 || lt.ndl[i] <= 0 || lt.ndt[i] <= 0) continue;
+      int32_t r0 = lt.nstrtl[i] - 1, r1 = r0 + lt.ndl[i];
+      for (int32_t ti = row_tile[r0]; ti < nrt && trow0[ti] < r1; ti++) dcount[ti + 1]++;
+    }
+    for (int32_t g = 0; g < nrg; g++) {
+      int32_t i = rg_members[g][0];
+      int32_t r0 = lt.nstrtl[i] - 1, r1 = r0 + lt.ndl[i];
+      for (int32_t ti = row_tile[r0]; ti < nrt && trow0[ti] < r1; ti++) gcount[ti + 1]++;
+    }
+    for (int32_t ti = 0; ti < nrt; ti++) {
+      dcount[ti + 1] += dcount[ti];
+      gcount[ti + 1] += gcount[ti];
+    }
+    std::vector<int32_t> dlist(dcount[nrt]), glist(gcount[nrt]);
+    {
+      std::vector<int32_t> dpos(dcount.begin(), dcount.end() - 1), gpos(gcount.begin(), gcount.end() - 1);
+      for (int32_t i = 0; i < nlf; i++) {
+        if (lt.ltmtx[i] != 2 || lt.ndl[i] <= 0 || lt.ndt[i] <= 0) continue;
+        int32_t r0 = lt.nstrtl[i] - 1, r1 = r0 + lt.ndl[i];
+        for (int32_t ti = row_tile[r0]; ti < nrt && trow0[ti] < r1; ti++) dlist[dpos[ti]++] = i;
+      }
+      for (int32_t g = 0; g < nrg; g++) {
+        int32_t i = rg_members[g][0];
+        int32_t r0 = lt.nstrtl[i] - 1, r1 = r0 + lt.ndl[i];
+        for (int32_t ti = row_tile[r0]; ti < nrt && trow0[ti] < r1; ti++) glist[gpos[ti]++] = g;
+      }
+    }
+    for (int32_t ti = 0; ti < nrt; ti++) {
+      TileBuild t;
+      t.stage = 2;
+      t.row0 = trow0[ti];
+      t.nrows = tnrows[ti];
+      t.mode = 0;
+      t.out_base = trow0[ti];
+      t.seg_first = (int32_t)sb.size();
+      int32_t nvec = 0;
+      // dense segments: merge leaves whose column ranges are adjacent
+      for (int32_t d = dcount[ti]; d < dcount[ti + 1]; d++) {
+        int32_t i = dlist[d];
+        int32_t src = lt.nstrtt[i] - 1;
+        if (t.nseg > 0) {
+          SegBuild &last = sb.back();
+          if (last.src >= 0 && last.src + last.ncols == src) {
+            last.ncols += lt.ndt[i];
+            last.nparts++;
+            parts.push_back(Part{i, -1, lt.ndt[i]});
+            continue;
+          }
+        }
+        sb.push_back(SegBuild{src, lt.ndt[i], (int32_t)parts.size(), 1});
+        parts.push_back(Part{i, -1, lt.ndt[i]});
+        t.nseg++;
+      }
+      for (int32_t gg = gcount[ti]; gg < gcount[ti + 1]; gg++) {
+        int32_t g = glist[gg];
+        sb.push_back(SegBuild{kTFlag | rg_slot[g], rg_k[g], (int32_t)parts.size(), 1});
+        parts.push_back(Part{-1, g, rg_k[g]});
+        t.nseg++;
+      }
+      for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) nvec += (sb[s].ncols + VEC - 1) / VEC;
+      t.nvec = nvec;
+      t.cost = (int64_t)nvec * t.nrows * 16 + 1024 + 128 * t.nseg;
+      tb.push_back(t);
+    }
+    const int32_t n2 = (int32_t)tb.size() - n1;
+
+    // ---- team assignment (LPT) and ordering --------------------------------
+    auto assign = [&](int32_t first, int32_t count, int32_t nteams, std::vector<int32_t> &order,
+                      std::vector<int32_t> &team_begin) {
+      std::vector<int32_t> idx(count);
+      for (int32_t k = 0; k < count; k++) idx[k] = first + k;
+      std::stable_sort(idx.begin(), idx.end(), [&](int32_t a, int32_t b) { return tb[a].cost > tb[b].cost; });
+      using HE = std::pair<int64_t, int32_t>;
+      std::priority_queue<HE, std::vector<HE>, std::greater<HE>> heap;
+      for (int32_t k = 0; k < nteams; k++) heap.emplace(0, k);
+      std::vector<int32_t> team_of(count);
+      for (int32_t k : idx) {
+        HE h = heap.top();
+        heap.pop();
+        team_of[k - first] = h.second;
+        heap.emplace(h.first + tb[k].cost, h.second);
+      }
+      std::vector<int32_t> cnt(nteams + 1, 0);
+      for (int32_t k = 0; k < count; k++) cnt[team_of[k] + 1]++;
+      for (int32_t k = 0; k < nteams; k++) cnt[k + 1] += cnt[k];
+      team_begin.assign(cnt.begin(), cnt.end());
+      std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1);
+      order.resize(count);
+      for (int32_t k = 0; k < count; k++) order[pos[team_of[k]]++] = first + k;  // tile order within team
+    };
+    const int32_t ctas = L.num_sms * L.ctas_per_sm;
+    L.stage1_teams = ctas * kCfgs[L.stage1_cfg].tpc;
+    L.stage2_teams = ctas * kCfgs[L.stage2_cfg].tpc;
+    std::vector<int32_t> ord1, ord2, tb1, tb2;
+    assign(0, n1, L.stage1_teams, ord1, tb1);
+    assign(n1, n2, L.stage2_teams, ord2, tb2);
+    std::vector<int32_t> order;
+    order.reserve(tb.size());
+    order.insert(order.end(), ord1.begin(), ord1.end());
+    order.insert(order.end(), ord2.begin(), ord2.end());
+    L.team_begin1 = tb1;
+    L.team_begin2.resize(tb2.size());
+    for (size_t k = 0; k < tb2.size(); k++) L.team_begin2[k] = tb2[k] + n1;
+    L.stage1_tiles = n1;
+    L.stage2_tiles = n2;
+
+    // ---- final descriptors, data offsets ---------------------------------
+    const int32_t ntiles = (int32_t)tb.size();
+    L.tiles.resize(ntiles);
+    L.segs.clear();
+    L.segs.reserve(sb.size());
+    std::vector<int64_t> data_off(ntiles);
+    int64_t off = 0;
+    for (int32_t k = 0; k < ntiles; k++) {
+      const TileBuild &t = tb[order[k]];
+      hmvm_tile_desc &d = L.tiles[k];
+      d.data_off = off;
+      d.seg_begin = (int32_t)L.segs.size();
+      d.nseg = t.nseg;
+      d.nvec = t.nvec;
+      d.out_base = t.out_base;
+      d.nrows = (int16_t)t.nrows;
+      d.mode = (int16_t)t.mode;
+      d._pad = 0;
+      for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) L.segs.push_back(hmvm_seg_desc{sb[s].src, sb[s].ncols});
+      data_off[k] = off;
+      off += (int64_t)t.nvec * t.nrows;
+    }
+    L.data.resize((size_t)off);
+
+    // ---- pack ------------------------------------------------------------
+    const bool srcf = lt.rowmat_is_float;
+    const bool dstf = L.precision == HMVM_FP32;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int32_t k = 0; k < ntiles; k++) {
+      const TileBuild &t = tb[order[k]];
+      const int32_t R = t.nrows;
+      const int64_t tile_elems = (int64_t)t.nvec * R * VEC;
+      char *base = reinterpret_cast<char *>(L.data.data() + data_off[k]);
+      std::memset(base, 0, (size_t)tile_elems * L.elem_size);
+      auto put = [&](int64_t c, int32_t r, double v) {
+        int64_t vi = c / VEC, e = c % VEC;
+        int64_t at = (vi * R + r) * VEC + e;
+        if (dstf) reinterpret_cast<float *>(base)[at] = (float)v;
+        else reinterpret_cast<double *>(base)[at] = v;
+      };
+      auto get = [&](int64_t idx) { return srcf ? rd<float>(lt.rowmat, idx) : rd<double>(lt.rowmat, idx); };
+      if (t.stage == 1) {
+        const SegBuild &s = sb[t.seg_first];
+        for (int32_t r = 0; r < R; r++) {
+          auto lk = panel_rows[t.panel_row0 + r];
+          int32_t i = lk.first, kk = lk.second;
+          int64_t src0 = lt.a1(i) + (int64_t)kk * lt.ndt[i] + t.col0;
+          for (int32_t c = 0; c < s.ncols; c++) put(c, r, get(src0 + c));
+        }
+      } else {
+        int64_t col = 0;
+        for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) {
+          const SegBuild &sg = sb[s];
+          int64_t segcol0 = col;
+          int64_t pc = 0;  // column within segment
+          for (int32_t p = sg.part_first; p < sg.part_first + sg.nparts; p++) {
+            const Part &pt = parts[p];
+            if (pt.leaf >= 0) {
+              int32_t i = pt.leaf, ndt = lt.ndt[i];
+              int32_t rs = lt.nstrtl[i] - 1;
+              for (int32_t r = 0; r < R; r++) {
+                int64_t src0 = lt.a1(i) + (int64_t)(t.row0 + r - rs) * ndt;
+                for (int32_t c = 0; c < ndt; c++) put(segcol0 + pc + c, r, get(src0 + c));
+              }
+              pc += ndt;
+            } else {
+              int64_t kc = 0;
+              for (int32_t i : rg_members[pt.group]) {
+                int32_t ndl = lt.ndl[i], rs = lt.nstrtl[i] - 1;
+                for (int32_t kk = 0; kk < lt.kt[i]; kk++) {
+                  int64_t src0 = lt.a2(i) + (int64_t)kk * ndl + (t.row0 - rs);
+                  for (int32_t r = 0; r < R; r++) put(segcol0 + pc + kc, r, get(src0 + r));
+                  kc++;
+                }
+              }
+              pc += kc;
+            }
+          }
+          // next segment starts at the next vector boundary
+          col = round_up(segcol0 + sg.ncols, VEC);
+        }
+      }
+    }
+  } catch (const std::bad_alloc &) {
+    msg = "host allocation failed while building the layout";
+    return HMVM_ENOMEM;
+  }
+  return HMVM_OK;
+}
+
+}  // namespace hmvm

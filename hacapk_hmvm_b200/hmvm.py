@@ -1,0 +1,189 @@
+"""HMVM on the GPU through the C ABI (include/hmvm_b200.h).
+
+``Plan``       one H-matrix repacked and resident on the device; ``apply`` runs
+               y = H x on device buffers, ``apply_host`` on numpy arrays.
+``hmvm``       one-shot y = H x from host arrays (the C ``hmvm_cuda_d/f``).
+``hmvm_cuda``  mirror of the reference harness entry point
+               ``hmvm_cuda<T>(mat2, b, kernel, dump_result, nbench)``
+               (src_hmvm/src_cpp/hmvm_cuda.h:4-7): optional result dump at
+               %.3E and a TIME line over nbench timed runs after 5 warm-ups.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+from . import _lib
+from .hmatrix import HMatrix
+
+PRECISIONS = {"fp64": _lib.HMVM_FP64, "fp32": _lib.HMVM_FP32, "double": _lib.HMVM_FP64, "float": _lib.HMVM_FP32}
+
+
+def _dev_ptr(t):
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    return int(t.data_ptr())
+
+
+def _stream_handle(stream):
+    if stream is None:
+        try:
+            import torch
+
+            if torch.cuda.is_available():
+                return int(torch.cuda.current_stream().cuda_stream)
+        except ImportError:
+            pass
+        return 0
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)
+
+
+def default_opts(**kw) -> _lib.PlanOpts:
+    o = _lib.PlanOpts()
+    _lib.hmvm_lib().hmvm_b200_default_opts(C.byref(o))
+    for k, v in kw.items():
+        if v is not None:
+            setattr(o, k, int(v))
+    return o
+
+
+class Plan:
+    """A resident, repacked H-matrix on one GPU."""
+
+    def __init__(self, hm: HMatrix, precision: str = "fp64", device: int = -1, **opts):
+        lib = _lib.hmvm_lib()
+        prec = PRECISIONS[precision]
+        o = default_opts(precision=prec, device=device, **opts)
+        h = C.c_void_p()
+        t0 = time.perf_counter()
+        if hm.fits_matrix2():
+            m2 = hm.as_matrix2()
+            if hm.rowmat.dtype == np.float32:
+                rc = lib.hmvm_b200_plan_create_f(C.byref(m2), C.byref(o), C.byref(h))
+            else:
+                rc = lib.hmvm_b200_plan_create_d(C.byref(m2), C.byref(o), C.byref(h))
+        else:
+            lv = hm.as_leaves64()
+            fn = lib.hmvm_b200_plan_create64_f if hm.rowmat.dtype == np.float32 else lib.hmvm_b200_plan_create64_d
+            rc = fn(C.byref(lv), C.byref(o), C.byref(h))
+        _lib.check(rc, "plan create")
+        self.setup_seconds = time.perf_counter() - t0
+        self._h = h
+        self.hm = hm
+        self.precision = "fp64" if prec == _lib.HMVM_FP64 else "fp32"
+        self.dtype = np.float64 if prec == _lib.HMVM_FP64 else np.float32
+        self.nd = hm.nd
+
+    @property
+    def handle(self):
+        if not self._h:
+            raise RuntimeError("plan is closed")
+        return self._h
+
+    def info(self) -> dict:
+        inf = _lib.PlanInfo()
+        _lib.check(_lib.hmvm_lib().hmvm_b200_plan_get_info(self.handle, C.byref(inf)), "plan info")
+        return {f: getattr(inf, f) for f, _ in _lib.PlanInfo._fields_ if not f.startswith("_")}
+
+    def profile(self, enable: bool = True) -> None:
+        _lib.check(_lib.hmvm_lib().hmvm_b200_plan_profile(self.handle, int(enable)), "profile")
+
+    def profile_read(self) -> tuple[list[float], int]:
+        """(summed ms of [V stage, reduction, row stage], number of applies)."""
+        ms = (C.c_double * 3)()
+        n = C.c_int32()
+        _lib.check(_lib.hmvm_lib().hmvm_b200_plan_profile_read(self.handle, ms, C.byref(n)), "profile_read")
+        return [ms[0], ms[1], ms[2]], int(n.value)
+
+    def kernel_count(self) -> int:
+        return int(_lib.hmvm_lib().hmvm_b200_plan_kernel_count(self.handle))
+
+    def apply(self, x, y, stream=None) -> None:
+        """y = H x; x and y are CUDA tensors (or raw device addresses)."""
+        rc = _lib.hmvm_lib().hmvm_b200_apply(self.handle, _dev_ptr(x), _dev_ptr(y), _stream_handle(stream))
+        _lib.check(rc, "apply")
+
+    def apply_host(self, x: np.ndarray, y: np.ndarray | None = None, stream=None) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=self.dtype)
+        if x.shape != (self.nd,):
+            raise ValueError(f"x must have shape ({self.nd},)")
+        if y is None:
+            y = np.empty(self.nd, dtype=self.dtype)
+        rc = _lib.hmvm_lib().hmvm_b200_apply_host(self.handle, x.ctypes.data, y.ctypes.data,
+                                                  _stream_handle(stream) if stream is not None else 0)
+        _lib.check(rc, "apply_host")
+        return y
+
+    def close(self) -> None:
+        if self._h:
+            _lib.hmvm_lib().hmvm_b200_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def hmvm(hm: HMatrix, x: np.ndarray, mode: int = 0) -> tuple[np.ndarray, dict]:
+    """One-shot y = H x (plan, run, release) through hmvm_cuda_d / hmvm_cuda_f."""
+    lib = _lib.hmvm_lib()
+    st = _lib.Stats()
+    m2 = hm.as_matrix2()
+    if hm.rowmat.dtype == np.float32:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.empty(hm.nd, np.float32)
+        rc = lib.hmvm_cuda_f(C.byref(m2), x.ctypes.data, y.ctypes.data, int(mode), C.byref(st))
+    else:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(hm.nd, np.float64)
+        rc = lib.hmvm_cuda_d(C.byref(m2), x.ctypes.data, y.ctypes.data, int(mode), C.byref(st))
+    _lib.check(rc, "hmvm_cuda")
+    return y, {f: getattr(st, f) for f, _ in _lib.Stats._fields_}
+
+
+def hmvm_cuda(hm: HMatrix, b: np.ndarray, kernel: int = 0, dump_result: int = 0, nbench: int = 5,
+              name: str | None = None) -> np.ndarray:
+    """Reference-shaped entry: dump y to result_cuda_b200_<name>.txt at %.3E when
+    dump_result, and print ``TIME <nbench> hmvm_cuda_<name> min .. max .. avg ..``
+    over nbench timed runs after 5 untimed ones (the reference's M=5 warm-ups,
+    hmvm_cuda2.cu:234-302).  Times are device times (CUDA events)."""
+    tname = "d" if hm.rowmat.dtype == np.float64 else "f"
+    name = name or f"b200_k{kernel}_{tname}"
+    with Plan(hm, "fp64" if tname == "d" else "fp32") as plan:
+        y = plan.apply_host(b)
+        if dump_result:
+            with open(f"result_cuda_{name}.txt", "w") as f:
+                for v in y:
+                    f.write("%.3E\n" % v)
+        if nbench > 0:
+            import torch
+
+            dt = torch.float64 if tname == "d" else torch.float32
+            xd = torch.from_numpy(np.ascontiguousarray(b, dtype=plan.dtype)).to("cuda")
+            yd = torch.empty(hm.nd, dtype=dt, device="cuda")
+            times = []
+            for _ in range(5 + nbench):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                plan.apply(xd, yd)
+                e1.record()
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1) * 1e-3)
+            t = np.array(times[5:])
+            print(f"TIME {nbench} hmvm_cuda_{name} min {t.min():e} max {t.max():e} avg {t.mean():e}")
+    return y

@@ -1,0 +1,245 @@
+/*
+ * hmvm_b200.h -- H-matrix-vector multiplication on one NVIDIA B200 (C ABI).
+ *
+ * A drop-in for the HMVM path of the reference harness (hacapk_hmvm,
+ * src_hmvm/src_cpp): the same H-matrix structures and files, and y = H x over
+ * the HACApK leaf list, computed by hand-written sm_100a kernels.
+ *
+ * Conventions
+ *   - Every function returns HMVM_OK (0) or a negative HMVM_E* status; none of
+ *     them exits the process (the reference prints and calls exit(-1),
+ *     src_hmvm/src_cpp/hmvm_cuda0.cu:11).  hmvm_b200_last_error() gives the
+ *     message of the calling thread's last failure.
+ *   - Row/column indices nstrtl/nstrtt are 1-based, as written by HACApK.
+ *   - The library owns the device memory of a plan; the caller owns x and y.
+ *   - There is no CPU fallback: without a usable CUDA device, plan creation and
+ *     every compute call return HMVM_ENODEV.
+ */
+#ifndef HMVM_B200_H
+#define HMVM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define HMVM_OK 0
+#define HMVM_EINVAL -1   /* bad argument or inconsistent leaf table */
+#define HMVM_ENOMEM -2   /* host or device allocation failed */
+#define HMVM_ECUDA -3    /* a CUDA runtime call failed */
+#define HMVM_EIO -4      /* file could not be opened or read */
+#define HMVM_EFORMAT -5  /* file is not a well-formed hmatrix_1.bin / hmatrix_2.bin */
+#define HMVM_ERANGE -6   /* a count exceeds what the structure or format can hold */
+#define HMVM_ENODEV -7   /* no usable CUDA device */
+#define HMVM_EDEVICE -8  /* a kernel reported an error status */
+
+/* ---- H-matrix structures ------------------------------------------------ */
+/* Byte-compatible with the reference templates (src_hmvm/src_cpp/hacapk.h:5-36)
+ * instantiated for double / float.  Low-rank leaf (ltmtx==1): rowmat[a1..] is
+ * V^T as [kt][ndt], rowmat[a2..] is U as [kt][ndl]; dense leaf (ltmtx==2):
+ * rowmat[a1..] is [ndl][ndt] row-major.  rowmat_t holds the same data with U
+ * transposed to [ndl][kt] (loadmatrix.cpp:227-234). */
+typedef struct hmvm_submatrix_d {
+  int ltmtx, kt, ndl, ndt, nstrtl, nstrtt;
+  double *a1, *a2, *a2t;
+} hmvm_submatrix_d;
+typedef struct hmvm_submatrix_f {
+  int ltmtx, kt, ndl, ndt, nstrtl, nstrtt;
+  float *a1, *a2, *a2t;
+} hmvm_submatrix_f;
+
+typedef struct hmvm_matrix_d {
+  int nd, nlf, ktmax;
+  int *nleavs;
+  hmvm_submatrix_d *submat;
+  int b1, b2, b3, e1, e2, e3;
+} hmvm_matrix_d;
+typedef struct hmvm_matrix_f {
+  int nd, nlf, ktmax;
+  int *nleavs;
+  hmvm_submatrix_f *submat;
+  int b1, b2, b3, e1, e2, e3;
+} hmvm_matrix_f;
+
+typedef struct hmvm_matrix2_d {
+  int nd, nlf, ktmax, len;
+  int *nleavs;
+  int *ltmtx, *kt, *ndl, *ndt, *nstrtl, *nstrtt;
+  int *a1, *a2;
+  double *rowmat, *rowmat_t;
+  int napprox, ndense;
+  int *approx, *dense;
+} hmvm_matrix2_d;
+typedef struct hmvm_matrix2_f {
+  int nd, nlf, ktmax, len;
+  int *nleavs;
+  int *ltmtx, *kt, *ndl, *ndt, *nstrtl, *nstrtt;
+  int *a1, *a2;
+  float *rowmat, *rowmat_t;
+  int napprox, ndense;
+  int *approx, *dense;
+} hmvm_matrix2_f;
+
+/* The same leaf table with 64-bit element offsets, for matrices whose stored
+ * element count overflows matrix2's int `len` / `a1` / `a2`
+ * (src_hmvm/src_cpp/hacapk.h:28,31).  `rowmat` is double or float as named by
+ * the create call it is passed to. */
+typedef struct hmvm_leaves64 {
+  int32_t nd, nlf, ktmax, _pad0;
+  int64_t len;
+  const int32_t *ltmtx, *kt, *ndl, *ndt, *nstrtl, *nstrtt;
+  const int64_t *a1, *a2;
+  const void *rowmat;
+} hmvm_leaves64;
+
+/* ---- loaders (replace src_hmvm/src_cpp/loadmatrix.cpp) ------------------ */
+/* Replaces loadHmatrix (loadmatrix.cpp:7-150): reads hmatrix_1.bin into the AoS
+ * and SoA forms (mat may be NULL to skip the AoS copies).  Record markers and
+ * leaf fields are validated; on error nothing is left allocated. */
+int hmvm_b200_load_hmatrix(const char *fname, hmvm_matrix_d *mat, hmvm_matrix2_d *mat2);
+/* Replaces loadHmatrix2 (loadmatrix.cpp:152-250): reads hmatrix_2.bin into SoA. */
+int hmvm_b200_load_hmatrix2(const char *fname, hmvm_matrix2_d *mat2);
+/* Replaces convertD2F (loadmatrix.cpp:252-342): FP64 -> FP32 copies; either
+ * source may be NULL. */
+int hmvm_b200_convert_d2f(hmvm_matrix_f *matF, hmvm_matrix2_f *matF2, const hmvm_matrix_d *matD,
+                          const hmvm_matrix2_d *matD2);
+/* Release what the loaders / convert allocated (the reference never frees). */
+void hmvm_b200_free_matrix_d(hmvm_matrix_d *mat);
+void hmvm_b200_free_matrix_f(hmvm_matrix_f *mat);
+void hmvm_b200_free_matrix2_d(hmvm_matrix2_d *mat2);
+void hmvm_b200_free_matrix2_f(hmvm_matrix2_f *mat2);
+
+/* ---- plans: a leaf table repacked and resident on the GPU ---------------- */
+typedef struct hmvm_plan hmvm_plan;
+
+enum hmvm_precision {
+  HMVM_FP64 = 0, /* FP64 storage, FP64 arithmetic */
+  HMVM_FP32 = 1  /* FP32 storage, FP32 arithmetic (the reference's float mode) */
+};
+
+typedef struct hmvm_plan_opts {
+  int32_t precision;      /* enum hmvm_precision */
+  int32_t device;         /* CUDA device ordinal, -1 = current device */
+  int32_t max_tile_rows;  /* rows per row tile, 1..32 (0 = 32) */
+  int32_t split_cols;     /* low-rank column panels wider than this are split (0 = auto) */
+  int32_t stage1_cfg;     /* kernel configuration index for the V stage (-1 = default) */
+  int32_t stage2_cfg;     /* kernel configuration index for the row stage (-1 = default) */
+  int32_t ctas_per_sm;    /* persistent CTAs per SM (0 = default) */
+  int32_t _reserved;
+} hmvm_plan_opts;
+
+typedef struct hmvm_plan_info {
+  int32_t nd, nlf, n_lowrank, n_dense;
+  int32_t precision, device, num_sms, _pad0;
+  int64_t algorithmic_bytes; /* stored leaf elements once + x + y, as the reference stores them */
+  int64_t device_bytes;      /* repacked matrix bytes resident on the GPU (incl. padding) */
+  int64_t t_len;             /* length of the intermediate V x vector */
+  int32_t stage1_tiles, stage2_tiles, stage1_teams, stage2_teams;
+  int32_t split_rows, kernels_per_apply, stage1_cfg, stage2_cfg;
+  int64_t flops;             /* 2 * stored elements */
+  int64_t stage1_bytes;      /* algorithmic bytes of the V stage: V elements + x */
+  int64_t stage2_bytes;      /* algorithmic bytes of the row stage: U + dense elements + x + y */
+} hmvm_plan_info;
+
+void hmvm_b200_default_opts(hmvm_plan_opts *opts);
+
+/* Build a plan from the reference's SoA structure (replaces the per-call
+ * cudaMalloc/cudaMemcpy of every matrix2 array in hmvm_cuda1.cu:333-353 with a
+ * one-time repack + upload).  For HMVM_FP32 from a double matrix the elements
+ * are rounded to float exactly as convertD2F does. */
+int hmvm_b200_plan_create_d(const hmvm_matrix2_d *mat2, const hmvm_plan_opts *opts, hmvm_plan **plan);
+int hmvm_b200_plan_create_f(const hmvm_matrix2_f *mat2, const hmvm_plan_opts *opts, hmvm_plan **plan);
+/* 64-bit leaf table, rowmat in double / float. */
+int hmvm_b200_plan_create64_d(const hmvm_leaves64 *lv, const hmvm_plan_opts *opts, hmvm_plan **plan);
+int hmvm_b200_plan_create64_f(const hmvm_leaves64 *lv, const hmvm_plan_opts *opts, hmvm_plan **plan);
+void hmvm_b200_plan_destroy(hmvm_plan *plan);
+int hmvm_b200_plan_get_info(const hmvm_plan *plan, hmvm_plan_info *info);
+
+/* y = H x with x, y in device memory of the plan's device (double for FP64
+ * plans, float for FP32 plans); y is overwritten, x and y must not overlap.
+ * Launches asynchronously on `stream` (a cudaStream_t, NULL = legacy default
+ * stream).  The kernels sum in a fixed order, so repeated calls on the same
+ * inputs give bitwise-identical y.  Replaces the kernel launch of
+ * hmvm_cuda{0,1,2,3} (e.g. hmvm_cuda2.cu:262-306). */
+int hmvm_b200_apply(hmvm_plan *plan, const void *x_dev, void *y_dev, void *stream);
+/* The same with host buffers: copies x in, runs, copies y out, and waits for
+ * the stream. */
+int hmvm_b200_apply_host(hmvm_plan *plan, const void *x_host, void *y_host, void *stream);
+
+/* Per-stage device timing.  While enabled, every apply records CUDA events
+ * around its launches on the launch stream (up to 4096 applies are kept);
+ * profile_read waits for the last recorded apply, returns the summed
+ * milliseconds of stage 0 (V stage), 1 (split-panel reduction), 2 (row stage)
+ * and the number of applies, and clears the record. */
+int hmvm_b200_plan_profile(hmvm_plan *plan, int enable);
+int hmvm_b200_plan_profile_read(hmvm_plan *plan, double *stage_ms3, int32_t *napplies);
+
+/* ---- one-shot call with the reference's shape ---------------------------- */
+typedef struct hmvm_stats {
+  double seconds_setup;  /* plan creation (repack + upload) */
+  double seconds_apply;  /* device time of the HMVM itself (CUDA events) */
+  int64_t algorithmic_bytes;
+  double gbytes_per_s;   /* algorithmic bytes / seconds_apply / 1e9 */
+} hmvm_stats;
+
+/* y = H x from host arrays: plan, apply once, release (the reference's
+ * hmvm_cuda<T>(mat2, b, kernel, dump, nbench) minus the dump and timing loop,
+ * with an output argument the reference lacks).  stats may be NULL. */
+int hmvm_cuda_d(const hmvm_matrix2_d *mat2, const double *x, double *y, int mode, hmvm_stats *stats);
+int hmvm_cuda_f(const hmvm_matrix2_f *mat2, const float *x, float *y, int mode, hmvm_stats *stats);
+
+/* ---- inspection (host only; no GPU needed) ------------------------------ */
+/* Builds the repacked layout on the host exactly as plan creation does, so it
+ * can be checked without a device.  Arrays stay owned by the layout. */
+typedef struct hmvm_layout hmvm_layout;
+typedef struct hmvm_layout_view {
+  int32_t precision, vec;            /* vec = elements per 16-byte vector */
+  int32_t n_tiles, n_segs;           /* all stages */
+  int32_t stage1_tiles, stage2_tiles; /* tiles [0,stage1) are stage 1, then stage 2 */
+  int32_t stage1_teams, stage2_teams;
+  int32_t n_red, nd;
+  int64_t data_vectors;              /* 16-byte vectors in the data stream */
+  int64_t t_len, p_len;
+  const void *tiles;                 /* hmvm_tile_desc[n_tiles] */
+  const void *segs;                  /* hmvm_seg_desc[n_segs] */
+  const int32_t *team_begin1;        /* [stage1_teams+1], indexes tiles */
+  const int32_t *team_begin2;        /* [stage2_teams+1], indexes tiles */
+  const int32_t *out_idx;            /* stage-1 output slots */
+  const int32_t *red;                /* [n_red][4]: slot, pbase, nchunk, 0 */
+  const void *data;                  /* data_vectors * 16 bytes */
+} hmvm_layout_view;
+
+/* Tile and segment records as stored in the data structures above. */
+typedef struct hmvm_tile_desc {
+  int64_t data_off;  /* first 16-byte vector of the tile in the data stream */
+  int32_t seg_begin, nseg, nvec, out_base;
+  int16_t nrows, mode; /* mode 0: y[out_base+r]; 1: t[out_idx[out_base+r]]; 2: partial[out_base+r] */
+  int32_t _pad;
+} hmvm_tile_desc;
+typedef struct hmvm_seg_desc {
+  int32_t src;   /* x index, or (t index | 0x80000000) */
+  int32_t ncols;
+} hmvm_seg_desc;
+
+int hmvm_b200_layout_build_d(const hmvm_matrix2_d *mat2, const hmvm_plan_opts *opts, int32_t num_sms,
+                             hmvm_layout **layout);
+int hmvm_b200_layout_build64(const hmvm_leaves64 *lv, int32_t rowmat_is_float, const hmvm_plan_opts *opts,
+                             int32_t num_sms, hmvm_layout **layout);
+int hmvm_b200_layout_view(const hmvm_layout *layout, hmvm_layout_view *view);
+void hmvm_b200_layout_destroy(hmvm_layout *layout);
+
+/* ---- misc --------------------------------------------------------------- */
+const char *hmvm_b200_strerror(int status);
+const char *hmvm_b200_last_error(void);
+int hmvm_b200_version(void);
+/* Number of kernel launches one apply issues for this plan. */
+int hmvm_b200_plan_kernel_count(const hmvm_plan *plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HMVM_B200_H */

@@ -107,7 +107,19 @@ void* ref_wrap2(int nd, int nlf, int ktmax, int len, int* ltmtx, int* kt, int* n
   m->a1 = a1;
   m->a2 = a2;
   m->rowmat = rowmat;
-  m->rowmat_t = nullptr;
+  // rowmat_t as the reference loader builds it (loadmatrix.cpp:216-242): the
+  // reference's convertD2F copies it, so it must exist.
+  m->rowmat_t = (double*)malloc(sizeof(double) * (size_t)(len > 0 ? len : 1));
+  for (int i = 0; i < nlf; i++) {
+    if (ltmtx[i] == 1) {
+      memcpy(&m->rowmat_t[a1[i]], &rowmat[a1[i]], sizeof(double) * (size_t)kt[i] * ndt[i]);
+      for (int y = 0; y < kt[i]; y++)
+        for (int x = 0; x < ndl[i]; x++)
+          m->rowmat_t[a2[i] + y + x * kt[i]] = rowmat[a2[i] + y * ndl[i] + x];
+    } else {
+      memcpy(&m->rowmat_t[a1[i]], &rowmat[a1[i]], sizeof(double) * (size_t)ndl[i] * ndt[i]);
+    }
+  }
   m->napprox = 0;
   m->ndense = 0;
   m->approx = nullptr;
@@ -199,6 +211,7 @@ void ref_free(void* hv) {
   RefHandle* h = static_cast<RefHandle*>(hv);
   if (!h) return;
   // The reference never frees its matrices; release what the loaders allocated.
+  if (h->matD2 && h->wrapped) free(h->matD2->rowmat_t);
   if (h->matD2 && !h->wrapped) {
     free(h->matD2->ltmtx); free(h->matD2->kt); free(h->matD2->ndl); free(h->matD2->ndt);
     free(h->matD2->nstrtl); free(h->matD2->nstrtt); free(h->matD2->a1); free(h->matD2->a2);

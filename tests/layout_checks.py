@@ -1,0 +1,57 @@
+"""Bounds checks of a layout: every address the kernels form stays inside its buffer."""
+import ctypes as C
+
+import numpy as np
+
+
+def check_layout_bounds(view):
+    from hacapk_hmvm_b200 import _lib
+
+    VEC = view.vec
+    nt = view.n_tiles
+    tiles = np.ctypeslib.as_array((_lib.TileDesc * nt).from_address(view.tiles)) if nt else None
+    segs = np.ctypeslib.as_array((_lib.SegDesc * view.n_segs).from_address(view.segs)) if view.n_segs else None
+    tb1 = np.ctypeslib.as_array(view.team_begin1, (view.stage1_teams + 1,))
+    tb2 = np.ctypeslib.as_array(view.team_begin2, (view.stage2_teams + 1,))
+    assert tb1[0] == 0 and tb1[-1] == view.stage1_tiles and np.all(np.diff(tb1) >= 0)
+    assert tb2[0] == view.stage1_tiles and tb2[-1] == nt and np.all(np.diff(tb2) >= 0)
+    n_out = 0
+    covered = np.zeros(view.nd, np.int32)
+    for k in range(nt):
+        td = tiles[k]
+        R, nvec, off = int(td["nrows"]), int(td["nvec"]), int(td["data_off"])
+        assert 1 <= R <= 32 and nvec >= 0
+        assert 0 <= off and off + nvec * R <= view.data_vectors
+        s0, ns = int(td["seg_begin"]), int(td["nseg"])
+        assert 0 <= s0 and s0 + ns <= view.n_segs
+        tot = 0
+        for s in range(s0, s0 + ns):
+            src, ncols = int(segs[s]["src"]), int(segs[s]["ncols"])
+            assert ncols >= 1
+            if src < 0:
+                slot = src & 0x7FFFFFFF
+                assert slot % VEC == 0
+                assert slot + -(-ncols // VEC) * VEC <= view.t_len
+            else:
+                assert 0 <= src and src + ncols <= view.nd
+            tot += -(-ncols // VEC)
+        assert tot == nvec
+        ob, mode = int(td["out_base"]), int(td["mode"])
+        if k < view.stage1_tiles:
+            assert mode in (1, 2)
+            if mode == 2:
+                assert 0 <= ob and ob + R <= view.p_len
+            else:
+                n_out = max(n_out, ob + R)
+        else:
+            assert mode == 0 and 0 <= ob and ob + R <= view.nd
+            covered[ob:ob + R] += 1
+    assert np.all(covered == 1), "stage-2 tiles must cover every row exactly once"
+    if n_out:
+        out_idx = np.ctypeslib.as_array(view.out_idx, (n_out,))
+        assert np.all((out_idx >= 0) & (out_idx < view.t_len))
+        assert len(np.unique(out_idx)) == len(out_idx)
+    if view.n_red:
+        red = np.ctypeslib.as_array(view.red, (view.n_red * 4,)).reshape(-1, 4)
+        assert np.all((red[:, 0] >= 0) & (red[:, 0] < view.t_len))
+        assert np.all(red[:, 1] >= 0) and np.all(red[:, 1] + (red[:, 2] - 1) * 32 < view.p_len)
