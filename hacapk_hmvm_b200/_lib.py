@@ -26,6 +26,8 @@ HMVM_EDEVICE = -8
 HMVM_FP64 = 0
 HMVM_FP32 = 1
 
+HMVM_NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024
+
 _ip = C.POINTER(C.c_int)
 
 
@@ -151,6 +153,7 @@ HMVM_SIGNATURES = {
     "hmvm_b200_plan_get_info": (C.c_int, [C.c_void_p, C.POINTER(PlanInfo)]),
     "hmvm_b200_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hmvm_b200_apply_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "hmvm_b200_apply_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hmvm_cuda_d": (C.c_int, [C.POINTER(Matrix2_d), C.c_void_p, C.c_void_p, C.c_int, C.POINTER(Stats)]),
     "hmvm_cuda_f": (C.c_int, [C.POINTER(Matrix2_f), C.c_void_p, C.c_void_p, C.c_int, C.POINTER(Stats)]),
     "hmvm_b200_layout_build_d": (C.c_int, [C.POINTER(Matrix2_d), C.POINTER(PlanOpts), C.c_int32,

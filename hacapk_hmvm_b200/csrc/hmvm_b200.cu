@@ -6,6 +6,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -541,6 +542,107 @@ int hmvm_cuda_f(const hmvm_matrix2_f* mat2, const float* x, float* y, int mode, 
   }
   hmvm_b200_plan_destroy(plan);
   return rc;
+}
+
+}  // extern "C"
+
+// ---- apply without allocation ----------------------------------------------
+// The scratch of hmvm_b200_apply_noalloc: a file-scope device array, reserved
+// on every GPU that loads the library until the process exits.  Host code must
+// not pass its name to a kernel: on the host it only stands in for the symbol,
+// so its device address is looked up with cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[HMVM_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoallocMaxDevices] = {};
+
+// Device address of the scratch array on `dev`, which must be the current
+// device; looked up once per device and cached.
+int noalloc_scratch(int dev, void** out) {
+  if (dev < 0 || dev >= kNoallocMaxDevices) return set_error(HMVM_EINVAL, "device ordinal beyond the scratch table");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* addr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress of the no-alloc scratch");
+    g_noalloc_addr[dev] = addr;
+  }
+  *out = g_noalloc_addr[dev];
+  return HMVM_OK;
+}
+
+// The stages of launch_apply with t and the partial sums in caller-provided
+// scratch.  t's padding slots must read as zero, and earlier calls (of any
+// plan) left other values there, so t is cleared first; the partial sums are
+// written in full before they are read.
+template <typename T>
+int launch_apply_noalloc(hmvm_plan* p, const void* x, void* y, void* tbuf, size_t tbytes, void* pbuf,
+                         cudaStream_t st) {
+  HMVM_CUDA_TRY(cudaMemsetAsync(tbuf, 0, tbytes, st), "clear the no-alloc scratch");
+  TileArgs a;
+  a.tiles = p->d_tiles;
+  a.segs = p->d_segs;
+  a.data = p->d_data;
+  a.x = x;
+  a.t = tbuf;
+  a.y = y;
+  a.p = pbuf;
+  a.out_idx = p->d_out_idx;
+  const int ctas = p->num_sms * p->ctas_per_sm;
+  if (p->stage1_tiles > 0) {
+    const KernelCfg c = kCfgs[p->stage1_cfg];
+    a.team_begin = p->d_tb1;
+    a.nteams = p->stage1_teams;
+    tile_kernel_for<T>(p->stage1_cfg)<<<ctas, 32 * c.wg * c.tpc, 0, st>>>(a);
+    HMVM_CUDA_TRY(cudaGetLastError(), "stage-1 launch");
+  }
+  if (p->n_red > 0) {
+    int blocks = (p->n_red + 255) / 256;
+    hmvm_reduce_kernel<T><<<blocks, 256, 0, st>>>(p->d_red, p->n_red, static_cast<const T*>(pbuf),
+                                                  static_cast<T*>(tbuf));
+    HMVM_CUDA_TRY(cudaGetLastError(), "reduction launch");
+  }
+  const KernelCfg c = kCfgs[p->stage2_cfg];
+  a.team_begin = p->d_tb2;
+  a.nteams = p->stage2_teams;
+  tile_kernel_for<T>(p->stage2_cfg)<<<ctas, 32 * c.wg * c.tpc, 0, st>>>(a);
+  HMVM_CUDA_TRY(cudaGetLastError(), "stage-2 launch");
+  return HMVM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hmvm_b200_apply_noalloc(hmvm_plan* p, const void* x, void* y, void* stream) {
+  if (!p) return set_error(HMVM_EINVAL, "plan is NULL");
+  if (p->nd > 0 && (!x || !y)) return set_error(HMVM_EINVAL, "x or y is NULL");
+  const char* xb = static_cast<const char*>(x);
+  const char* yb = static_cast<const char*>(y);
+  const size_t nb = (size_t)p->nd * p->elem;
+  if (p->nd > 0 && xb < yb + nb && yb < xb + nb) return set_error(HMVM_EINVAL, "x and y overlap");
+  auto round256 = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t tbytes = round256((size_t)(p->t_len + 16) * p->elem);
+  const size_t pbytes = round256((size_t)(p->p_len + 16) * p->elem);
+  if (tbytes + pbytes > (size_t)HMVM_NOALLOC_SCRATCH_BYTES)
+    return set_error(HMVM_ERANGE, "this plan needs " + std::to_string(tbytes + pbytes) +
+                                      " bytes of scratch but hmvm_b200_apply_noalloc has " +
+                                      std::to_string((size_t)HMVM_NOALLOC_SCRATCH_BYTES) +
+                                      "; use hmvm_b200_apply");
+  if (p->nd == 0) return HMVM_OK;
+  DeviceGuard g(p->device);
+  if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
+  void* base = nullptr;
+  int rc = noalloc_scratch(p->device, &base);
+  if (rc) return rc;
+  char* tbuf = static_cast<char*>(base);
+  char* pbuf = tbuf + tbytes;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (p->precision == HMVM_FP64) return launch_apply_noalloc<double>(p, x, y, tbuf, tbytes, pbuf, st);
+  return launch_apply_noalloc<float>(p, x, y, tbuf, tbytes, pbuf, st);
 }
 
 // ---- inspection --------------------------------------------------------

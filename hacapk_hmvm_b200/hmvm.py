@@ -109,6 +109,13 @@ class Plan:
         rc = _lib.hmvm_lib().hmvm_b200_apply(self.handle, _dev_ptr(x), _dev_ptr(y), _stream_handle(stream))
         _lib.check(rc, "apply")
 
+    def apply_noalloc(self, x, y, stream=None) -> None:
+        """y = H x without any GPU allocation: the scratch comes from the
+        library's fixed 16 MiB device array (hmvm_b200_apply_noalloc), for
+        callers that may not call cudaMalloc while they run."""
+        rc = _lib.hmvm_lib().hmvm_b200_apply_noalloc(self.handle, _dev_ptr(x), _dev_ptr(y), _stream_handle(stream))
+        _lib.check(rc, "apply_noalloc")
+
     def apply_host(self, x: np.ndarray, y: np.ndarray | None = None, stream=None) -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=self.dtype)
         if x.shape != (self.nd,):

@@ -169,6 +169,28 @@ int hmvm_b200_apply(hmvm_plan *plan, const void *x_dev, void *y_dev, void *strea
  * the stream. */
 int hmvm_b200_apply_host(hmvm_plan *plan, const void *x_host, void *y_host, void *stream);
 
+/* Capacity of the scratch array used by hmvm_b200_apply_noalloc: 16 MiB. */
+#define HMVM_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+
+/* y = H x exactly like hmvm_b200_apply, for callers that must not allocate GPU
+ * memory while they run: a solver embedded in an application that hands out
+ * all device memory from its own pool and forbids further cudaMalloc/cudaFree
+ * once it is running, or code whose device-memory budget is fixed at start-up.
+ * This call allocates nothing.  Its scratch -- the intermediate V x vector and
+ * the partial sums of split panels -- lives in one library-wide array of
+ * HMVM_NOALLOC_SCRATCH_BYTES in device memory, which every GPU that loads the
+ * library holds until the process exits.  A plan whose scratch (t_len + 16 and
+ * p_len + 16 elements, each rounded up to 256 bytes; see hmvm_plan_info.t_len)
+ * does not fit is rejected with HMVM_ERANGE.  The first call on each device
+ * looks up that array's device address (once per device, with that device
+ * current); make that first call before any stream capture.  All calls share
+ * the array and it keeps the last call's contents: the call clears, on
+ * `stream` and before its kernels, the part that has to start at zero.  Calls
+ * whose work overlaps on the GPU (other streams, threads or plans running at
+ * the same time) race on the array; order them on one stream or synchronise
+ * between them.  No counterpart in the reference. */
+int hmvm_b200_apply_noalloc(hmvm_plan *plan, const void *x_dev, void *y_dev, void *stream);
+
 /* Per-stage device timing.  While enabled, every apply records CUDA events
  * around its launches on the launch stream (up to 4096 applies are kept);
  * profile_read waits for the last recorded apply, returns the summed
