@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--stage1-cfg", type=int, default=-1)
     ap.add_argument("--stage2-cfg", type=int, default=-1)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
+    ap.add_argument("--kernel", type=int, default=-1, help="0: register-streaming, 1: TMA-ring (default)")
     return ap.parse_args()
 
 
@@ -256,7 +257,7 @@ def run_b200(a, rank, world, local_rank):
     x = rng.uniform(-1.0, 1.0, hm.nd)
     t0 = time.perf_counter()
     plan = Plan(hm, a.precision, device=local_rank, stage1_cfg=a.stage1_cfg, stage2_cfg=a.stage2_cfg,
-                ctas_per_sm=a.ctas_per_sm)
+                ctas_per_sm=a.ctas_per_sm, kernel=a.kernel)
     setup_s = time.perf_counter() - t0
     info = plan.info()
     tdt = torch.float64 if a.precision == "fp64" else torch.float32
@@ -338,13 +339,16 @@ def run_b200(a, rank, world, local_rank):
 
     # ---- roofline of the dominant kernel ----
     peak, peak_kind = measured_peak_gbs()
-    stage_bytes = [info["stage1_bytes"], 0, info["stage2_bytes"]]
+    stage_bytes = [info["stage1_bytes"], 0, info["stage2_bytes"], 0]
     dom = int(np.argmax(stage_ms))
     dom_avg_s = stage_ms[dom] / max(napplies, 1) * 1e-3
     achieved = stage_bytes[dom] / dom_avg_s / 1e9 if dom_avg_s > 0 else 0.0
     alg_bytes = info["algorithmic_bytes"]
+    kname = "hmvm_stream_kernel" if info["kernel"] == 1 else "hmvm_tile_kernel"
     roof = {
-        "bound": "hbm", "kernel": ["hmvm_tile_kernel (V stage)", "hmvm_reduce_kernel", "hmvm_tile_kernel (row stage)"][dom],
+        "bound": "hbm",
+        "kernel": [f"{kname} (V stage)", "hmvm_reduce_kernel (V stage)", f"{kname} (row stage)",
+                   "hmvm_reduce_kernel (row stage)"][dom],
         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
         "traffic": None,
         "whole_hmvm_gbs": alg_bytes / (ms_step * 1e-3) / 1e9,
@@ -356,7 +360,8 @@ def run_b200(a, rank, world, local_rank):
     if rank == 0:
         value = world * 1e3 / ms_step
         cfg = workload_config(a, hm)
-        cfg.update({"stage1_cfg": info["stage1_cfg"], "stage2_cfg": info["stage2_cfg"],
+        cfg.update({"kernel": kname, "stage1_cfg": info["stage1_cfg"], "stage2_cfg": info["stage2_cfg"],
+                    "ctas_per_sm": info["ctas_per_sm"],
                     "device_bytes": info["device_bytes"], "plan_setup_s": setup_s})
         line = {
             "metric": "HMVM/s", "value": value, "unit": "HMVM/s", "n_gpus": world, "steps": a.steps,

@@ -81,7 +81,7 @@ class Leaves64(C.Structure):
 class PlanOpts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("device", C.c_int32), ("max_tile_rows", C.c_int32),
                 ("split_cols", C.c_int32), ("stage1_cfg", C.c_int32), ("stage2_cfg", C.c_int32),
-                ("ctas_per_sm", C.c_int32), ("_reserved", C.c_int32)]
+                ("ctas_per_sm", C.c_int32), ("kernel", C.c_int32)]
 
 
 class PlanInfo(C.Structure):
@@ -91,7 +91,8 @@ class PlanInfo(C.Structure):
                 ("stage1_tiles", C.c_int32), ("stage2_tiles", C.c_int32), ("stage1_teams", C.c_int32),
                 ("stage2_teams", C.c_int32), ("split_rows", C.c_int32), ("kernels_per_apply", C.c_int32),
                 ("stage1_cfg", C.c_int32), ("stage2_cfg", C.c_int32), ("flops", C.c_int64),
-                ("stage1_bytes", C.c_int64), ("stage2_bytes", C.c_int64)]
+                ("stage1_bytes", C.c_int64), ("stage2_bytes", C.c_int64),
+                ("kernel", C.c_int32), ("ctas_per_sm", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -111,11 +112,12 @@ class SegDesc(C.Structure):
 class LayoutView(C.Structure):
     _fields_ = [("precision", C.c_int32), ("vec", C.c_int32), ("n_tiles", C.c_int32), ("n_segs", C.c_int32),
                 ("stage1_tiles", C.c_int32), ("stage2_tiles", C.c_int32), ("stage1_teams", C.c_int32),
-                ("stage2_teams", C.c_int32), ("n_red", C.c_int32), ("nd", C.c_int32),
+                ("stage2_teams", C.c_int32), ("n_red1", C.c_int32), ("n_red2", C.c_int32), ("nd", C.c_int32),
+                ("kernel", C.c_int32),
                 ("data_vectors", C.c_int64), ("t_len", C.c_int64), ("p_len", C.c_int64),
                 ("tiles", C.c_void_p), ("segs", C.c_void_p), ("team_begin1", C.POINTER(C.c_int32)),
                 ("team_begin2", C.POINTER(C.c_int32)), ("out_idx", C.POINTER(C.c_int32)),
-                ("red", C.POINTER(C.c_int32)), ("data", C.c_void_p)]
+                ("red1", C.POINTER(C.c_int32)), ("red2", C.POINTER(C.c_int32)), ("data", C.c_void_p)]
 
 
 class HgenParams(C.Structure):
@@ -168,6 +170,7 @@ HMVM_SIGNATURES = {
     "hmvm_b200_plan_kernel_count": (C.c_int, [C.c_void_p]),
     "hmvm_b200_plan_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "hmvm_b200_plan_profile_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
+    "hmvm_b200_plan_status": (C.c_int, [C.c_void_p]),
 }
 
 HGEN_SIGNATURES = {

@@ -1,8 +1,10 @@
 // C-ABI of the B200 HMVM library: plan creation (host planner + upload),
-// kernel dispatch, host-buffer apply and the one-shot reference-shaped call.
+// kernel dispatch, host-buffer apply, the one-shot reference-shaped call, and
+// the allocation-free apply.
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -29,9 +31,9 @@ int cuda_fail(cudaError_t e, const char* what) {
   return set_error(e == cudaErrorMemoryAllocation ? HMVM_ENOMEM : HMVM_ECUDA, m);
 }
 
-#define HMVM_CUDA_TRY(call, what)          \
-  do {                                     \
-    cudaError_t e_ = (call);               \
+#define HMVM_CUDA_TRY(call, what)                      \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
     if (e_ != cudaSuccess) return cuda_fail(e_, what); \
   } while (0)
 
@@ -49,10 +51,10 @@ struct DeviceGuard {
   }
 };
 
-using TileKernelFn = void (*)(TileArgs);
+using KernelFn = void (*)(TileArgs);
 
 template <typename T>
-TileKernelFn tile_kernel_for(int cfg) {
+KernelFn tile_kernel_for(int cfg) {
   switch (cfg) {
     case 0: return hmvm_tile_kernel<T, 1, 8>;
     case 1: return hmvm_tile_kernel<T, 2, 4>;
@@ -65,6 +67,31 @@ TileKernelFn tile_kernel_for(int cfg) {
   }
 }
 
+// Must list kStreamCfgs (layout.hpp) in order.
+template <typename T>
+KernelFn stream_kernel_for(int cfg) {
+  switch (cfg) {
+    case 0: return hmvm_stream_kernel<T, 8, 4, 1024, 256>;
+    case 1: return hmvm_stream_kernel<T, 4, 4, 2048, 512>;
+    case 2: return hmvm_stream_kernel<T, 8, 4, 2048, 256>;
+    case 3: return hmvm_stream_kernel<T, 16, 4, 1024, 128>;
+    case 4: return hmvm_stream_kernel<T, 4, 8, 1024, 512>;
+    default: return hmvm_stream_kernel<T, 8, 8, 512, 256>;
+  }
+}
+
+struct Launch {
+  KernelFn fn;
+  int threads, smem;
+};
+
+template <typename T>
+Launch stage_launch(int kernel, int cfg) {
+  if (kernel == 0) return Launch{tile_kernel_for<T>(cfg), 32 * kCfgs[cfg].wg * kCfgs[cfg].tpc, 0};
+  const StreamCfg& c = kStreamCfgs[cfg];
+  return Launch{stream_kernel_for<T>(cfg), 32 * c.wpb, stream_smem_bytes(c, (int)sizeof(T))};
+}
+
 }  // namespace hmvm
 
 using namespace hmvm;
@@ -74,8 +101,8 @@ struct hmvm_plan {
   int precision = HMVM_FP64;
   int elem = 8;
   int32_t nd = 0, nlf = 0, n_lowrank = 0, n_dense = 0;
-  int num_sms = 0, ctas_per_sm = 2, stage1_cfg = 0, stage2_cfg = 0;
-  int32_t stage1_tiles = 0, stage2_tiles = 0, stage1_teams = 0, stage2_teams = 0, n_red = 0;
+  int num_sms = 0, kernel = 1, ctas_per_sm = 3, stage1_cfg = 0, stage2_cfg = 0;
+  int32_t stage1_tiles = 0, stage2_tiles = 0, stage1_teams = 0, stage2_teams = 0, n_red1 = 0, n_red2 = 0;
   int64_t stored_elems = 0, device_bytes = 0, t_len = 0, p_len = 0;
   // device buffers
   void* d_data = nullptr;
@@ -84,13 +111,15 @@ struct hmvm_plan {
   int32_t* d_tb1 = nullptr;
   int32_t* d_tb2 = nullptr;
   int32_t* d_out_idx = nullptr;
-  int4* d_red = nullptr;
+  int4* d_red1 = nullptr;
+  int4* d_red2 = nullptr;
   void* d_t = nullptr;
   void* d_p = nullptr;
+  int* d_err = nullptr;
   void* d_x = nullptr;  // staging for apply_host
   void* d_y = nullptr;
   int64_t stage1_bytes = 0, stage2_bytes = 0;
-  // profiling: 4 events per recorded apply (before stage 1, reduce, stage 2, after)
+  // profiling: kEventsPerApply events per recorded apply
   bool profiling = false;
   std::vector<cudaEvent_t> prof_events;
   int prof_count = 0;
@@ -103,12 +132,13 @@ struct hmvm_layout {
 namespace {
 
 constexpr int kMaxProfiled = 4096;
+constexpr int kEventsPerApply = 5;
 
 void free_plan_buffers(hmvm_plan* p) {
   for (cudaEvent_t e : p->prof_events) cudaEventDestroy(e);
   p->prof_events.clear();
-  void* bufs[] = {p->d_data, p->d_tiles, p->d_segs, p->d_tb1, p->d_tb2, p->d_out_idx,
-                  p->d_red,  p->d_t,     p->d_p,    p->d_x,   p->d_y};
+  void* bufs[] = {p->d_data, p->d_tiles, p->d_segs, p->d_tb1, p->d_tb2, p->d_out_idx, p->d_red1,
+                  p->d_red2, p->d_t,     p->d_p,    p->d_err, p->d_x,  p->d_y};
   for (void* b : bufs)
     if (b) cudaFree(b);
 }
@@ -145,6 +175,50 @@ int upload(Buf** dst, const void* src, size_t bytes, int64_t* total) {
   return HMVM_OK;
 }
 
+// Dynamic shared memory beyond 48 KB must be enabled per kernel.
+template <typename T>
+int prepare_kernels(const hmvm_plan* p) {
+  for (int cfg : {p->stage1_cfg, p->stage2_cfg}) {
+    Launch l = stage_launch<T>(p->kernel, cfg);
+    if (l.smem > 0)
+      HMVM_CUDA_TRY(cudaFuncSetAttribute((const void*)l.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, l.smem),
+                    "cudaFuncSetAttribute");
+  }
+  return HMVM_OK;
+}
+
+// CTAs per SM that stay resident for both stage kernels of the configuration
+// `o` selects (its defaults resolved as the planner resolves them).
+template <typename T>
+int resident_ctas_t(int kernel, int cfg1, int cfg2, int* out) {
+  int best = 64;
+  for (int cfg : {cfg1, cfg2}) {
+    const Launch l = stage_launch<T>(kernel, cfg);
+    if (l.smem > 0)
+      HMVM_CUDA_TRY(cudaFuncSetAttribute((const void*)l.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, l.smem),
+                    "cudaFuncSetAttribute");
+    int nb = 0;
+    HMVM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)l.fn, l.threads, l.smem),
+                  "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    best = std::min(best, std::max(nb, 1));
+  }
+  *out = best;
+  return HMVM_OK;
+}
+
+int resident_ctas(const hmvm_plan_opts& o, int dev, int* out) {
+  DeviceGuard g(dev);
+  if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
+  const int kernel = o.kernel == 0 ? 0 : 1;
+  const int ncfg = kernel == 0 ? kNumCfgs : kNumStreamCfgs;
+  const int c1 = (o.stage1_cfg >= 0 && o.stage1_cfg < ncfg) ? o.stage1_cfg
+                 : (kernel == 0 ? kDefaultStage1Cfg : kDefaultStreamCfg);
+  const int c2 = (o.stage2_cfg >= 0 && o.stage2_cfg < ncfg) ? o.stage2_cfg
+                 : (kernel == 0 ? kDefaultStage2Cfg : kDefaultStreamCfg);
+  return o.precision == HMVM_FP64 ? resident_ctas_t<double>(kernel, c1, c2, out)
+                                  : resident_ctas_t<float>(kernel, c1, c2, out);
+}
+
 int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** out) {
   if (!out) return set_error(HMVM_EINVAL, "plan output pointer is NULL");
   *out = nullptr;
@@ -154,6 +228,12 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   int dev = 0, sms = 0;
   int rc = check_device(opts.device, &dev, &sms);
   if (rc) return rc;
+  if (opts.ctas_per_sm <= 0) {
+    // Persistent grids: as many CTAs per SM as can be resident at once, so no
+    // CTA waits for another to finish.
+    rc = resident_ctas(opts, dev, &opts.ctas_per_sm);
+    if (rc) return rc;
+  }
   HostLayout* L = new (std::nothrow) HostLayout();
   if (!L) return set_error(HMVM_ENOMEM, "host allocation failed");
   std::string msg;
@@ -175,6 +255,7 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   p->n_lowrank = L->n_lowrank;
   p->n_dense = L->n_dense;
   p->num_sms = sms;
+  p->kernel = L->kernel;
   p->ctas_per_sm = L->ctas_per_sm;
   p->stage1_cfg = L->stage1_cfg;
   p->stage2_cfg = L->stage2_cfg;
@@ -182,7 +263,8 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   p->stage2_tiles = L->stage2_tiles;
   p->stage1_teams = L->stage1_teams;
   p->stage2_teams = L->stage2_teams;
-  p->n_red = (int32_t)(L->red.size() / 4);
+  p->n_red1 = (int32_t)(L->red1.size() / 4);
+  p->n_red2 = (int32_t)(L->red2.size() / 4);
   p->stored_elems = L->stored_elems;
   p->t_len = L->t_len;
   p->p_len = L->p_len;
@@ -206,7 +288,8 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
     if (!rc) rc = upload(&p->d_tb1, L->team_begin1.data(), L->team_begin1.size() * 4, nullptr);
     if (!rc) rc = upload(&p->d_tb2, L->team_begin2.data(), L->team_begin2.size() * 4, nullptr);
     if (!rc) rc = upload(&p->d_out_idx, L->out_idx.data(), L->out_idx.size() * 4, nullptr);
-    if (!rc) rc = upload(&p->d_red, L->red.data(), L->red.size() * 4, nullptr);
+    if (!rc) rc = upload(&p->d_red1, L->red1.data(), L->red1.size() * 4, nullptr);
+    if (!rc) rc = upload(&p->d_red2, L->red2.data(), L->red2.size() * 4, nullptr);
     // t: the padding slots of every row group must read as zero; stage 1 only
     // ever writes real slots, so one clear at creation keeps them zero.
     size_t tbytes = (size_t)(L->t_len + 16) * L->elem_size;
@@ -219,6 +302,12 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
       cudaError_t e = cudaMalloc(&p->d_p, (size_t)(L->p_len + 16) * L->elem_size);
       if (e != cudaSuccess) rc = cuda_fail(e, "partial buffer");
     }
+    if (!rc) {
+      cudaError_t e = cudaMalloc(&p->d_err, sizeof(int));
+      if (e == cudaSuccess) e = cudaMemset(p->d_err, 0, sizeof(int));
+      if (e != cudaSuccess) rc = cuda_fail(e, "status word");
+    }
+    if (!rc) rc = p->precision == HMVM_FP64 ? prepare_kernels<double>(p) : prepare_kernels<float>(p);
     if (!rc) {
       cudaError_t e = cudaDeviceSynchronize();
       if (e != cudaSuccess) rc = cuda_fail(e, "plan upload");
@@ -234,59 +323,77 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   return HMVM_OK;
 }
 
+// The launches of one HMVM: V stage, its reduction into t, row stage, its
+// reduction into y.  t and the partial sums live in tbuf / pbuf.
 template <typename T>
-int launch_apply(hmvm_plan* p, const void* x, void* y, cudaStream_t st) {
+int launch_stages(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, cudaStream_t st) {
   TileArgs a;
+  a.err = p->d_err;
   a.tiles = p->d_tiles;
   a.segs = p->d_segs;
   a.data = p->d_data;
   a.x = x;
-  a.t = p->d_t;
+  a.t = tbuf;
   a.y = y;
-  a.p = p->d_p;
+  a.p = pbuf;
   a.out_idx = p->d_out_idx;
   const int ctas = p->num_sms * p->ctas_per_sm;
   cudaEvent_t* ev = nullptr;
   if (p->profiling && p->prof_count < kMaxProfiled) {
-    ev = &p->prof_events[4 * (size_t)p->prof_count];
+    ev = &p->prof_events[kEventsPerApply * (size_t)p->prof_count];
     p->prof_count++;
   }
   if (ev) cudaEventRecord(ev[0], st);
   if (p->stage1_tiles > 0) {
-    const KernelCfg c = kCfgs[p->stage1_cfg];
+    const Launch l = stage_launch<T>(p->kernel, p->stage1_cfg);
     a.team_begin = p->d_tb1;
     a.nteams = p->stage1_teams;
-    tile_kernel_for<T>(p->stage1_cfg)<<<ctas, 32 * c.wg * c.tpc, 0, st>>>(a);
-    HMVM_CUDA_TRY(cudaGetLastError(), "stage-1 launch");
+    l.fn<<<ctas, l.threads, l.smem, st>>>(a);
+    HMVM_CUDA_TRY(cudaGetLastError(), "V-stage launch");
   }
   if (ev) cudaEventRecord(ev[1], st);
-  if (p->n_red > 0) {
-    int blocks = (p->n_red + 255) / 256;
-    hmvm_reduce_kernel<T><<<blocks, 256, 0, st>>>(p->d_red, p->n_red, static_cast<const T*>(p->d_p),
-                                                  static_cast<T*>(p->d_t));
-    HMVM_CUDA_TRY(cudaGetLastError(), "reduction launch");
+  if (p->n_red1 > 0) {
+    hmvm_reduce_kernel<T><<<(p->n_red1 + 255) / 256, 256, 0, st>>>(p->d_red1, p->n_red1,
+                                                                   static_cast<const T*>(pbuf), static_cast<T*>(tbuf));
+    HMVM_CUDA_TRY(cudaGetLastError(), "V-stage reduction launch");
   }
   if (ev) cudaEventRecord(ev[2], st);
   {
-    const KernelCfg c = kCfgs[p->stage2_cfg];
+    const Launch l = stage_launch<T>(p->kernel, p->stage2_cfg);
     a.team_begin = p->d_tb2;
     a.nteams = p->stage2_teams;
-    tile_kernel_for<T>(p->stage2_cfg)<<<ctas, 32 * c.wg * c.tpc, 0, st>>>(a);
-    HMVM_CUDA_TRY(cudaGetLastError(), "stage-2 launch");
+    l.fn<<<ctas, l.threads, l.smem, st>>>(a);
+    HMVM_CUDA_TRY(cudaGetLastError(), "row-stage launch");
   }
   if (ev) cudaEventRecord(ev[3], st);
+  if (p->n_red2 > 0) {
+    hmvm_reduce_kernel<T><<<(p->n_red2 + 255) / 256, 256, 0, st>>>(p->d_red2, p->n_red2,
+                                                                   static_cast<const T*>(pbuf), static_cast<T*>(y));
+    HMVM_CUDA_TRY(cudaGetLastError(), "row-stage reduction launch");
+  }
+  if (ev) cudaEventRecord(ev[4], st);
   return HMVM_OK;
 }
 
 int apply_impl(hmvm_plan* p, const void* x, void* y, cudaStream_t st) {
   if (p->nd == 0) return HMVM_OK;
-  if (p->precision == HMVM_FP64) return launch_apply<double>(p, x, y, st);
-  return launch_apply<float>(p, x, y, st);
+  if (p->precision == HMVM_FP64) return launch_stages<double>(p, x, y, p->d_t, p->d_p, st);
+  return launch_stages<float>(p, x, y, p->d_t, p->d_p, st);
 }
 
-int make_table_from_matrix2(int nd, int nlf, int ktmax, int len, const int* ltmtx, const int* kt, const int* ndl,
-                            const int* ndt, const int* nstrtl, const int* nstrtt, const int* a1, const int* a2,
-                            const void* rowmat, bool is_float, LeafTable& lt) {
+int check_xy(const hmvm_plan* p, const void* x, const void* y) {
+  if (!p) return set_error(HMVM_EINVAL, "plan is NULL");
+  if (p->nd > 0 && (!x || !y)) return set_error(HMVM_EINVAL, "x or y is NULL");
+  const char* xb = static_cast<const char*>(x);
+  const char* yb = static_cast<const char*>(y);
+  const size_t nb = (size_t)p->nd * p->elem;
+  if (p->nd > 0 && xb < yb + nb && yb < xb + nb) return set_error(HMVM_EINVAL, "x and y overlap");
+  return HMVM_OK;
+}
+
+void make_table_from_matrix2(int nd, int nlf, int ktmax, int len, const int* ltmtx, const int* kt, const int* ndl,
+                             const int* ndt, const int* nstrtl, const int* nstrtt, const int* a1, const int* a2,
+                             const void* rowmat, bool is_float, LeafTable& lt) {
   lt.nd = nd;
   lt.nlf = nlf;
   lt.ktmax = ktmax;
@@ -301,7 +408,6 @@ int make_table_from_matrix2(int nd, int nlf, int ktmax, int len, const int* ltmt
   lt.a2_32 = a2;
   lt.rowmat = rowmat;
   lt.rowmat_is_float = is_float;
-  return HMVM_OK;
 }
 
 void table_from_leaves64(const hmvm_leaves64* lv, bool is_float, LeafTable& lt) {
@@ -335,6 +441,7 @@ void hmvm_b200_default_opts(hmvm_plan_opts* o) {
   o->stage1_cfg = -1;
   o->stage2_cfg = -1;
   o->ctas_per_sm = 0;
+  o->kernel = -1;
 }
 
 int hmvm_b200_plan_create_d(const hmvm_matrix2_d* m, const hmvm_plan_opts* opts, hmvm_plan** plan) {
@@ -401,13 +508,15 @@ int hmvm_b200_plan_get_info(const hmvm_plan* p, hmvm_plan_info* info) {
   info->stage2_tiles = p->stage2_tiles;
   info->stage1_teams = p->stage1_teams;
   info->stage2_teams = p->stage2_teams;
-  info->split_rows = p->n_red;
+  info->split_rows = p->n_red1 + p->n_red2;
   info->kernels_per_apply = hmvm_b200_plan_kernel_count(p);
   info->stage1_cfg = p->stage1_cfg;
   info->stage2_cfg = p->stage2_cfg;
   info->flops = 2 * p->stored_elems;
   info->stage1_bytes = p->stage1_bytes;
   info->stage2_bytes = p->stage2_bytes;
+  info->kernel = p->kernel;
+  info->ctas_per_sm = p->ctas_per_sm;
   return HMVM_OK;
 }
 
@@ -416,7 +525,7 @@ int hmvm_b200_plan_profile(hmvm_plan* p, int enable) {
   DeviceGuard g(p->device);
   if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
   if (enable && p->prof_events.empty()) {
-    p->prof_events.resize(4 * (size_t)kMaxProfiled);
+    p->prof_events.resize(kEventsPerApply * (size_t)kMaxProfiled);
     for (auto& e : p->prof_events) HMVM_CUDA_TRY(cudaEventCreate(&e), "cudaEventCreate");
   }
   p->profiling = enable != 0;
@@ -424,18 +533,21 @@ int hmvm_b200_plan_profile(hmvm_plan* p, int enable) {
   return HMVM_OK;
 }
 
-int hmvm_b200_plan_profile_read(hmvm_plan* p, double* ms3, int32_t* napplies) {
-  if (!p || !ms3) return set_error(HMVM_EINVAL, "NULL argument");
+int hmvm_b200_plan_profile_read(hmvm_plan* p, double* ms4, int32_t* napplies) {
+  if (!p || !ms4) return set_error(HMVM_EINVAL, "NULL argument");
   DeviceGuard g(p->device);
-  ms3[0] = ms3[1] = ms3[2] = 0.0;
-  int n = p->prof_count;
-  if (n > 0) HMVM_CUDA_TRY(cudaEventSynchronize(p->prof_events[4 * (size_t)(n - 1) + 3]), "event sync");
+  for (int s = 0; s < 4; s++) ms4[s] = 0.0;
+  const int n = p->prof_count;
+  if (n > 0)
+    HMVM_CUDA_TRY(cudaEventSynchronize(p->prof_events[kEventsPerApply * (size_t)(n - 1) + kEventsPerApply - 1]),
+                  "event sync");
   for (int k = 0; k < n; k++) {
-    for (int s = 0; s < 3; s++) {
+    for (int s = 0; s < kEventsPerApply - 1; s++) {
       float ms = 0.f;
-      HMVM_CUDA_TRY(cudaEventElapsedTime(&ms, p->prof_events[4 * (size_t)k + s], p->prof_events[4 * (size_t)k + s + 1]),
+      HMVM_CUDA_TRY(cudaEventElapsedTime(&ms, p->prof_events[kEventsPerApply * (size_t)k + s],
+                                         p->prof_events[kEventsPerApply * (size_t)k + s + 1]),
                     "cudaEventElapsedTime");
-      ms3[s] += ms;
+      ms4[s] += ms;
     }
   }
   if (napplies) *napplies = n;
@@ -443,18 +555,25 @@ int hmvm_b200_plan_profile_read(hmvm_plan* p, double* ms3, int32_t* napplies) {
   return HMVM_OK;
 }
 
+int hmvm_b200_plan_status(hmvm_plan* p) {
+  if (!p) return set_error(HMVM_EINVAL, "plan is NULL");
+  DeviceGuard g(p->device);
+  int h = 0;
+  HMVM_CUDA_TRY(cudaMemcpy(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost), "read status word");
+  if (h == 0) return HMVM_OK;
+  HMVM_CUDA_TRY(cudaMemset(p->d_err, 0, sizeof(int)), "clear status word");
+  return set_error(HMVM_EDEVICE, h == 1 ? "a kernel gave up waiting for its bulk copies"
+                                        : "a kernel found a stream region too large");
+}
+
 int hmvm_b200_plan_kernel_count(const hmvm_plan* p) {
   if (!p || p->nd == 0) return 0;
-  return (p->stage1_tiles > 0) + (p->n_red > 0) + 1;
+  return (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1 + (p->n_red2 > 0);
 }
 
 int hmvm_b200_apply(hmvm_plan* p, const void* x, void* y, void* stream) {
-  if (!p) return set_error(HMVM_EINVAL, "plan is NULL");
-  if (p->nd > 0 && (!x || !y)) return set_error(HMVM_EINVAL, "x or y is NULL");
-  const char* xb = static_cast<const char*>(x);
-  const char* yb = static_cast<const char*>(y);
-  size_t nb = (size_t)p->nd * p->elem;
-  if (p->nd > 0 && xb < yb + nb && yb < xb + nb) return set_error(HMVM_EINVAL, "x and y overlap");
+  int rc = check_xy(p, x, y);
+  if (rc) return rc;
   DeviceGuard g(p->device);
   if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
   return apply_impl(p, x, y, static_cast<cudaStream_t>(stream));
@@ -497,6 +616,7 @@ static int one_shot(hmvm_plan* plan, const void* x, void* y, hmvm_stats* stats, 
       cudaError_t e = cudaMemcpy(y, plan->d_y, nb, cudaMemcpyDeviceToHost);
       if (e != cudaSuccess) rc = cuda_fail(e, "copy y");
     }
+    if (!rc) rc = hmvm_b200_plan_status(plan);
   }
   float ms = 0.f;
   if (!rc && plan->nd > 0) cudaEventElapsedTime(&ms, e0, e1);
@@ -574,56 +694,13 @@ int noalloc_scratch(int dev, void** out) {
   return HMVM_OK;
 }
 
-// The stages of launch_apply with t and the partial sums in caller-provided
-// scratch.  t's padding slots must read as zero, and earlier calls (of any
-// plan) left other values there, so t is cleared first; the partial sums are
-// written in full before they are read.
-template <typename T>
-int launch_apply_noalloc(hmvm_plan* p, const void* x, void* y, void* tbuf, size_t tbytes, void* pbuf,
-                         cudaStream_t st) {
-  HMVM_CUDA_TRY(cudaMemsetAsync(tbuf, 0, tbytes, st), "clear the no-alloc scratch");
-  TileArgs a;
-  a.tiles = p->d_tiles;
-  a.segs = p->d_segs;
-  a.data = p->d_data;
-  a.x = x;
-  a.t = tbuf;
-  a.y = y;
-  a.p = pbuf;
-  a.out_idx = p->d_out_idx;
-  const int ctas = p->num_sms * p->ctas_per_sm;
-  if (p->stage1_tiles > 0) {
-    const KernelCfg c = kCfgs[p->stage1_cfg];
-    a.team_begin = p->d_tb1;
-    a.nteams = p->stage1_teams;
-    tile_kernel_for<T>(p->stage1_cfg)<<<ctas, 32 * c.wg * c.tpc, 0, st>>>(a);
-    HMVM_CUDA_TRY(cudaGetLastError(), "stage-1 launch");
-  }
-  if (p->n_red > 0) {
-    int blocks = (p->n_red + 255) / 256;
-    hmvm_reduce_kernel<T><<<blocks, 256, 0, st>>>(p->d_red, p->n_red, static_cast<const T*>(pbuf),
-                                                  static_cast<T*>(tbuf));
-    HMVM_CUDA_TRY(cudaGetLastError(), "reduction launch");
-  }
-  const KernelCfg c = kCfgs[p->stage2_cfg];
-  a.team_begin = p->d_tb2;
-  a.nteams = p->stage2_teams;
-  tile_kernel_for<T>(p->stage2_cfg)<<<ctas, 32 * c.wg * c.tpc, 0, st>>>(a);
-  HMVM_CUDA_TRY(cudaGetLastError(), "stage-2 launch");
-  return HMVM_OK;
-}
-
 }  // namespace
 
 extern "C" {
 
 int hmvm_b200_apply_noalloc(hmvm_plan* p, const void* x, void* y, void* stream) {
-  if (!p) return set_error(HMVM_EINVAL, "plan is NULL");
-  if (p->nd > 0 && (!x || !y)) return set_error(HMVM_EINVAL, "x or y is NULL");
-  const char* xb = static_cast<const char*>(x);
-  const char* yb = static_cast<const char*>(y);
-  const size_t nb = (size_t)p->nd * p->elem;
-  if (p->nd > 0 && xb < yb + nb && yb < xb + nb) return set_error(HMVM_EINVAL, "x and y overlap");
+  int rc = check_xy(p, x, y);
+  if (rc) return rc;
   auto round256 = [](size_t b) { return (b + 255) / 256 * 256; };
   const size_t tbytes = round256((size_t)(p->t_len + 16) * p->elem);
   const size_t pbytes = round256((size_t)(p->p_len + 16) * p->elem);
@@ -636,13 +713,16 @@ int hmvm_b200_apply_noalloc(hmvm_plan* p, const void* x, void* y, void* stream) 
   DeviceGuard g(p->device);
   if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
   void* base = nullptr;
-  int rc = noalloc_scratch(p->device, &base);
+  rc = noalloc_scratch(p->device, &base);
   if (rc) return rc;
   char* tbuf = static_cast<char*>(base);
   char* pbuf = tbuf + tbytes;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (p->precision == HMVM_FP64) return launch_apply_noalloc<double>(p, x, y, tbuf, tbytes, pbuf, st);
-  return launch_apply_noalloc<float>(p, x, y, tbuf, tbytes, pbuf, st);
+  // t's padding slots must read as zero, and earlier calls (of any plan) left
+  // other values there; the partial sums are written in full before they are read.
+  HMVM_CUDA_TRY(cudaMemsetAsync(tbuf, 0, tbytes, st), "clear the no-alloc scratch");
+  if (p->precision == HMVM_FP64) return launch_stages<double>(p, x, y, tbuf, pbuf, st);
+  return launch_stages<float>(p, x, y, tbuf, pbuf, st);
 }
 
 // ---- inspection --------------------------------------------------------
@@ -701,8 +781,10 @@ int hmvm_b200_layout_view(const hmvm_layout* h, hmvm_layout_view* v) {
   v->stage2_tiles = L.stage2_tiles;
   v->stage1_teams = L.stage1_teams;
   v->stage2_teams = L.stage2_teams;
-  v->n_red = (int32_t)(L.red.size() / 4);
+  v->n_red1 = (int32_t)(L.red1.size() / 4);
+  v->n_red2 = (int32_t)(L.red2.size() / 4);
   v->nd = L.nd;
+  v->kernel = L.kernel;
   v->data_vectors = (int64_t)L.data.size();
   v->t_len = L.t_len;
   v->p_len = L.p_len;
@@ -711,7 +793,8 @@ int hmvm_b200_layout_view(const hmvm_layout* h, hmvm_layout_view* v) {
   v->team_begin1 = L.team_begin1.data();
   v->team_begin2 = L.team_begin2.data();
   v->out_idx = L.out_idx.data();
-  v->red = L.red.data();
+  v->red1 = L.red1.data();
+  v->red2 = L.red2.data();
   v->data = L.data.data();
   return HMVM_OK;
 }
@@ -735,6 +818,6 @@ const char* hmvm_b200_strerror(int s) {
 
 const char* hmvm_b200_last_error(void) { return g_last_error.c_str(); }
 
-int hmvm_b200_version(void) { return 1; }
+int hmvm_b200_version(void) { return 2; }
 
 }  // extern "C"

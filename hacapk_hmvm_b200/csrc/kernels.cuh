@@ -14,8 +14,23 @@
 // No global atomics; the summation order is fixed by the layout, so results
 // are bitwise reproducible.
 //
-// hmvm_reduce_kernel<T>: for column panels that were split into chunks, adds
-// the chunk partial sums in chunk order and writes the t slot.
+// hmvm_stream_kernel<T, WPB, S, CHUNK, ZCAP>: persistent; every warp is a team
+// and owns one contiguous region of the data stream (its items in order).
+//   * Matrix bytes: lane 0 keeps S chunks of CHUNK bytes in flight into the
+//     warp's shared-memory ring with cp.async.bulk (TMA bulk copies, completion
+//     counted on one mbarrier per slot), refilling a slot as soon as the warp
+//     has moved past it, so loads run ahead across item boundaries.
+//   * Inputs: the x / t columns an item reads (<= ZCAP) are gathered into one of
+//     two shared-memory buffers with cp.async while the previous item runs;
+//     item descriptors are loaded two items ahead.
+//   * The inner loop then only reads shared memory: lane r takes its row's
+//     16-byte vector from the ring and the vector's VEC input values from the
+//     buffer (a broadcast), and accumulates as in hmvm_tile_kernel.
+// Every wait on an mbarrier is bounded by time; a warp that gives up sets
+// *err, waits (bounded) for its copies in flight and stops.
+//
+// hmvm_reduce_kernel<T>: for tiles that were cut into parts, adds the parts'
+// partial sums in part order and writes the t slot or y row.
 #pragma once
 
 #include <cstdint>
@@ -39,6 +54,7 @@ struct VecT<float> {
 };
 
 struct TileArgs {
+  int* err;                   // device status word (0 = ok)
   const hmvm_tile_desc* tiles;
   const hmvm_seg_desc* segs;
   const int32_t* team_begin;  // [nteams+1] absolute tile indices
@@ -188,14 +204,276 @@ __global__ void __launch_bounds__(32 * WG * TPC) hmvm_tile_kernel(TileArgs a) {
   }
 }
 
+// ---- TMA bulk-copy ring -------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Global -> shared bulk copy (no multicast); completion is counted on `bar`.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// Give up on an mbarrier after this long (the copies it waits for take
+// microseconds; only a broken copy would get near this).
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+
+// Warp-uniform bounded wait for the phase with parity `parity` of `bar`.
+__device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t parity) {
+  if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;  // usually already landed
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    bool ok = mbar_try_wait(bar, parity);
+    if (__all_sync(0xffffffffu, ok)) return true;
+    if (global_ns() - t0 > kWaitLimitNs) return false;
+  }
+}
+
+// Asynchronous 4/8/16-byte global -> shared copy (completion by group).
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Copy the x / t columns item `d` reads into zb (one column per element, each
+// segment padded with zeros to whole vectors), with cp.async; `sreg` holds the
+// item's first 32 segment descriptors (lane j: segment j).
+template <typename T>
+__device__ __forceinline__ void gather_inputs(const hmvm_tile_desc& d, const hmvm_seg_desc& sreg,
+                                              const hmvm_seg_desc* __restrict__ segs, const T* __restrict__ x,
+                                              const T* __restrict__ tv, T* zb, int lane) {
+  constexpr int VN = VecT<T>::N;
+  int col0 = 0;
+  for (int base = 0; base < d.nseg; base += 32) {
+    hmvm_seg_desc my = sreg;
+    if (base > 0) my = (base + lane < d.nseg) ? segs[d.seg_begin + base + lane] : hmvm_seg_desc{0, 0};
+    const int cnt = min(32, d.nseg - base);
+    for (int j = 0; j < cnt; j++) {
+      const int src = __shfl_sync(0xffffffffu, my.src, j);
+      const int nc = __shfl_sync(0xffffffffu, my.ncols, j);
+      const int ncp = (nc + VN - 1) / VN * VN;
+      const T* zs = src < 0 ? tv + (src & 0x7fffffff) : x + src;
+      for (int c = lane; c < ncp; c += 32) {
+        if (c < nc) cp_async<sizeof(T)>(zb + col0 + c, zs + c);
+        else zb[col0 + c] = T(0);
+      }
+      col0 += ncp;
+    }
+  }
+}
+
+// CTAs of a configuration that fit one SM's 227 KB of shared memory (at most
+// 24 warps): the register budget the kernel is compiled for.
+template <typename T, int WPB, int S, int CHUNK, int ZCAP>
+constexpr int stream_min_blocks() {
+  constexpr int smem = WPB * (S * CHUNK + 2 * ZCAP * (int)sizeof(T) + S * 8);
+  constexpr int by_smem = (227 * 1024) / smem;
+  constexpr int by_warps = 24 / WPB;
+  constexpr int m = by_smem < by_warps ? by_smem : by_warps;
+  return m > 0 ? m : 1;
+}
+
+template <typename T, int WPB, int S, int CHUNK, int ZCAP>
+__global__ void __launch_bounds__(32 * WPB, (stream_min_blocks<T, WPB, S, CHUNK, ZCAP>()))
+    hmvm_stream_kernel(TileArgs a) {
+  using V = typename VecT<T>::V;
+  constexpr uint32_t RING = (uint32_t)S * CHUNK;
+  // vectors per batch: 8 when the ring has room for them (see the assert below)
+  constexpr int B = ((S - 1) * CHUNK / (32 * 16) >= 8) ? 8 : 4;
+  static_assert((RING & (RING - 1)) == 0, "ring size must be a power of two");
+  static_assert(CHUNK % 16 == 0 && CHUNK >= 512, "bulk copies move multiples of 16 bytes");
+  // A batch (B vectors of <= 32 rows x 16 bytes) must fit in the S-1 slots
+  // after the first one it touches, or its wait could need an unissued chunk.
+  static_assert(B * 32 * 16 <= (S - 1) * CHUNK, "ring too small for one batch");
+  static_assert(ZCAP % 4 == 0, "input buffers hold whole vectors");
+  extern __shared__ __align__(128) unsigned char smem[];
+
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int team = blockIdx.x * WPB + warp;
+  if (team >= a.nteams) return;
+  const int tb = a.team_begin[team], te = a.team_begin[team + 1];
+  if (tb >= te) return;
+  unsigned char* ring = smem + (size_t)warp * RING;
+  T* zbase = reinterpret_cast<T*>(smem + (size_t)WPB * RING) + (size_t)warp * 2 * ZCAP;
+  uint64_t* bars =
+      reinterpret_cast<uint64_t*>(smem + (size_t)WPB * RING + (size_t)WPB * 2 * ZCAP * sizeof(T)) + warp * S;
+
+  const hmvm_tile_desc* __restrict__ tiles = a.tiles;
+  const hmvm_seg_desc* __restrict__ segs = a.segs;
+  const T* __restrict__ x = static_cast<const T*>(a.x);
+  const T* __restrict__ tv = static_cast<const T*>(a.t);
+  const hmvm_tile_desc dzero = {0, 0, 0, 0, 0, 1, 0, 0};
+  const hmvm_seg_desc szero = {0, 0};
+
+  // ---- the matrix stream: this warp's items are one contiguous region ----
+  hmvm_tile_desc cur = tiles[tb];
+  const int64_t vbase = cur.data_off;
+  const hmvm_tile_desc tl = tiles[te - 1];
+  const int64_t total64 = (tl.data_off + (int64_t)tl.nvec * tl.nrows - vbase) * 16;
+  if (total64 >= (int64_t)1 << 31) {  // the planner keeps regions far below this
+    if (lane == 0) atomicExch(a.err, 2);
+    return;
+  }
+  const uint32_t total = (uint32_t)total64;
+  const char* gsrc = static_cast<const char*>(a.data) + vbase * 16;
+  const uint32_t nchunks = (total + CHUNK - 1) / CHUNK;
+  if (lane == 0) {
+#pragma unroll
+    for (int s = 0; s < S; s++) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  // Lane 0 only: start the copy of chunk q into slot q % S.
+  auto issue = [&](uint32_t q) {
+    const uint32_t off = q * (uint32_t)CHUNK;
+    const uint32_t bytes = min((uint32_t)CHUNK, total - off);
+    uint64_t* bar = &bars[q % S];
+    mbar_expect_tx(bar, bytes);
+    bulk_g2s(ring + (q % S) * CHUNK, gsrc + off, bytes, bar);
+  };
+  if (lane == 0)
+    for (uint32_t q = 0; q < min((uint32_t)S, nchunks); q++) issue(q);
+
+  // ---- descriptor pipeline: item i+1's inputs are gathered during item i ----
+  hmvm_seg_desc cur_seg = lane < cur.nseg ? segs[cur.seg_begin + lane] : szero;
+  gather_inputs<T>(cur, cur_seg, segs, x, tv, zbase, lane);
+  cp_async_commit();
+  hmvm_tile_desc nxt = tb + 1 < te ? tiles[tb + 1] : dzero;
+  hmvm_seg_desc nxt_seg = (tb + 1 < te && lane < nxt.nseg) ? segs[nxt.seg_begin + lane] : szero;
+  int nxt_oidx = (tb + 1 < te && nxt.mode == 1 && lane < nxt.nrows) ? a.out_idx[nxt.out_base + lane] : 0;
+  int cur_oidx = (cur.mode == 1 && lane < cur.nrows) ? a.out_idx[cur.out_base + lane] : 0;
+  hmvm_tile_desc nn = tb + 2 < te ? tiles[tb + 2] : dzero;
+
+  uint32_t q_ready = 0, q_rel = 0;  // chunks < q_ready have landed; chunks < q_rel are released
+  bool failed = false;
+  for (int ti = tb, k = 0; ti < te; ++ti, ++k) {
+    T* zcur = zbase + (k & 1) * ZCAP;
+    __syncwarp();  // every lane is done with the buffer the next gather overwrites
+    if (ti + 1 < te) gather_inputs<T>(nxt, nxt_seg, segs, x, tv, zbase + ((k + 1) & 1) * ZCAP, lane);
+    cp_async_commit();
+    // loads for two items ahead; they land while this item runs
+    const hmvm_seg_desc nn_seg = (ti + 2 < te && lane < nn.nseg) ? segs[nn.seg_begin + lane] : szero;
+    const int nn_oidx = (ti + 2 < te && nn.mode == 1 && lane < nn.nrows) ? a.out_idx[nn.out_base + lane] : 0;
+    const hmvm_tile_desc nnn = ti + 3 < te ? tiles[ti + 3] : dzero;
+    cp_async_wait<1>();
+    __syncwarp();  // this item's inputs are in zcur
+
+    const int R = cur.nrows;
+    const bool act = lane < R;
+    const uint32_t rstride = (uint32_t)R * 16;
+    const int nvt = cur.nvec;
+    // Lanes >= R read ring bytes of other rows (always inside the ring); their
+    // sums are never written, so the loop needs no per-lane predicate.
+    uint32_t o = (uint32_t)((cur.data_off - vbase) * 16);  // byte offset of vector v in the region
+    const unsigned char* zc = reinterpret_cast<const unsigned char*>(zcur);
+    T acc0 = T(0), acc1 = T(0), acc2 = T(0), acc3 = T(0);
+    for (int v = 0; v < nvt; v += B) {
+      const int nb = min(B, nvt - v);
+      const uint32_t o_end = o + (uint32_t)nb * rstride;
+      // Release the slots the warp has moved past, then wait for the batch's chunks.
+      if (o >= (q_rel + 1) * (uint32_t)CHUNK) {
+        const uint32_t qf = o / CHUNK;
+        __syncwarp();
+        if (lane == 0) {
+          fence_proxy_async();
+          for (uint32_t q = q_rel; q < qf; q++)
+            if (q + S < nchunks) issue(q + S);
+        }
+        q_rel = qf;
+      }
+      if (o_end > q_ready * (uint32_t)CHUNK) {
+        const uint32_t ql = (o_end - 1) / CHUNK;
+        while (q_ready <= ql) {
+          if (!warp_wait(&bars[q_ready % S], (q_ready / S) & 1)) {
+            failed = true;
+            break;
+          }
+          q_ready++;
+        }
+        if (failed) break;
+      }
+      const uint32_t ol = o + (uint32_t)lane * 16;
+      if (nb == B) {
+        V m[B], z[B];
+#pragma unroll
+        for (int u = 0; u < B; u++) {
+          m[u] = *reinterpret_cast<const V*>(ring + ((ol + (uint32_t)u * rstride) & (RING - 1)));
+          z[u] = *reinterpret_cast<const V*>(zc + (size_t)(v + u) * 16);
+        }
+#pragma unroll
+        for (int u = 0; u < B; u += 2) {
+          fma_vec(acc0, acc1, m[u], z[u]);
+          fma_vec(acc2, acc3, m[u + 1], z[u + 1]);
+        }
+      } else {
+        for (int u = 0; u < nb; u++) {
+          const V m = *reinterpret_cast<const V*>(ring + ((ol + (uint32_t)u * rstride) & (RING - 1)));
+          const V z = *reinterpret_cast<const V*>(zc + (size_t)(v + u) * 16);
+          fma_vec(acc0, acc1, m, z);
+        }
+      }
+      o = o_end;
+    }
+    if (failed) break;
+    const T acc = (acc0 + acc1) + (acc2 + acc3);
+    if (act) {
+      if (cur.mode == 0) static_cast<T*>(a.y)[cur.out_base + lane] = acc;
+      else if (cur.mode == 1) static_cast<T*>(a.t)[cur_oidx] = acc;
+      else static_cast<T*>(a.p)[cur.out_base + lane] = acc;
+    }
+    cur = nxt;
+    cur_oidx = nxt_oidx;
+    nxt = nn;
+    nxt_seg = nn_seg;
+    nxt_oidx = nn_oidx;
+    nn = nnn;
+  }
+  cp_async_wait<0>();
+  if (failed) {
+    // Let every copy still in flight land before the CTA's shared memory goes away.
+    const uint32_t issued = min(nchunks, q_rel + (uint32_t)S);
+    for (uint32_t q = q_ready; q < issued; q++) warp_wait(&bars[q % S], (q / S) & 1);
+    if (lane == 0) atomicExch(a.err, 1);
+  }
+}
+
 template <typename T>
 __global__ void hmvm_reduce_kernel(const int4* __restrict__ red, int n, const T* __restrict__ p,
-                                   T* __restrict__ t) {
+                                   T* __restrict__ dst) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int4 e = red[i];
+    const int4 e = red[i];  // destination, first partial, parts, stride
     T s = p[e.y];
-    for (int c = 1; c < e.z; c++) s += p[e.y + c * 32];
-    t[e.x] = s;
+    for (int c = 1; c < e.z; c++) s += p[e.y + c * e.w];
+    dst[e.x] = s;
   }
 }
 

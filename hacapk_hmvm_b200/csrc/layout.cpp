@@ -114,9 +114,14 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     L.nd = lt.nd;
     L.nlf = lt.nlf;
     L.num_sms = num_sms > 0 ? num_sms : 148;
-    L.stage1_cfg = (opts.stage1_cfg >= 0 && opts.stage1_cfg < kNumCfgs) ? opts.stage1_cfg : kDefaultStage1Cfg;
-    L.stage2_cfg = (opts.stage2_cfg >= 0 && opts.stage2_cfg < kNumCfgs) ? opts.stage2_cfg : kDefaultStage2Cfg;
-    L.ctas_per_sm = opts.ctas_per_sm > 0 ? opts.ctas_per_sm : kDefaultCtasPerSm;
+    L.kernel = (opts.kernel == 0) ? 0 : 1;
+    const int ncfg = L.kernel == 0 ? kNumCfgs : kNumStreamCfgs;
+    L.stage1_cfg = (opts.stage1_cfg >= 0 && opts.stage1_cfg < ncfg) ? opts.stage1_cfg
+                   : (L.kernel == 0 ? kDefaultStage1Cfg : kDefaultStreamCfg);
+    L.stage2_cfg = (opts.stage2_cfg >= 0 && opts.stage2_cfg < ncfg) ? opts.stage2_cfg
+                   : (L.kernel == 0 ? kDefaultStage2Cfg : kDefaultStreamCfg);
+    L.ctas_per_sm = opts.ctas_per_sm > 0 ? opts.ctas_per_sm
+                    : (L.kernel == 0 ? kDefaultCtasPerSm : kDefaultStreamCtasPerSm);
     const int VEC = L.vec;
     const int RMAX = (opts.max_tile_rows >= 1 && opts.max_tile_rows <= kMaxRows) ? opts.max_tile_rows : kMaxRows;
     const int32_t nd = lt.nd, nlf = lt.nlf;
@@ -213,21 +218,16 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     L.t_len = t_len;
 
     // ---- stage 1: column panels ------------------------------------------
-    const int32_t split = opts.split_cols > 0 ? std::max<int32_t>(opts.split_cols, VEC) : 4096;
     std::vector<TileBuild> tb;
     std::vector<SegBuild> sb;
     std::vector<Part> parts;
     std::vector<std::pair<int32_t, int32_t>> panel_rows;  // (leaf, k) per out_idx entry
-    int64_t p_len = 0;
     for (int32_t c = 0; c < (int32_t)cg_members.size(); c++) {
       const auto &mem = cg_members[c];
       int32_t ndt = lt.ndt[mem[0]], st = lt.nstrtt[mem[0]];
       std::vector<std::pair<int32_t, int32_t>> rows;
       for (int32_t i : mem)
         for (int32_t k = 0; k < lt.kt[i]; k++) rows.emplace_back(i, k);
-      // Column chunks of width w (a multiple of VEC) when the panel is wider than `split`.
-      const int32_t w = ndt > split ? std::max<int32_t>(VEC, split / VEC * VEC) : (int32_t)round_up(ndt, VEC);
-      const int32_t nchunks = ndt > split ? (ndt + w - 1) / w : 1;
       for (size_t p0 = 0; p0 < rows.size(); p0 += kMaxRows) {
         int32_t R = (int32_t)std::min<size_t>(kMaxRows, rows.size() - p0);
         int32_t ob = (int32_t)L.out_idx.size();
@@ -236,42 +236,20 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
           L.out_idx.push_back((int32_t)(slot_of_leaf[lk.first] + lk.second));
           panel_rows.push_back(lk);
         }
-        int64_t pb = p_len;
-        if (nchunks > 1) {
-          p_len += (int64_t)nchunks * kMaxRows;
-          for (int32_t r = 0; r < R; r++) {
-            L.red.push_back(L.out_idx[ob + r]);
-            L.red.push_back((int32_t)(pb + r));
-            L.red.push_back(nchunks);
-            L.red.push_back(0);
-          }
-          L.split_rows += R;
-        }
-        for (int32_t ch = 0; ch < nchunks; ch++) {
-          int32_t c0 = ch * w, c1 = std::min(ndt, c0 + w);
-          TileBuild t;
-          t.stage = 1;
-          t.cgroup = c;
-          t.nrows = R;
-          t.panel_row0 = ob;  // index into panel_rows / out_idx
-          t.col0 = c0;
-          t.mode = nchunks > 1 ? 2 : 1;
-          t.out_base = nchunks > 1 ? (int32_t)(pb + (int64_t)ch * kMaxRows) : ob;
-          t.seg_first = (int32_t)sb.size();
-          t.nseg = 1;
-          int32_t ncols = c1 - c0;
-          sb.push_back(SegBuild{st - 1 + c0, ncols, -1, 0});
-          t.nvec = (ncols + VEC - 1) / VEC;
-          t.cost = (int64_t)t.nvec * R * 16 + 1024;
-          tb.push_back(t);
-        }
+        TileBuild t;
+        t.stage = 1;
+        t.cgroup = c;
+        t.nrows = R;
+        t.panel_row0 = ob;  // index into panel_rows / out_idx
+        t.mode = 1;
+        t.out_base = ob;
+        t.seg_first = (int32_t)sb.size();
+        t.nseg = 1;
+        sb.push_back(SegBuild{st - 1, ndt, -1, 0});
+        t.nvec = (ndt + VEC - 1) / VEC;
+        tb.push_back(t);
       }
     }
-    if (p_len > INT32_MAX / 2) {
-      msg = "partial-sum buffer too long";
-      return HMVM_ERANGE;
-    }
-    L.p_len = p_len;
     const int32_t n1 = (int32_t)tb.size();
 
     // ---- stage 2: row tiles ---------------------------------------------
@@ -339,17 +317,84 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
       }
       for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) nvec += (sb[s].ncols + VEC - 1) / VEC;
       t.nvec = nvec;
-      t.cost = (int64_t)nvec * t.nrows * 16 + 1024 + 128 * t.nseg;
       tb.push_back(t);
     }
-    const int32_t n2 = (int32_t)tb.size() - n1;
+    const int32_t ntb = (int32_t)tb.size();
+
+    // ---- items: tiles cut into contiguous vector ranges ----------------------
+    // A tile whose bytes exceed the stage's bound is cut into near-equal vector
+    // ranges that write partial sums; the reduction lists add them in order.
+    const int32_t ctas = L.num_sms * L.ctas_per_sm;
+    L.stage1_teams = ctas * teams_per_cta(L.kernel, L.stage1_cfg);
+    L.stage2_teams = ctas * teams_per_cta(L.kernel, L.stage2_cfg);
+    int64_t stage_bytes[2] = {0, 0};
+    for (int32_t k = 0; k < ntb; k++) stage_bytes[k < n1 ? 0 : 1] += (int64_t)tb[k].nvec * tb[k].nrows * 16;
+    int64_t max_item[2];
+    for (int st = 0; st < 2; st++) {
+      int32_t nteams = st == 0 ? L.stage1_teams : L.stage2_teams;
+      max_item[st] = std::max<int64_t>(kMinItemBytes, stage_bytes[st] / std::max<int64_t>(1, (int64_t)nteams * kItemsPerTeam));
+    }
+    struct Item {
+      int32_t tile, va, vb, mode, out_base;
+      int64_t cost;
+    };
+    std::vector<Item> items;
+    items.reserve((size_t)ntb + ntb / 2);
+    std::vector<int32_t> tile_item0(ntb + 1);
+    int64_t p_len = 0;
+    for (int32_t k = 0; k < ntb; k++) {
+      const TileBuild &t = tb[k];
+      tile_item0[k] = (int32_t)items.size();
+      const int st = k < n1 ? 0 : 1;
+      int64_t bytes = (int64_t)t.nvec * t.nrows * 16;
+      int32_t nparts = (int32_t)std::min<int64_t>(std::max<int64_t>(1, t.nvec),
+                                                  (bytes + max_item[st] - 1) / max_item[st]);
+      if (st == 0 && opts.split_cols > 0) {
+        int32_t vmax = std::max(1, opts.split_cols / VEC);
+        nparts = std::max(nparts, (t.nvec + vmax - 1) / vmax);
+      }
+      if (L.kernel == 1) {
+        // an item's x/t columns must fit the kernel's input buffer
+        const int32_t cfg = st == 0 ? L.stage1_cfg : L.stage2_cfg;
+        const int32_t vmax = std::max(1, kStreamCfgs[cfg].zcap / VEC);
+        nparts = std::max(nparts, (t.nvec + vmax - 1) / vmax);
+      }
+      if (nparts <= 1) {
+        items.push_back(Item{k, 0, t.nvec, t.mode, t.out_base, bytes + kItemOverheadBytes});
+        continue;
+      }
+      // part q of the tile writes its R partial sums at pb + q*R
+      int64_t pb = p_len;
+      p_len += (int64_t)nparts * t.nrows;
+      std::vector<int32_t> &red = st == 0 ? L.red1 : L.red2;
+      for (int32_t r = 0; r < t.nrows; r++) {
+        red.push_back(st == 0 ? L.out_idx[t.panel_row0 + r] : t.row0 + r);
+        red.push_back((int32_t)(pb + r));
+        red.push_back(nparts);
+        red.push_back(t.nrows);
+      }
+      for (int32_t q = 0; q < nparts; q++) {
+        int32_t va = (int32_t)((int64_t)t.nvec * q / nparts), vb = (int32_t)((int64_t)t.nvec * (q + 1) / nparts);
+        items.push_back(Item{k, va, vb, 2, (int32_t)(pb + (int64_t)q * t.nrows),
+                             (int64_t)(vb - va) * t.nrows * 16 + kItemOverheadBytes});
+      }
+    }
+    tile_item0[ntb] = (int32_t)items.size();
+    if (p_len > INT32_MAX / 2) {
+      msg = "partial-sum buffer too long";
+      return HMVM_ERANGE;
+    }
+    L.p_len = p_len;
+    L.split_rows = (int32_t)((L.red1.size() + L.red2.size()) / 4);
+    const int32_t ni1 = tile_item0[n1];
+    const int32_t ni2 = (int32_t)items.size() - ni1;
 
     // ---- team assignment (LPT) and ordering --------------------------------
     auto assign = [&](int32_t first, int32_t count, int32_t nteams, std::vector<int32_t> &order,
                       std::vector<int32_t> &team_begin) {
       std::vector<int32_t> idx(count);
       for (int32_t k = 0; k < count; k++) idx[k] = first + k;
-      std::stable_sort(idx.begin(), idx.end(), [&](int32_t a, int32_t b) { return tb[a].cost > tb[b].cost; });
+      std::stable_sort(idx.begin(), idx.end(), [&](int32_t a, int32_t b) { return items[a].cost > items[b].cost; });
       using HE = std::pair<int64_t, int32_t>;
       std::priority_queue<HE, std::vector<HE>, std::greater<HE>> heap;
       for (int32_t k = 0; k < nteams; k++) heap.emplace(0, k);
@@ -358,7 +403,7 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
         HE h = heap.top();
         heap.pop();
         team_of[k - first] = h.second;
-        heap.emplace(h.first + tb[k].cost, h.second);
+        heap.emplace(h.first + items[k].cost, h.second);
       }
       std::vector<int32_t> cnt(nteams + 1, 0);
       for (int32_t k = 0; k < count; k++) cnt[team_of[k] + 1]++;
@@ -366,104 +411,121 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
       team_begin.assign(cnt.begin(), cnt.end());
       std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1);
       order.resize(count);
-      for (int32_t k = 0; k < count; k++) order[pos[team_of[k]]++] = first + k;  // tile order within team
+      for (int32_t k = 0; k < count; k++) order[pos[team_of[k]]++] = first + k;  // item order within team
     };
-    const int32_t ctas = L.num_sms * L.ctas_per_sm;
-    L.stage1_teams = ctas * kCfgs[L.stage1_cfg].tpc;
-    L.stage2_teams = ctas * kCfgs[L.stage2_cfg].tpc;
     std::vector<int32_t> ord1, ord2, tb1, tb2;
-    assign(0, n1, L.stage1_teams, ord1, tb1);
-    assign(n1, n2, L.stage2_teams, ord2, tb2);
+    assign(0, ni1, L.stage1_teams, ord1, tb1);
+    assign(ni1, ni2, L.stage2_teams, ord2, tb2);
     std::vector<int32_t> order;
-    order.reserve(tb.size());
+    order.reserve(items.size());
     order.insert(order.end(), ord1.begin(), ord1.end());
     order.insert(order.end(), ord2.begin(), ord2.end());
     L.team_begin1 = tb1;
     L.team_begin2.resize(tb2.size());
-    for (size_t k = 0; k < tb2.size(); k++) L.team_begin2[k] = tb2[k] + n1;
-    L.stage1_tiles = n1;
-    L.stage2_tiles = n2;
+    for (size_t k = 0; k < tb2.size(); k++) L.team_begin2[k] = tb2[k] + ni1;
+    L.stage1_tiles = ni1;
+    L.stage2_tiles = ni2;
 
-    // ---- final descriptors, data offsets ---------------------------------
-    const int32_t ntiles = (int32_t)tb.size();
-    L.tiles.resize(ntiles);
+    // ---- final descriptors (segments trimmed to each item's vector range) --
+    const int32_t nitems = (int32_t)items.size();
+    L.tiles.resize(nitems);
     L.segs.clear();
-    L.segs.reserve(sb.size());
-    std::vector<int64_t> data_off(ntiles);
+    L.segs.reserve(sb.size() + nitems);
+    std::vector<int64_t> item_off(nitems);  // by item index
     int64_t off = 0;
-    for (int32_t k = 0; k < ntiles; k++) {
-      const TileBuild &t = tb[order[k]];
+    for (int32_t k = 0; k < nitems; k++) {
+      const Item &it = items[order[k]];
+      const TileBuild &t = tb[it.tile];
       hmvm_tile_desc &d = L.tiles[k];
       d.data_off = off;
       d.seg_begin = (int32_t)L.segs.size();
-      d.nseg = t.nseg;
-      d.nvec = t.nvec;
-      d.out_base = t.out_base;
+      d.nvec = it.vb - it.va;
+      d.out_base = it.out_base;
       d.nrows = (int16_t)t.nrows;
-      d.mode = (int16_t)t.mode;
+      d.mode = (int16_t)it.mode;
       d._pad = 0;
-      for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) L.segs.push_back(hmvm_seg_desc{sb[s].src, sb[s].ncols});
-      data_off[k] = off;
-      off += (int64_t)t.nvec * t.nrows;
+      int32_t nseg = 0, sv0 = 0;
+      for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) {
+        int32_t nv = (sb[s].ncols + VEC - 1) / VEC;
+        int32_t lo = std::max(sv0, it.va), hi = std::min(sv0 + nv, it.vb);
+        if (lo < hi) {
+          int32_t skip = (lo - sv0) * VEC;  // columns of the segment before this item
+          int32_t ncols = std::min(sb[s].ncols - skip, (hi - lo) * VEC);
+          L.segs.push_back(hmvm_seg_desc{sb[s].src + skip, ncols});
+          nseg++;
+        }
+        sv0 += nv;
+      }
+      d.nseg = nseg;
+      item_off[order[k]] = off;
+      off += (int64_t)d.nvec * t.nrows;
     }
     L.data.resize((size_t)off);
 
-    // ---- pack ------------------------------------------------------------
+    // ---- pack: each tile into a scratch buffer, then its items' ranges -----
     const bool srcf = lt.rowmat_is_float;
     const bool dstf = L.precision == HMVM_FP32;
-#pragma omp parallel for schedule(dynamic, 4)
-    for (int32_t k = 0; k < ntiles; k++) {
-      const TileBuild &t = tb[order[k]];
-      const int32_t R = t.nrows;
-      const int64_t tile_elems = (int64_t)t.nvec * R * VEC;
-      char *base = reinterpret_cast<char *>(L.data.data() + data_off[k]);
-      std::memset(base, 0, (size_t)tile_elems * L.elem_size);
-      auto put = [&](int64_t c, int32_t r, double v) {
-        int64_t vi = c / VEC, e = c % VEC;
-        int64_t at = (vi * R + r) * VEC + e;
-        if (dstf) reinterpret_cast<float *>(base)[at] = (float)v;
-        else reinterpret_cast<double *>(base)[at] = v;
-      };
-      auto get = [&](int64_t idx) { return srcf ? rd<float>(lt.rowmat, idx) : rd<double>(lt.rowmat, idx); };
-      if (t.stage == 1) {
-        const SegBuild &s = sb[t.seg_first];
-        for (int32_t r = 0; r < R; r++) {
-          auto lk = panel_rows[t.panel_row0 + r];
-          int32_t i = lk.first, kk = lk.second;
-          int64_t src0 = lt.a1(i) + (int64_t)kk * lt.ndt[i] + t.col0;
-          for (int32_t c = 0; c < s.ncols; c++) put(c, r, get(src0 + c));
-        }
-      } else {
-        int64_t col = 0;
-        for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) {
-          const SegBuild &sg = sb[s];
-          int64_t segcol0 = col;
-          int64_t pc = 0;  // column within segment
-          for (int32_t p = sg.part_first; p < sg.part_first + sg.nparts; p++) {
-            const Part &pt = parts[p];
-            if (pt.leaf >= 0) {
-              int32_t i = pt.leaf, ndt = lt.ndt[i];
-              int32_t rs = lt.nstrtl[i] - 1;
-              for (int32_t r = 0; r < R; r++) {
-                int64_t src0 = lt.a1(i) + (int64_t)(t.row0 + r - rs) * ndt;
-                for (int32_t c = 0; c < ndt; c++) put(segcol0 + pc + c, r, get(src0 + c));
-              }
-              pc += ndt;
-            } else {
-              int64_t kc = 0;
-              for (int32_t i : rg_members[pt.group]) {
-                int32_t ndl = lt.ndl[i], rs = lt.nstrtl[i] - 1;
-                for (int32_t kk = 0; kk < lt.kt[i]; kk++) {
-                  int64_t src0 = lt.a2(i) + (int64_t)kk * ndl + (t.row0 - rs);
-                  for (int32_t r = 0; r < R; r++) put(segcol0 + pc + kc, r, get(src0 + r));
-                  kc++;
-                }
-              }
-              pc += kc;
-            }
+#pragma omp parallel
+    {
+      std::vector<Vec16> buf;
+#pragma omp for schedule(dynamic, 4)
+      for (int32_t k = 0; k < ntb; k++) {
+        const TileBuild &t = tb[k];
+        const int32_t R = t.nrows;
+        buf.assign((size_t)t.nvec * R, Vec16{{0, 0, 0, 0}});
+        char *base = reinterpret_cast<char *>(buf.data());
+        auto put = [&](int64_t c, int32_t r, double v) {
+          int64_t vi = c / VEC, e = c % VEC;
+          int64_t at = (vi * R + r) * VEC + e;
+          if (dstf) reinterpret_cast<float *>(base)[at] = (float)v;
+          else reinterpret_cast<double *>(base)[at] = v;
+        };
+        auto get = [&](int64_t idx) { return srcf ? rd<float>(lt.rowmat, idx) : rd<double>(lt.rowmat, idx); };
+        if (t.stage == 1) {
+          const SegBuild &s = sb[t.seg_first];
+          for (int32_t r = 0; r < R; r++) {
+            auto lk = panel_rows[t.panel_row0 + r];
+            int32_t i = lk.first, kk = lk.second;
+            int64_t src0 = lt.a1(i) + (int64_t)kk * lt.ndt[i];
+            for (int32_t c = 0; c < s.ncols; c++) put(c, r, get(src0 + c));
           }
-          // next segment starts at the next vector boundary
-          col = round_up(segcol0 + sg.ncols, VEC);
+        } else {
+          int64_t col = 0;
+          for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) {
+            const SegBuild &sg = sb[s];
+            int64_t segcol0 = col;
+            int64_t pc = 0;  // column within segment
+            for (int32_t p = sg.part_first; p < sg.part_first + sg.nparts; p++) {
+              const Part &pt = parts[p];
+              if (pt.leaf >= 0) {
+                int32_t i = pt.leaf, ndt = lt.ndt[i];
+                int32_t rs = lt.nstrtl[i] - 1;
+                for (int32_t r = 0; r < R; r++) {
+                  int64_t src0 = lt.a1(i) + (int64_t)(t.row0 + r - rs) * ndt;
+                  for (int32_t c = 0; c < ndt; c++) put(segcol0 + pc + c, r, get(src0 + c));
+                }
+                pc += ndt;
+              } else {
+                int64_t kc = 0;
+                for (int32_t i : rg_members[pt.group]) {
+                  int32_t ndl = lt.ndl[i], rs = lt.nstrtl[i] - 1;
+                  for (int32_t kk = 0; kk < lt.kt[i]; kk++) {
+                    int64_t src0 = lt.a2(i) + (int64_t)kk * ndl + (t.row0 - rs);
+                    for (int32_t r = 0; r < R; r++) put(segcol0 + pc + kc, r, get(src0 + r));
+                    kc++;
+                  }
+                }
+                pc += kc;
+              }
+            }
+            // next segment starts at the next vector boundary
+            col = round_up(segcol0 + sg.ncols, VEC);
+          }
+        }
+        for (int32_t q = tile_item0[k]; q < tile_item0[k + 1]; q++) {
+          const Item &it = items[q];
+          std::memcpy(L.data.data() + item_off[q], buf.data() + (size_t)it.va * R,
+                      (size_t)(it.vb - it.va) * R * sizeof(Vec16));
         }
       }
     }

@@ -21,11 +21,12 @@
 //    of row r), so one warp-wide load reads R*16 contiguous bytes and every
 //    lane accumulates its own row: no shuffles and no atomics, and the
 //    summation order is fixed by the layout.
-//  * Column panels wider than split_cols are cut into chunks that write
-//    partial sums; a small reduction adds the chunks in chunk order.
-//  * Tiles are assigned to persistent "teams" (groups of warps) by LPT on
-//    their byte cost and stored in team order, so a team streams one
-//    contiguous region.
+//  * Tiles larger than a per-stage bound are cut into "items": contiguous
+//    vector ranges (segments trimmed to the range) that write partial sums; a
+//    small reduction adds the parts in order into t (stage 1) or y (stage 2).
+//  * Items are assigned to persistent "teams" (a warp, or a group of warps) by
+//    LPT on their byte cost and stored in team order, so a team streams one
+//    contiguous region of HBM.
 #pragma once
 
 #include <cstdint>
@@ -54,29 +55,58 @@ struct LeafTable {
   int64_t a2(int32_t i) const { return a2_64 ? a2_64[i] : (int64_t)a2_32[i]; }
 };
 
-// Kernel configurations: warps per team (WG) and teams per CTA (TPC).
+// Kernel variants.
+//   0: hmvm_tile_kernel   -- teams of WG warps split a tile's vectors; data
+//                            streamed with 16-byte register loads.
+//   1: hmvm_stream_kernel -- one warp per team; each warp streams its contiguous
+//                            region through a private shared-memory ring filled
+//                            by cp.async.bulk (TMA bulk copies) ahead of use.
+// Configurations of variant 0: warps per team (WG) and teams per CTA (TPC).
 struct KernelCfg {
   int wg, tpc;
 };
 constexpr int kNumCfgs = 8;
 constexpr KernelCfg kCfgs[kNumCfgs] = {{1, 8}, {2, 4}, {4, 2}, {8, 1}, {2, 8}, {4, 4}, {8, 2}, {16, 1}};
-constexpr int kDefaultStage1Cfg = 4;
+// Configurations of variant 1: warps per CTA, ring slots per warp, slot bytes,
+// and zcap, the x/t columns one item may read (the size of each of the warp's
+// two input buffers in shared memory).
+struct StreamCfg {
+  int wpb, slots, chunk, zcap;
+};
+constexpr int kNumStreamCfgs = 6;
+constexpr StreamCfg kStreamCfgs[kNumStreamCfgs] = {{8, 4, 1024, 256}, {4, 4, 2048, 512}, {8, 4, 2048, 256},
+                                                   {16, 4, 1024, 128}, {4, 8, 1024, 512}, {8, 8, 512, 256}};
+inline int stream_smem_bytes(const StreamCfg& c, int elem) {
+  return c.wpb * (c.slots * c.chunk + 2 * c.zcap * elem + c.slots * 8);
+}
+inline int teams_per_cta(int kernel, int cfg) { return kernel == 0 ? kCfgs[cfg].tpc : kStreamCfgs[cfg].wpb; }
+constexpr int kDefaultKernel = 1;
+constexpr int kDefaultStage1Cfg = 4;  // variant 0 defaults
 constexpr int kDefaultStage2Cfg = 5;
 constexpr int kDefaultCtasPerSm = 2;
+constexpr int kDefaultStreamCfg = 2;  // variant 1 defaults
+constexpr int kDefaultStreamCtasPerSm = 2;  // plans use the occupancy the device reports
 constexpr int kMaxRows = 32;
+// Item split: a stage's tiles are cut so that no item exceeds
+// max(kMinItemBytes, stage bytes / (teams * kItemsPerTeam)).
+constexpr int64_t kMinItemBytes = 32 * 1024;
+constexpr int64_t kItemsPerTeam = 6;
+constexpr int64_t kItemOverheadBytes = 1024;
 
 struct HostLayout {
   int precision = HMVM_FP64;
   int vec = 2;
   int elem_size = 8;
   int32_t nd = 0, nlf = 0, n_lowrank = 0, n_dense = 0;
-  int stage1_cfg = kDefaultStage1Cfg, stage2_cfg = kDefaultStage2Cfg, ctas_per_sm = kDefaultCtasPerSm;
+  int kernel = kDefaultKernel;
+  int stage1_cfg = kDefaultStreamCfg, stage2_cfg = kDefaultStreamCfg, ctas_per_sm = kDefaultStreamCtasPerSm;
   int num_sms = 148;
   std::vector<hmvm_tile_desc> tiles;  // [stage1 tiles][stage2 tiles], each in team order
   std::vector<hmvm_seg_desc> segs;
   std::vector<int32_t> team_begin1, team_begin2;  // absolute tile indices
   std::vector<int32_t> out_idx;
-  std::vector<int32_t> red;  // 4 ints per entry
+  std::vector<int32_t> red1;  // 4 ints per entry: t slot, first partial, parts, stride between parts
+  std::vector<int32_t> red2;  // 4 ints per entry: y row, first partial, parts, stride between parts
   std::vector<Vec16> data;
   int32_t stage1_tiles = 0, stage2_tiles = 0, stage1_teams = 0, stage2_teams = 0;
   int64_t t_len = 0, p_len = 0;

@@ -95,11 +95,16 @@ class Plan:
         _lib.check(_lib.hmvm_lib().hmvm_b200_plan_profile(self.handle, int(enable)), "profile")
 
     def profile_read(self) -> tuple[list[float], int]:
-        """(summed ms of [V stage, reduction, row stage], number of applies)."""
-        ms = (C.c_double * 3)()
+        """(summed ms of [V stage, its reduction, row stage, its reduction],
+        number of applies)."""
+        ms = (C.c_double * 4)()
         n = C.c_int32()
         _lib.check(_lib.hmvm_lib().hmvm_b200_plan_profile_read(self.handle, ms, C.byref(n)), "profile_read")
-        return [ms[0], ms[1], ms[2]], int(n.value)
+        return [ms[0], ms[1], ms[2], ms[3]], int(n.value)
+
+    def status(self) -> None:
+        """Raise if a kernel of this plan reported a device-side error."""
+        _lib.check(_lib.hmvm_lib().hmvm_b200_plan_status(self.handle), "device status")
 
     def kernel_count(self) -> int:
         return int(_lib.hmvm_lib().hmvm_b200_plan_kernel_count(self.handle))

@@ -124,11 +124,11 @@ typedef struct hmvm_plan_opts {
   int32_t precision;      /* enum hmvm_precision */
   int32_t device;         /* CUDA device ordinal, -1 = current device */
   int32_t max_tile_rows;  /* rows per row tile, 1..32 (0 = 32) */
-  int32_t split_cols;     /* low-rank column panels wider than this are split (0 = auto) */
+  int32_t split_cols;     /* V panels are also cut every split_cols columns (0 = only by size) */
   int32_t stage1_cfg;     /* kernel configuration index for the V stage (-1 = default) */
   int32_t stage2_cfg;     /* kernel configuration index for the row stage (-1 = default) */
   int32_t ctas_per_sm;    /* persistent CTAs per SM (0 = default) */
-  int32_t _reserved;
+  int32_t kernel;         /* 0: register-streaming tile kernel; 1 (default, -1): TMA-ring stream kernel */
 } hmvm_plan_opts;
 
 typedef struct hmvm_plan_info {
@@ -138,10 +138,11 @@ typedef struct hmvm_plan_info {
   int64_t device_bytes;      /* repacked matrix bytes resident on the GPU (incl. padding) */
   int64_t t_len;             /* length of the intermediate V x vector */
   int32_t stage1_tiles, stage2_tiles, stage1_teams, stage2_teams;
-  int32_t split_rows, kernels_per_apply, stage1_cfg, stage2_cfg;
+  int32_t split_rows, kernels_per_apply, stage1_cfg, stage2_cfg;  /* split_rows: rows finished by a reduction */
   int64_t flops;             /* 2 * stored elements */
   int64_t stage1_bytes;      /* algorithmic bytes of the V stage: V elements + x */
   int64_t stage2_bytes;      /* algorithmic bytes of the row stage: U + dense elements + x + y */
+  int32_t kernel, ctas_per_sm;
 } hmvm_plan_info;
 
 void hmvm_b200_default_opts(hmvm_plan_opts *opts);
@@ -194,10 +195,16 @@ int hmvm_b200_apply_noalloc(hmvm_plan *plan, const void *x_dev, void *y_dev, voi
 /* Per-stage device timing.  While enabled, every apply records CUDA events
  * around its launches on the launch stream (up to 4096 applies are kept);
  * profile_read waits for the last recorded apply, returns the summed
- * milliseconds of stage 0 (V stage), 1 (split-panel reduction), 2 (row stage)
- * and the number of applies, and clears the record. */
+ * milliseconds of stage 0 (V stage), 1 (its reduction), 2 (row stage), 3 (its
+ * reduction) and the number of applies, and clears the record. */
 int hmvm_b200_plan_profile(hmvm_plan *plan, int enable);
-int hmvm_b200_plan_profile_read(hmvm_plan *plan, double *stage_ms3, int32_t *napplies);
+int hmvm_b200_plan_profile_read(hmvm_plan *plan, double *stage_ms4, int32_t *napplies);
+
+/* Device-side status of the plan's kernels: HMVM_OK, or HMVM_EDEVICE if a
+ * kernel gave up on a bounded wait since the last call (the wait's results are
+ * not valid then).  Waits for the plan's device to finish its work; clears the
+ * flag. */
+int hmvm_b200_plan_status(hmvm_plan *plan);
 
 /* ---- one-shot call with the reference's shape ---------------------------- */
 typedef struct hmvm_stats {
@@ -222,7 +229,7 @@ typedef struct hmvm_layout_view {
   int32_t n_tiles, n_segs;           /* all stages */
   int32_t stage1_tiles, stage2_tiles; /* tiles [0,stage1) are stage 1, then stage 2 */
   int32_t stage1_teams, stage2_teams;
-  int32_t n_red, nd;
+  int32_t n_red1, n_red2, nd, kernel;
   int64_t data_vectors;              /* 16-byte vectors in the data stream */
   int64_t t_len, p_len;
   const void *tiles;                 /* hmvm_tile_desc[n_tiles] */
@@ -230,7 +237,8 @@ typedef struct hmvm_layout_view {
   const int32_t *team_begin1;        /* [stage1_teams+1], indexes tiles */
   const int32_t *team_begin2;        /* [stage2_teams+1], indexes tiles */
   const int32_t *out_idx;            /* stage-1 output slots */
-  const int32_t *red;                /* [n_red][4]: slot, pbase, nchunk, 0 */
+  const int32_t *red1;               /* [n_red1][4]: t slot, partial base, parts, 0 */
+  const int32_t *red2;               /* [n_red2][4]: y row, partial base, parts, 0 */
   const void *data;                  /* data_vectors * 16 bytes */
 } hmvm_layout_view;
 

@@ -171,7 +171,9 @@ def emulate_layout(view, x: np.ndarray) -> np.ndarray:
             if view.n_segs else [])
     data = np.ctypeslib.as_array((C.c_uint8 * (16 * view.data_vectors)).from_address(view.data)).view(dt) \
         if view.data_vectors else np.zeros(0, dt)
-    out_idx = np.ctypeslib.as_array(view.out_idx, (max(1, len(tiles)) * 32,))
+    n_out = max([int(tiles[k]["out_base"]) + int(tiles[k]["nrows"]) for k in range(view.stage1_tiles)
+                 if tiles[k]["mode"] == 1] or [0])
+    out_idx = np.ctypeslib.as_array(view.out_idx, (n_out,)) if n_out else np.zeros(0, np.int32)
     x = np.asarray(x, dtype=dt)
     t = np.zeros(view.t_len + 16, dt)
     p = np.zeros(view.p_len + 16, dt)
@@ -201,15 +203,22 @@ def emulate_layout(view, x: np.ndarray) -> np.ndarray:
             t[out_idx[ob:ob + R]] = acc
         else:
             p[ob:ob + R] = acc
-    if view.n_red:
-        red = np.ctypeslib.as_array(view.red, (view.n_red * 4,)).reshape(-1, 4)
-        for slot, pb, nch, _ in red:
-            t[slot] = sum(p[pb + c * 32] for c in range(nch))
+    if view.n_red1:
+        red = np.ctypeslib.as_array(view.red1, (view.n_red1 * 4,)).reshape(-1, 4)
+        for slot, pb, nch, stride in red:
+            t[slot] = sum(p[pb + c * stride] for c in range(nch))
     for k in range(view.stage1_tiles, view.n_tiles):
         td = tiles[k]
         acc = run_tile(td)
         R, ob = int(td["nrows"]), int(td["out_base"])
-        y[ob:ob + R] = acc
+        if td["mode"] == 0:
+            y[ob:ob + R] = acc
+        else:
+            p[ob:ob + R] = acc
+    if view.n_red2:
+        red = np.ctypeslib.as_array(view.red2, (view.n_red2 * 4,)).reshape(-1, 4)
+        for row, pb, nch, stride in red:
+            y[row] = sum(p[pb + c * stride] for c in range(nch))
     return y
 
 

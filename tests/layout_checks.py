@@ -44,14 +44,29 @@ def check_layout_bounds(view):
             else:
                 n_out = max(n_out, ob + R)
         else:
-            assert mode == 0 and 0 <= ob and ob + R <= view.nd
-            covered[ob:ob + R] += 1
-    assert np.all(covered == 1), "stage-2 tiles must cover every row exactly once"
+            assert mode in (0, 2)
+            if mode == 0:
+                assert 0 <= ob and ob + R <= view.nd
+                covered[ob:ob + R] += 1
+            else:
+                assert 0 <= ob and ob + R <= view.p_len
     if n_out:
         out_idx = np.ctypeslib.as_array(view.out_idx, (n_out,))
         assert np.all((out_idx >= 0) & (out_idx < view.t_len))
         assert len(np.unique(out_idx)) == len(out_idx)
-    if view.n_red:
-        red = np.ctypeslib.as_array(view.red, (view.n_red * 4,)).reshape(-1, 4)
+    if view.n_red1:
+        red = np.ctypeslib.as_array(view.red1, (view.n_red1 * 4,)).reshape(-1, 4)
         assert np.all((red[:, 0] >= 0) & (red[:, 0] < view.t_len))
-        assert np.all(red[:, 1] >= 0) and np.all(red[:, 1] + (red[:, 2] - 1) * 32 < view.p_len)
+        assert np.all(red[:, 1] >= 0) and np.all(red[:, 1] + (red[:, 2] - 1) * red[:, 3] < view.p_len)
+    if view.n_red2:
+        red = np.ctypeslib.as_array(view.red2, (view.n_red2 * 4,)).reshape(-1, 4)
+        assert np.all((red[:, 0] >= 0) & (red[:, 0] < view.nd))
+        assert np.all(red[:, 1] >= 0) and np.all(red[:, 1] + (red[:, 2] - 1) * red[:, 3] < view.p_len)
+        covered[red[:, 0]] += 1
+    assert np.all(covered == 1), "every row must be written exactly once (by a tile or a reduction)"
+    # the items of one team form one contiguous region of the data stream
+    for tbeg in (tb1, tb2):
+        for a, b in zip(tbeg[:-1], tbeg[1:]):
+            for k in range(a + 1, b):
+                prev = tiles[k - 1]
+                assert int(tiles[k]["data_off"]) == int(prev["data_off"]) + int(prev["nvec"]) * int(prev["nrows"])
