@@ -180,6 +180,17 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(value: float, dist, device) -> float:
+    """The largest `value` over all ranks (timings are reported as the slowest rank)."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peak_gbs():
     try:
         with open(PEAKS) as f:
@@ -293,10 +304,7 @@ def run_b200(a, rank, world, local_rank):
     stage_ms, napplies = plan.profile_read()
     plan.profile(False)
     clk = clocks.stop()
-    if dist:
-        tt = torch.tensor([ms_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_total = float(tt.item())
+    ms_total = max_over_ranks(ms_total, dist, dev)
     ms_step = ms_total / a.steps
     y_gpu = yd.cpu().numpy().astype(np.float64)
 
@@ -317,10 +325,7 @@ def run_b200(a, rank, world, local_rank):
     f1.record(stream)
     torch.cuda.synchronize(dev)
     e2e_ms = f0.elapsed_time(f1)
-    if dist:
-        tt = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = max_over_ranks(e2e_ms, dist, dev)
     e2e_step = e2e_ms / a.e2e_steps
 
     # ---- CPU baseline (rank 0, N=1 only) and parity of this run ----

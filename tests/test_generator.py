@@ -1,0 +1,101 @@
+"""The H-matrix generator (include/hacapk_hgen.h): HACApK's construction rules
+hold on its output, and the reference's own loaders read its files."""
+import numpy as np
+import pytest
+
+from hacapk_hmvm_b200 import HMatrix
+from helpers import RefMatrix, ref_available, relerr
+
+
+def _boxes(hm, r0, n):
+    pts = hm.meta["coords"][hm.meta["lod"][r0:r0 + n] - 1]
+    return pts.min(axis=0), pts.max(axis=0)
+
+
+@pytest.mark.parametrize("geo,eta,eps,leaf", [("sphere", 2.0, 1e-4, 32), ("cube", 1.0, 1e-6, 16),
+                                              ("plate", 2.0, 1e-3, 8)])
+def test_structure(geo, eta, eps, leaf):
+    hm = HMatrix.generate(1500, geo, eta=eta, eps=eps, leaf_size=leaf, seed=4)
+    n = hm.nd
+    # leaves tile the n x n matrix exactly once
+    cov = np.zeros((n, n), np.int8)
+    for i in range(hm.nlf):
+        r, c = hm.nstrtl[i] - 1, hm.nstrtt[i] - 1
+        cov[r:r + hm.ndl[i], c:c + hm.ndt[i]] += 1
+    assert np.all(cov == 1)
+    # rows nondecreasing (HACApK's row sort, m_HACApK_base.f90:245)
+    assert np.all(np.diff(hm.nstrtl) >= 0)
+    # lod is a permutation
+    assert np.array_equal(np.sort(hm.meta["lod"]), np.arange(1, n + 1))
+    lr = hm.ltmtx == 1
+    # admissibility of every low-rank leaf and size rules (:860-877)
+    for i in np.where(lr)[0]:
+        lo1, hi1 = _boxes(hm, hm.nstrtl[i] - 1, hm.ndl[i])
+        lo2, hi2 = _boxes(hm, hm.nstrtt[i] - 1, hm.ndt[i])
+        gap = np.maximum(0, np.maximum(lo2 - hi1, lo1 - hi2))
+        dist = np.sqrt((gap ** 2).sum())
+        w1, w2 = np.linalg.norm(hi1 - lo1), np.linalg.norm(hi2 - lo2)
+        assert min(w1, w2) <= eta * dist * (1 + 1e-12)
+        assert hm.ndl[i] >= leaf + 1 and hm.ndt[i] >= leaf + 1
+    assert hm.ktmax == hm.kt[lr].max()
+    assert hm.meta["aca_incomplete"] == 0
+
+
+def test_aca_accuracy_and_entries():
+    hm = HMatrix.generate(2000, "sphere", eta=2.0, eps=1e-4, leaf_size=32, seed=6)
+    rm = hm.rowmat
+    errs = []
+    for i in np.where(hm.ltmtx == 1)[0][:40]:
+        k, l, t = hm.kt[i], hm.ndl[i], hm.ndt[i]
+        V = rm[hm.a1[i]:hm.a1[i] + k * t].reshape(k, t)
+        U = rm[hm.a2[i]:hm.a2[i] + k * l].reshape(k, l)
+        E = np.array([[hm.entry(hm.nstrtl[i] + r, hm.nstrtt[i] + c) for c in range(t)] for r in range(l)])
+        errs.append(np.linalg.norm(U.T @ V - E) / np.linalg.norm(E))
+    assert max(errs) < 1e-2 and np.median(errs) < 1e-3
+    # dense leaves hold exact kernel entries; the diagonal is the self term 1.0
+    for i in np.where(hm.ltmtx == 2)[0][:20]:
+        l, t = hm.ndl[i], hm.ndt[i]
+        D = rm[hm.a1[i]:hm.a1[i] + l * t].reshape(l, t)
+        E = np.array([[hm.entry(hm.nstrtl[i] + r, hm.nstrtt[i] + c) for c in range(t)] for r in range(l)])
+        assert np.array_equal(D, E)
+    assert hm.entry(5, 5) == 1.0
+
+
+def test_deterministic():
+    a = HMatrix.generate(3000, "cube", seed=12, nthreads=1)
+    b = HMatrix.generate(3000, "cube", seed=12, nthreads=4)
+    assert np.array_equal(a.rowmat, b.rowmat) and np.array_equal(a.kt, b.kt)
+    c = HMatrix.generate(3000, "cube", seed=13)
+    assert not np.array_equal(a.rowmat[:100], c.rowmat[:100])
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference build oracle/_ref absent")
+def test_reference_reads_generated_files(tmp_path):
+    import ctypes as C
+
+    from helpers import ref_lib
+
+    hm = HMatrix.generate(1000, "sphere", seed=2)
+    p1, p2 = str(tmp_path / "hmatrix_1.bin"), str(tmp_path / "hmatrix_2.bin")
+    hm.write_bin1(p1)
+    hm.write_bin2(p2)
+    r = ref_lib()
+    x = np.sin(np.arange(1, hm.nd + 1, dtype=np.float64))
+    h1, h2 = r.ref_load1(p1.encode()), r.ref_load2(p2.encode())
+    y1, y2, y3 = np.empty(hm.nd), np.empty(hm.nd), np.empty(hm.nd)
+    r.ref_seq1_d(h1, x.ctypes.data, y1.ctypes.data, 0)  # AoS from hmatrix_1.bin
+    r.ref_seq2_d(h1, x.ctypes.data, y2.ctypes.data, 0)  # SoA from hmatrix_1.bin
+    r.ref_seq2_d(h2, x.ctypes.data, y3.ctypes.data, 0)  # SoA from hmatrix_2.bin
+    r.ref_free(h1)
+    r.ref_free(h2)
+    assert np.array_equal(y1, y2) and np.array_equal(y2, y3)
+    # and it approximates the dense kernel matrix to the ACA tolerance
+    A = np.array([[hm.entry(i, j) for j in range(1, hm.nd + 1)] for i in range(1, hm.nd + 1)])
+    assert relerr(y2, A @ x) < 1e-3
+
+
+def test_write_rejects_range(tmp_path):
+    # a leaf record beyond the format's int32 byte count is refused, not wrapped
+    hm = HMatrix.from_arrays(1, 1, [2], [0], [1], [1], [1], [1], [0], [0], np.array([1.0]))
+    hm.write_bin1(str(tmp_path / "ok.bin"))
+    assert HMatrix.load(str(tmp_path / "ok.bin")).rowmat[0] == 1.0

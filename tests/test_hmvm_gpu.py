@@ -274,3 +274,25 @@ def test_streams(gpu):
             plan.apply(xd, yd, stream=s)
         s.synchronize()
         assert np.array_equal(yd.cpu().numpy(), y0)
+
+
+def test_golden_fixtures(gpu):
+    """The committed fixtures: inputs as bytes, y from the reference's own hmvm_seq_2."""
+    import json
+    import os
+
+    from helpers import GOLDEN
+
+    meta = json.load(open(os.path.join(GOLDEN, "golden.json")))
+    Y = np.load(os.path.join(GOLDEN, "golden_y.npz"))
+    for name, m in meta["matrices"].items():
+        hm = HMatrix.load(os.path.join(GOLDEN, m["file"]))
+        for xn in ("sin", "uniform"):
+            x = Y[f"{name}/x_{xn}"]
+            with Plan(hm, "fp64") as plan:
+                y = _run(plan, x)
+            assert relerr(y, Y[f"{name}/y_seq2_d_{xn}"]) <= TOL64, (name, xn)
+            with Plan(hm, "fp32") as plan:
+                yf = _run(plan, x)
+            assert relerr(yf, Y[f"{name}/y_seq2_f_{xn}"]) <= TOL32, (name, xn)
+            assert relerr(yf, Y[f"{name}/y_seq2_d_{xn}"]) <= TOL32
