@@ -191,6 +191,22 @@ def max_over_ranks(value: float, dist, device) -> float:
     return float(t.item())
 
 
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "stream_kernel_fp64_sphere65536.md")
+
+
+def traffic_ratio(stage: int):
+    """DRAM bytes per algorithmic byte of a stage kernel, from the committed ncu
+    summary (a capture of a smaller case of the same kernel), or None."""
+    try:
+        for line in open(TRAFFIC_PROFILE):
+            parts = line.split()
+            if len(parts) == 3 and parts[0] == "traffic_per_algorithmic_byte" and parts[1] == f"stage{stage}":
+                return float(parts[2])
+    except OSError:
+        pass
+    return None
+
+
 def measured_peak_gbs():
     try:
         with open(PEAKS) as f:
@@ -355,7 +371,11 @@ def run_b200(a, rank, world, local_rank):
         "kernel": [f"{kname} (V stage)", "hmvm_reduce_kernel (V stage)", f"{kname} (row stage)",
                    "hmvm_reduce_kernel (row stage)"][dom],
         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-        "traffic": None,
+        "traffic": (stage_bytes[dom] * traffic_ratio(1 if dom == 0 else 2)
+                    if dom in (0, 2) and info["kernel"] == 1 and a.precision == "fp64"
+                    and traffic_ratio(1 if dom == 0 else 2) else None),
+        "traffic_source": "ncu capture of the same kernel at N=65536, scaled by algorithmic bytes "
+                          "(profiles/stream_kernel_fp64_sphere65536.md)",
         "whole_hmvm_gbs": alg_bytes / (ms_step * 1e-3) / 1e9,
         "whole_hmvm_frac": alg_bytes / (ms_step * 1e-3) / 1e9 / peak,
         "stage_ms_avg": [s / max(napplies, 1) for s in stage_ms],
