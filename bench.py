@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "mixed"])
     ap.add_argument("--n", type=int, default=262144)
     ap.add_argument("--geometry", default="sphere")
     ap.add_argument("--eps", type=float, default=1e-4)
@@ -191,6 +191,9 @@ def max_over_ranks(value: float, dist, device) -> float:
     return float(t.item())
 
 
+DTYPES = {"fp64": "f64", "fp32": "f32",
+          "mixed": "mixed: f32/f16/e4m3 low-rank, f32/f64 dense storage; f32 segment sums, f64 rows and x, y"}
+
 TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "stream_kernel_fp64_sphere65536.md")
 
 
@@ -287,9 +290,10 @@ def run_b200(a, rank, world, local_rank):
                 ctas_per_sm=a.ctas_per_sm, kernel=a.kernel)
     setup_s = time.perf_counter() - t0
     info = plan.info()
-    tdt = torch.float64 if a.precision == "fp64" else torch.float32
-    ndt = np.float64 if a.precision == "fp64" else np.float32
-    elem = 8 if a.precision == "fp64" else 4
+    # x and y: FP64 for FP64 and mixed plans, FP32 for FP32 plans
+    tdt = torch.float32 if a.precision == "fp32" else torch.float64
+    ndt = np.float32 if a.precision == "fp32" else np.float64
+    elem = 4 if a.precision == "fp32" else 8
     xd = torch.from_numpy(x.astype(ndt)).to(dev)
     yd = torch.empty(hm.nd, dtype=tdt, device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -365,7 +369,7 @@ def run_b200(a, rank, world, local_rank):
     dom_avg_s = stage_ms[dom] / max(napplies, 1) * 1e-3
     achieved = stage_bytes[dom] / dom_avg_s / 1e9 if dom_avg_s > 0 else 0.0
     alg_bytes = info["algorithmic_bytes"]
-    kname = "hmvm_stream_kernel" if info["kernel"] == 1 else "hmvm_tile_kernel"
+    kname = {0: "hmvm_tile_kernel", 1: "hmvm_stream_kernel", 2: "hmvm_mixed_kernel"}[info["kernel"]]
     roof = {
         "bound": "hbm",
         "kernel": [f"{kname} (V stage)", "hmvm_reduce_kernel (V stage)", f"{kname} (row stage)",
@@ -391,7 +395,7 @@ def run_b200(a, rank, world, local_rank):
         line = {
             "metric": "HMVM/s", "value": value, "unit": "HMVM/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f32",
+            "vs_baseline": None, "dtype": DTYPES[a.precision],
             "data": "synthetic (seeded HACApK-rule H-matrix; x uniform[-1,1])",
             "config": cfg,
             "gbytes_per_s": alg_bytes / (ms_step * 1e-3) / 1e9,

@@ -25,6 +25,12 @@ HMVM_EDEVICE = -8
 
 HMVM_FP64 = 0
 HMVM_FP32 = 1
+HMVM_MIXED = 2
+HMVM_LR_FP16 = 0
+HMVM_LR_BF16 = 1
+# storage types of mixed-plan segments (high bits of hmvm_seg_desc.ncols)
+ST_F64, ST_F32, ST_F16, ST_E4M3, ST_BF16 = 0, 1, 2, 3, 4
+SEG_TYPE_SHIFT = 28
 
 HMVM_NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024
 
@@ -81,7 +87,8 @@ class Leaves64(C.Structure):
 class PlanOpts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("device", C.c_int32), ("max_tile_rows", C.c_int32),
                 ("split_cols", C.c_int32), ("stage1_cfg", C.c_int32), ("stage2_cfg", C.c_int32),
-                ("ctas_per_sm", C.c_int32), ("kernel", C.c_int32)]
+                ("ctas_per_sm", C.c_int32), ("kernel", C.c_int32), ("mixed_fp8_eps", C.c_double),
+                ("mixed_fp32_tau", C.c_double), ("mixed_lr_format", C.c_int32), ("_reserved", C.c_int32)]
 
 
 class PlanInfo(C.Structure):
@@ -92,7 +99,8 @@ class PlanInfo(C.Structure):
                 ("stage2_teams", C.c_int32), ("split_rows", C.c_int32), ("kernels_per_apply", C.c_int32),
                 ("stage1_cfg", C.c_int32), ("stage2_cfg", C.c_int32), ("flops", C.c_int64),
                 ("stage1_bytes", C.c_int64), ("stage2_bytes", C.c_int64),
-                ("kernel", C.c_int32), ("ctas_per_sm", C.c_int32)]
+                ("kernel", C.c_int32), ("ctas_per_sm", C.c_int32),
+                ("cols_fp32", C.c_int64), ("cols_lr16", C.c_int64), ("cols_fp8", C.c_int64)]
 
 
 class Stats(C.Structure):
@@ -117,7 +125,8 @@ class LayoutView(C.Structure):
                 ("data_vectors", C.c_int64), ("t_len", C.c_int64), ("p_len", C.c_int64),
                 ("tiles", C.c_void_p), ("segs", C.c_void_p), ("team_begin1", C.POINTER(C.c_int32)),
                 ("team_begin2", C.POINTER(C.c_int32)), ("out_idx", C.POINTER(C.c_int32)),
-                ("red1", C.POINTER(C.c_int32)), ("red2", C.POINTER(C.c_int32)), ("data", C.c_void_p)]
+                ("red1", C.POINTER(C.c_int32)), ("red2", C.POINTER(C.c_int32)), ("data", C.c_void_p),
+                ("rowscale", C.POINTER(C.c_double)), ("n_rowscale", C.c_int64)]
 
 
 class HgenParams(C.Structure):

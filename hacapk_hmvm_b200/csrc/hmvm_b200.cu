@@ -80,14 +80,28 @@ KernelFn stream_kernel_for(int cfg) {
   }
 }
 
+// Must list kMixedCfgs (layout.hpp) in order.
+inline KernelFn mixed_kernel_for(int cfg) {
+  switch (cfg) {
+    case 0: return hmvm_mixed_kernel<8, 4, 2048, 2048>;
+    case 1: return hmvm_mixed_kernel<8, 4, 1024, 4096>;
+    case 2: return hmvm_mixed_kernel<8, 4, 2048, 4096>;
+    case 3: return hmvm_mixed_kernel<4, 4, 2048, 4096>;
+    case 4: return hmvm_mixed_kernel<6, 4, 2048, 4096>;
+    default: return hmvm_mixed_kernel<16, 4, 1024, 2048>;
+  }
+}
+
 struct Launch {
   KernelFn fn;
   int threads, smem;
 };
 
+// kernel: 0 tile kernel, 1 stream kernel, 2 mixed-precision kernel
 template <typename T>
 Launch stage_launch(int kernel, int cfg) {
   if (kernel == 0) return Launch{tile_kernel_for<T>(cfg), 32 * kCfgs[cfg].wg * kCfgs[cfg].tpc, 0};
+  if (kernel == 2) return Launch{mixed_kernel_for(cfg), 32 * kMixedCfgs[cfg].wpb, mixed_smem_bytes(kMixedCfgs[cfg])};
   const StreamCfg& c = kStreamCfgs[cfg];
   return Launch{stream_kernel_for<T>(cfg), 32 * c.wpb, stream_smem_bytes(c, (int)sizeof(T))};
 }
@@ -118,6 +132,12 @@ struct hmvm_plan {
   int* d_err = nullptr;
   void* d_x = nullptr;  // staging for apply_host
   void* d_y = nullptr;
+  // mixed precision
+  bool mixed = false;
+  float* d_x32 = nullptr;
+  double* d_scale = nullptr;
+  int64_t cols_fp32 = 0, cols_lr16 = 0, cols_fp8 = 0, stored_bytes = 0;
+  int t_elem = 8, p_elem = 8;  // bytes per t slot and per partial sum
   int64_t stage1_bytes = 0, stage2_bytes = 0;
   // profiling: kEventsPerApply events per recorded apply
   bool profiling = false;
@@ -137,8 +157,8 @@ constexpr int kEventsPerApply = 5;
 void free_plan_buffers(hmvm_plan* p) {
   for (cudaEvent_t e : p->prof_events) cudaEventDestroy(e);
   p->prof_events.clear();
-  void* bufs[] = {p->d_data, p->d_tiles, p->d_segs, p->d_tb1, p->d_tb2, p->d_out_idx, p->d_red1,
-                  p->d_red2, p->d_t,     p->d_p,    p->d_err, p->d_x,  p->d_y};
+  void* bufs[] = {p->d_data, p->d_tiles, p->d_segs, p->d_tb1, p->d_tb2, p->d_out_idx, p->d_red1, p->d_red2,
+                  p->d_t,    p->d_p,     p->d_err,  p->d_x,   p->d_y,   p->d_x32,     p->d_scale};
   for (void* b : bufs)
     if (b) cudaFree(b);
 }
@@ -179,7 +199,7 @@ int upload(Buf** dst, const void* src, size_t bytes, int64_t* total) {
 template <typename T>
 int prepare_kernels(const hmvm_plan* p) {
   for (int cfg : {p->stage1_cfg, p->stage2_cfg}) {
-    Launch l = stage_launch<T>(p->kernel, cfg);
+    Launch l = stage_launch<T>(p->mixed ? 2 : p->kernel, cfg);
     if (l.smem > 0)
       HMVM_CUDA_TRY(cudaFuncSetAttribute((const void*)l.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, l.smem),
                     "cudaFuncSetAttribute");
@@ -209,14 +229,15 @@ int resident_ctas_t(int kernel, int cfg1, int cfg2, int* out) {
 int resident_ctas(const hmvm_plan_opts& o, int dev, int* out) {
   DeviceGuard g(dev);
   if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
-  const int kernel = o.kernel == 0 ? 0 : 1;
-  const int ncfg = kernel == 0 ? kNumCfgs : kNumStreamCfgs;
-  const int c1 = (o.stage1_cfg >= 0 && o.stage1_cfg < ncfg) ? o.stage1_cfg
-                 : (kernel == 0 ? kDefaultStage1Cfg : kDefaultStreamCfg);
-  const int c2 = (o.stage2_cfg >= 0 && o.stage2_cfg < ncfg) ? o.stage2_cfg
-                 : (kernel == 0 ? kDefaultStage2Cfg : kDefaultStreamCfg);
-  return o.precision == HMVM_FP64 ? resident_ctas_t<double>(kernel, c1, c2, out)
-                                  : resident_ctas_t<float>(kernel, c1, c2, out);
+  const bool mixed = o.precision == HMVM_MIXED;
+  const int kernel = mixed ? 2 : (o.kernel == 0 ? 0 : 1);
+  const int ncfg = mixed ? kNumMixedCfgs : (kernel == 0 ? kNumCfgs : kNumStreamCfgs);
+  const int d1 = mixed ? kDefaultMixedCfg : (kernel == 0 ? kDefaultStage1Cfg : kDefaultStreamCfg);
+  const int d2 = mixed ? kDefaultMixedCfg : (kernel == 0 ? kDefaultStage2Cfg : kDefaultStreamCfg);
+  const int c1 = (o.stage1_cfg >= 0 && o.stage1_cfg < ncfg) ? o.stage1_cfg : d1;
+  const int c2 = (o.stage2_cfg >= 0 && o.stage2_cfg < ncfg) ? o.stage2_cfg : d2;
+  return o.precision == HMVM_FP32 ? resident_ctas_t<float>(kernel, c1, c2, out)
+                                  : resident_ctas_t<double>(kernel, c1, c2, out);
 }
 
 int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** out) {
@@ -268,12 +289,25 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   p->stored_elems = L->stored_elems;
   p->t_len = L->t_len;
   p->p_len = L->p_len;
-  {
+  p->mixed = L->mixed;
+  p->cols_fp32 = L->cols_fp32;
+  p->cols_lr16 = L->cols_lr16;
+  p->cols_fp8 = L->cols_fp8;
+  p->t_elem = L->mixed ? 4 : L->elem_size;
+  p->p_elem = L->elem_size;
+  if (L->mixed) {
+    // Algorithmic bytes: the stored elements in their storage formats, the
+    // per-column scales, x and y once.
+    p->stored_bytes = L->stored_bytes + 8 * (int64_t)L->rowscale.size();
+    p->stage1_bytes = L->stored_bytes1 + 8 * (int64_t)L->rowscale.size() + 8 * (int64_t)lt.nd;
+    p->stage2_bytes = L->stored_bytes - L->stored_bytes1 + 16 * (int64_t)lt.nd;
+  } else {
     // Algorithmic bytes per stage: stored elements of the stage once, plus the
     // vectors it reads/writes once (the intermediate t is not counted).
     int64_t v_elems = 0;
     for (int32_t i = 0; i < lt.nlf; i++)
       if (lt.ltmtx[i] == 1) v_elems += (int64_t)lt.kt[i] * lt.ndt[i];
+    p->stored_bytes = L->stored_elems * L->elem_size;
     p->stage1_bytes = (v_elems + (int64_t)lt.nd) * L->elem_size;
     p->stage2_bytes = (L->stored_elems - v_elems + 2 * (int64_t)lt.nd) * L->elem_size;
   }
@@ -292,22 +326,27 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
     if (!rc) rc = upload(&p->d_red2, L->red2.data(), L->red2.size() * 4, nullptr);
     // t: the padding slots of every row group must read as zero; stage 1 only
     // ever writes real slots, so one clear at creation keeps them zero.
-    size_t tbytes = (size_t)(L->t_len + 16) * L->elem_size;
+    size_t tbytes = (size_t)(L->t_len + 16) * p->t_elem;
     if (!rc) {
       cudaError_t e = cudaMalloc(&p->d_t, tbytes);
       if (e == cudaSuccess) e = cudaMemset(p->d_t, 0, tbytes);
       if (e != cudaSuccess) rc = cuda_fail(e, "t buffer");
     }
     if (!rc) {
-      cudaError_t e = cudaMalloc(&p->d_p, (size_t)(L->p_len + 16) * L->elem_size);
+      cudaError_t e = cudaMalloc(&p->d_p, (size_t)(L->p_len + 16) * p->p_elem);
       if (e != cudaSuccess) rc = cuda_fail(e, "partial buffer");
+    }
+    if (!rc && L->mixed) {
+      cudaError_t e = cudaMalloc(&p->d_x32, (size_t)(L->nd + 16) * sizeof(float));
+      if (e != cudaSuccess) rc = cuda_fail(e, "x32 buffer");
+      if (!rc) rc = upload(&p->d_scale, L->rowscale.data(), L->rowscale.size() * sizeof(double), nullptr);
     }
     if (!rc) {
       cudaError_t e = cudaMalloc(&p->d_err, sizeof(int));
       if (e == cudaSuccess) e = cudaMemset(p->d_err, 0, sizeof(int));
       if (e != cudaSuccess) rc = cuda_fail(e, "status word");
     }
-    if (!rc) rc = p->precision == HMVM_FP64 ? prepare_kernels<double>(p) : prepare_kernels<float>(p);
+    if (!rc) rc = p->precision == HMVM_FP32 ? prepare_kernels<float>(p) : prepare_kernels<double>(p);
     if (!rc) {
       cudaError_t e = cudaDeviceSynchronize();
       if (e != cudaSuccess) rc = cuda_fail(e, "plan upload");
@@ -320,6 +359,63 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
     return rc;
   }
   *out = p;
+  return HMVM_OK;
+}
+
+// Mixed plans: x rounded to FP32, V stage (scaled t in FP32), its reduction,
+// row stage, its reduction into y (partials in FP64).
+int launch_stages_mixed(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, float* x32, cudaStream_t st) {
+  TileArgs a;
+  a.err = p->d_err;
+  a.tiles = p->d_tiles;
+  a.segs = p->d_segs;
+  a.data = p->d_data;
+  a.x = x;
+  a.t = tbuf;
+  a.y = y;
+  a.p = pbuf;
+  a.out_idx = p->d_out_idx;
+  a.x32 = x32;
+  const int ctas = p->num_sms * p->ctas_per_sm;
+  cudaEvent_t* ev = nullptr;
+  if (p->profiling && p->prof_count < kMaxProfiled) {
+    ev = &p->prof_events[kEventsPerApply * (size_t)p->prof_count];
+    p->prof_count++;
+  }
+  if (ev) cudaEventRecord(ev[0], st);
+  hmvm_round_f32_kernel<<<std::min((p->nd + 255) / 256, p->num_sms * 8), 256, 0, st>>>(
+      static_cast<const double*>(x), x32, p->nd);
+  HMVM_CUDA_TRY(cudaGetLastError(), "x rounding launch");
+  if (p->stage1_tiles > 0) {
+    const Launch l = stage_launch<double>(2, p->stage1_cfg);
+    a.team_begin = p->d_tb1;
+    a.nteams = p->stage1_teams;
+    a.scale = p->d_scale;
+    l.fn<<<ctas, l.threads, l.smem, st>>>(a);
+    HMVM_CUDA_TRY(cudaGetLastError(), "V-stage launch");
+  }
+  if (ev) cudaEventRecord(ev[1], st);
+  if (p->n_red1 > 0) {
+    hmvm_reduce_kernel<double, float><<<(p->n_red1 + 255) / 256, 256, 0, st>>>(
+        p->d_red1, p->n_red1, static_cast<const double*>(pbuf), static_cast<float*>(tbuf));
+    HMVM_CUDA_TRY(cudaGetLastError(), "V-stage reduction launch");
+  }
+  if (ev) cudaEventRecord(ev[2], st);
+  {
+    const Launch l = stage_launch<double>(2, p->stage2_cfg);
+    a.team_begin = p->d_tb2;
+    a.nteams = p->stage2_teams;
+    a.scale = nullptr;
+    l.fn<<<ctas, l.threads, l.smem, st>>>(a);
+    HMVM_CUDA_TRY(cudaGetLastError(), "row-stage launch");
+  }
+  if (ev) cudaEventRecord(ev[3], st);
+  if (p->n_red2 > 0) {
+    hmvm_reduce_kernel<double, double><<<(p->n_red2 + 255) / 256, 256, 0, st>>>(
+        p->d_red2, p->n_red2, static_cast<const double*>(pbuf), static_cast<double*>(y));
+    HMVM_CUDA_TRY(cudaGetLastError(), "row-stage reduction launch");
+  }
+  if (ev) cudaEventRecord(ev[4], st);
   return HMVM_OK;
 }
 
@@ -337,6 +433,8 @@ int launch_stages(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, 
   a.y = y;
   a.p = pbuf;
   a.out_idx = p->d_out_idx;
+  a.x32 = nullptr;
+  a.scale = nullptr;
   const int ctas = p->num_sms * p->ctas_per_sm;
   cudaEvent_t* ev = nullptr;
   if (p->profiling && p->prof_count < kMaxProfiled) {
@@ -353,8 +451,8 @@ int launch_stages(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, 
   }
   if (ev) cudaEventRecord(ev[1], st);
   if (p->n_red1 > 0) {
-    hmvm_reduce_kernel<T><<<(p->n_red1 + 255) / 256, 256, 0, st>>>(p->d_red1, p->n_red1,
-                                                                   static_cast<const T*>(pbuf), static_cast<T*>(tbuf));
+    hmvm_reduce_kernel<T, T><<<(p->n_red1 + 255) / 256, 256, 0, st>>>(p->d_red1, p->n_red1,
+                                                                      static_cast<const T*>(pbuf), static_cast<T*>(tbuf));
     HMVM_CUDA_TRY(cudaGetLastError(), "V-stage reduction launch");
   }
   if (ev) cudaEventRecord(ev[2], st);
@@ -367,8 +465,8 @@ int launch_stages(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, 
   }
   if (ev) cudaEventRecord(ev[3], st);
   if (p->n_red2 > 0) {
-    hmvm_reduce_kernel<T><<<(p->n_red2 + 255) / 256, 256, 0, st>>>(p->d_red2, p->n_red2,
-                                                                   static_cast<const T*>(pbuf), static_cast<T*>(y));
+    hmvm_reduce_kernel<T, T><<<(p->n_red2 + 255) / 256, 256, 0, st>>>(p->d_red2, p->n_red2,
+                                                                      static_cast<const T*>(pbuf), static_cast<T*>(y));
     HMVM_CUDA_TRY(cudaGetLastError(), "row-stage reduction launch");
   }
   if (ev) cudaEventRecord(ev[4], st);
@@ -377,6 +475,7 @@ int launch_stages(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, 
 
 int apply_impl(hmvm_plan* p, const void* x, void* y, cudaStream_t st) {
   if (p->nd == 0) return HMVM_OK;
+  if (p->mixed) return launch_stages_mixed(p, x, y, p->d_t, p->d_p, p->d_x32, st);
   if (p->precision == HMVM_FP64) return launch_stages<double>(p, x, y, p->d_t, p->d_p, st);
   return launch_stages<float>(p, x, y, p->d_t, p->d_p, st);
 }
@@ -442,6 +541,9 @@ void hmvm_b200_default_opts(hmvm_plan_opts* o) {
   o->stage2_cfg = -1;
   o->ctas_per_sm = 0;
   o->kernel = -1;
+  o->mixed_fp8_eps = 1e-4;
+  o->mixed_fp32_tau = 0.5;
+  o->mixed_lr_format = HMVM_LR_FP16;
 }
 
 int hmvm_b200_plan_create_d(const hmvm_matrix2_d* m, const hmvm_plan_opts* opts, hmvm_plan** plan) {
@@ -501,7 +603,7 @@ int hmvm_b200_plan_get_info(const hmvm_plan* p, hmvm_plan_info* info) {
   info->precision = p->precision;
   info->device = p->device;
   info->num_sms = p->num_sms;
-  info->algorithmic_bytes = (p->stored_elems + 2 * (int64_t)p->nd) * p->elem;
+  info->algorithmic_bytes = p->stored_bytes + 2 * (int64_t)p->nd * p->elem;
   info->device_bytes = p->device_bytes;
   info->t_len = p->t_len;
   info->stage1_tiles = p->stage1_tiles;
@@ -515,8 +617,11 @@ int hmvm_b200_plan_get_info(const hmvm_plan* p, hmvm_plan_info* info) {
   info->flops = 2 * p->stored_elems;
   info->stage1_bytes = p->stage1_bytes;
   info->stage2_bytes = p->stage2_bytes;
-  info->kernel = p->kernel;
+  info->kernel = p->mixed ? 2 : p->kernel;
   info->ctas_per_sm = p->ctas_per_sm;
+  info->cols_fp32 = p->cols_fp32;
+  info->cols_lr16 = p->cols_lr16;
+  info->cols_fp8 = p->cols_fp8;
   return HMVM_OK;
 }
 
@@ -568,7 +673,7 @@ int hmvm_b200_plan_status(hmvm_plan* p) {
 
 int hmvm_b200_plan_kernel_count(const hmvm_plan* p) {
   if (!p || p->nd == 0) return 0;
-  return (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1 + (p->n_red2 > 0);
+  return (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1 + (p->n_red2 > 0) + (p->mixed ? 1 : 0);
 }
 
 int hmvm_b200_apply(hmvm_plan* p, const void* x, void* y, void* stream) {
@@ -625,7 +730,7 @@ static int one_shot(hmvm_plan* plan, const void* x, void* y, hmvm_stats* stats, 
   if (!rc && stats) {
     stats->seconds_setup = setup_s;
     stats->seconds_apply = ms * 1e-3;
-    stats->algorithmic_bytes = (plan->stored_elems + 2 * (int64_t)plan->nd) * plan->elem;
+    stats->algorithmic_bytes = plan->stored_bytes + 2 * (int64_t)plan->nd * plan->elem;
     stats->gbytes_per_s = ms > 0 ? stats->algorithmic_bytes / (ms * 1e-3) / 1e9 : 0.0;
   }
   return rc;
@@ -702,10 +807,11 @@ int hmvm_b200_apply_noalloc(hmvm_plan* p, const void* x, void* y, void* stream) 
   int rc = check_xy(p, x, y);
   if (rc) return rc;
   auto round256 = [](size_t b) { return (b + 255) / 256 * 256; };
-  const size_t tbytes = round256((size_t)(p->t_len + 16) * p->elem);
-  const size_t pbytes = round256((size_t)(p->p_len + 16) * p->elem);
-  if (tbytes + pbytes > (size_t)HMVM_NOALLOC_SCRATCH_BYTES)
-    return set_error(HMVM_ERANGE, "this plan needs " + std::to_string(tbytes + pbytes) +
+  const size_t tbytes = round256((size_t)(p->t_len + 16) * p->t_elem);
+  const size_t pbytes = round256((size_t)(p->p_len + 16) * p->p_elem);
+  const size_t xbytes = p->mixed ? round256((size_t)(p->nd + 16) * sizeof(float)) : 0;
+  if (tbytes + pbytes + xbytes > (size_t)HMVM_NOALLOC_SCRATCH_BYTES)
+    return set_error(HMVM_ERANGE, "this plan needs " + std::to_string(tbytes + pbytes + xbytes) +
                                       " bytes of scratch but hmvm_b200_apply_noalloc has " +
                                       std::to_string((size_t)HMVM_NOALLOC_SCRATCH_BYTES) +
                                       "; use hmvm_b200_apply");
@@ -721,6 +827,7 @@ int hmvm_b200_apply_noalloc(hmvm_plan* p, const void* x, void* y, void* stream) 
   // t's padding slots must read as zero, and earlier calls (of any plan) left
   // other values there; the partial sums are written in full before they are read.
   HMVM_CUDA_TRY(cudaMemsetAsync(tbuf, 0, tbytes, st), "clear the no-alloc scratch");
+  if (p->mixed) return launch_stages_mixed(p, x, y, tbuf, pbuf, reinterpret_cast<float*>(pbuf + pbytes), st);
   if (p->precision == HMVM_FP64) return launch_stages<double>(p, x, y, tbuf, pbuf, st);
   return launch_stages<float>(p, x, y, tbuf, pbuf, st);
 }
@@ -788,6 +895,8 @@ int hmvm_b200_layout_view(const hmvm_layout* h, hmvm_layout_view* v) {
   v->data_vectors = (int64_t)L.data.size();
   v->t_len = L.t_len;
   v->p_len = L.p_len;
+  v->rowscale = L.rowscale.empty() ? nullptr : L.rowscale.data();
+  v->n_rowscale = (int64_t)L.rowscale.size();
   v->tiles = L.tiles.data();
   v->segs = L.segs.data();
   v->team_begin1 = L.team_begin1.data();

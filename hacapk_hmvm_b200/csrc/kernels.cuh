@@ -34,6 +34,8 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
 #include "hmvm_b200.h"
@@ -65,6 +67,8 @@ struct TileArgs {
   void* y;                    // output (T)
   void* p;                    // partial sums of split panels (T)
   const int32_t* out_idx;     // stage-1 output slots
+  const float* x32;           // mixed: x rounded to FP32
+  const double* scale;        // mixed, V stage: per panel-row column scale (NULL in the row stage)
 };
 
 __device__ __forceinline__ void fma_vec(double& a0, double& a1, const double2& m, const double2& z) {
@@ -466,14 +470,282 @@ __global__ void __launch_bounds__(32 * WPB, (stream_min_blocks<T, WPB, S, CHUNK,
   }
 }
 
-template <typename T>
-__global__ void hmvm_reduce_kernel(const int4* __restrict__ red, int n, const T* __restrict__ p,
-                                   T* __restrict__ dst) {
+template <typename TP, typename TD>
+__global__ void hmvm_reduce_kernel(const int4* __restrict__ red, int n, const TP* __restrict__ p,
+                                   TD* __restrict__ dst) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int4 e = red[i];  // destination, first partial, parts, stride
-    T s = p[e.y];
+    TP s = p[e.y];
     for (int c = 1; c < e.z; c++) s += p[e.y + c * e.w];
-    dst[e.x] = s;
+    dst[e.x] = (TD)s;
+  }
+}
+
+// x rounded to FP32 once per HMVM (the inputs of the FP32 / FP16 / FP8 segments).
+__global__ void hmvm_round_f32_kernel(const double* __restrict__ x, float* __restrict__ x32, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x32[i] = (float)x[i];
+}
+
+// ---- mixed precision ---------------------------------------------------------
+// Segment element types (the top 4 bits of hmvm_seg_desc.ncols in mixed plans).
+enum : int { kF64 = 0, kF32 = 1, kF16 = 2, kE4M3 = 3, kBF16 = 4 };
+__device__ __forceinline__ int mixed_vec(int type) {
+  return type == kF64 ? 2 : type == kF32 ? 4 : type == kE4M3 ? 16 : 8;
+}
+
+// Copy the inputs item `d` reads into zb: FP64 segments take x (8-byte
+// elements), the others x rounded to FP32 or t (4-byte elements); every
+// segment is padded with zeros to whole vectors.  d has at most 32 segments.
+__device__ __forceinline__ void gather_inputs_mixed(const hmvm_tile_desc& d, const hmvm_seg_desc& sreg,
+                                                    const double* __restrict__ x, const float* __restrict__ x32,
+                                                    const float* __restrict__ tv, unsigned char* zb, int lane) {
+  int zoff = 0;
+  for (int j = 0; j < d.nseg; j++) {
+    const int src = __shfl_sync(0xffffffffu, sreg.src, j);
+    const int enc = __shfl_sync(0xffffffffu, sreg.ncols, j);
+    const int type = enc >> 28, nc = enc & 0x0fffffff;
+    const int vs = mixed_vec(type);
+    const int ncp = (nc + vs - 1) / vs * vs;
+    if (type == kF64) {
+      double* z = reinterpret_cast<double*>(zb + zoff);
+      for (int c = lane; c < ncp; c += 32) {
+        if (c < nc) cp_async<8>(z + c, x + src + c);
+        else z[c] = 0.0;
+      }
+      zoff += ncp * 8;
+    } else {
+      float* z = reinterpret_cast<float*>(zb + zoff);
+      const float* zs = src < 0 ? tv + (src & 0x7fffffff) : x32 + src;
+      for (int c = lane; c < ncp; c += 32) {
+        if (c < nc) cp_async<4>(z + c, zs + c);
+        else z[c] = 0.0f;
+      }
+      zoff += ncp * 4;
+    }
+  }
+}
+
+__device__ __forceinline__ void fma8(float& a0, float& a1, const float2 m01, const float2 m23, const float2 m45,
+                                     const float2 m67, const float4 z0, const float4 z1) {
+  a0 = fmaf(m01.x, z0.x, a0);
+  a1 = fmaf(m01.y, z0.y, a1);
+  a0 = fmaf(m23.x, z0.z, a0);
+  a1 = fmaf(m23.y, z0.w, a1);
+  a0 = fmaf(m45.x, z1.x, a0);
+  a1 = fmaf(m45.y, z1.y, a1);
+  a0 = fmaf(m67.x, z1.z, a0);
+  a1 = fmaf(m67.y, z1.w, a1);
+}
+__device__ __forceinline__ float2 h2f(uint32_t w) {
+  return __half22float2(*reinterpret_cast<const __half2*>(&w));
+}
+__device__ __forceinline__ float2 bf2f(uint32_t w) {
+  return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+}
+__device__ __forceinline__ float2 e4m3x2f(uint16_t w) {
+  __half2_raw h = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)w, __NV_E4M3);
+  return __half22float2(*reinterpret_cast<const __half2*>(&h));
+}
+
+// hmvm_mixed_kernel<WPB, S, CHUNK, ZBYTES>: the stream kernel's pipeline (TMA
+// bulk ring for the matrix, cp.async-gathered inputs one item ahead) for
+// mixed-precision plans, whose items hold segments of different element types
+// (FP64, FP32, FP16, BF16, FP8 E4M3).  Each segment's products are summed in
+// FP32 (FP64 for FP64 segments) and added to the row's FP64 total; the V stage
+// multiplies a row's total by its column scale before storing t (FP32).
+template <int WPB, int S, int CHUNK, int ZBYTES>
+constexpr int mixed_min_blocks() {
+  constexpr int smem = WPB * (S * CHUNK + 2 * ZBYTES + S * 8);
+  constexpr int by_smem = (227 * 1024) / smem;
+  constexpr int by_warps = 24 / WPB;
+  constexpr int m = by_smem < by_warps ? by_smem : by_warps;
+  return m > 0 ? m : 1;
+}
+
+template <int WPB, int S, int CHUNK, int ZBYTES>
+__global__ void __launch_bounds__(32 * WPB, (mixed_min_blocks<WPB, S, CHUNK, ZBYTES>()))
+    hmvm_mixed_kernel(TileArgs a) {
+  constexpr uint32_t RING = (uint32_t)S * CHUNK;
+  constexpr int B = 4;
+  static_assert((RING & (RING - 1)) == 0, "ring size must be a power of two");
+  static_assert(CHUNK % 16 == 0 && CHUNK >= 512, "bulk copies move multiples of 16 bytes");
+  static_assert(B * 32 * 16 <= (S - 1) * CHUNK, "ring too small for one batch");
+  extern __shared__ __align__(128) unsigned char smem[];
+
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int team = blockIdx.x * WPB + warp;
+  if (team >= a.nteams) return;
+  const int tb = a.team_begin[team], te = a.team_begin[team + 1];
+  if (tb >= te) return;
+  unsigned char* ring = smem + (size_t)warp * RING;
+  unsigned char* zbase = smem + (size_t)WPB * RING + (size_t)warp * 2 * ZBYTES;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)WPB * RING + (size_t)WPB * 2 * ZBYTES) + warp * S;
+
+  const hmvm_tile_desc* __restrict__ tiles = a.tiles;
+  const hmvm_seg_desc* __restrict__ segs = a.segs;
+  const double* __restrict__ x = static_cast<const double*>(a.x);
+  const float* __restrict__ x32 = a.x32;
+  const float* __restrict__ tv = static_cast<const float*>(a.t);
+  const double* __restrict__ scl = a.scale;
+  const hmvm_tile_desc dzero = {0, 0, 0, 0, 0, 1, 0, 0};
+  const hmvm_seg_desc szero = {0, 0};
+
+  hmvm_tile_desc cur = tiles[tb];
+  const int64_t vbase = cur.data_off;
+  const hmvm_tile_desc tl = tiles[te - 1];
+  const int64_t total64 = (tl.data_off + (int64_t)tl.nvec * tl.nrows - vbase) * 16;
+  if (total64 >= (int64_t)1 << 31) {
+    if (lane == 0) atomicExch(a.err, 2);
+    return;
+  }
+  const uint32_t total = (uint32_t)total64;
+  const char* gsrc = static_cast<const char*>(a.data) + vbase * 16;
+  const uint32_t nchunks = (total + CHUNK - 1) / CHUNK;
+  if (lane == 0) {
+#pragma unroll
+    for (int s = 0; s < S; s++) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  auto issue = [&](uint32_t q) {
+    const uint32_t off = q * (uint32_t)CHUNK;
+    const uint32_t bytes = min((uint32_t)CHUNK, total - off);
+    uint64_t* bar = &bars[q % S];
+    mbar_expect_tx(bar, bytes);
+    bulk_g2s(ring + (q % S) * CHUNK, gsrc + off, bytes, bar);
+  };
+  if (lane == 0)
+    for (uint32_t q = 0; q < min((uint32_t)S, nchunks); q++) issue(q);
+
+  auto row_scale = [&](const hmvm_tile_desc& d) {
+    return (scl != nullptr && lane < d.nrows) ? scl[d._pad + lane] : 1.0;
+  };
+  auto out_slot = [&](const hmvm_tile_desc& d) {
+    return (d.mode == 1 && lane < d.nrows) ? a.out_idx[d.out_base + lane] : 0;
+  };
+  hmvm_seg_desc cur_seg = lane < cur.nseg ? segs[cur.seg_begin + lane] : szero;
+  gather_inputs_mixed(cur, cur_seg, x, x32, tv, zbase, lane);
+  cp_async_commit();
+  int cur_oidx = out_slot(cur);
+  double cur_scale = row_scale(cur);
+  hmvm_tile_desc nxt = tb + 1 < te ? tiles[tb + 1] : dzero;
+  hmvm_seg_desc nxt_seg = (tb + 1 < te && lane < nxt.nseg) ? segs[nxt.seg_begin + lane] : szero;
+  int nxt_oidx = tb + 1 < te ? out_slot(nxt) : 0;
+  double nxt_scale = tb + 1 < te ? row_scale(nxt) : 1.0;
+  hmvm_tile_desc nn = tb + 2 < te ? tiles[tb + 2] : dzero;
+
+  uint32_t q_ready = 0, q_rel = 0;
+  bool failed = false;
+  for (int ti = tb, k = 0; ti < te; ++ti, ++k) {
+    unsigned char* zcur = zbase + (k & 1) * ZBYTES;
+    __syncwarp();
+    if (ti + 1 < te) gather_inputs_mixed(nxt, nxt_seg, x, x32, tv, zbase + ((k + 1) & 1) * ZBYTES, lane);
+    cp_async_commit();
+    const bool has_nn = ti + 2 < te;
+    const hmvm_seg_desc nn_seg = (has_nn && lane < nn.nseg) ? segs[nn.seg_begin + lane] : szero;
+    const int nn_oidx = has_nn ? out_slot(nn) : 0;
+    const double nn_scale = has_nn ? row_scale(nn) : 1.0;
+    const hmvm_tile_desc nnn = ti + 3 < te ? tiles[ti + 3] : dzero;
+    cp_async_wait<1>();
+    __syncwarp();
+
+    const int R = cur.nrows;
+    const uint32_t rstride = (uint32_t)R * 16;
+    uint32_t o = (uint32_t)((cur.data_off - vbase) * 16);
+    const uint32_t ol_lane = (uint32_t)lane * 16;
+    double row = 0.0;
+    int zoff = 0;
+    for (int j = 0; j < cur.nseg && !failed; j++) {
+      const int enc = __shfl_sync(0xffffffffu, cur_seg.ncols, j);
+      const int type = enc >> 28, nc = enc & 0x0fffffff;
+      const int vs = mixed_vec(type);
+      const int nv = (nc + vs - 1) / vs;
+      const unsigned char* zs = zcur + zoff;
+      zoff += nv * vs * (type == kF64 ? 8 : 4);
+      float f0 = 0.f, f1 = 0.f, f2 = 0.f, f3 = 0.f;
+      double d0 = 0.0, d1 = 0.0;
+      for (int v = 0; v < nv; v += B) {
+        const int nb = min(B, nv - v);
+        const uint32_t o_end = o + (uint32_t)nb * rstride;
+        if (o >= (q_rel + 1) * (uint32_t)CHUNK) {
+          const uint32_t qf = o / CHUNK;
+          __syncwarp();
+          if (lane == 0) {
+            fence_proxy_async();
+            for (uint32_t q = q_rel; q < qf; q++)
+              if (q + S < nchunks) issue(q + S);
+          }
+          q_rel = qf;
+        }
+        if (o_end > q_ready * (uint32_t)CHUNK) {
+          const uint32_t ql = (o_end - 1) / CHUNK;
+          while (q_ready <= ql) {
+            if (!warp_wait(&bars[q_ready % S], (q_ready / S) & 1)) {
+              failed = true;
+              break;
+            }
+            q_ready++;
+          }
+          if (failed) break;
+        }
+        for (int u = 0; u < nb; u++) {
+          const uint4 m = *reinterpret_cast<const uint4*>(ring + ((o + ol_lane + (uint32_t)u * rstride) & (RING - 1)));
+          const int vv = v + u;
+          if (type == kF64) {
+            const double2 z = *reinterpret_cast<const double2*>(zs + vv * 16);
+            d0 = fma(__hiloint2double(m.y, m.x), z.x, d0);
+            d1 = fma(__hiloint2double(m.w, m.z), z.y, d1);
+          } else if (type == kF32) {
+            const float4 z = *reinterpret_cast<const float4*>(zs + vv * 16);
+            f0 = fmaf(__uint_as_float(m.x), z.x, f0);
+            f1 = fmaf(__uint_as_float(m.y), z.y, f1);
+            f2 = fmaf(__uint_as_float(m.z), z.z, f2);
+            f3 = fmaf(__uint_as_float(m.w), z.w, f3);
+          } else if (type == kE4M3) {
+            const float4* z = reinterpret_cast<const float4*>(zs + vv * 64);
+            fma8(f0, f1, e4m3x2f((uint16_t)m.x), e4m3x2f((uint16_t)(m.x >> 16)), e4m3x2f((uint16_t)m.y),
+                 e4m3x2f((uint16_t)(m.y >> 16)), z[0], z[1]);
+            fma8(f2, f3, e4m3x2f((uint16_t)m.z), e4m3x2f((uint16_t)(m.z >> 16)), e4m3x2f((uint16_t)m.w),
+                 e4m3x2f((uint16_t)(m.w >> 16)), z[2], z[3]);
+          } else if (type == kBF16) {
+            const float4* z = reinterpret_cast<const float4*>(zs + vv * 32);
+            fma8(f0, f1, bf2f(m.x), bf2f(m.y), bf2f(m.z), bf2f(m.w), z[0], z[1]);
+          } else {
+            const float4* z = reinterpret_cast<const float4*>(zs + vv * 32);
+            fma8(f0, f1, h2f(m.x), h2f(m.y), h2f(m.z), h2f(m.w), z[0], z[1]);
+          }
+        }
+        o = o_end;
+      }
+      row += (d0 + d1) + (double)((f0 + f1) + (f2 + f3));
+    }
+    if (failed) break;
+    if (lane < R) {
+      if (scl != nullptr) {  // V stage
+        const double val = row * cur_scale;
+        if (cur.mode == 1) const_cast<float*>(tv)[cur_oidx] = (float)val;
+        else static_cast<double*>(a.p)[cur.out_base + lane] = val;
+      } else {
+        if (cur.mode == 0) static_cast<double*>(a.y)[cur.out_base + lane] = row;
+        else static_cast<double*>(a.p)[cur.out_base + lane] = row;
+      }
+    }
+    cur = nxt;
+    cur_seg = nxt_seg;
+    cur_oidx = nxt_oidx;
+    cur_scale = nxt_scale;
+    nxt = nn;
+    nxt_seg = nn_seg;
+    nxt_oidx = nn_oidx;
+    nxt_scale = nn_scale;
+    nn = nnn;
+  }
+  cp_async_wait<0>();
+  if (failed) {
+    const uint32_t issued = min(nchunks, q_rel + (uint32_t)S);
+    for (uint32_t q = q_ready; q < issued; q++) warp_wait(&bars[q % S], (q / S) & 1);
+    if (lane == 0) atomicExch(a.err, 1);
   }
 }
 

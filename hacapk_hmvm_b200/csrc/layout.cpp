@@ -3,12 +3,14 @@
 #include "layout.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
-#include <map>
 #include <new>
 #include <queue>
 #include <unordered_map>
 #include <utility>
+
+#include "numfmt.hpp"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -28,22 +30,21 @@ inline uint64_t key2(int32_t a, int32_t b) { return ((uint64_t)(uint32_t)a << 32
 struct Part {
   int32_t leaf;   // dense leaf, or -1 for a low-rank row group
   int32_t group;  // row group index when leaf < 0
+  int32_t cls;    // column class of the row group's columns
   int32_t ncols;
 };
 
 struct TileBuild {
-  int32_t row0 = 0, nrows = 0;       // stage 2
+  int32_t row0 = 0, nrows = 0;  // stage 2
   int32_t stage = 2;
-  // stage 1 panel chunk
-  int32_t cgroup = -1, panel_row0 = 0, col0 = 0;
+  int32_t panel_row0 = 0;       // stage 1: index into panel_rows / out_idx
+  int32_t scale_base = 0;       // stage 1, mixed: index into rowscale
   int32_t mode = 0, out_base = 0;
-  // segments: [seg_first, seg_first+nseg) in the temp segment list
   int32_t seg_first = 0, nseg = 0, nvec = 0;
-  int64_t cost = 0;
 };
 
 struct SegBuild {
-  int32_t src, ncols;
+  int32_t src, ncols, type;
   int32_t part_first, nparts;  // into parts (stage 2)
 };
 
@@ -51,6 +52,34 @@ template <class S>
 inline double rd(const void *base, int64_t i) {
   return (double)static_cast<const S *>(base)[i];
 }
+
+// Writes one element of `type` (value already scaled) at byte `off` of buf.
+inline void store_elem(char *buf, int64_t off, int type, double v) {
+  switch (type) {
+    case ST_F64: std::memcpy(buf + off, &v, 8); break;
+    case ST_F32: {
+      float f = (float)v;
+      std::memcpy(buf + off, &f, 4);
+      break;
+    }
+    case ST_F16: {
+      uint16_t h = to_fp16(v);
+      std::memcpy(buf + off, &h, 2);
+      break;
+    }
+    case ST_BF16: {
+      uint16_t h = to_bf16(v);
+      std::memcpy(buf + off, &h, 2);
+      break;
+    }
+    default: {
+      uint8_t b = to_e4m3(v);
+      std::memcpy(buf + off, &b, 1);
+    }
+  }
+}
+
+inline int elem_bytes(int type) { return 16 / seg_vec(type); }
 
 }  // namespace
 
@@ -102,40 +131,109 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
                  std::string &msg) {
   int rc = validate_leaves(lt, msg);
   if (rc) return rc;
-  if (opts.precision != HMVM_FP64 && opts.precision != HMVM_FP32) {
+  if (opts.precision != HMVM_FP64 && opts.precision != HMVM_FP32 && opts.precision != HMVM_MIXED) {
     msg = "unsupported precision";
     return HMVM_EINVAL;
   }
   try {
     L = HostLayout();
     L.precision = opts.precision;
-    L.elem_size = opts.precision == HMVM_FP64 ? 8 : 4;
+    L.mixed = opts.precision == HMVM_MIXED;
+    L.elem_size = opts.precision == HMVM_FP32 ? 4 : 8;  // of x, y and the partial sums
     L.vec = 16 / L.elem_size;
     L.nd = lt.nd;
     L.nlf = lt.nlf;
     L.num_sms = num_sms > 0 ? num_sms : 148;
-    L.kernel = (opts.kernel == 0) ? 0 : 1;
-    const int ncfg = L.kernel == 0 ? kNumCfgs : kNumStreamCfgs;
+    L.kernel = (opts.kernel == 0 && !L.mixed) ? 0 : 1;
+    const int ncfg = L.mixed ? kNumMixedCfgs : (L.kernel == 0 ? kNumCfgs : kNumStreamCfgs);
+    const int dcfg = L.mixed ? kDefaultMixedCfg : (L.kernel == 0 ? -1 : kDefaultStreamCfg);
     L.stage1_cfg = (opts.stage1_cfg >= 0 && opts.stage1_cfg < ncfg) ? opts.stage1_cfg
-                   : (L.kernel == 0 ? kDefaultStage1Cfg : kDefaultStreamCfg);
+                   : (dcfg >= 0 ? dcfg : kDefaultStage1Cfg);
     L.stage2_cfg = (opts.stage2_cfg >= 0 && opts.stage2_cfg < ncfg) ? opts.stage2_cfg
-                   : (L.kernel == 0 ? kDefaultStage2Cfg : kDefaultStreamCfg);
+                   : (dcfg >= 0 ? dcfg : kDefaultStage2Cfg);
     L.ctas_per_sm = opts.ctas_per_sm > 0 ? opts.ctas_per_sm
                     : (L.kernel == 0 ? kDefaultCtasPerSm : kDefaultStreamCtasPerSm);
-    const int VEC = L.vec;
+    const int VEC = L.vec;  // plain plans: elements per vector
     const int RMAX = (opts.max_tile_rows >= 1 && opts.max_tile_rows <= kMaxRows) ? opts.max_tile_rows : kMaxRows;
     const int32_t nd = lt.nd, nlf = lt.nlf;
+    const bool srcf = lt.rowmat_is_float;
+    auto get = [&](int64_t idx) { return srcf ? rd<float>(lt.rowmat, idx) : rd<double>(lt.rowmat, idx); };
+
+    // Column classes: plain plans have one (FP64 or FP32); mixed plans have
+    // FP32 (leading terms), FP16/BF16 and FP8 E4M3 (terms below eps).
+    const int base_type = opts.precision == HMVM_FP32 ? ST_F32 : ST_F64;
+    const int lr16 = opts.mixed_lr_format == HMVM_LR_BF16 ? ST_BF16 : ST_F16;
+    const int ncls = L.mixed ? 3 : 1;
+    const int cls_type[3] = {L.mixed ? (int)ST_F32 : base_type, lr16, ST_E4M3};
 
     // ---- leaf classes ---------------------------------------------------
     std::vector<uint8_t> live_lr(nlf, 0);
+    std::vector<int64_t> colbase(nlf, -1);  // first flat column (leaf, k=0) of a live low-rank leaf
+    int64_t ncolflat = 0;
     for (int32_t i = 0; i < nlf; i++) {
       if (lt.ltmtx[i] == 1) {
         L.n_lowrank++;
         L.stored_elems += (int64_t)lt.kt[i] * (lt.ndl[i] + (int64_t)lt.ndt[i]);
         live_lr[i] = lt.kt[i] > 0 && lt.ndl[i] > 0 && lt.ndt[i] > 0;
+        if (live_lr[i]) {
+          colbase[i] = ncolflat;
+          ncolflat += lt.kt[i];
+        }
       } else {
         L.n_dense++;
         L.stored_elems += (int64_t)lt.ndl[i] * lt.ndt[i];
+      }
+    }
+    // Per column: class and (mixed) the scales of its U and V factors.
+    std::vector<uint8_t> col_cls(ncolflat, 0);
+    std::vector<float> sc_u, sc_v;
+    if (L.mixed) {
+      sc_u.assign(ncolflat, 1.0f);
+      sc_v.assign(ncolflat, 1.0f);
+      const double fp8_eps = opts.mixed_fp8_eps;
+      const double tau = opts.mixed_fp32_tau;
+#pragma omp parallel for schedule(dynamic, 64)
+      for (int32_t i = 0; i < nlf; i++) {
+        if (!live_lr[i]) continue;
+        const int32_t kt = lt.kt[i], ndl = lt.ndl[i], ndt = lt.ndt[i];
+        std::vector<double> nu(kt), nv(kt), mu(kt), mv(kt);
+        double block = 0.0;
+        for (int32_t k = 0; k < kt; k++) {
+          double su = 0, sv = 0, au = 0, av = 0;
+          for (int32_t r = 0; r < ndl; r++) {
+            double u = get(lt.a2(i) + (int64_t)k * ndl + r);
+            su += u * u;
+            au = std::max(au, std::fabs(u));
+          }
+          for (int32_t c = 0; c < ndt; c++) {
+            double v = get(lt.a1(i) + (int64_t)k * ndt + c);
+            sv += v * v;
+            av = std::max(av, std::fabs(v));
+          }
+          nu[k] = std::sqrt(su);
+          nv[k] = std::sqrt(sv);
+          mu[k] = au;
+          mv[k] = av;
+          block = std::max(block, nu[k] * nv[k]);
+        }
+        for (int32_t k = 0; k < kt; k++) {
+          const int64_t f = colbase[i] + k;
+          const double term = nu[k] * nv[k];
+          int cl = 1;
+          if (term >= tau * block) cl = 0;
+          else if (term < fp8_eps * block) cl = 2;
+          col_cls[f] = (uint8_t)cl;
+          if (cl == 1) {  // FP16/BF16: scale each factor to max |value| 1
+            sc_u[f] = mu[k] > 0 ? (float)mu[k] : 1.0f;
+            sc_v[f] = mv[k] > 0 ? (float)mv[k] : 1.0f;
+          } else if (cl == 2) {  // E4M3: scale to max |value| 448
+            sc_u[f] = mu[k] > 0 ? (float)(mu[k] / 448.0) : 1.0f;
+            sc_v[f] = mv[k] > 0 ? (float)(mv[k] / 448.0) : 1.0f;
+          }
+        }
+      }
+      for (int64_t f = 0; f < ncolflat; f++) {
+        (col_cls[f] == 0 ? L.cols_fp32 : col_cls[f] == 1 ? L.cols_lr16 : L.cols_fp8)++;
       }
     }
 
@@ -166,9 +264,8 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     for (int32_t ti = 0; ti < nrt; ti++)
       for (int32_t r = trow0[ti]; r < trow0[ti] + tnrows[ti]; r++) row_tile[r] = ti;
 
-    // ---- low-rank row groups and t slots ---------------------------------
+    // ---- low-rank row groups / column groups and t slots ------------------
     std::unordered_map<uint64_t, int32_t> rgmap, cgmap;
-    std::vector<int32_t> rg_of(nlf, -1), cg_of(nlf, -1);
     std::vector<std::vector<int32_t>> rg_members, cg_members;
     for (int32_t i = 0; i < nlf; i++) {
       if (!live_lr[i]) continue;
@@ -182,7 +279,6 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
       } else {
         g = it->second;
       }
-      rg_of[i] = g;
       rg_members[g].push_back(i);
       uint64_t kc = key2(lt.nstrtt[i], lt.ndt[i]);
       auto jt = cgmap.find(kc);
@@ -194,22 +290,28 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
       } else {
         c = jt->second;
       }
-      cg_of[i] = c;
       cg_members[c].push_back(i);
     }
     const int32_t nrg = (int32_t)rg_members.size();
-    std::vector<int64_t> slot_of_leaf(nlf, -1);  // slot of (leaf, k=0)
-    std::vector<int32_t> rg_slot(nrg), rg_k(nrg);
+    // slots ordered by (row group, column class, leaf in file order, k)
+    std::vector<int64_t> slot_of_col(ncolflat, -1);
+    std::vector<int32_t> rg_slot((size_t)nrg * ncls), rg_k((size_t)nrg * ncls);
     int64_t t_len = 0;
+    const int slot_align = L.mixed ? 4 : VEC;
     for (int32_t g = 0; g < nrg; g++) {
-      rg_slot[g] = (int32_t)t_len;
-      int32_t k = 0;
-      for (int32_t i : rg_members[g]) {
-        slot_of_leaf[i] = t_len + k;
-        k += lt.kt[i];
+      for (int cl = 0; cl < ncls; cl++) {
+        rg_slot[(size_t)g * ncls + cl] = (int32_t)t_len;
+        int32_t k = 0;
+        for (int32_t i : rg_members[g])
+          for (int32_t kk = 0; kk < lt.kt[i]; kk++) {
+            const int64_t f = colbase[i] + kk;
+            if (col_cls[f] != cl) continue;
+            slot_of_col[f] = t_len + k;
+            k++;
+          }
+        rg_k[(size_t)g * ncls + cl] = k;
+        t_len += round_up(k, slot_align);
       }
-      rg_k[g] = k;
-      t_len += round_up(k, VEC);
       if (t_len > INT32_MAX / 2) {
         msg = "intermediate vector too long";
         return HMVM_ERANGE;
@@ -217,7 +319,7 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     }
     L.t_len = t_len;
 
-    // ---- stage 1: column panels ------------------------------------------
+    // ---- stage 1: column panels (one column class per panel) ---------------
     std::vector<TileBuild> tb;
     std::vector<SegBuild> sb;
     std::vector<Part> parts;
@@ -225,35 +327,40 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     for (int32_t c = 0; c < (int32_t)cg_members.size(); c++) {
       const auto &mem = cg_members[c];
       int32_t ndt = lt.ndt[mem[0]], st = lt.nstrtt[mem[0]];
-      std::vector<std::pair<int32_t, int32_t>> rows;
-      for (int32_t i : mem)
-        for (int32_t k = 0; k < lt.kt[i]; k++) rows.emplace_back(i, k);
-      for (size_t p0 = 0; p0 < rows.size(); p0 += kMaxRows) {
-        int32_t R = (int32_t)std::min<size_t>(kMaxRows, rows.size() - p0);
-        int32_t ob = (int32_t)L.out_idx.size();
-        for (int32_t r = 0; r < R; r++) {
-          auto lk = rows[p0 + r];
-          L.out_idx.push_back((int32_t)(slot_of_leaf[lk.first] + lk.second));
-          panel_rows.push_back(lk);
+      for (int cl = 0; cl < ncls; cl++) {
+        std::vector<std::pair<int32_t, int32_t>> rows;
+        for (int32_t i : mem)
+          for (int32_t k = 0; k < lt.kt[i]; k++)
+            if (col_cls[colbase[i] + k] == cl) rows.emplace_back(i, k);
+        const int type = cls_type[cl];
+        for (size_t p0 = 0; p0 < rows.size(); p0 += kMaxRows) {
+          int32_t R = (int32_t)std::min<size_t>(kMaxRows, rows.size() - p0);
+          int32_t ob = (int32_t)L.out_idx.size();
+          TileBuild t;
+          t.stage = 1;
+          t.nrows = R;
+          t.panel_row0 = ob;
+          t.scale_base = (int32_t)L.rowscale.size();
+          for (int32_t r = 0; r < R; r++) {
+            auto lk = rows[p0 + r];
+            const int64_t f = colbase[lk.first] + lk.second;
+            L.out_idx.push_back((int32_t)slot_of_col[f]);
+            panel_rows.push_back(lk);
+            if (L.mixed) L.rowscale.push_back((double)sc_u[f] * (double)sc_v[f]);
+          }
+          t.mode = 1;
+          t.out_base = ob;
+          t.seg_first = (int32_t)sb.size();
+          t.nseg = 1;
+          sb.push_back(SegBuild{st - 1, ndt, type, -1, 0});
+          t.nvec = (ndt + seg_vec(type) - 1) / seg_vec(type);
+          tb.push_back(t);
         }
-        TileBuild t;
-        t.stage = 1;
-        t.cgroup = c;
-        t.nrows = R;
-        t.panel_row0 = ob;  // index into panel_rows / out_idx
-        t.mode = 1;
-        t.out_base = ob;
-        t.seg_first = (int32_t)sb.size();
-        t.nseg = 1;
-        sb.push_back(SegBuild{st - 1, ndt, -1, 0});
-        t.nvec = (ndt + VEC - 1) / VEC;
-        tb.push_back(t);
       }
     }
     const int32_t n1 = (int32_t)tb.size();
 
     // ---- stage 2: row tiles ---------------------------------------------
-    // Per tile: dense leaves (file order) and row groups touching it.
     std::vector<int32_t> dcount(nrt + 1, 0), gcount(nrt + 1, 0);
     for (int32_t i = 0; i < nlf; i++) {
       if (lt.ltmtx[i] != 2 || lt.ndl[i] <= 0 || lt.ndt[i] <= 0) continue;
@@ -283,6 +390,11 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
         for (int32_t ti = row_tile[r0]; ti < nrt && trow0[ti] < r1; ti++) glist[gpos[ti]++] = g;
       }
     }
+    auto dense_type = [&](int32_t i) {
+      if (!L.mixed) return base_type;
+      // diagonal near-field blocks keep FP64
+      return (lt.nstrtl[i] == lt.nstrtt[i] && lt.ndl[i] == lt.ndt[i]) ? (int)ST_F64 : (int)ST_F32;
+    };
     for (int32_t ti = 0; ti < nrt; ti++) {
       TileBuild t;
       t.stage = 2;
@@ -292,41 +404,48 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
       t.out_base = trow0[ti];
       t.seg_first = (int32_t)sb.size();
       int32_t nvec = 0;
-      // dense segments: merge leaves whose column ranges are adjacent
+      // dense segments: merge leaves whose column ranges are adjacent (same type)
       for (int32_t d = dcount[ti]; d < dcount[ti + 1]; d++) {
         int32_t i = dlist[d];
         int32_t src = lt.nstrtt[i] - 1;
+        const int type = dense_type(i);
         if (t.nseg > 0) {
           SegBuild &last = sb.back();
-          if (last.src >= 0 && last.src + last.ncols == src) {
+          if (last.src >= 0 && last.type == type && last.src + last.ncols == src) {
             last.ncols += lt.ndt[i];
             last.nparts++;
-            parts.push_back(Part{i, -1, lt.ndt[i]});
+            parts.push_back(Part{i, -1, 0, lt.ndt[i]});
             continue;
           }
         }
-        sb.push_back(SegBuild{src, lt.ndt[i], (int32_t)parts.size(), 1});
-        parts.push_back(Part{i, -1, lt.ndt[i]});
+        sb.push_back(SegBuild{src, lt.ndt[i], type, (int32_t)parts.size(), 1});
+        parts.push_back(Part{i, -1, 0, lt.ndt[i]});
         t.nseg++;
       }
       for (int32_t gg = gcount[ti]; gg < gcount[ti + 1]; gg++) {
         int32_t g = glist[gg];
-        sb.push_back(SegBuild{kTFlag | rg_slot[g], rg_k[g], (int32_t)parts.size(), 1});
-        parts.push_back(Part{-1, g, rg_k[g]});
-        t.nseg++;
+        for (int cl = 0; cl < ncls; cl++) {
+          const int32_t k = rg_k[(size_t)g * ncls + cl];
+          if (k == 0) continue;
+          sb.push_back(SegBuild{kTFlag | rg_slot[(size_t)g * ncls + cl], k, cls_type[cl], (int32_t)parts.size(), 1});
+          parts.push_back(Part{-1, g, cl, k});
+          t.nseg++;
+        }
       }
-      for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) nvec += (sb[s].ncols + VEC - 1) / VEC;
+      for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++)
+        nvec += (sb[s].ncols + seg_vec(sb[s].type) - 1) / seg_vec(sb[s].type);
       t.nvec = nvec;
       tb.push_back(t);
     }
     const int32_t ntb = (int32_t)tb.size();
 
     // ---- items: tiles cut into contiguous vector ranges ----------------------
-    // A tile whose bytes exceed the stage's bound is cut into near-equal vector
-    // ranges that write partial sums; the reduction lists add them in order.
+    // A tile whose bytes exceed the stage's bound, or (stream kernels) whose
+    // inputs exceed the kernel's input buffer, is cut into vector ranges that
+    // write partial sums; the reduction lists add them in order.
     const int32_t ctas = L.num_sms * L.ctas_per_sm;
-    L.stage1_teams = ctas * teams_per_cta(L.kernel, L.stage1_cfg);
-    L.stage2_teams = ctas * teams_per_cta(L.kernel, L.stage2_cfg);
+    L.stage1_teams = ctas * (L.mixed ? kMixedCfgs[L.stage1_cfg].wpb : teams_per_cta(L.kernel, L.stage1_cfg));
+    L.stage2_teams = ctas * (L.mixed ? kMixedCfgs[L.stage2_cfg].wpb : teams_per_cta(L.kernel, L.stage2_cfg));
     int64_t stage_bytes[2] = {0, 0};
     for (int32_t k = 0; k < ntb; k++) stage_bytes[k < n1 ? 0 : 1] += (int64_t)tb[k].nvec * tb[k].nrows * 16;
     int64_t max_item[2];
@@ -346,19 +465,65 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
       const TileBuild &t = tb[k];
       tile_item0[k] = (int32_t)items.size();
       const int st = k < n1 ? 0 : 1;
-      int64_t bytes = (int64_t)t.nvec * t.nrows * 16;
-      int32_t nparts = (int32_t)std::min<int64_t>(std::max<int64_t>(1, t.nvec),
-                                                  (bytes + max_item[st] - 1) / max_item[st]);
-      if (st == 0 && opts.split_cols > 0) {
-        int32_t vmax = std::max(1, opts.split_cols / VEC);
-        nparts = std::max(nparts, (t.nvec + vmax - 1) / vmax);
+      const int64_t bytes = (int64_t)t.nvec * t.nrows * 16;
+      std::vector<int32_t> cuts;  // vector indices where items start (after 0)
+      if (!L.mixed) {
+        int32_t nparts = (int32_t)std::min<int64_t>(std::max<int64_t>(1, t.nvec),
+                                                    (bytes + max_item[st] - 1) / max_item[st]);
+        if (st == 0 && opts.split_cols > 0) {
+          int32_t vmax = std::max(1, opts.split_cols / VEC);
+          nparts = std::max(nparts, (t.nvec + vmax - 1) / vmax);
+        }
+        if (L.kernel == 1) {
+          // an item's x/t columns must fit the kernel's input buffer
+          const int32_t cfg = st == 0 ? L.stage1_cfg : L.stage2_cfg;
+          const int32_t vmax = std::max(1, kStreamCfgs[cfg].zcap / VEC);
+          nparts = std::max(nparts, (t.nvec + vmax - 1) / vmax);
+        }
+        for (int32_t q = 1; q < nparts; q++) cuts.push_back((int32_t)((int64_t)t.nvec * q / nparts));
+      } else {
+        // greedy: close an item before it exceeds the byte bound, the input
+        // buffer or kMixedMaxSegs segments
+        const int cfg = st == 0 ? L.stage1_cfg : L.stage2_cfg;
+        const int64_t zcap = kMixedCfgs[cfg].zbytes;
+        const int64_t bcap = std::max<int64_t>(max_item[st], (int64_t)t.nrows * 16);
+        const int32_t vsplit = (st == 0 && opts.split_cols > 0) ? std::max(1, opts.split_cols / 4) : INT32_MAX;
+        int64_t zb = 0, by = 0;
+        int32_t nseg = 0, nv_item = 0, v = 0;
+        for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) {
+          const int32_t nvs = (sb[s].ncols + seg_vec(sb[s].type) - 1) / seg_vec(sb[s].type);
+          const int64_t zv = seg_zbytes(sb[s].type);
+          int32_t done = 0;
+          bool seg_open = false;
+          while (done < nvs) {
+            if (!seg_open && nseg == kMixedMaxSegs) {  // segment cap: start a new item
+              cuts.push_back(v);
+              zb = by = 0;
+              nseg = nv_item = 0;
+            }
+            if (!seg_open) {
+              nseg++;
+              seg_open = true;
+            }
+            int64_t room = std::min<int64_t>((zcap - zb) / zv, (bcap - by) / ((int64_t)t.nrows * 16));
+            room = std::min<int64_t>(room, (int64_t)vsplit - nv_item);
+            if (room <= 0) {  // full: the rest of this segment goes to a new item
+              cuts.push_back(v);
+              zb = by = 0;
+              nseg = 1;
+              nv_item = 0;
+              continue;
+            }
+            const int32_t take = (int32_t)std::min<int64_t>(room, nvs - done);
+            done += take;
+            v += take;
+            nv_item += take;
+            zb += take * zv;
+            by += (int64_t)take * t.nrows * 16;
+          }
+        }
       }
-      if (L.kernel == 1) {
-        // an item's x/t columns must fit the kernel's input buffer
-        const int32_t cfg = st == 0 ? L.stage1_cfg : L.stage2_cfg;
-        const int32_t vmax = std::max(1, kStreamCfgs[cfg].zcap / VEC);
-        nparts = std::max(nparts, (t.nvec + vmax - 1) / vmax);
-      }
+      const int32_t nparts = (int32_t)cuts.size() + 1;
       if (nparts <= 1) {
         items.push_back(Item{k, 0, t.nvec, t.mode, t.out_base, bytes + kItemOverheadBytes});
         continue;
@@ -374,7 +539,7 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
         red.push_back(t.nrows);
       }
       for (int32_t q = 0; q < nparts; q++) {
-        int32_t va = (int32_t)((int64_t)t.nvec * q / nparts), vb = (int32_t)((int64_t)t.nvec * (q + 1) / nparts);
+        int32_t va = q == 0 ? 0 : cuts[q - 1], vb = q + 1 < nparts ? cuts[q] : t.nvec;
         items.push_back(Item{k, va, vb, 2, (int32_t)(pb + (int64_t)q * t.nrows),
                              (int64_t)(vb - va) * t.nrows * 16 + kItemOverheadBytes});
       }
@@ -443,15 +608,17 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
       d.out_base = it.out_base;
       d.nrows = (int16_t)t.nrows;
       d.mode = (int16_t)it.mode;
-      d._pad = 0;
+      d._pad = (L.mixed && t.stage == 1) ? t.scale_base : 0;
       int32_t nseg = 0, sv0 = 0;
       for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) {
-        int32_t nv = (sb[s].ncols + VEC - 1) / VEC;
+        const int vs = seg_vec(sb[s].type);
+        int32_t nv = (sb[s].ncols + vs - 1) / vs;
         int32_t lo = std::max(sv0, it.va), hi = std::min(sv0 + nv, it.vb);
         if (lo < hi) {
-          int32_t skip = (lo - sv0) * VEC;  // columns of the segment before this item
-          int32_t ncols = std::min(sb[s].ncols - skip, (hi - lo) * VEC);
-          L.segs.push_back(hmvm_seg_desc{sb[s].src + skip, ncols});
+          int32_t skip = (lo - sv0) * vs;  // columns of the segment before this item
+          int32_t ncols = std::min(sb[s].ncols - skip, (hi - lo) * vs);
+          int32_t enc = L.mixed ? (ncols | (sb[s].type << kSegTypeShift)) : ncols;
+          L.segs.push_back(hmvm_seg_desc{sb[s].src + skip, enc});
           nseg++;
         }
         sv0 += nv;
@@ -463,9 +630,8 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     L.data.resize((size_t)off);
 
     // ---- pack: each tile into a scratch buffer, then its items' ranges -----
-    const bool srcf = lt.rowmat_is_float;
-    const bool dstf = L.precision == HMVM_FP32;
-#pragma omp parallel
+    int64_t stored_bytes = 0, stored_bytes1 = 0;
+#pragma omp parallel reduction(+ : stored_bytes, stored_bytes1)
     {
       std::vector<Vec16> buf;
 #pragma omp for schedule(dynamic, 4)
@@ -474,26 +640,22 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
         const int32_t R = t.nrows;
         buf.assign((size_t)t.nvec * R, Vec16{{0, 0, 0, 0}});
         char *base = reinterpret_cast<char *>(buf.data());
-        auto put = [&](int64_t c, int32_t r, double v) {
-          int64_t vi = c / VEC, e = c % VEC;
-          int64_t at = (vi * R + r) * VEC + e;
-          if (dstf) reinterpret_cast<float *>(base)[at] = (float)v;
-          else reinterpret_cast<double *>(base)[at] = v;
-        };
-        auto get = [&](int64_t idx) { return srcf ? rd<float>(lt.rowmat, idx) : rd<double>(lt.rowmat, idx); };
-        if (t.stage == 1) {
-          const SegBuild &s = sb[t.seg_first];
-          for (int32_t r = 0; r < R; r++) {
-            auto lk = panel_rows[t.panel_row0 + r];
-            int32_t i = lk.first, kk = lk.second;
-            int64_t src0 = lt.a1(i) + (int64_t)kk * lt.ndt[i];
-            for (int32_t c = 0; c < s.ncols; c++) put(c, r, get(src0 + c));
-          }
-        } else {
-          int64_t col = 0;
-          for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) {
-            const SegBuild &sg = sb[s];
-            int64_t segcol0 = col;
+        int64_t vs0 = 0;  // first vector of the current segment
+        for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) {
+          const SegBuild &sg = sb[s];
+          const int type = sg.type, vs = seg_vec(type), eb = elem_bytes(type);
+          auto put = [&](int64_t c, int32_t r, double v) {
+            store_elem(base, ((vs0 + c / vs) * R + r) * 16 + (c % vs) * eb, type, v);
+          };
+          if (t.stage == 1) {
+            for (int32_t r = 0; r < R; r++) {
+              auto lk = panel_rows[t.panel_row0 + r];
+              int32_t i = lk.first, kk = lk.second;
+              const double inv = L.mixed ? 1.0 / sc_v[colbase[i] + kk] : 1.0;
+              int64_t src0 = lt.a1(i) + (int64_t)kk * lt.ndt[i];
+              for (int32_t c = 0; c < sg.ncols; c++) put(c, r, get(src0 + c) * inv);
+            }
+          } else {
             int64_t pc = 0;  // column within segment
             for (int32_t p = sg.part_first; p < sg.part_first + sg.nparts; p++) {
               const Part &pt = parts[p];
@@ -502,7 +664,7 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
                 int32_t rs = lt.nstrtl[i] - 1;
                 for (int32_t r = 0; r < R; r++) {
                   int64_t src0 = lt.a1(i) + (int64_t)(t.row0 + r - rs) * ndt;
-                  for (int32_t c = 0; c < ndt; c++) put(segcol0 + pc + c, r, get(src0 + c));
+                  for (int32_t c = 0; c < ndt; c++) put(pc + c, r, get(src0 + c));
                 }
                 pc += ndt;
               } else {
@@ -510,17 +672,21 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
                 for (int32_t i : rg_members[pt.group]) {
                   int32_t ndl = lt.ndl[i], rs = lt.nstrtl[i] - 1;
                   for (int32_t kk = 0; kk < lt.kt[i]; kk++) {
+                    const int64_t f = colbase[i] + kk;
+                    if (col_cls[f] != pt.cls) continue;
+                    const double inv = L.mixed ? 1.0 / sc_u[f] : 1.0;
                     int64_t src0 = lt.a2(i) + (int64_t)kk * ndl + (t.row0 - rs);
-                    for (int32_t r = 0; r < R; r++) put(segcol0 + pc + kc, r, get(src0 + r));
+                    for (int32_t r = 0; r < R; r++) put(pc + kc, r, get(src0 + r) * inv);
                     kc++;
                   }
                 }
                 pc += kc;
               }
             }
-            // next segment starts at the next vector boundary
-            col = round_up(segcol0 + sg.ncols, VEC);
           }
+          stored_bytes += (int64_t)sg.ncols * R * eb;
+          if (t.stage == 1) stored_bytes1 += (int64_t)sg.ncols * R * eb;
+          vs0 += (sg.ncols + vs - 1) / vs;  // the next segment starts at the next vector
         }
         for (int32_t q = tile_item0[k]; q < tile_item0[k + 1]; q++) {
           const Item &it = items[q];
@@ -529,6 +695,8 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
         }
       }
     }
+    L.stored_bytes = stored_bytes;
+    L.stored_bytes1 = stored_bytes1;
   } catch (const std::bad_alloc &) {
     msg = "host allocation failed while building the layout";
     return HMVM_ENOMEM;

@@ -93,6 +93,30 @@ constexpr int64_t kMinItemBytes = 32 * 1024;
 constexpr int64_t kItemsPerTeam = 6;
 constexpr int64_t kItemOverheadBytes = 1024;
 
+// Element type of a segment's matrix data (mixed-precision plans encode it in
+// the top bits of hmvm_seg_desc.ncols; plain plans leave those bits zero).
+enum SegType : int32_t { ST_F64 = 0, ST_F32 = 1, ST_F16 = 2, ST_E4M3 = 3, ST_BF16 = 4 };
+constexpr int kSegTypeShift = 28;
+constexpr int32_t kSegColsMask = (1 << kSegTypeShift) - 1;
+inline int seg_vec(int type) {  // matrix elements per 16-byte vector
+  return type == ST_F64 ? 2 : type == ST_F32 ? 4 : type == ST_E4M3 ? 16 : 8;
+}
+inline int seg_zbytes(int type) {  // input bytes per 16-byte vector (x in FP64 for F64, else FP32)
+  return type == ST_F64 ? 16 : seg_vec(type) * 4;
+}
+// Mixed-precision stream kernel: segments per item (one descriptor per lane)
+// and configurations: warps per CTA, ring slots, slot bytes, and the bytes of
+// each of the warp's two input buffers.
+constexpr int kMixedMaxSegs = 32;
+struct MixedCfg {
+  int wpb, slots, chunk, zbytes;
+};
+constexpr int kNumMixedCfgs = 6;
+constexpr MixedCfg kMixedCfgs[kNumMixedCfgs] = {{8, 4, 2048, 2048}, {8, 4, 1024, 4096}, {8, 4, 2048, 4096},
+                                                {4, 4, 2048, 4096}, {6, 4, 2048, 4096}, {16, 4, 1024, 2048}};
+inline int mixed_smem_bytes(const MixedCfg& c) { return c.wpb * (c.slots * c.chunk + 2 * c.zbytes + c.slots * 8); }
+constexpr int kDefaultMixedCfg = 0;
+
 struct HostLayout {
   int precision = HMVM_FP64;
   int vec = 2;
@@ -112,6 +136,12 @@ struct HostLayout {
   int64_t t_len = 0, p_len = 0;
   int64_t stored_elems = 0;  // sum of leaf element counts (the reference's len)
   int32_t split_rows = 0;
+  // mixed precision
+  bool mixed = false;
+  std::vector<double> rowscale;  // per V-stage panel row: s_u * s_v of its (leaf, k) column
+  int64_t cols_fp32 = 0, cols_lr16 = 0, cols_fp8 = 0;
+  int64_t stored_bytes = 0;      // bytes of the stored elements in their storage formats
+  int64_t stored_bytes1 = 0;     // ... of the V stage
 };
 
 // Returns HMVM_OK or a status; msg receives a description on failure.

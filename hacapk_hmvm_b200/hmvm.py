@@ -18,7 +18,9 @@ import numpy as np
 from . import _lib
 from .hmatrix import HMatrix
 
-PRECISIONS = {"fp64": _lib.HMVM_FP64, "fp32": _lib.HMVM_FP32, "double": _lib.HMVM_FP64, "float": _lib.HMVM_FP32}
+PRECISIONS = {"fp64": _lib.HMVM_FP64, "fp32": _lib.HMVM_FP32, "double": _lib.HMVM_FP64, "float": _lib.HMVM_FP32,
+              "mixed": _lib.HMVM_MIXED}
+LR_FORMATS = {"fp16": _lib.HMVM_LR_FP16, "bf16": _lib.HMVM_LR_BF16}
 
 
 def _dev_ptr(t):
@@ -48,8 +50,11 @@ def default_opts(**kw) -> _lib.PlanOpts:
     o = _lib.PlanOpts()
     _lib.hmvm_lib().hmvm_b200_default_opts(C.byref(o))
     for k, v in kw.items():
-        if v is not None:
-            setattr(o, k, int(v))
+        if v is None:
+            continue
+        if k == "mixed_lr_format" and isinstance(v, str):
+            v = LR_FORMATS[v]
+        setattr(o, k, float(v) if isinstance(getattr(o, k), float) else int(v))
     return o
 
 
@@ -76,8 +81,9 @@ class Plan:
         self.setup_seconds = time.perf_counter() - t0
         self._h = h
         self.hm = hm
-        self.precision = "fp64" if prec == _lib.HMVM_FP64 else "fp32"
-        self.dtype = np.float64 if prec == _lib.HMVM_FP64 else np.float32
+        self.precision = {_lib.HMVM_FP64: "fp64", _lib.HMVM_FP32: "fp32", _lib.HMVM_MIXED: "mixed"}[prec]
+        # x and y: FP64 for FP64 and mixed plans, FP32 for FP32 plans
+        self.dtype = np.float32 if prec == _lib.HMVM_FP32 else np.float64
         self.nd = hm.nd
 
     @property

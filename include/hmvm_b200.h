@@ -116,9 +116,16 @@ void hmvm_b200_free_matrix2_f(hmvm_matrix2_f *mat2);
 typedef struct hmvm_plan hmvm_plan;
 
 enum hmvm_precision {
-  HMVM_FP64 = 0, /* FP64 storage, FP64 arithmetic */
-  HMVM_FP32 = 1  /* FP32 storage, FP32 arithmetic (the reference's float mode) */
+  HMVM_FP64 = 0,  /* FP64 storage, FP64 arithmetic */
+  HMVM_FP32 = 1,  /* FP32 storage, FP32 arithmetic (the reference's float mode) */
+  HMVM_MIXED = 2  /* x, y in FP64; low-rank factors FP16 (or BF16) with per-column FP32-range
+                     scales, FP8 E4M3 for columns whose rank-1 term is below
+                     mixed_fp8_eps * |block|, FP32 for columns at or above
+                     mixed_fp32_tau * |block|; dense leaves FP32, diagonal dense blocks FP64;
+                     products summed in FP32 per segment, rows summed in FP64 */
 };
+
+enum hmvm_lr_format { HMVM_LR_FP16 = 0, HMVM_LR_BF16 = 1 };
 
 typedef struct hmvm_plan_opts {
   int32_t precision;      /* enum hmvm_precision */
@@ -129,6 +136,11 @@ typedef struct hmvm_plan_opts {
   int32_t stage2_cfg;     /* kernel configuration index for the row stage (-1 = default) */
   int32_t ctas_per_sm;    /* persistent CTAs per SM (0 = default) */
   int32_t kernel;         /* 0: register-streaming tile kernel; 1 (default, -1): TMA-ring stream kernel */
+  /* HMVM_MIXED only.  |block| is the largest rank-1 term norm |u_k||v_k| of the leaf. */
+  double mixed_fp8_eps;   /* FP8 below this * |block| (default 1e-4, the ACA tolerance; 0 = no FP8) */
+  double mixed_fp32_tau;  /* FP32 at or above this * |block| (default 0.5; > 1 = none) */
+  int32_t mixed_lr_format;/* enum hmvm_lr_format (default FP16) */
+  int32_t _reserved;
 } hmvm_plan_opts;
 
 typedef struct hmvm_plan_info {
@@ -143,6 +155,7 @@ typedef struct hmvm_plan_info {
   int64_t stage1_bytes;      /* algorithmic bytes of the V stage: V elements + x */
   int64_t stage2_bytes;      /* algorithmic bytes of the row stage: U + dense elements + x + y */
   int32_t kernel, ctas_per_sm;
+  int64_t cols_fp32, cols_lr16, cols_fp8; /* HMVM_MIXED: low-rank columns per storage format */
 } hmvm_plan_info;
 
 void hmvm_b200_default_opts(hmvm_plan_opts *opts);
@@ -240,6 +253,9 @@ typedef struct hmvm_layout_view {
   const int32_t *red1;               /* [n_red1][4]: t slot, partial base, parts, 0 */
   const int32_t *red2;               /* [n_red2][4]: y row, partial base, parts, 0 */
   const void *data;                  /* data_vectors * 16 bytes */
+  const double *rowscale;            /* HMVM_MIXED: [n_rowscale] s_u * s_v per V-stage output row, in
+                                        stage-1 item order (tile _pad = first index of the tile) */
+  int64_t n_rowscale;
 } hmvm_layout_view;
 
 /* Tile and segment records as stored in the data structures above. */
@@ -251,7 +267,8 @@ typedef struct hmvm_tile_desc {
 } hmvm_tile_desc;
 typedef struct hmvm_seg_desc {
   int32_t src;   /* x index, or (t index | 0x80000000) */
-  int32_t ncols;
+  int32_t ncols; /* HMVM_MIXED: low 28 bits columns, high bits the storage type
+                    (0 FP64, 1 FP32, 2 FP16, 3 FP8 E4M3, 4 BF16) */
 } hmvm_seg_desc;
 
 int hmvm_b200_layout_build_d(const hmvm_matrix2_d *mat2, const hmvm_plan_opts *opts, int32_t num_sms,

@@ -163,6 +163,8 @@ def emulate_layout(view, x: np.ndarray) -> np.ndarray:
     panels -> t / partial sums, the chunk reduction, stage 2 row tiles)."""
     from hacapk_hmvm_b200 import _lib
 
+    if view.precision == 2:
+        return emulate_mixed(view, x)
     VEC = view.vec
     dt = np.float64 if view.precision == 0 else np.float32
     ntiles = view.n_tiles
@@ -211,6 +213,108 @@ def emulate_layout(view, x: np.ndarray) -> np.ndarray:
         td = tiles[k]
         acc = run_tile(td)
         R, ob = int(td["nrows"]), int(td["out_base"])
+        if td["mode"] == 0:
+            y[ob:ob + R] = acc
+        else:
+            p[ob:ob + R] = acc
+    if view.n_red2:
+        red = np.ctypeslib.as_array(view.red2, (view.n_red2 * 4,)).reshape(-1, 4)
+        for row, pb, nch, stride in red:
+            y[row] = sum(p[pb + c * stride] for c in range(nch))
+    return y
+
+
+def _e4m3_table():
+    """Values of the 256 OCP FP8 E4M3 (fn) codes."""
+    out = np.empty(256)
+    for b in range(256):
+        e, m = (b >> 3) & 15, b & 7
+        s = -1.0 if b & 0x80 else 1.0
+        if e == 15 and m == 7:
+            out[b] = np.nan
+        elif e == 0:
+            out[b] = s * m * 2.0 ** -9
+        else:
+            out[b] = s * (8 + m) * 2.0 ** (e - 10)
+    return out
+
+
+E4M3 = _e4m3_table()
+
+
+def decode_vectors(raw, ty):
+    """raw: uint8 [nv, R, 16] -> float64 [R, nv * elements per vector]."""
+    nv, R = raw.shape[:2]
+    flat = np.ascontiguousarray(raw).reshape(-1)
+    if ty == 0:
+        v = flat.view("<f8")
+    elif ty == 1:
+        v = flat.view("<f4")
+    elif ty == 2:
+        v = flat.view("<f2")
+    elif ty == 4:
+        v = (flat.view("<u2").astype(np.uint32) << 16).view("<f4")
+    else:
+        v = E4M3[flat]
+    vs = 16 * v.size // max(flat.size, 1) if flat.size else 1
+    return v.astype(np.float64).reshape(nv, R, vs).transpose(1, 0, 2).reshape(R, nv * vs)
+
+
+def emulate_mixed(view, x: np.ndarray) -> np.ndarray:
+    """y = H x for a mixed-precision layout: decodes each segment's stored
+    elements, uses x (FP64 segments) or x rounded to FP32 / the FP32 t (other
+    segments), scales the V-stage rows and rounds t to FP32 as the kernels do;
+    the products are summed in FP64 here (the kernels use FP32 per segment)."""
+    from hacapk_hmvm_b200 import _lib
+    from layout_checks import SEG_VEC
+
+    tiles = np.ctypeslib.as_array((_lib.TileDesc * view.n_tiles).from_address(view.tiles)) if view.n_tiles else []
+    segs = np.ctypeslib.as_array((_lib.SegDesc * view.n_segs).from_address(view.segs)) if view.n_segs else []
+    raw = (np.ctypeslib.as_array((C.c_uint8 * (16 * view.data_vectors)).from_address(view.data)).reshape(-1, 16)
+           if view.data_vectors else np.zeros((0, 16), np.uint8))
+    scale = np.ctypeslib.as_array(view.rowscale, (view.n_rowscale,)) if view.n_rowscale else np.zeros(0)
+    n_out = max([int(tiles[k]["out_base"]) + int(tiles[k]["nrows"]) for k in range(view.stage1_tiles)
+                 if tiles[k]["mode"] == 1] or [0])
+    out_idx = np.ctypeslib.as_array(view.out_idx, (n_out,)) if n_out else np.zeros(0, np.int32)
+    x = np.asarray(x, dtype=np.float64)
+    x32 = x.astype(np.float32).astype(np.float64)
+    t = np.zeros(view.t_len + 16, np.float32)
+    p = np.zeros(view.p_len + 16)
+    y = np.full(view.nd, np.nan)
+
+    def run_tile(td):
+        R = int(td["nrows"])
+        v0 = int(td["data_off"])
+        row = np.zeros(R)
+        for s in range(int(td["seg_begin"]), int(td["seg_begin"]) + int(td["nseg"])):
+            src, enc = int(segs[s]["src"]), int(segs[s]["ncols"])
+            ty, nc = enc >> 28, enc & 0x0FFFFFFF
+            nv = -(-nc // SEG_VEC[ty])
+            M = decode_vectors(raw[v0:v0 + nv * R].reshape(nv, R, 16), ty)[:, :nc]
+            v0 += nv * R
+            if src < 0:
+                z = t[(src & 0x7FFFFFFF):(src & 0x7FFFFFFF) + nc].astype(np.float64)
+            else:
+                z = (x if ty == 0 else x32)[src:src + nc]
+            row += M @ z
+        return row
+
+    for k in range(view.stage1_tiles):
+        td = tiles[k]
+        R, ob, sb = int(td["nrows"]), int(td["out_base"]), int(td["_pad"])
+        val = run_tile(td) * scale[sb:sb + R]
+        if td["mode"] == 1:
+            t[out_idx[ob:ob + R]] = val.astype(np.float32)
+        else:
+            p[ob:ob + R] = val
+    if view.n_red1:
+        red = np.ctypeslib.as_array(view.red1, (view.n_red1 * 4,)).reshape(-1, 4)
+        for slot, pb, nch, stride in red:
+            t[slot] = np.float32(sum(p[pb + c * stride] for c in range(nch)))
+    for k in range(view.stage1_tiles, view.n_tiles):
+        td = tiles[k]
+        R, ob = int(td["nrows"]), int(td["out_base"])
+        acc = run_tile(td)
         if td["mode"] == 0:
             y[ob:ob + R] = acc
         else:

@@ -4,9 +4,22 @@ import ctypes as C
 import numpy as np
 
 
-def check_layout_bounds(view):
+SEG_VEC = {0: 2, 1: 4, 2: 8, 3: 16, 4: 8}  # elements per 16-byte vector by storage type
+
+
+def seg_type(view, enc):
+    """(storage type, columns) of a segment descriptor's ncols field."""
+    if view.precision == 2:
+        return enc >> 28, enc & 0x0FFFFFFF
+    return (0 if view.precision == 0 else 1), enc
+
+
+def check_layout_bounds(view, zbytes=None):
+    """zbytes: (mixed plans) the kernels' input buffers per item, in bytes,
+    as (V stage, row stage)."""
     from hacapk_hmvm_b200 import _lib
 
+    mixed = view.precision == 2
     VEC = view.vec
     nt = view.n_tiles
     tiles = np.ctypeslib.as_array((_lib.TileDesc * nt).from_address(view.tiles)) if nt else None
@@ -24,18 +37,30 @@ def check_layout_bounds(view):
         assert 0 <= off and off + nvec * R <= view.data_vectors
         s0, ns = int(td["seg_begin"]), int(td["nseg"])
         assert 0 <= s0 and s0 + ns <= view.n_segs
-        tot = 0
+        tot = zb = 0
+        if mixed:
+            assert ns <= 32
         for s in range(s0, s0 + ns):
-            src, ncols = int(segs[s]["src"]), int(segs[s]["ncols"])
-            assert ncols >= 1
+            src = int(segs[s]["src"])
+            ty, ncols = seg_type(view, int(segs[s]["ncols"]))
+            vs = SEG_VEC[ty]
+            assert ncols >= 1 and ty in SEG_VEC
             if src < 0:
                 slot = src & 0x7FFFFFFF
-                assert slot % VEC == 0
-                assert slot + -(-ncols // VEC) * VEC <= view.t_len
+                if mixed:  # t is FP32; the kernel reads exactly ncols slots
+                    assert ty != 0 and slot + ncols <= view.t_len
+                else:
+                    assert slot % VEC == 0
+                    assert slot + -(-ncols // VEC) * VEC <= view.t_len
             else:
                 assert 0 <= src and src + ncols <= view.nd
-            tot += -(-ncols // VEC)
+            tot += -(-ncols // vs)
+            zb += -(-ncols // vs) * vs * (8 if ty == 0 else 4)
         assert tot == nvec
+        if mixed and zbytes is not None:
+            assert zb <= zbytes[0 if k < view.stage1_tiles else 1]
+        if mixed and k < view.stage1_tiles:
+            assert 0 <= int(td["_pad"]) and int(td["_pad"]) + R <= view.n_rowscale
         ob, mode = int(td["out_base"]), int(td["mode"])
         if k < view.stage1_tiles:
             assert mode in (1, 2)

@@ -30,6 +30,58 @@ def test_layout_bounds_and_emulation(case):
             _lib.hmvm_lib().hmvm_b200_layout_destroy(h)
 
 
+MIXED_ZBYTES = {0: 2048, 1: 4096, 2: 4096, 3: 4096, 4: 4096, 5: 2048}  # kMixedCfgs (layout.hpp)
+MIXED_OPTS = [dict(), dict(mixed_lr_format="bf16"), dict(mixed_fp8_eps=0.0), dict(mixed_fp32_tau=2.0),
+              dict(split_cols=8), dict(max_tile_rows=5), dict(stage1_cfg=5, stage2_cfg=1, ctas_per_sm=1)]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[1]}{c[0]}")
+def test_mixed_layout_bounds_and_emulation(case):
+    """Mixed plans: bounds, the per-item input buffer, and the decoded formats
+    give relerr <= 1e-4 against the FP64 oracle."""
+    n, geo, eta, eps, leaf = case
+    hm = HMatrix.generate(n, geo, eta=eta, eps=eps, leaf_size=leaf, seed=5)
+    x = np.random.default_rng(1).uniform(-1, 1, n)
+    yo = oracle_hmvm(hm, x)
+    for opts in MIXED_OPTS:
+        h, v = layout_for(hm, precision=2, **opts)
+        check_layout_bounds(v, zbytes=(MIXED_ZBYTES[opts.get("stage1_cfg", 0)], MIXED_ZBYTES[opts.get("stage2_cfg", 0)]))
+        err = relerr(emulate_layout(v, x), yo)
+        assert err < 1e-4, (opts, err)
+        _lib.hmvm_lib().hmvm_b200_layout_destroy(h)
+
+
+def test_mixed_column_classes():
+    """Columns at or above tau*|block| are FP32, below eps*|block| FP8, the
+    rest FP16; the stage-1 rows carry scale s_u*s_v."""
+    from helpers import decode_vectors
+
+    hm = HMatrix.generate(1500, "sphere", eps=1e-6, leaf_size=24, seed=3)
+    h, v = layout_for(hm, precision=2)
+    segs = np.ctypeslib.as_array((_lib.SegDesc * v.n_segs).from_address(v.segs))
+    types = segs["ncols"].astype(np.int64) >> 28
+    assert set(np.unique(types)) <= {0, 1, 2, 3}
+    assert (types == 3).any() and (types == 2).any() and (types == 1).any() and (types == 0).any()
+    assert np.all(np.ctypeslib.as_array(v.rowscale, (v.n_rowscale,)) > 0)
+    _lib.hmvm_lib().hmvm_b200_layout_destroy(h)
+    # the FP8 share grows with the threshold, the FP32 share with 1/tau
+    def counts(**o):
+        h, v = layout_for(hm, precision=2, **o)
+        segs = np.ctypeslib.as_array((_lib.SegDesc * v.n_segs).from_address(v.segs))
+        ty, nc = segs["ncols"].astype(np.int64) >> 28, segs["ncols"].astype(np.int64) & 0x0FFFFFFF
+        tiles = np.ctypeslib.as_array((_lib.TileDesc * v.n_tiles).from_address(v.tiles))
+        first = tiles[:v.stage1_tiles]["seg_begin"]
+        rows = tiles[:v.stage1_tiles]["nrows"]
+        out = {t: int(rows[ty[first] == t].sum()) for t in (1, 2, 3)}
+        _lib.hmvm_lib().hmvm_b200_layout_destroy(h)
+        return out
+    a, b = counts(mixed_fp8_eps=1e-5), counts(mixed_fp8_eps=1e-3)
+    assert b[3] > a[3]
+    c, d = counts(mixed_fp32_tau=0.9), counts(mixed_fp32_tau=0.1)
+    assert d[1] > c[1]
+    assert counts(mixed_fp8_eps=0.0)[3] == 0
+
+
 def test_stream_items_fit_input_buffer():
     from hacapk_hmvm_b200._lib import TileDesc
 
