@@ -81,15 +81,20 @@ KernelFn stream_kernel_for(int cfg) {
 }
 
 // Must list kMixedCfgs (layout.hpp) in order.
-inline KernelFn mixed_kernel_for(int cfg) {
+template <int LR16, bool VST>
+KernelFn mixed_kernel_lr(int cfg) {
   switch (cfg) {
-    case 0: return hmvm_mixed_kernel<8, 4, 2048, 2048>;
-    case 1: return hmvm_mixed_kernel<8, 4, 1024, 4096>;
-    case 2: return hmvm_mixed_kernel<8, 4, 2048, 4096>;
-    case 3: return hmvm_mixed_kernel<4, 4, 2048, 4096>;
-    case 4: return hmvm_mixed_kernel<6, 4, 2048, 4096>;
-    default: return hmvm_mixed_kernel<16, 4, 1024, 2048>;
+    case 0: return hmvm_mixed_kernel<8, 4, 2048, 2048, LR16, VST>;
+    case 1: return hmvm_mixed_kernel<8, 4, 1024, 4096, LR16, VST>;
+    case 2: return hmvm_mixed_kernel<8, 4, 2048, 4096, LR16, VST>;
+    case 3: return hmvm_mixed_kernel<4, 4, 2048, 4096, LR16, VST>;
+    case 4: return hmvm_mixed_kernel<6, 4, 2048, 4096, LR16, VST>;
+    default: return hmvm_mixed_kernel<16, 4, 1024, 2048, LR16, VST>;
   }
+}
+inline KernelFn mixed_kernel_for(int cfg, bool bf16, int stage) {
+  if (stage == 1) return bf16 ? mixed_kernel_lr<kBF16, true>(cfg) : mixed_kernel_lr<kF16, true>(cfg);
+  return bf16 ? mixed_kernel_lr<kBF16, false>(cfg) : mixed_kernel_lr<kF16, false>(cfg);
 }
 
 struct Launch {
@@ -97,11 +102,14 @@ struct Launch {
   int threads, smem;
 };
 
-// kernel: 0 tile kernel, 1 stream kernel, 2 mixed-precision kernel
+// kernel: 0 tile kernel, 1 stream kernel, 2 / 3 mixed-precision kernel with FP16 / BF16 factors;
+// stage: 1 (V stage) or 2 (row stage)
 template <typename T>
-Launch stage_launch(int kernel, int cfg) {
+Launch stage_launch(int kernel, int cfg, int stage) {
   if (kernel == 0) return Launch{tile_kernel_for<T>(cfg), 32 * kCfgs[cfg].wg * kCfgs[cfg].tpc, 0};
-  if (kernel == 2) return Launch{mixed_kernel_for(cfg), 32 * kMixedCfgs[cfg].wpb, mixed_smem_bytes(kMixedCfgs[cfg])};
+  if (kernel >= 2)
+    return Launch{mixed_kernel_for(cfg, kernel == 3, stage), 32 * kMixedCfgs[cfg].wpb,
+                  mixed_smem_bytes(kMixedCfgs[cfg])};
   const StreamCfg& c = kStreamCfgs[cfg];
   return Launch{stream_kernel_for<T>(cfg), 32 * c.wpb, stream_smem_bytes(c, (int)sizeof(T))};
 }
@@ -134,6 +142,7 @@ struct hmvm_plan {
   void* d_y = nullptr;
   // mixed precision
   bool mixed = false;
+  int mixed_kcode = 2;  // stage_launch code: 2 FP16 factors, 3 BF16 factors
   float* d_x32 = nullptr;
   double* d_scale = nullptr;
   int64_t cols_fp32 = 0, cols_lr16 = 0, cols_fp8 = 0, stored_bytes = 0;
@@ -198,8 +207,8 @@ int upload(Buf** dst, const void* src, size_t bytes, int64_t* total) {
 // Dynamic shared memory beyond 48 KB must be enabled per kernel.
 template <typename T>
 int prepare_kernels(const hmvm_plan* p) {
-  for (int cfg : {p->stage1_cfg, p->stage2_cfg}) {
-    Launch l = stage_launch<T>(p->mixed ? 2 : p->kernel, cfg);
+  for (int st = 1; st <= 2; st++) {
+    Launch l = stage_launch<T>(p->mixed ? p->mixed_kcode : p->kernel, st == 1 ? p->stage1_cfg : p->stage2_cfg, st);
     if (l.smem > 0)
       HMVM_CUDA_TRY(cudaFuncSetAttribute((const void*)l.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, l.smem),
                     "cudaFuncSetAttribute");
@@ -212,8 +221,8 @@ int prepare_kernels(const hmvm_plan* p) {
 template <typename T>
 int resident_ctas_t(int kernel, int cfg1, int cfg2, int* out) {
   int best = 64;
-  for (int cfg : {cfg1, cfg2}) {
-    const Launch l = stage_launch<T>(kernel, cfg);
+  for (int st = 1; st <= 2; st++) {
+    const Launch l = stage_launch<T>(kernel, st == 1 ? cfg1 : cfg2, st);
     if (l.smem > 0)
       HMVM_CUDA_TRY(cudaFuncSetAttribute((const void*)l.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, l.smem),
                     "cudaFuncSetAttribute");
@@ -230,7 +239,7 @@ int resident_ctas(const hmvm_plan_opts& o, int dev, int* out) {
   DeviceGuard g(dev);
   if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
   const bool mixed = o.precision == HMVM_MIXED;
-  const int kernel = mixed ? 2 : (o.kernel == 0 ? 0 : 1);
+  const int kernel = mixed ? (o.mixed_lr_format == HMVM_LR_BF16 ? 3 : 2) : (o.kernel == 0 ? 0 : 1);
   const int ncfg = mixed ? kNumMixedCfgs : (kernel == 0 ? kNumCfgs : kNumStreamCfgs);
   const int d1 = mixed ? kDefaultMixedCfg : (kernel == 0 ? kDefaultStage1Cfg : kDefaultStreamCfg);
   const int d2 = mixed ? kDefaultMixedCfg : (kernel == 0 ? kDefaultStage2Cfg : kDefaultStreamCfg);
@@ -290,6 +299,7 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   p->t_len = L->t_len;
   p->p_len = L->p_len;
   p->mixed = L->mixed;
+  p->mixed_kcode = opts.mixed_lr_format == HMVM_LR_BF16 ? 3 : 2;
   p->cols_fp32 = L->cols_fp32;
   p->cols_lr16 = L->cols_lr16;
   p->cols_fp8 = L->cols_fp8;
@@ -387,7 +397,7 @@ int launch_stages_mixed(hmvm_plan* p, const void* x, void* y, void* tbuf, void* 
       static_cast<const double*>(x), x32, p->nd);
   HMVM_CUDA_TRY(cudaGetLastError(), "x rounding launch");
   if (p->stage1_tiles > 0) {
-    const Launch l = stage_launch<double>(2, p->stage1_cfg);
+    const Launch l = stage_launch<double>(p->mixed_kcode, p->stage1_cfg, 1);
     a.team_begin = p->d_tb1;
     a.nteams = p->stage1_teams;
     a.scale = p->d_scale;
@@ -402,7 +412,7 @@ int launch_stages_mixed(hmvm_plan* p, const void* x, void* y, void* tbuf, void* 
   }
   if (ev) cudaEventRecord(ev[2], st);
   {
-    const Launch l = stage_launch<double>(2, p->stage2_cfg);
+    const Launch l = stage_launch<double>(p->mixed_kcode, p->stage2_cfg, 2);
     a.team_begin = p->d_tb2;
     a.nteams = p->stage2_teams;
     a.scale = nullptr;
@@ -443,7 +453,7 @@ int launch_stages(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, 
   }
   if (ev) cudaEventRecord(ev[0], st);
   if (p->stage1_tiles > 0) {
-    const Launch l = stage_launch<T>(p->kernel, p->stage1_cfg);
+    const Launch l = stage_launch<T>(p->kernel, p->stage1_cfg, 1);
     a.team_begin = p->d_tb1;
     a.nteams = p->stage1_teams;
     l.fn<<<ctas, l.threads, l.smem, st>>>(a);
@@ -457,7 +467,7 @@ int launch_stages(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, 
   }
   if (ev) cudaEventRecord(ev[2], st);
   {
-    const Launch l = stage_launch<T>(p->kernel, p->stage2_cfg);
+    const Launch l = stage_launch<T>(p->kernel, p->stage2_cfg, 2);
     a.team_begin = p->d_tb2;
     a.nteams = p->stage2_teams;
     l.fn<<<ctas, l.threads, l.smem, st>>>(a);

@@ -525,17 +525,6 @@ __device__ __forceinline__ void gather_inputs_mixed(const hmvm_tile_desc& d, con
   }
 }
 
-__device__ __forceinline__ void fma8(float& a0, float& a1, const float2 m01, const float2 m23, const float2 m45,
-                                     const float2 m67, const float4 z0, const float4 z1) {
-  a0 = fmaf(m01.x, z0.x, a0);
-  a1 = fmaf(m01.y, z0.y, a1);
-  a0 = fmaf(m23.x, z0.z, a0);
-  a1 = fmaf(m23.y, z0.w, a1);
-  a0 = fmaf(m45.x, z1.x, a0);
-  a1 = fmaf(m45.y, z1.y, a1);
-  a0 = fmaf(m67.x, z1.z, a0);
-  a1 = fmaf(m67.y, z1.w, a1);
-}
 __device__ __forceinline__ float2 h2f(uint32_t w) {
   return __half22float2(*reinterpret_cast<const __half2*>(&w));
 }
@@ -547,12 +536,75 @@ __device__ __forceinline__ float2 e4m3x2f(uint16_t w) {
   return __half22float2(*reinterpret_cast<const __half2*>(&h));
 }
 
-// hmvm_mixed_kernel<WPB, S, CHUNK, ZBYTES>: the stream kernel's pipeline (TMA
+template <int V>
+struct TypeTag {
+  static constexpr int value = V;
+};
+// Input bytes per 16-byte matrix vector: FP64 segments read x in FP64, the
+// others x rounded to FP32 or t (FP32), one per stored element.
+template <int TY>
+struct MixedZ {
+  static constexpr int bytes = TY == kF64 ? 16 : TY == kF32 ? 16 : TY == kE4M3 ? 64 : 32;
+};
+// Vectors per batch: 4 (2 for FP8, whose vectors carry 16 products), fewer
+// when the ring cannot hold a batch of 32-row vectors beside the chunk being
+// refilled.
+template <int TY, int S, int CHUNK, bool VST>
+__host__ __device__ constexpr int mixed_batch() {
+  constexpr int want = TY == kE4M3 ? 2 : 4;
+  constexpr int room = (S - 1) * CHUNK / (32 * 16);
+  return want <= room ? want : (room >= 4 ? 4 : (room >= 2 ? 2 : 1));
+}
+
+// acc += the products of one matrix vector m (element type TY) with its
+// inputs at z.  Each of a vector's products goes to its own accumulator of
+// acc[8] (FP32 vectors use half of them: the caller passes acc or acc + 4 by
+// vector parity); FP64 vectors add to e[2].
+__device__ __forceinline__ void fma2(float& a0, float& a1, const float2 m, const float2 z) {
+  a0 = fmaf(m.x, z.x, a0);
+  a1 = fmaf(m.y, z.y, a1);
+}
+template <int TY>
+__device__ __forceinline__ void mixed_fma(const uint4 m, const unsigned char* z, float* acc, double* e) {
+  if constexpr (TY == kF64) {
+    const double2 zz = *reinterpret_cast<const double2*>(z);
+    e[0] = fma(__hiloint2double(m.y, m.x), zz.x, e[0]);
+    e[1] = fma(__hiloint2double(m.w, m.z), zz.y, e[1]);
+  } else if constexpr (TY == kF32) {
+    const float4 zz = *reinterpret_cast<const float4*>(z);
+    acc[0] = fmaf(__uint_as_float(m.x), zz.x, acc[0]);
+    acc[1] = fmaf(__uint_as_float(m.y), zz.y, acc[1]);
+    acc[2] = fmaf(__uint_as_float(m.z), zz.z, acc[2]);
+    acc[3] = fmaf(__uint_as_float(m.w), zz.w, acc[3]);
+  } else if constexpr (TY == kE4M3) {
+    const float4* zz = reinterpret_cast<const float4*>(z);
+    const uint32_t w[4] = {m.x, m.y, m.z, m.w};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const float4 zi = zz[i];
+      fma2(acc[2 * i], acc[2 * i + 1], e4m3x2f((uint16_t)w[i]), make_float2(zi.x, zi.y));
+      fma2(acc[(2 * i + 4) & 7], acc[(2 * i + 5) & 7], e4m3x2f((uint16_t)(w[i] >> 16)), make_float2(zi.z, zi.w));
+    }
+  } else {
+    const float4* zz = reinterpret_cast<const float4*>(z);
+    const uint32_t w[4] = {m.x, m.y, m.z, m.w};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const float4 zi = zz[i >> 1];
+      const float2 zp = (i & 1) ? make_float2(zi.z, zi.w) : make_float2(zi.x, zi.y);
+      fma2(acc[2 * i], acc[2 * i + 1], TY == kBF16 ? bf2f(w[i]) : h2f(w[i]), zp);
+    }
+  }
+}
+
+// hmvm_mixed_kernel<WPB, S, CHUNK, ZBYTES, LR16, VST>: the stream kernel's pipeline (TMA
 // bulk ring for the matrix, cp.async-gathered inputs one item ahead) for
 // mixed-precision plans, whose items hold segments of different element types
-// (FP64, FP32, FP16, BF16, FP8 E4M3).  Each segment's products are summed in
-// FP32 (FP64 for FP64 segments) and added to the row's FP64 total; the V stage
-// multiplies a row's total by its column scale before storing t (FP32).
+// (FP64, FP32, FP8 E4M3 and LR16 = the plan's 16-bit format, kF16 or kBF16).
+// Each run of same-type segments is summed in FP32 (FP64 for FP64 segments)
+// and added to the row's FP64 total.  VST: the V-stage instance, which
+// multiplies a row's total by its column scale before storing t (FP32); the
+// row-stage instance carries neither scales nor t slots.
 template <int WPB, int S, int CHUNK, int ZBYTES>
 constexpr int mixed_min_blocks() {
   constexpr int smem = WPB * (S * CHUNK + 2 * ZBYTES + S * 8);
@@ -562,14 +614,13 @@ constexpr int mixed_min_blocks() {
   return m > 0 ? m : 1;
 }
 
-template <int WPB, int S, int CHUNK, int ZBYTES>
+template <int WPB, int S, int CHUNK, int ZBYTES, int LR16, bool VST>
 __global__ void __launch_bounds__(32 * WPB, (mixed_min_blocks<WPB, S, CHUNK, ZBYTES>()))
     hmvm_mixed_kernel(TileArgs a) {
   constexpr uint32_t RING = (uint32_t)S * CHUNK;
-  constexpr int B = 4;
   static_assert((RING & (RING - 1)) == 0, "ring size must be a power of two");
   static_assert(CHUNK % 16 == 0 && CHUNK >= 512, "bulk copies move multiples of 16 bytes");
-  static_assert(B * 32 * 16 <= (S - 1) * CHUNK, "ring too small for one batch");
+  static_assert(mixed_batch<kF32, S, CHUNK, VST>() * 32 * 16 <= (S - 1) * CHUNK, "ring too small for one batch");
   extern __shared__ __align__(128) unsigned char smem[];
 
   const int lane = threadIdx.x & 31;
@@ -619,10 +670,12 @@ __global__ void __launch_bounds__(32 * WPB, (mixed_min_blocks<WPB, S, CHUNK, ZBY
     for (uint32_t q = 0; q < min((uint32_t)S, nchunks); q++) issue(q);
 
   auto row_scale = [&](const hmvm_tile_desc& d) {
-    return (scl != nullptr && lane < d.nrows) ? scl[d._pad + lane] : 1.0;
+    if constexpr (VST) return lane < d.nrows ? scl[d._pad + lane] : 1.0;
+    else return 1.0;
   };
   auto out_slot = [&](const hmvm_tile_desc& d) {
-    return (d.mode == 1 && lane < d.nrows) ? a.out_idx[d.out_base + lane] : 0;
+    if constexpr (VST) return (d.mode == 1 && lane < d.nrows) ? a.out_idx[d.out_base + lane] : 0;
+    else return 0;
   };
   hmvm_seg_desc cur_seg = lane < cur.nseg ? segs[cur.seg_begin + lane] : szero;
   gather_inputs_mixed(cur, cur_seg, x, x32, tv, zbase, lane);
@@ -656,19 +709,17 @@ __global__ void __launch_bounds__(32 * WPB, (mixed_min_blocks<WPB, S, CHUNK, ZBY
     const uint32_t ol_lane = (uint32_t)lane * 16;
     double row = 0.0;
     int zoff = 0;
-    for (int j = 0; j < cur.nseg && !failed; j++) {
-      const int enc = __shfl_sync(0xffffffffu, cur_seg.ncols, j);
-      const int type = enc >> 28, nc = enc & 0x0fffffff;
-      const int vs = mixed_vec(type);
-      const int nv = (nc + vs - 1) / vs;
-      const unsigned char* zs = zcur + zoff;
-      zoff += nv * vs * (type == kF64 ? 8 : 4);
-      float f0 = 0.f, f1 = 0.f, f2 = 0.f, f3 = 0.f;
-      double d0 = 0.0, d1 = 0.0;
+    // One segment of element type TY: batches of B vectors whose matrix and
+    // input loads are issued together; FP32 (FP64) partial sums per segment.
+    auto run_seg = [&](auto tag, const unsigned char* zs, int nv) -> bool {
+      constexpr int TY = decltype(tag)::value;
+      constexpr int B = mixed_batch<TY, S, CHUNK, VST>();
+      float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      double e[4] = {0.0, 0.0, 0.0, 0.0};
       for (int v = 0; v < nv; v += B) {
         const int nb = min(B, nv - v);
         const uint32_t o_end = o + (uint32_t)nb * rstride;
-        if (o >= (q_rel + 1) * (uint32_t)CHUNK) {
+        if (o >= (q_rel + 1) * (uint32_t)CHUNK) {  // release the slots the warp has moved past
           const uint32_t qf = o / CHUNK;
           __syncwarp();
           if (lane == 0) {
@@ -678,51 +729,67 @@ __global__ void __launch_bounds__(32 * WPB, (mixed_min_blocks<WPB, S, CHUNK, ZBY
           }
           q_rel = qf;
         }
-        if (o_end > q_ready * (uint32_t)CHUNK) {
+        if (o_end > q_ready * (uint32_t)CHUNK) {  // wait for the batch's chunks
           const uint32_t ql = (o_end - 1) / CHUNK;
           while (q_ready <= ql) {
-            if (!warp_wait(&bars[q_ready % S], (q_ready / S) & 1)) {
-              failed = true;
-              break;
-            }
+            if (!warp_wait(&bars[q_ready % S], (q_ready / S) & 1)) return false;
             q_ready++;
           }
-          if (failed) break;
         }
-        for (int u = 0; u < nb; u++) {
-          const uint4 m = *reinterpret_cast<const uint4*>(ring + ((o + ol_lane + (uint32_t)u * rstride) & (RING - 1)));
-          const int vv = v + u;
-          if (type == kF64) {
-            const double2 z = *reinterpret_cast<const double2*>(zs + vv * 16);
-            d0 = fma(__hiloint2double(m.y, m.x), z.x, d0);
-            d1 = fma(__hiloint2double(m.w, m.z), z.y, d1);
-          } else if (type == kF32) {
-            const float4 z = *reinterpret_cast<const float4*>(zs + vv * 16);
-            f0 = fmaf(__uint_as_float(m.x), z.x, f0);
-            f1 = fmaf(__uint_as_float(m.y), z.y, f1);
-            f2 = fmaf(__uint_as_float(m.z), z.z, f2);
-            f3 = fmaf(__uint_as_float(m.w), z.w, f3);
-          } else if (type == kE4M3) {
-            const float4* z = reinterpret_cast<const float4*>(zs + vv * 64);
-            fma8(f0, f1, e4m3x2f((uint16_t)m.x), e4m3x2f((uint16_t)(m.x >> 16)), e4m3x2f((uint16_t)m.y),
-                 e4m3x2f((uint16_t)(m.y >> 16)), z[0], z[1]);
-            fma8(f2, f3, e4m3x2f((uint16_t)m.z), e4m3x2f((uint16_t)(m.z >> 16)), e4m3x2f((uint16_t)m.w),
-                 e4m3x2f((uint16_t)(m.w >> 16)), z[2], z[3]);
-          } else if (type == kBF16) {
-            const float4* z = reinterpret_cast<const float4*>(zs + vv * 32);
-            fma8(f0, f1, bf2f(m.x), bf2f(m.y), bf2f(m.z), bf2f(m.w), z[0], z[1]);
-          } else {
-            const float4* z = reinterpret_cast<const float4*>(zs + vv * 32);
-            fma8(f0, f1, h2f(m.x), h2f(m.y), h2f(m.z), h2f(m.w), z[0], z[1]);
-          }
+        const uint32_t ol = o + ol_lane;
+        const unsigned char* zv = zs + (size_t)v * MixedZ<TY>::bytes;
+        // the last batch of a stretch is predicated (vectors past nb are
+        // neither loaded nor used)
+        uint4 m[B];
+#pragma unroll
+        for (int u = 0; u < B; u++)
+          if (u < nb) m[u] = *reinterpret_cast<const uint4*>(ring + ((ol + (uint32_t)u * rstride) & (RING - 1)));
+#pragma unroll
+        for (int u = 0; u < B; u++) {
+          if (u < nb)
+            mixed_fma<TY>(m[u], zv + u * MixedZ<TY>::bytes, acc + (TY == kF32 ? (u & 1) * 4 : 0), e + (u & 1) * 2);
         }
         o = o_end;
       }
-      row += (d0 + d1) + (double)((f0 + f1) + (f2 + f3));
+      row += ((e[0] + e[1]) + (e[2] + e[3])) +
+             (double)(((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7])));
+      return true;
+    };
+    // Segments come sorted by type: each run of one type is one stretch of
+    // vectors (matrix and inputs both contiguous).  V-stage items are one
+    // segment.
+    int j = 0;
+    while (j < (VST ? 1 : cur.nseg)) {
+      const int type = __shfl_sync(0xffffffffu, cur_seg.ncols, j) >> 28;
+      const int vs = mixed_vec(type);
+      const unsigned char* zs = zcur + zoff;
+      int nv = 0;
+      if constexpr (VST) {
+        nv = cur.nvec;
+        j = 1;
+      } else {
+        for (; j < cur.nseg; j++) {
+          const int enc = __shfl_sync(0xffffffffu, cur_seg.ncols, j);
+          if ((enc >> 28) != type) break;
+          nv += ((enc & 0x0fffffff) + vs - 1) / vs;
+        }
+      }
+      zoff += nv * vs * (type == kF64 ? 8 : 4);
+      bool ok;
+      switch (type) {
+        case kF64: ok = run_seg(TypeTag<kF64>{}, zs, nv); break;
+        case kF32: ok = run_seg(TypeTag<kF32>{}, zs, nv); break;
+        case kE4M3: ok = run_seg(TypeTag<kE4M3>{}, zs, nv); break;
+        default: ok = run_seg(TypeTag<LR16>{}, zs, nv); break;
+      }
+      if (!ok) {
+        failed = true;
+        break;
+      }
     }
     if (failed) break;
     if (lane < R) {
-      if (scl != nullptr) {  // V stage
+      if constexpr (VST) {
         const double val = row * cur_scale;
         if (cur.mode == 1) const_cast<float*>(tv)[cur_oidx] = (float)val;
         else static_cast<double*>(a.p)[cur.out_base + lane] = val;

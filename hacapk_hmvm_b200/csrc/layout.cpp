@@ -432,6 +432,13 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
           t.nseg++;
         }
       }
+      if (L.mixed) {
+        // segments of one storage type next to each other: the kernel runs
+        // each type's vectors as one stretch
+        auto rank = [](int ty) { return ty == ST_F64 ? 0 : ty == ST_F32 ? 1 : ty == ST_E4M3 ? 3 : 2; };
+        std::stable_sort(sb.begin() + t.seg_first, sb.begin() + t.seg_first + t.nseg,
+                         [&](const SegBuild &a, const SegBuild &b) { return rank(a.type) < rank(b.type); });
+      }
       for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++)
         nvec += (sb[s].ncols + seg_vec(sb[s].type) - 1) / seg_vec(sb[s].type);
       t.nvec = nvec;

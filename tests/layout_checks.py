@@ -40,6 +40,7 @@ def check_layout_bounds(view, zbytes=None):
         tot = zb = 0
         if mixed:
             assert ns <= 32
+            assert k >= view.stage1_tiles or ns == 1  # the V-stage kernel runs one segment per item
         for s in range(s0, s0 + ns):
             src = int(segs[s]["src"])
             ty, ncols = seg_type(view, int(segs[s]["ncols"]))
