@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--stage2-cfg", type=int, default=-1)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--kernel", type=int, default=-1, help="0: register-streaming, 1: TMA-ring (default)")
+    ap.add_argument("--nrhs", type=int, default=1, help="right-hand sides per step (multi-RHS HMVM when > 1)")
+    ap.add_argument("--lr-format", default="fp16", choices=["fp16", "bf16"], help="mixed plans: 16-bit factor format")
     return ap.parse_args()
 
 
@@ -226,8 +228,10 @@ def build_matrix(a):
 
 def workload_config(a, hm):
     return {
-        "workload": f"{a.geometry} N={a.n} leaf={a.leaf} eta={a.eta} ACA eps={a.eps:g}, single-vector HMVM, "
-                    f"{a.precision.upper()}",
+        "workload": f"{a.geometry} N={a.n} leaf={a.leaf} eta={a.eta} ACA eps={a.eps:g}, "
+                    + ("single-vector HMVM, " if a.nrhs == 1 else f"multi-RHS HMVM nrhs={a.nrhs}, ")
+                    + f"{a.precision.upper()}" + (f" ({a.lr_format} factors)" if a.precision == "mixed" else ""),
+        "nrhs": a.nrhs,
         "n": a.n, "geometry": a.geometry, "leaf_size": a.leaf, "eta": a.eta, "aca_eps": a.eps,
         "nlf": hm.nlf, "n_lowrank": int((hm.ltmtx == 1).sum()), "n_dense": int((hm.ltmtx == 2).sum()),
         "stored_elements": hm.stored_elements(), "precision": a.precision,
@@ -284,22 +288,30 @@ def run_b200(a, rank, world, local_rank):
         dist = dist_mod
     hm = build_matrix(a)
     rng = np.random.default_rng(a.seed)
-    x = rng.uniform(-1.0, 1.0, hm.nd)
+    X = rng.uniform(-1.0, 1.0, (a.nrhs, hm.nd))
+    x = X[0]
     t0 = time.perf_counter()
     plan = Plan(hm, a.precision, device=local_rank, stage1_cfg=a.stage1_cfg, stage2_cfg=a.stage2_cfg,
-                ctas_per_sm=a.ctas_per_sm, kernel=a.kernel)
+                ctas_per_sm=a.ctas_per_sm, kernel=a.kernel, nrhs_max=min(a.nrhs, 8),
+                mixed_lr_format=a.lr_format if a.precision == "mixed" else None)
     setup_s = time.perf_counter() - t0
     info = plan.info()
     # x and y: FP64 for FP64 and mixed plans, FP32 for FP32 plans
     tdt = torch.float32 if a.precision == "fp32" else torch.float64
     ndt = np.float32 if a.precision == "fp32" else np.float64
     elem = 4 if a.precision == "fp32" else 8
-    xd = torch.from_numpy(x.astype(ndt)).to(dev)
-    yd = torch.empty(hm.nd, dtype=tdt, device=dev)
+    xd = torch.from_numpy(X.astype(ndt)).to(dev)
+    yd = torch.empty((a.nrhs, hm.nd), dtype=tdt, device=dev)
     stream = torch.cuda.current_stream(dev)
+    if a.nrhs == 1:
+        def step():
+            plan.apply(xd[0], yd[0], stream)
+    else:
+        def step():
+            plan.apply_multi(xd, yd, stream)
 
     for _ in range(a.warmup):
-        plan.apply(xd, yd, stream)
+        step()
     torch.cuda.synchronize(dev)
 
     # ---- timed region: K device-resident HMVMs ----
@@ -315,7 +327,7 @@ def run_b200(a, rank, world, local_rank):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(a.steps):
-        plan.apply(xd, yd, stream)
+        step()
     e1.record(stream)
     torch.cuda.synchronize(dev)
     if dist:
@@ -326,14 +338,21 @@ def run_b200(a, rank, world, local_rank):
     clk = clocks.stop()
     ms_total = max_over_ranks(ms_total, dist, dev)
     ms_step = ms_total / a.steps
-    y_gpu = yd.cpu().numpy().astype(np.float64)
+    Y_gpu = yd.cpu().numpy().astype(np.float64)
+    y_gpu = Y_gpu[0]
 
     # ---- e2e: the C-ABI host-buffer call, pinned buffers, copies inside ----
-    xh = torch.from_numpy(x.astype(ndt)).pin_memory()
-    yh = torch.empty(hm.nd, dtype=tdt).pin_memory()
+    xh = torch.from_numpy(X.astype(ndt)).pin_memory()
+    yh = torch.empty((a.nrhs, hm.nd), dtype=tdt).pin_memory()
     xh_np, yh_np = xh.numpy(), yh.numpy()
+    if a.nrhs == 1:
+        def host_step():
+            plan.apply_host(xh_np[0], yh_np[0], stream)
+    else:
+        def host_step():
+            plan.apply_multi_host(xh_np, yh_np, stream)
     for _ in range(3):
-        plan.apply_host(xh_np, yh_np, stream)
+        host_step()
     if dist:
         dist.barrier()
     torch.cuda.synchronize(dev)
@@ -341,13 +360,14 @@ def run_b200(a, rank, world, local_rank):
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for _ in range(a.e2e_steps):
-        plan.apply_host(xh_np, yh_np, stream)
+        host_step()
     f1.record(stream)
     torch.cuda.synchronize(dev)
     e2e_ms = f0.elapsed_time(f1)
     e2e_ms = max_over_ranks(e2e_ms, dist, dev)
     e2e_step = e2e_ms / a.e2e_steps
 
+    unit = "HMVM/s" if a.nrhs == 1 else "vectors/s"
     # ---- CPU baseline (rank 0, N=1 only) and parity of this run ----
     cpu_line = None
     rel = None
@@ -355,9 +375,13 @@ def run_b200(a, rank, world, local_rank):
         cpu = CpuReference(hm)
         y_cpu, st = cpu.time_sample(x, a.cpu_seconds)
         rel = float(np.linalg.norm(y_gpu - y_cpu) / np.linalg.norm(y_cpu))
-        cpu_line = {"value": 1.0 / st["min"], "unit": "HMVM/s", "cores": cpu.threads, "kind": cpu.kind,
-                    "sample": f"hmvm_omp_2<double,0> on the full matrix, {st['runs']} runs, first 5 discarded, "
-                              f"min of {st['kept']} (avg {st['avg'] * 1e3:.2f} ms)",
+        for r in range(1, min(a.nrhs, 4)):  # a few more columns of a multi-RHS step
+            yc = np.empty(hm.nd)
+            cpu.run(X[r], yc)
+            rel = max(rel, float(np.linalg.norm(Y_gpu[r] - yc) / np.linalg.norm(yc)))
+        cpu_line = {"value": 1.0 / st["min"], "unit": unit, "cores": cpu.threads, "kind": cpu.kind,
+                    "sample": f"hmvm_omp_2<double,0> on the full matrix (one vector per call), {st['runs']} runs, "
+                              f"first 5 discarded, min of {st['kept']} (avg {st['avg'] * 1e3:.2f} ms)",
                     "relerr_gpu_vs_cpu": rel}
     if dist:
         dist.barrier()
@@ -368,8 +392,14 @@ def run_b200(a, rank, world, local_rank):
     dom = int(np.argmax(stage_ms))
     dom_avg_s = stage_ms[dom] / max(napplies, 1) * 1e-3
     achieved = stage_bytes[dom] / dom_avg_s / 1e9 if dom_avg_s > 0 else 0.0
-    alg_bytes = info["algorithmic_bytes"]
+    # a multi-RHS step streams the matrix once per pass and reads/writes every column once
+    elem_xy = 4 if a.precision == "fp32" else 8
+    passes = max(1, plan.multi_kernel_count(a.nrhs) // max(plan.multi_kernel_count(min(a.nrhs, 8)), 1)) \
+        if a.nrhs > 1 else 1
+    alg_bytes = info["algorithmic_bytes"] * passes + 2 * hm.nd * elem_xy * (a.nrhs - passes)
     kname = {0: "hmvm_tile_kernel", 1: "hmvm_stream_kernel", 2: "hmvm_mixed_kernel"}[info["kernel"]]
+    if a.nrhs > 1:
+        kname = "hmvm_multi_kernel"
     roof = {
         "bound": "hbm",
         "kernel": [f"{kname} (V stage)", "hmvm_reduce_kernel (V stage)", f"{kname} (row stage)",
@@ -387,13 +417,13 @@ def run_b200(a, rank, world, local_rank):
     }
 
     if rank == 0:
-        value = world * 1e3 / ms_step
+        value = world * 1e3 / ms_step * a.nrhs
         cfg = workload_config(a, hm)
         cfg.update({"kernel": kname, "stage1_cfg": info["stage1_cfg"], "stage2_cfg": info["stage2_cfg"],
                     "ctas_per_sm": info["ctas_per_sm"],
                     "device_bytes": info["device_bytes"], "plan_setup_s": setup_s})
         line = {
-            "metric": "HMVM/s", "value": value, "unit": "HMVM/s", "n_gpus": world, "steps": a.steps,
+            "metric": unit, "value": value, "unit": unit, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": DTYPES[a.precision],
             "data": "synthetic (seeded HACApK-rule H-matrix; x uniform[-1,1])",
@@ -403,10 +433,11 @@ def run_b200(a, rank, world, local_rank):
             "relerr_vs_fp64_cpu_reference": rel, "aca_eps": a.eps,
             "roofline": roof,
             "cpu_baseline": cpu_line,
-            "e2e": {"value": world * 1e3 / e2e_step, "unit": "HMVM/s", "h2d_bytes_per_step": hm.nd * elem,
-                    "d2h_bytes_per_step": hm.nd * elem, "ms_per_step": e2e_step},
+            "e2e": {"value": world * 1e3 / e2e_step * a.nrhs, "unit": unit,
+                    "h2d_bytes_per_step": hm.nd * elem * a.nrhs, "d2h_bytes_per_step": hm.nd * elem * a.nrhs,
+                    "ms_per_step": e2e_step},
             "clocks": clk,
-            "gpu_launches": a.steps * plan.kernel_count(),
+            "gpu_launches": a.steps * (plan.kernel_count() if a.nrhs == 1 else plan.multi_kernel_count(a.nrhs)),
         }
         print(json.dumps(line), flush=True)
     plan.close()

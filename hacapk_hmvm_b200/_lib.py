@@ -88,7 +88,7 @@ class PlanOpts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("device", C.c_int32), ("max_tile_rows", C.c_int32),
                 ("split_cols", C.c_int32), ("stage1_cfg", C.c_int32), ("stage2_cfg", C.c_int32),
                 ("ctas_per_sm", C.c_int32), ("kernel", C.c_int32), ("mixed_fp8_eps", C.c_double),
-                ("mixed_fp32_tau", C.c_double), ("mixed_lr_format", C.c_int32), ("_reserved", C.c_int32)]
+                ("mixed_fp32_tau", C.c_double), ("mixed_lr_format", C.c_int32), ("nrhs_max", C.c_int32)]
 
 
 class PlanInfo(C.Structure):
@@ -177,6 +177,11 @@ HMVM_SIGNATURES = {
     "hmvm_b200_last_error": (C.c_char_p, []),
     "hmvm_b200_version": (C.c_int, []),
     "hmvm_b200_plan_kernel_count": (C.c_int, [C.c_void_p]),
+    "hmvm_b200_apply_multi": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32,
+                                        C.c_void_p]),
+    "hmvm_b200_apply_multi_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32,
+                                             C.c_void_p]),
+    "hmvm_b200_plan_multi_kernel_count": (C.c_int, [C.c_void_p, C.c_int32]),
     "hmvm_b200_plan_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "hmvm_b200_plan_profile_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "hmvm_b200_plan_status": (C.c_int, [C.c_void_p]),

@@ -14,7 +14,7 @@
 #include <vector>
 
 #include "hmvm_b200.h"
-#include "kernels.cuh"
+#include "kernels_multi.cuh"
 #include "layout.hpp"
 
 namespace hmvm {
@@ -52,6 +52,7 @@ struct DeviceGuard {
 };
 
 using KernelFn = void (*)(TileArgs);
+using MultiFn = void (*)(MultiArgs);
 
 template <typename T>
 KernelFn tile_kernel_for(int cfg) {
@@ -148,6 +149,15 @@ struct hmvm_plan {
   int64_t cols_fp32 = 0, cols_lr16 = 0, cols_fp8 = 0, stored_bytes = 0;
   int t_elem = 8, p_elem = 8;  // bytes per t slot and per partial sum
   int64_t stage1_bytes = 0, stage2_bytes = 0;
+  // multi-RHS (nrhs_max > 1): packed inputs, t and partial sums for up to nrhs_max rhs
+  int nrhs_max = 1;
+  double* d_xm64 = nullptr;
+  float* d_xm32 = nullptr;
+  void* d_tm = nullptr;
+  void* d_pm = nullptr;
+  void* d_xh = nullptr;  // staging for apply_multi_host
+  void* d_yh = nullptr;
+  size_t xh_bytes = 0;
   // profiling: kEventsPerApply events per recorded apply
   bool profiling = false;
   std::vector<cudaEvent_t> prof_events;
@@ -166,8 +176,9 @@ constexpr int kEventsPerApply = 5;
 void free_plan_buffers(hmvm_plan* p) {
   for (cudaEvent_t e : p->prof_events) cudaEventDestroy(e);
   p->prof_events.clear();
-  void* bufs[] = {p->d_data, p->d_tiles, p->d_segs, p->d_tb1, p->d_tb2, p->d_out_idx, p->d_red1, p->d_red2,
-                  p->d_t,    p->d_p,     p->d_err,  p->d_x,   p->d_y,   p->d_x32,     p->d_scale};
+  void* bufs[] = {p->d_data, p->d_tiles, p->d_segs, p->d_tb1, p->d_tb2,  p->d_out_idx, p->d_red1,
+                  p->d_red2, p->d_t,     p->d_p,    p->d_err, p->d_x,    p->d_y,       p->d_x32,
+                  p->d_scale, p->d_xm64, p->d_xm32, p->d_tm,  p->d_pm,   p->d_xh,      p->d_yh};
   for (void* b : bufs)
     if (b) cudaFree(b);
 }
@@ -204,9 +215,21 @@ int upload(Buf** dst, const void* src, size_t bytes, int64_t* total) {
   return HMVM_OK;
 }
 
+int plan_mode(const hmvm_plan* p);
+template <bool VST>
+MultiFn multi_kernel_for(int mode, int nr, int cfg);
+
 // Dynamic shared memory beyond 48 KB must be enabled per kernel.
 template <typename T>
 int prepare_kernels(const hmvm_plan* p) {
+  if (p->nrhs_max > 1) {
+    const int smem = multi_smem_bytes(kMultiCfgs[kDefaultMultiCfg]);
+    for (int nr : {2, 4, 8})
+      for (MultiFn f : {multi_kernel_for<true>(plan_mode(p), nr, kDefaultMultiCfg),
+                        multi_kernel_for<false>(plan_mode(p), nr, kDefaultMultiCfg)})
+        HMVM_CUDA_TRY(cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                      "cudaFuncSetAttribute");
+  }
   for (int st = 1; st <= 2; st++) {
     Launch l = stage_launch<T>(p->mixed ? p->mixed_kcode : p->kernel, st == 1 ? p->stage1_cfg : p->stage2_cfg, st);
     if (l.smem > 0)
@@ -299,6 +322,7 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   p->t_len = L->t_len;
   p->p_len = L->p_len;
   p->mixed = L->mixed;
+  p->nrhs_max = L->nrhs_max;
   p->mixed_kcode = opts.mixed_lr_format == HMVM_LR_BF16 ? 3 : 2;
   p->cols_fp32 = L->cols_fp32;
   p->cols_lr16 = L->cols_lr16;
@@ -350,6 +374,16 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
       cudaError_t e = cudaMalloc(&p->d_x32, (size_t)(L->nd + 16) * sizeof(float));
       if (e != cudaSuccess) rc = cuda_fail(e, "x32 buffer");
       if (!rc) rc = upload(&p->d_scale, L->rowscale.data(), L->rowscale.size() * sizeof(double), nullptr);
+    }
+    if (!rc && p->nrhs_max > 1) {
+      const size_t nr = (size_t)p->nrhs_max;
+      cudaError_t e = cudaSuccess;
+      if (p->precision != HMVM_FP32) e = cudaMalloc(&p->d_xm64, (size_t)(L->nd + 16) * nr * sizeof(double));
+      if (e == cudaSuccess && p->precision != HMVM_FP64)
+        e = cudaMalloc(&p->d_xm32, (size_t)(L->nd + 16) * nr * sizeof(float));
+      if (e == cudaSuccess) e = cudaMalloc(&p->d_tm, (size_t)(L->t_len + 16) * nr * p->t_elem);
+      if (e == cudaSuccess) e = cudaMalloc(&p->d_pm, (size_t)(L->p_len + 16) * nr * p->p_elem);
+      if (e != cudaSuccess) rc = cuda_fail(e, "multi-RHS buffers");
     }
     if (!rc) {
       cudaError_t e = cudaMalloc(&p->d_err, sizeof(int));
@@ -483,6 +517,175 @@ int launch_stages(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, 
   return HMVM_OK;
 }
 
+int apply_impl(hmvm_plan* p, const void* x, void* y, cudaStream_t st);
+inline int apply_impl_fwd(hmvm_plan* p, const void* x, void* y, cudaStream_t st) { return apply_impl(p, x, y, st); }
+
+// ---- multi-RHS ---------------------------------------------------------------
+// Must list kMultiCfgs (layout.hpp) in order.
+template <int NR, int MODE, bool VST>
+MultiFn multi_kernel_cfg(int cfg) {
+  switch (cfg) {
+    default: return hmvm_multi_kernel<4, 4, 2048, NR, MODE, VST>;
+  }
+}
+template <int MODE, bool VST>
+MultiFn multi_kernel_nr(int nr, int cfg) {
+  switch (nr) {
+    case 2: return multi_kernel_cfg<2, MODE, VST>(cfg);
+    case 4: return multi_kernel_cfg<4, MODE, VST>(cfg);
+    default: return multi_kernel_cfg<8, MODE, VST>(cfg);
+  }
+}
+template <bool VST>
+MultiFn multi_kernel_for(int mode, int nr, int cfg) {
+  switch (mode) {
+    case kModePlain64: return multi_kernel_nr<kModePlain64, VST>(nr, cfg);
+    case kModePlain32: return multi_kernel_nr<kModePlain32, VST>(nr, cfg);
+    case kModeMixed16: return multi_kernel_nr<kModeMixed16, VST>(nr, cfg);
+    default: return multi_kernel_nr<kModeMixedBF16, VST>(nr, cfg);
+  }
+}
+int plan_mode(const hmvm_plan* p) {
+  if (p->mixed) return p->mixed_kcode == 3 ? kModeMixedBF16 : kModeMixed16;
+  return p->precision == HMVM_FP64 ? kModePlain64 : kModePlain32;
+}
+
+template <typename TP, typename TD, bool VST>
+void launch_reduce_multi(int nr_inst, const int4* red, int n, const void* pbuf, void* dst, int64_t ldy, int nr,
+                         cudaStream_t st) {
+  const int64_t work = (int64_t)n * nr_inst;
+  const int blocks = (int)std::min<int64_t>((work + 255) / 256, 65535);
+  const TP* pp = static_cast<const TP*>(pbuf);
+  TD* dd = static_cast<TD*>(dst);
+  switch (nr_inst) {
+    case 2: hmvm_reduce_multi_kernel<TP, TD, 2, VST><<<blocks, 256, 0, st>>>(red, n, pp, dd, ldy, nr); break;
+    case 4: hmvm_reduce_multi_kernel<TP, TD, 4, VST><<<blocks, 256, 0, st>>>(red, n, pp, dd, ldy, nr); break;
+    default: hmvm_reduce_multi_kernel<TP, TD, 8, VST><<<blocks, 256, 0, st>>>(red, n, pp, dd, ldy, nr); break;
+  }
+}
+
+template <int NR>
+void launch_pack(const hmvm_plan* p, const void* X, int64_t ldx, int nr, cudaStream_t st) {
+  const int64_t work = (int64_t)(p->nd + 16) * NR;
+  const int blocks = (int)std::min<int64_t>((work + 255) / 256, (int64_t)p->num_sms * 8);
+  double* x64 = p->precision != HMVM_FP32 ? p->d_xm64 : nullptr;
+  float* x32 = p->precision != HMVM_FP64 ? p->d_xm32 : nullptr;
+  if (p->precision == HMVM_FP32)
+    hmvm_pack_x_kernel<float, NR><<<blocks, 256, 0, st>>>(static_cast<const float*>(X), ldx, p->nd, 16, nr, x64, x32);
+  else
+    hmvm_pack_x_kernel<double, NR><<<blocks, 256, 0, st>>>(static_cast<const double*>(X), ldx, p->nd, 16, nr, x64,
+                                                           x32);
+}
+
+// One pass: nr (<= nr_inst) right-hand sides X[:, 0:nr] -> Y[:, 0:nr].
+int launch_multi_pass(hmvm_plan* p, const void* X, int64_t ldx, void* Y, int64_t ldy, int nr, int nr_inst,
+                      cudaStream_t st) {
+  switch (nr_inst) {
+    case 2: launch_pack<2>(p, X, ldx, nr, st); break;
+    case 4: launch_pack<4>(p, X, ldx, nr, st); break;
+    default: launch_pack<8>(p, X, ldx, nr, st); break;
+  }
+  HMVM_CUDA_TRY(cudaGetLastError(), "input packing launch");
+  MultiArgs a;
+  a.err = p->d_err;
+  a.tiles = p->d_tiles;
+  a.segs = p->d_segs;
+  a.data = p->d_data;
+  a.x64 = p->d_xm64;
+  a.x32 = p->d_xm32;
+  a.t = p->d_tm;
+  a.y = Y;
+  a.ldy = ldy;
+  a.nr = nr;
+  a.p = p->d_pm;
+  a.out_idx = p->d_out_idx;
+  a.scale = p->d_scale;
+  const int mode = plan_mode(p);
+  const MultiCfg& c = kMultiCfgs[kDefaultMultiCfg];
+  const int threads = 32 * c.wpb, smem = multi_smem_bytes(c);
+  cudaEvent_t* ev = nullptr;
+  if (p->profiling && p->prof_count < kMaxProfiled) {
+    ev = &p->prof_events[kEventsPerApply * (size_t)p->prof_count];
+    p->prof_count++;
+  }
+  if (ev) cudaEventRecord(ev[0], st);
+  if (p->stage1_tiles > 0) {
+    a.team_begin = p->d_tb1;
+    a.nteams = p->stage1_teams;
+    const int ctas = (p->stage1_teams + c.wpb - 1) / c.wpb;
+    multi_kernel_for<true>(mode, nr_inst, kDefaultMultiCfg)<<<ctas, threads, smem, st>>>(a);
+    HMVM_CUDA_TRY(cudaGetLastError(), "multi-RHS V-stage launch");
+  }
+  if (ev) cudaEventRecord(ev[1], st);
+  const bool f32 = p->precision == HMVM_FP32;
+  if (p->n_red1 > 0) {
+    if (mode == kModePlain64) launch_reduce_multi<double, double, true>(nr_inst, p->d_red1, p->n_red1, p->d_pm, p->d_tm, 0, nr, st);
+    else if (f32) launch_reduce_multi<float, float, true>(nr_inst, p->d_red1, p->n_red1, p->d_pm, p->d_tm, 0, nr, st);
+    else launch_reduce_multi<double, float, true>(nr_inst, p->d_red1, p->n_red1, p->d_pm, p->d_tm, 0, nr, st);
+    HMVM_CUDA_TRY(cudaGetLastError(), "multi-RHS V-stage reduction launch");
+  }
+  if (ev) cudaEventRecord(ev[2], st);
+  {
+    a.team_begin = p->d_tb2;
+    a.nteams = p->stage2_teams;
+    const int ctas = (p->stage2_teams + c.wpb - 1) / c.wpb;
+    multi_kernel_for<false>(mode, nr_inst, kDefaultMultiCfg)<<<ctas, threads, smem, st>>>(a);
+    HMVM_CUDA_TRY(cudaGetLastError(), "multi-RHS row-stage launch");
+  }
+  if (ev) cudaEventRecord(ev[3], st);
+  if (p->n_red2 > 0) {
+    if (f32) launch_reduce_multi<float, float, false>(nr_inst, p->d_red2, p->n_red2, p->d_pm, Y, ldy, nr, st);
+    else launch_reduce_multi<double, double, false>(nr_inst, p->d_red2, p->n_red2, p->d_pm, Y, ldy, nr, st);
+    HMVM_CUDA_TRY(cudaGetLastError(), "multi-RHS row-stage reduction launch");
+  }
+  if (ev) cudaEventRecord(ev[4], st);
+  return HMVM_OK;
+}
+
+// Right-hand sides per pass: the largest of 8, 4, 2 that is <= nrhs_max and
+// not above what is left (a last single column runs in a 2-wide pass).
+int multi_pass_width(int nrhs_max, int left) {
+  for (int w : {8, 4, 2})
+    if (w <= nrhs_max && w <= std::max(left, 2)) return w;
+  return 2;
+}
+
+int apply_multi_impl(hmvm_plan* p, const void* X, int64_t ldx, void* Y, int64_t ldy, int nrhs, cudaStream_t st) {
+  if (p->nd == 0 || nrhs == 0) return HMVM_OK;
+  const size_t ex = (size_t)p->elem;
+  if (p->nrhs_max <= 1) {
+    // single-vector passes
+    for (int r = 0; r < nrhs; r++) {
+      int rc = apply_impl_fwd(p, static_cast<const char*>(X) + (size_t)r * ldx * ex,
+                              static_cast<char*>(Y) + (size_t)r * ldy * ex, st);
+      if (rc) return rc;
+    }
+    return HMVM_OK;
+  }
+  for (int r0 = 0; r0 < nrhs;) {
+    const int w = multi_pass_width(p->nrhs_max, nrhs - r0);
+    const int nr = std::min(w, nrhs - r0);
+    int rc = launch_multi_pass(p, static_cast<const char*>(X) + (size_t)r0 * ldx * ex, ldx,
+                               static_cast<char*>(Y) + (size_t)r0 * ldy * ex, ldy, nr, w, st);
+    if (rc) return rc;
+    r0 += nr;
+  }
+  return HMVM_OK;
+}
+
+int check_multi(const hmvm_plan* p, const void* X, int64_t ldx, const void* Y, int64_t ldy, int32_t nrhs) {
+  if (!p) return set_error(HMVM_EINVAL, "plan is NULL");
+  if (nrhs < 0) return set_error(HMVM_EINVAL, "nrhs < 0");
+  if (p->nd == 0 || nrhs == 0) return HMVM_OK;
+  if (!X || !Y) return set_error(HMVM_EINVAL, "X or Y is NULL");
+  if (ldx < p->nd || ldy < p->nd) return set_error(HMVM_EINVAL, "ldx and ldy must be >= N");
+  const char* xb = static_cast<const char*>(X);
+  const char* yb = static_cast<const char*>(Y);
+  const size_t xe = ((size_t)(nrhs - 1) * ldx + p->nd) * p->elem, ye = ((size_t)(nrhs - 1) * ldy + p->nd) * p->elem;
+  if (xb < yb + ye && yb < xb + xe) return set_error(HMVM_EINVAL, "X and Y overlap");
+  return HMVM_OK;
+}
+
 int apply_impl(hmvm_plan* p, const void* x, void* y, cudaStream_t st) {
   if (p->nd == 0) return HMVM_OK;
   if (p->mixed) return launch_stages_mixed(p, x, y, p->d_t, p->d_p, p->d_x32, st);
@@ -552,8 +755,9 @@ void hmvm_b200_default_opts(hmvm_plan_opts* o) {
   o->ctas_per_sm = 0;
   o->kernel = -1;
   o->mixed_fp8_eps = 1e-4;
-  o->mixed_fp32_tau = 0.5;
+  o->mixed_fp32_tau = -1.0;
   o->mixed_lr_format = HMVM_LR_FP16;
+  o->nrhs_max = 1;
 }
 
 int hmvm_b200_plan_create_d(const hmvm_matrix2_d* m, const hmvm_plan_opts* opts, hmvm_plan** plan) {
@@ -710,6 +914,62 @@ int hmvm_b200_apply_host(hmvm_plan* p, const void* x_host, void* y_host, void* s
   HMVM_CUDA_TRY(cudaMemcpyAsync(y_host, p->d_y, nb, cudaMemcpyDeviceToHost, st), "copy y to host");
   HMVM_CUDA_TRY(cudaStreamSynchronize(st), "stream synchronize");
   return HMVM_OK;
+}
+
+int hmvm_b200_apply_multi(hmvm_plan* p, const void* X, int64_t ldx, void* Y, int64_t ldy, int32_t nrhs,
+                          void* stream) {
+  int rc = check_multi(p, X, ldx, Y, ldy, nrhs);
+  if (rc) return rc;
+  DeviceGuard g(p->device);
+  if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
+  return apply_multi_impl(p, X, ldx, Y, ldy, nrhs, static_cast<cudaStream_t>(stream));
+}
+
+int hmvm_b200_apply_multi_host(hmvm_plan* p, const void* X_host, int64_t ldx, void* Y_host, int64_t ldy,
+                               int32_t nrhs, void* stream) {
+  int rc = check_multi(p, X_host, ldx, Y_host, ldy, nrhs);
+  if (rc) return rc;
+  if (p->nd == 0 || nrhs == 0) return HMVM_OK;
+  DeviceGuard g(p->device);
+  if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
+  // device copies with leading dimension N, grown on demand
+  const size_t col = (size_t)p->nd * p->elem, nb = col * (size_t)nrhs;
+  if (nb > p->xh_bytes) {
+    if (p->d_xh) cudaFree(p->d_xh);
+    if (p->d_yh) cudaFree(p->d_yh);
+    p->d_xh = p->d_yh = nullptr;
+    p->xh_bytes = 0;
+    HMVM_CUDA_TRY(cudaMalloc(&p->d_xh, nb), "cudaMalloc X staging");
+    HMVM_CUDA_TRY(cudaMalloc(&p->d_yh, nb), "cudaMalloc Y staging");
+    p->xh_bytes = nb;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (ldx == p->nd) {
+    HMVM_CUDA_TRY(cudaMemcpyAsync(p->d_xh, X_host, nb, cudaMemcpyHostToDevice, st), "copy X to device");
+  } else {
+    HMVM_CUDA_TRY(cudaMemcpy2DAsync(p->d_xh, col, X_host, (size_t)ldx * p->elem, col, (size_t)nrhs,
+                                    cudaMemcpyHostToDevice, st),
+                  "copy X to device");
+  }
+  rc = apply_multi_impl(p, p->d_xh, p->nd, p->d_yh, p->nd, nrhs, st);
+  if (rc) return rc;
+  if (ldy == p->nd) {
+    HMVM_CUDA_TRY(cudaMemcpyAsync(Y_host, p->d_yh, nb, cudaMemcpyDeviceToHost, st), "copy Y to host");
+  } else {
+    HMVM_CUDA_TRY(cudaMemcpy2DAsync(Y_host, (size_t)ldy * p->elem, p->d_yh, col, col, (size_t)nrhs,
+                                    cudaMemcpyDeviceToHost, st),
+                  "copy Y to host");
+  }
+  HMVM_CUDA_TRY(cudaStreamSynchronize(st), "stream synchronize");
+  return HMVM_OK;
+}
+
+int hmvm_b200_plan_multi_kernel_count(const hmvm_plan* p, int32_t nrhs) {
+  if (!p || p->nd == 0 || nrhs <= 0) return 0;
+  if (p->nrhs_max <= 1) return nrhs * hmvm_b200_plan_kernel_count(p);
+  int passes = 0;
+  for (int r0 = 0; r0 < nrhs; passes++) r0 += std::min(multi_pass_width(p->nrhs_max, nrhs - r0), nrhs - r0);
+  return passes * (1 + (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1 + (p->n_red2 > 0));
 }
 
 static int one_shot(hmvm_plan* plan, const void* x, void* y, hmvm_stats* stats, double setup_s) {

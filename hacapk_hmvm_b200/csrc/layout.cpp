@@ -154,6 +154,8 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     L.ctas_per_sm = opts.ctas_per_sm > 0 ? opts.ctas_per_sm
                     : (L.kernel == 0 ? kDefaultCtasPerSm : kDefaultStreamCtasPerSm);
     const int VEC = L.vec;  // plain plans: elements per vector
+    const int nrhs_max = std::min(std::max(opts.nrhs_max, 1), kMaxNrhsPass);
+    L.nrhs_max = nrhs_max;
     const int RMAX = (opts.max_tile_rows >= 1 && opts.max_tile_rows <= kMaxRows) ? opts.max_tile_rows : kMaxRows;
     const int32_t nd = lt.nd, nlf = lt.nlf;
     const bool srcf = lt.rowmat_is_float;
@@ -191,7 +193,8 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
       sc_u.assign(ncolflat, 1.0f);
       sc_v.assign(ncolflat, 1.0f);
       const double fp8_eps = opts.mixed_fp8_eps;
-      const double tau = opts.mixed_fp32_tau;
+      const double tau = opts.mixed_fp32_tau >= 0.0 ? opts.mixed_fp32_tau
+                         : (opts.mixed_lr_format == HMVM_LR_BF16 ? 0.05 : 0.5);
 #pragma omp parallel for schedule(dynamic, 64)
       for (int32_t i = 0; i < nlf; i++) {
         if (!live_lr[i]) continue;
@@ -453,6 +456,12 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     const int32_t ctas = L.num_sms * L.ctas_per_sm;
     L.stage1_teams = ctas * (L.mixed ? kMixedCfgs[L.stage1_cfg].wpb : teams_per_cta(L.kernel, L.stage1_cfg));
     L.stage2_teams = ctas * (L.mixed ? kMixedCfgs[L.stage2_cfg].wpb : teams_per_cta(L.kernel, L.stage2_cfg));
+    if (nrhs_max > 1) {
+      // teams for the multi-RHS kernel, all resident at once (and no more than
+      // the single-vector kernels launch)
+      L.stage1_teams = std::min(L.stage1_teams, L.num_sms * kMultiWarpsPerSm);
+      L.stage2_teams = std::min(L.stage2_teams, L.num_sms * kMultiWarpsPerSm);
+    }
     int64_t stage_bytes[2] = {0, 0};
     for (int32_t k = 0; k < ntb; k++) stage_bytes[k < n1 ? 0 : 1] += (int64_t)tb[k].nvec * tb[k].nrows * 16;
     int64_t max_item[2];
@@ -481,10 +490,12 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
           int32_t vmax = std::max(1, opts.split_cols / VEC);
           nparts = std::max(nparts, (t.nvec + vmax - 1) / vmax);
         }
-        if (L.kernel == 1) {
-          // an item's x/t columns must fit the kernel's input buffer
+        if (L.kernel == 1 || nrhs_max > 1) {
+          // an item's x/t columns must fit the kernels' input buffers
           const int32_t cfg = st == 0 ? L.stage1_cfg : L.stage2_cfg;
-          const int32_t vmax = std::max(1, kStreamCfgs[cfg].zcap / VEC);
+          int32_t zcap = L.kernel == 1 ? kStreamCfgs[cfg].zcap : INT32_MAX;
+          if (nrhs_max > 1) zcap = std::min(zcap, kMultiZBytes / (nrhs_max * L.elem_size));
+          const int32_t vmax = std::max(1, zcap / VEC);
           nparts = std::max(nparts, (t.nvec + vmax - 1) / vmax);
         }
         for (int32_t q = 1; q < nparts; q++) cuts.push_back((int32_t)((int64_t)t.nvec * q / nparts));
@@ -492,7 +503,7 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
         // greedy: close an item before it exceeds the byte bound, the input
         // buffer or kMixedMaxSegs segments
         const int cfg = st == 0 ? L.stage1_cfg : L.stage2_cfg;
-        const int64_t zcap = kMixedCfgs[cfg].zbytes;
+        const int64_t zcap = std::min<int64_t>(kMixedCfgs[cfg].zbytes, kMultiZBytes / nrhs_max);
         const int64_t bcap = std::max<int64_t>(max_item[st], (int64_t)t.nrows * 16);
         const int32_t vsplit = (st == 0 && opts.split_cols > 0) ? std::max(1, opts.split_cols / 4) : INT32_MAX;
         int64_t zb = 0, by = 0;

@@ -117,6 +117,18 @@ constexpr MixedCfg kMixedCfgs[kNumMixedCfgs] = {{8, 4, 2048, 2048}, {8, 4, 1024,
 inline int mixed_smem_bytes(const MixedCfg& c) { return c.wpb * (c.slots * c.chunk + 2 * c.zbytes + c.slots * 8); }
 constexpr int kDefaultMixedCfg = 0;
 
+// Multi-RHS kernel (hmvm_multi_kernel): rhs per pass and its input buffer.
+constexpr int kMaxNrhsPass = 8;
+constexpr int kMultiZBytes = 8192;
+struct MultiCfg {
+  int wpb, slots, chunk;
+};
+constexpr int kNumMultiCfgs = 3;
+constexpr MultiCfg kMultiCfgs[kNumMultiCfgs] = {{4, 4, 2048}, {8, 4, 2048}, {4, 8, 1024}};
+inline int multi_smem_bytes(const MultiCfg& c) { return c.wpb * (c.slots * c.chunk + 2 * kMultiZBytes + c.slots * 8); }
+constexpr int kDefaultMultiCfg = 0;
+constexpr int kMultiWarpsPerSm = 8;  // resident warps (teams) per SM of the multi-RHS kernel
+
 struct HostLayout {
   int precision = HMVM_FP64;
   int vec = 2;
@@ -142,6 +154,7 @@ struct HostLayout {
   int64_t cols_fp32 = 0, cols_lr16 = 0, cols_fp8 = 0;
   int64_t stored_bytes = 0;      // bytes of the stored elements in their storage formats
   int64_t stored_bytes1 = 0;     // ... of the V stage
+  int nrhs_max = 1;              // items fit the multi-RHS input buffer for this many rhs
 };
 
 // Returns HMVM_OK or a status; msg receives a description on failure.

@@ -138,6 +138,32 @@ class Plan:
         _lib.check(rc, "apply_host")
         return y
 
+    def apply_multi(self, X, Y, stream=None) -> None:
+        """Y = H X for a block of right-hand sides: X and Y are CUDA tensors
+        of shape (nrhs, N) whose rows are the vectors (column-major N x nrhs
+        with leading dimension X.stride(0))."""
+        if X.dim() != 2 or Y.shape != X.shape or X.shape[1] != self.nd or X.stride(1) != 1 or Y.stride(1) != 1:
+            raise ValueError(f"X and Y must be (nrhs, {self.nd}) with unit stride along N")
+        rc = _lib.hmvm_lib().hmvm_b200_apply_multi(self.handle, _dev_ptr(X), X.stride(0), _dev_ptr(Y), Y.stride(0),
+                                                   X.shape[0], _stream_handle(stream))
+        _lib.check(rc, "apply_multi")
+
+    def apply_multi_host(self, X: np.ndarray, Y: np.ndarray | None = None, stream=None) -> np.ndarray:
+        """The same with host arrays of shape (nrhs, N)."""
+        X = np.ascontiguousarray(X, dtype=self.dtype)
+        if X.ndim != 2 or X.shape[1] != self.nd:
+            raise ValueError(f"X must have shape (nrhs, {self.nd})")
+        if Y is None:
+            Y = np.empty_like(X)
+        rc = _lib.hmvm_lib().hmvm_b200_apply_multi_host(self.handle, X.ctypes.data, self.nd, Y.ctypes.data, self.nd,
+                                                        X.shape[0],
+                                                        _stream_handle(stream) if stream is not None else 0)
+        _lib.check(rc, "apply_multi_host")
+        return Y
+
+    def multi_kernel_count(self, nrhs: int) -> int:
+        return int(_lib.hmvm_lib().hmvm_b200_plan_multi_kernel_count(self.handle, nrhs))
+
     def close(self) -> None:
         if self._h:
             _lib.hmvm_lib().hmvm_b200_plan_destroy(self._h)

@@ -138,9 +138,11 @@ typedef struct hmvm_plan_opts {
   int32_t kernel;         /* 0: register-streaming tile kernel; 1 (default, -1): TMA-ring stream kernel */
   /* HMVM_MIXED only.  |block| is the largest rank-1 term norm |u_k||v_k| of the leaf. */
   double mixed_fp8_eps;   /* FP8 below this * |block| (default 1e-4, the ACA tolerance; 0 = no FP8) */
-  double mixed_fp32_tau;  /* FP32 at or above this * |block| (default 0.5; > 1 = none) */
+  double mixed_fp32_tau;  /* FP32 at or above this * |block| (> 1 = none; < 0, the default = 0.5 for FP16
+                             factors, 0.05 for BF16, whose 8-bit significand needs more FP32 columns) */
   int32_t mixed_lr_format;/* enum hmvm_lr_format (default FP16) */
-  int32_t _reserved;
+  int32_t nrhs_max;       /* right-hand sides per pass of hmvm_b200_apply_multi, 1..8 (default 1; items are
+                             sized so that nrhs_max inputs per column fit the multi-RHS kernel's buffer) */
 } hmvm_plan_opts;
 
 typedef struct hmvm_plan_info {
@@ -182,6 +184,23 @@ int hmvm_b200_apply(hmvm_plan *plan, const void *x_dev, void *y_dev, void *strea
 /* The same with host buffers: copies x in, runs, copies y out, and waits for
  * the stream. */
 int hmvm_b200_apply_host(hmvm_plan *plan, const void *x_host, void *y_host, void *stream);
+
+/* Y = H X for nrhs right-hand sides: X and Y column-major in device memory
+ * (column r at X + r * ldx, ldx >= N; same for Y), element type as for
+ * hmvm_b200_apply.  Plans created with opts.nrhs_max > 1 run passes of up to
+ * nrhs_max (8 at most) columns through the multi-RHS kernel, each pass
+ * streaming the matrix once; plans with nrhs_max = 1 run nrhs single-vector
+ * applies.  Each column of Y is computed in a fixed order (repeatable bit for
+ * bit; it may differ in the last bits from the single-vector apply).  The
+ * reference has no multi-RHS entry point: its hmvm_cuda* wrappers take one b
+ * (hmvm_cuda.h:4-7). */
+int hmvm_b200_apply_multi(hmvm_plan *plan, const void *X_dev, int64_t ldx, void *Y_dev, int64_t ldy, int32_t nrhs,
+                          void *stream);
+/* The same with host buffers (copies in, runs, copies out, waits). */
+int hmvm_b200_apply_multi_host(hmvm_plan *plan, const void *X_host, int64_t ldx, void *Y_host, int64_t ldy,
+                               int32_t nrhs, void *stream);
+/* Kernels one hmvm_b200_apply_multi call with nrhs columns launches. */
+int hmvm_b200_plan_multi_kernel_count(const hmvm_plan *plan, int32_t nrhs);
 
 /* Capacity of the scratch array used by hmvm_b200_apply_noalloc: 16 MiB. */
 #define HMVM_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)

@@ -82,6 +82,32 @@ def test_mixed_column_classes():
     assert counts(mixed_fp8_eps=0.0)[3] == 0
 
 
+@pytest.mark.parametrize("nrhs_max", [2, 4, 8])
+def test_multi_rhs_items_fit_input_buffer(nrhs_max):
+    """Plans for the multi-RHS kernel: every item's inputs for nrhs_max
+    right-hand sides fit its 8 KiB buffer, and the teams are the multi-RHS
+    kernel's (8 per SM)."""
+    from layout_checks import SEG_VEC, seg_type
+
+    hm = HMatrix.generate(2500, "cube", eps=1e-6, leaf_size=24, seed=4)
+    x = np.random.default_rng(3).uniform(-1, 1, hm.nd)
+    yo = oracle_hmvm(hm, x)
+    for prec in (0, 1, 2):
+        h, v = layout_for(hm, precision=prec, nrhs_max=nrhs_max)
+        check_layout_bounds(v)
+        assert v.stage1_teams <= 148 * 8 and v.stage2_teams <= 148 * 8
+        tiles = np.ctypeslib.as_array((_lib.TileDesc * v.n_tiles).from_address(v.tiles))
+        segs = np.ctypeslib.as_array((_lib.SegDesc * v.n_segs).from_address(v.segs))
+        for td in tiles:
+            zb = 0
+            for sidx in range(int(td["seg_begin"]), int(td["seg_begin"]) + int(td["nseg"])):
+                ty, nc = seg_type(v, int(segs[sidx]["ncols"]))
+                zb += -(-nc // SEG_VEC[ty]) * SEG_VEC[ty] * (8 if ty == 0 else 4)
+            assert zb * nrhs_max <= 8192
+        assert relerr(emulate_layout(v, x), yo) < (1e-14 if prec == 0 else 1e-6 if prec == 1 else 1e-4)
+        _lib.hmvm_lib().hmvm_b200_layout_destroy(h)
+
+
 def test_stream_items_fit_input_buffer():
     from hacapk_hmvm_b200._lib import TileDesc
 
