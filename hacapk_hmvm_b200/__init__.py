@@ -6,5 +6,6 @@ behind the C ABI in include/hmvm_b200.h.
 """
 from .hmatrix import HMatrix  # noqa: F401
 from .hmvm import Plan, hmvm, hmvm_cuda  # noqa: F401
+from .batch import Batch  # noqa: F401
 
-__all__ = ["HMatrix", "Plan", "hmvm", "hmvm_cuda"]
+__all__ = ["HMatrix", "Plan", "Batch", "hmvm", "hmvm_cuda"]

@@ -578,6 +578,8 @@ void launch_pack(const hmvm_plan* p, const void* X, int64_t ldx, int nr, cudaStr
 }
 
 // One pass: nr (<= nr_inst) right-hand sides X[:, 0:nr] -> Y[:, 0:nr].
+int launch_multi_stages(hmvm_plan* p, void* Y, int64_t ldy, int nr, int nr_inst, cudaStream_t st);
+
 int launch_multi_pass(hmvm_plan* p, const void* X, int64_t ldx, void* Y, int64_t ldy, int nr, int nr_inst,
                       cudaStream_t st) {
   switch (nr_inst) {
@@ -586,6 +588,11 @@ int launch_multi_pass(hmvm_plan* p, const void* X, int64_t ldx, void* Y, int64_t
     default: launch_pack<8>(p, X, ldx, nr, st); break;
   }
   HMVM_CUDA_TRY(cudaGetLastError(), "input packing launch");
+  return launch_multi_stages(p, Y, ldy, nr, nr_inst, st);
+}
+
+// The stages of one pass, the packed inputs already in place.
+int launch_multi_stages(hmvm_plan* p, void* Y, int64_t ldy, int nr, int nr_inst, cudaStream_t st) {
   MultiArgs a;
   a.err = p->d_err;
   a.tiles = p->d_tiles;
@@ -1198,5 +1205,338 @@ const char* hmvm_b200_strerror(int s) {
 const char* hmvm_b200_last_error(void) { return g_last_error.c_str(); }
 
 int hmvm_b200_version(void) { return 2; }
+
+}  // extern "C"
+
+// ---- batches of independent H-matrices ----------------------------------------
+// A batch is planned as one block-diagonal H-matrix: instance m's leaves are
+// shifted by off[m] in rows and columns, so one persistent launch per stage
+// runs every instance's items, load-balanced together.
+
+struct hmvm_batch {
+  hmvm_plan* plan = nullptr;
+  int32_t count = 0;
+  int64_t ntot = 0;
+  int32_t nmax = 0;
+  std::vector<int32_t> n;
+  std::vector<int64_t> off;
+  std::vector<BatchIO> io;  // the table last uploaded
+  BatchIO* d_io = nullptr;
+  void* d_xcat = nullptr;   // single-vector plans: concatenated x (ntot + 16)
+  void* d_ycat = nullptr;   // concatenated Y, column r at d_ycat + r * ntot
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+void free_batch(hmvm_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  for (void* q : {(void*)b->d_io, b->d_xcat, b->d_ycat})
+    if (q) cudaFree(q);
+  b->d_io = nullptr;
+  b->d_xcat = b->d_ycat = nullptr;
+  if (b->plan) hmvm_b200_plan_destroy(b->plan);
+  b->plan = nullptr;
+}
+
+int batch_create(const std::vector<LeafTable>& tabs, bool is_float, const hmvm_plan_opts* opts, hmvm_batch** out) {
+  if (!out) return set_error(HMVM_EINVAL, "output handle is NULL");
+  *out = nullptr;
+  const int32_t count = (int32_t)tabs.size();
+  if (count <= 0) return set_error(HMVM_EINVAL, "a batch needs at least one matrix");
+  int64_t ntot = 0, nlf = 0, len = 0;
+  int32_t ktmax = 0, nmax = 0;
+  for (const LeafTable& t : tabs) {
+    std::string msg;
+    int rc = validate_leaves(t, msg);
+    if (rc) return set_error(rc, "batch instance: " + msg);
+    ntot += t.nd;
+    nlf += t.nlf;
+    len += t.len;
+    ktmax = std::max(ktmax, t.ktmax);
+    nmax = std::max(nmax, t.nd);
+  }
+  if (ntot > INT32_MAX - 64 || nlf > INT32_MAX) return set_error(HMVM_ERANGE, "batch too large for one plan");
+  // the block-diagonal leaf table
+  std::vector<int32_t> ltmtx, kt, ndl, ndt, sl, st;
+  std::vector<int64_t> a1, a2;
+  std::vector<unsigned char> rowmat;
+  const size_t esz = is_float ? 4 : 8;
+  try {
+    for (auto* v : {&ltmtx, &kt, &ndl, &ndt, &sl, &st}) v->reserve((size_t)nlf);
+    a1.reserve((size_t)nlf);
+    a2.reserve((size_t)nlf);
+    rowmat.resize((size_t)len * esz);
+  } catch (const std::bad_alloc&) {
+    return set_error(HMVM_ENOMEM, "host allocation failed while merging the batch");
+  }
+  hmvm_batch* b = new (std::nothrow) hmvm_batch();
+  if (!b) return set_error(HMVM_ENOMEM, "host allocation failed");
+  b->count = count;
+  b->ntot = ntot;
+  b->nmax = nmax;
+  int64_t roff = 0, loff = 0;
+  for (const LeafTable& t : tabs) {
+    b->n.push_back(t.nd);
+    b->off.push_back(roff);
+    for (int32_t i = 0; i < t.nlf; i++) {
+      ltmtx.push_back(t.ltmtx[i]);
+      kt.push_back(t.kt[i]);
+      ndl.push_back(t.ndl[i]);
+      ndt.push_back(t.ndt[i]);
+      sl.push_back(t.nstrtl[i] + (int32_t)roff);
+      st.push_back(t.nstrtt[i] + (int32_t)roff);
+      a1.push_back(t.a1(i) + loff);
+      a2.push_back(t.a2(i) + loff);
+    }
+    if (t.len > 0) std::memcpy(rowmat.data() + (size_t)loff * esz, t.rowmat, (size_t)t.len * esz);
+    roff += t.nd;
+    loff += t.len;
+  }
+  LeafTable m;
+  m.nd = (int32_t)ntot;
+  m.nlf = (int32_t)nlf;
+  m.ktmax = ktmax;
+  m.len = len;
+  m.ltmtx = ltmtx.data();
+  m.kt = kt.data();
+  m.ndl = ndl.data();
+  m.ndt = ndt.data();
+  m.nstrtl = sl.data();
+  m.nstrtt = st.data();
+  m.a1_64 = a1.data();
+  m.a2_64 = a2.data();
+  m.rowmat = rowmat.data();
+  m.rowmat_is_float = is_float;
+  int rc = create_plan(m, opts, &b->plan);
+  if (rc) {
+    delete b;
+    return rc;
+  }
+  hmvm_plan* p = b->plan;
+  DeviceGuard g(p->device);
+  const size_t ncols = (size_t)std::max(1, p->nrhs_max);
+  cudaError_t e = cudaMalloc(&b->d_io, sizeof(BatchIO) * (size_t)count);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_ycat, (size_t)(ntot + 16) * ncols * p->elem);
+  if (e == cudaSuccess && p->nrhs_max <= 1) {
+    e = cudaMalloc(&b->d_xcat, (size_t)(ntot + 16) * p->elem);
+    if (e == cudaSuccess) e = cudaMemset(b->d_xcat, 0, (size_t)(ntot + 16) * p->elem);
+  }
+  // the packed multi-RHS inputs: the batch packing kernels never write the pad rows
+  if (e == cudaSuccess && p->d_xm64) e = cudaMemset(p->d_xm64, 0, (size_t)(ntot + 16) * ncols * sizeof(double));
+  if (e == cudaSuccess && p->d_xm32) e = cudaMemset(p->d_xm32, 0, (size_t)(ntot + 16) * ncols * sizeof(float));
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    rc = cuda_fail(e, "batch buffers");
+    free_batch(b);
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return HMVM_OK;
+}
+
+int batch_set_io(hmvm_batch* b, const void* const* X, const int64_t* ldx, void* const* Y, const int64_t* ldy,
+                 const int32_t* nrhs) {
+  if (!b) return set_error(HMVM_EINVAL, "batch is NULL");
+  if (!X || !ldx || !Y || !ldy || !nrhs) return set_error(HMVM_EINVAL, "NULL argument array");
+  std::vector<BatchIO> io((size_t)b->count);
+  for (int32_t m = 0; m < b->count; m++) {
+    BatchIO& q = io[m];
+    q.X = X[m];
+    q.ldx = ldx[m];
+    q.Y = Y[m];
+    q.ldy = ldy[m];
+    q.off = b->off[m];
+    q.n = b->n[m];
+    q.nrhs = nrhs[m];
+    if (q.nrhs < 0) return set_error(HMVM_EINVAL, "instance " + std::to_string(m) + ": nrhs < 0");
+    if (q.n == 0 || q.nrhs == 0) continue;
+    if (!q.X || !q.Y) return set_error(HMVM_EINVAL, "instance " + std::to_string(m) + ": X or Y is NULL");
+    if (q.ldx < q.n || q.ldy < q.n) return set_error(HMVM_EINVAL, "instance " + std::to_string(m) + ": ld < N");
+  }
+  b->io.swap(io);
+  return HMVM_OK;
+}
+
+int batch_max_nrhs(const hmvm_batch* b) {
+  int mx = 0;
+  for (const BatchIO& q : b->io) mx = std::max(mx, (int)q.nrhs);
+  return mx;
+}
+
+template <typename T>
+int batch_run_t(hmvm_batch* b, cudaStream_t st) {
+  hmvm_plan* p = b->plan;
+  const int mx = batch_max_nrhs(b);
+  const unsigned cnt = (unsigned)b->count;
+  auto blocks = [&](int64_t work) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 64)); };
+  if (p->nrhs_max <= 1) {
+    for (int c = 0; c < mx; c++) {
+      hmvm_batch_pack1_kernel<T><<<dim3(blocks(b->nmax), cnt), 256, 0, st>>>(b->d_io, c, static_cast<T*>(b->d_xcat));
+      HMVM_CUDA_TRY(cudaGetLastError(), "batch packing launch");
+      int rc = apply_impl(p, b->d_xcat, b->d_ycat, st);
+      if (rc) return rc;
+      hmvm_batch_unpack_kernel<T><<<dim3(blocks(b->nmax), cnt), 256, 0, st>>>(
+          b->d_io, c, 1, static_cast<const T*>(b->d_ycat), b->ntot);
+      HMVM_CUDA_TRY(cudaGetLastError(), "batch unpacking launch");
+    }
+    return HMVM_OK;
+  }
+  for (int c0 = 0; c0 < mx;) {
+    const int w = multi_pass_width(p->nrhs_max, mx - c0);
+    const dim3 grid(blocks((int64_t)b->nmax * w), cnt);
+    double* x64 = p->d_xm64;
+    float* x32 = p->d_xm32;
+    switch (w) {
+      case 2: hmvm_batch_packm_kernel<T, 2><<<grid, 256, 0, st>>>(b->d_io, c0, x64, x32); break;
+      case 4: hmvm_batch_packm_kernel<T, 4><<<grid, 256, 0, st>>>(b->d_io, c0, x64, x32); break;
+      default: hmvm_batch_packm_kernel<T, 8><<<grid, 256, 0, st>>>(b->d_io, c0, x64, x32); break;
+    }
+    HMVM_CUDA_TRY(cudaGetLastError(), "batch packing launch");
+    int rc = launch_multi_stages(p, b->d_ycat, b->ntot, w, w, st);
+    if (rc) return rc;
+    hmvm_batch_unpack_kernel<T><<<grid, 256, 0, st>>>(b->d_io, c0, w, static_cast<const T*>(b->d_ycat), b->ntot);
+    HMVM_CUDA_TRY(cudaGetLastError(), "batch unpacking launch");
+    c0 += w;
+  }
+  return HMVM_OK;
+}
+
+int batch_run(hmvm_batch* b, cudaStream_t st) {
+  HMVM_CUDA_TRY(cudaMemcpyAsync(b->d_io, b->io.data(), sizeof(BatchIO) * b->io.size(), cudaMemcpyHostToDevice, st),
+                "batch table upload");
+  return b->plan->precision == HMVM_FP32 ? batch_run_t<float>(b, st) : batch_run_t<double>(b, st);
+}
+
+}  // namespace
+
+extern "C" {
+
+int hmvm_b200_batch_create64_d(const hmvm_leaves64* mats, int32_t count, const hmvm_plan_opts* opts,
+                               hmvm_batch** out) {
+  if (!mats || count <= 0) return set_error(HMVM_EINVAL, "no matrices");
+  std::vector<LeafTable> t((size_t)count);
+  for (int32_t m = 0; m < count; m++) table_from_leaves64(&mats[m], false, t[m]);
+  return batch_create(t, false, opts, out);
+}
+
+int hmvm_b200_batch_create64_f(const hmvm_leaves64* mats, int32_t count, const hmvm_plan_opts* opts,
+                               hmvm_batch** out) {
+  if (!mats || count <= 0) return set_error(HMVM_EINVAL, "no matrices");
+  hmvm_plan_opts o;
+  hmvm_b200_default_opts(&o);
+  if (opts) o = *opts;
+  o.precision = HMVM_FP32;
+  std::vector<LeafTable> t((size_t)count);
+  for (int32_t m = 0; m < count; m++) table_from_leaves64(&mats[m], true, t[m]);
+  return batch_create(t, true, &o, out);
+}
+
+int hmvm_b200_batch_create_d(const hmvm_matrix2_d* mats, int32_t count, const hmvm_plan_opts* opts,
+                             hmvm_batch** out) {
+  if (!mats || count <= 0) return set_error(HMVM_EINVAL, "no matrices");
+  std::vector<LeafTable> t((size_t)count);
+  for (int32_t m = 0; m < count; m++) {
+    const hmvm_matrix2_d* q = &mats[m];
+    make_table_from_matrix2(q->nd, q->nlf, q->ktmax, q->len, q->ltmtx, q->kt, q->ndl, q->ndt, q->nstrtl, q->nstrtt,
+                            q->a1, q->a2, q->rowmat, false, t[m]);
+  }
+  return batch_create(t, false, opts, out);
+}
+
+void hmvm_b200_batch_destroy(hmvm_batch* b) {
+  if (!b) return;
+  if (b->plan) {
+    DeviceGuard g(b->plan->device);
+    free_batch(b);
+  }
+  delete b;
+}
+
+int hmvm_b200_batch_get_info(const hmvm_batch* b, hmvm_plan_info* info) {
+  if (!b) return set_error(HMVM_EINVAL, "batch is NULL");
+  return hmvm_b200_plan_get_info(b->plan, info);
+}
+
+int hmvm_b200_batch_instance(const hmvm_batch* b, int32_t m, int32_t* n, int64_t* offset) {
+  if (!b || m < 0 || m >= b->count) return set_error(HMVM_EINVAL, "no such instance");
+  if (n) *n = b->n[m];
+  if (offset) *offset = b->off[m];
+  return HMVM_OK;
+}
+
+int hmvm_b200_batch_apply(hmvm_batch* b, const void* const* X, const int64_t* ldx, void* const* Y,
+                          const int64_t* ldy, const int32_t* nrhs, void* stream) {
+  int rc = batch_set_io(b, X, ldx, Y, ldy, nrhs);
+  if (rc) return rc;
+  DeviceGuard g(b->plan->device);
+  if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the batch's device");
+  return batch_run(b, static_cast<cudaStream_t>(stream));
+}
+
+int hmvm_b200_batch_capture(hmvm_batch* b, const void* const* X, const int64_t* ldx, void* const* Y,
+                            const int64_t* ldy, const int32_t* nrhs) {
+  int rc = batch_set_io(b, X, ldx, Y, ldy, nrhs);
+  if (rc) return rc;
+  DeviceGuard g(b->plan->device);
+  if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the batch's device");
+  if (b->plan->profiling) return set_error(HMVM_EINVAL, "profiling is on; a captured batch cannot record events");
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  cudaStream_t cs;
+  HMVM_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "cudaStreamCreate");
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(cs);
+    return cuda_fail(e, "cudaStreamBeginCapture");
+  }
+  rc = batch_run(b, cs);
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(cs, &graph);  // always end the capture
+  cudaStreamDestroy(cs);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&b->exec, graph, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return cuda_fail(e, "cudaGraphInstantiate");
+  }
+  b->graph = graph;
+  return HMVM_OK;
+}
+
+int hmvm_b200_batch_launch(hmvm_batch* b, void* stream) {
+  if (!b) return set_error(HMVM_EINVAL, "batch is NULL");
+  if (!b->exec) return set_error(HMVM_EINVAL, "nothing captured: call hmvm_b200_batch_capture first");
+  DeviceGuard g(b->plan->device);
+  if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the batch's device");
+  HMVM_CUDA_TRY(cudaGraphLaunch(b->exec, static_cast<cudaStream_t>(stream)), "cudaGraphLaunch");
+  return HMVM_OK;
+}
+
+int hmvm_b200_batch_status(hmvm_batch* b) {
+  if (!b) return set_error(HMVM_EINVAL, "batch is NULL");
+  return hmvm_b200_plan_status(b->plan);
+}
+
+int hmvm_b200_batch_kernel_count(const hmvm_batch* b, int32_t max_nrhs) {
+  if (!b || max_nrhs <= 0) return 0;
+  const hmvm_plan* p = b->plan;
+  if (p->nrhs_max <= 1) return max_nrhs * (2 + hmvm_b200_plan_kernel_count(p));  // pack, stages, unpack
+  int passes = 0;
+  for (int c0 = 0; c0 < max_nrhs; passes++) c0 += multi_pass_width(p->nrhs_max, max_nrhs - c0);
+  // per pass: pack, the stage kernels, unpack
+  return passes * (2 + (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1 + (p->n_red2 > 0));
+}
 
 }  // extern "C"

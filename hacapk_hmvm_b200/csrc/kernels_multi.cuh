@@ -439,4 +439,56 @@ __global__ void __launch_bounds__(32 * WPB, (multi_min_blocks<WPB, S, CHUNK>()))
   }
 }
 
+// ---- batches of independent H-matrices ----------------------------------------
+// A batch runs as one block-diagonal H-matrix over the concatenated index
+// space; instance m owns rows [off, off + n).  These kernels move each
+// instance's vectors between its own buffers and the concatenated ones
+// (blockIdx.y = instance).
+struct BatchIO {
+  const void* X;  // column c at X + c * ldx
+  int64_t ldx;
+  void* Y;
+  int64_t ldy;
+  int64_t off;
+  int32_t n, nrhs;
+};
+
+// Column c of every instance -> xcat[off + i] (zero where c >= nrhs).
+template <typename T>
+__global__ void hmvm_batch_pack1_kernel(const BatchIO* __restrict__ io, int c, T* __restrict__ xcat) {
+  const BatchIO b = io[blockIdx.y];
+  const T* X = static_cast<const T*>(b.X);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < b.n; i += gridDim.x * blockDim.x)
+    xcat[b.off + i] = c < b.nrhs ? X[i + c * b.ldx] : T(0);
+}
+// Columns [c0, c0 + NR) -> the row-interleaved packed inputs (zero past nrhs).
+template <typename TI, int NR>
+__global__ void hmvm_batch_packm_kernel(const BatchIO* __restrict__ io, int c0, double* __restrict__ x64,
+                                        float* __restrict__ x32) {
+  const BatchIO b = io[blockIdx.y];
+  const TI* X = static_cast<const TI*>(b.X);
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)b.n * NR;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = k / NR;
+    const int r = (int)(k % NR);
+    const double v = c0 + r < b.nrhs ? (double)X[i + (int64_t)(c0 + r) * b.ldx] : 0.0;
+    const int64_t dst = (b.off + i) * NR + r;
+    if (x64) x64[dst] = v;
+    if (x32) x32[dst] = (float)v;
+  }
+}
+// ycat (column r at ycat + r * ldc) -> Y[:, c0 + r] for r < w, c0 + r < nrhs.
+template <typename T>
+__global__ void hmvm_batch_unpack_kernel(const BatchIO* __restrict__ io, int c0, int w, const T* __restrict__ ycat,
+                                         int64_t ldc) {
+  const BatchIO b = io[blockIdx.y];
+  T* Y = static_cast<T*>(b.Y);
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)b.n * w;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(k / b.n);
+    const int64_t i = k % b.n;
+    if (c0 + r < b.nrhs) Y[i + (int64_t)(c0 + r) * b.ldy] = ycat[b.off + i + r * ldc];
+  }
+}
+
 }  // namespace hmvm

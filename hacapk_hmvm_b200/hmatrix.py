@@ -152,8 +152,10 @@ class HMatrix:
     # ---- conversions -----------------------------------------------------
     def to_float(self) -> "HMatrix":
         """FP32 copy (element-wise rounding, as convertD2F)."""
-        return HMatrix.from_arrays(self.nd, self.ktmax, self.ltmtx, self.kt, self.ndl, self.ndt, self.nstrtl,
-                                   self.nstrtt, self.a1, self.a2, self.rowmat.astype(np.float32), self.meta)
+        # copies of the index arrays: they may be views of memory this matrix owns
+        return HMatrix.from_arrays(self.nd, self.ktmax, *(a.copy() for a in (
+            self.ltmtx, self.kt, self.ndl, self.ndt, self.nstrtl, self.nstrtt, self.a1, self.a2)),
+            self.rowmat.astype(np.float32), self.meta)
 
     def fits_matrix2(self) -> bool:
         return self.len <= np.iinfo(np.int32).max
