@@ -182,19 +182,20 @@ HMVM_SIGNATURES = {
     "hmvm_b200_apply_multi_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32,
                                              C.c_void_p]),
     "hmvm_b200_plan_multi_kernel_count": (C.c_int, [C.c_void_p, C.c_int32]),
-    "hmvm_b200_batch_create64_d": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
-    "hmvm_b200_batch_create64_f": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
-    "hmvm_b200_batch_create_d": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "hmvm_b200_batch_create64_d": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "hmvm_b200_batch_create64_f": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "hmvm_b200_batch_create_d": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hmvm_b200_batch_destroy": (None, [C.c_void_p]),
     "hmvm_b200_batch_get_info": (C.c_int, [C.c_void_p, C.c_void_p]),
-    "hmvm_b200_batch_instance": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "hmvm_b200_batch_instance": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "hmvm_b200_batch_class_count": (C.c_int, [C.c_void_p]),
     "hmvm_b200_batch_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p]),
     "hmvm_b200_batch_capture": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p]),
     "hmvm_b200_batch_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
     "hmvm_b200_batch_status": (C.c_int, [C.c_void_p]),
-    "hmvm_b200_batch_kernel_count": (C.c_int, [C.c_void_p, C.c_int32]),
+    "hmvm_b200_batch_kernel_count": (C.c_int, [C.c_void_p]),
     "hmvm_b200_plan_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "hmvm_b200_plan_profile_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "hmvm_b200_plan_status": (C.c_int, [C.c_void_p]),

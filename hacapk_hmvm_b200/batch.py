@@ -1,7 +1,8 @@
-"""Batches of independent H-matrices (hmvm_b200_batch_*): one block-diagonal
-plan over the concatenated index space, so every stage is one persistent launch
-over all instances; apply() runs it directly, capture()/launch() replay it as a
-CUDA graph."""
+"""Batches of independent H-matrices (hmvm_b200_batch_*): instances grouped by
+their right-hand-side count into classes, each one block-diagonal plan over its
+instances' concatenated index space, so every stage of a class is one
+persistent launch over all its instances; apply() runs the classes directly,
+capture()/launch() replay them as one CUDA graph."""
 from __future__ import annotations
 
 import ctypes as C
@@ -14,7 +15,10 @@ from .hmvm import PRECISIONS, _dev_ptr, _stream_handle, default_opts
 
 
 class Batch:
-    def __init__(self, mats: list[HMatrix], precision: str = "fp32", device: int = -1, **opts):
+    def __init__(self, mats: list[HMatrix], precision: str = "fp32", device: int = -1,
+                 nrhs: list[int] | None = None, **opts):
+        """nrhs: right-hand sides each instance will be applied with (groups the
+        instances into pass-width classes); None = opts' nrhs_max for all."""
         lib = _lib.hmvm_lib()
         prec = PRECISIONS[precision]
         o = default_opts(precision=prec, device=device, **opts)
@@ -26,7 +30,8 @@ class Batch:
         self._lv = (_lib.Leaves64 * len(mats))(*[m.as_leaves64() for m in mats])
         h = C.c_void_p()
         fn = lib.hmvm_b200_batch_create64_f if f32 else lib.hmvm_b200_batch_create64_d
-        _lib.check(fn(self._lv, len(mats), C.byref(o), C.byref(h)), "batch create")
+        nr = None if nrhs is None else (C.c_int32 * len(mats))(*[int(k) for k in nrhs])
+        _lib.check(fn(self._lv, len(mats), C.byref(o), nr, C.byref(h)), "batch create")
         self._h = h
         self.mats = mats
         self.n = [m.nd for m in mats]
@@ -75,8 +80,19 @@ class Batch:
     def status(self) -> None:
         _lib.check(_lib.hmvm_lib().hmvm_b200_batch_status(self.handle), "batch status")
 
-    def kernel_count(self, max_nrhs: int) -> int:
-        return int(_lib.hmvm_lib().hmvm_b200_batch_kernel_count(self.handle, max_nrhs))
+    def kernel_count(self) -> int:
+        """Kernels one apply / graph replay launches for the columns last given."""
+        return int(_lib.hmvm_lib().hmvm_b200_batch_kernel_count(self.handle))
+
+    def class_count(self) -> int:
+        return int(_lib.hmvm_lib().hmvm_b200_batch_class_count(self.handle))
+
+    def instance(self, m: int) -> tuple[int, int, int]:
+        """(N, class, row offset within the class's plan) of instance m."""
+        n, c, off = C.c_int32(), C.c_int32(), C.c_int64()
+        _lib.check(_lib.hmvm_lib().hmvm_b200_batch_instance(self.handle, m, C.byref(n), C.byref(c), C.byref(off)),
+                   "batch instance")
+        return n.value, c.value, off.value
 
     def close(self) -> None:
         if self._h:

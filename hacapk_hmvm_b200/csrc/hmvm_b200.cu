@@ -1209,59 +1209,76 @@ int hmvm_b200_version(void) { return 2; }
 }  // extern "C"
 
 // ---- batches of independent H-matrices ----------------------------------------
-// A batch is planned as one block-diagonal H-matrix: instance m's leaves are
-// shifted by off[m] in rows and columns, so one persistent launch per stage
-// runs every instance's items, load-balanced together.
+// Instances are grouped into classes by the number of right-hand sides they
+// will be applied with (width 1, 2, 4 or 8 per pass, and the number of 8-wide
+// passes above 8).  Each class is planned as ONE block-diagonal H-matrix:
+// instance m's leaves are shifted by its offset in rows and columns, so each
+// stage of a class is one persistent launch over all its instances' items,
+// load-balanced together.  One apply (or one graph replay) runs the classes
+// one after the other.
 
-struct hmvm_batch {
+struct BatchClass {
   hmvm_plan* plan = nullptr;
-  int32_t count = 0;
-  int64_t ntot = 0;
-  int32_t nmax = 0;
+  int width = 1;                 // rhs per pass (the plan's nrhs_max)
+  std::vector<int32_t> members;  // instance ids
   std::vector<int32_t> n;
   std::vector<int64_t> off;
-  std::vector<BatchIO> io;  // the table last uploaded
+  int64_t ntot = 0;
+  int32_t nmax = 0;
+  std::vector<BatchIO> io;
   BatchIO* d_io = nullptr;
-  void* d_xcat = nullptr;   // single-vector plans: concatenated x (ntot + 16)
-  void* d_ycat = nullptr;   // concatenated Y, column r at d_ycat + r * ntot
+  void* d_xcat = nullptr;  // width 1: concatenated x (ntot + 16)
+  void* d_ycat = nullptr;  // concatenated Y, column r at d_ycat + r * ntot
+};
+
+struct hmvm_batch {
+  int32_t count = 0;
+  std::vector<int32_t> cls_of;  // class of each instance
+  std::vector<int32_t> pos_of;  // position within its class
+  std::vector<BatchClass> cls;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  int device = 0;
 };
 
 namespace {
+
+// Class key of an instance applied with k right-hand sides: the pass width
+// (1, 2, 4 or 8; a pass of width w runs ceil(k / 8) times when k > 8).
+int batch_width(int32_t k) {
+  if (k <= 1) return 1;
+  if (k <= 2) return 2;
+  if (k <= 4) return 4;
+  return 8;
+}
 
 void free_batch(hmvm_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
   b->graph = nullptr;
-  for (void* q : {(void*)b->d_io, b->d_xcat, b->d_ycat})
-    if (q) cudaFree(q);
-  b->d_io = nullptr;
-  b->d_xcat = b->d_ycat = nullptr;
-  if (b->plan) hmvm_b200_plan_destroy(b->plan);
-  b->plan = nullptr;
+  for (BatchClass& c : b->cls) {
+    for (void* q : {(void*)c.d_io, c.d_xcat, c.d_ycat})
+      if (q) cudaFree(q);
+    c.d_io = nullptr;
+    c.d_xcat = c.d_ycat = nullptr;
+    if (c.plan) hmvm_b200_plan_destroy(c.plan);
+    c.plan = nullptr;
+  }
 }
 
-int batch_create(const std::vector<LeafTable>& tabs, bool is_float, const hmvm_plan_opts* opts, hmvm_batch** out) {
-  if (!out) return set_error(HMVM_EINVAL, "output handle is NULL");
-  *out = nullptr;
-  const int32_t count = (int32_t)tabs.size();
-  if (count <= 0) return set_error(HMVM_EINVAL, "a batch needs at least one matrix");
+int class_create(BatchClass& c, const std::vector<LeafTable>& tabs, bool is_float, hmvm_plan_opts o) {
   int64_t ntot = 0, nlf = 0, len = 0;
   int32_t ktmax = 0, nmax = 0;
-  for (const LeafTable& t : tabs) {
-    std::string msg;
-    int rc = validate_leaves(t, msg);
-    if (rc) return set_error(rc, "batch instance: " + msg);
+  for (int32_t m : c.members) {
+    const LeafTable& t = tabs[m];
     ntot += t.nd;
     nlf += t.nlf;
     len += t.len;
     ktmax = std::max(ktmax, t.ktmax);
     nmax = std::max(nmax, t.nd);
   }
-  if (ntot > INT32_MAX - 64 || nlf > INT32_MAX) return set_error(HMVM_ERANGE, "batch too large for one plan");
-  // the block-diagonal leaf table
+  if (ntot > INT32_MAX - 64 || nlf > INT32_MAX) return set_error(HMVM_ERANGE, "batch class too large for one plan");
   std::vector<int32_t> ltmtx, kt, ndl, ndt, sl, st;
   std::vector<int64_t> a1, a2;
   std::vector<unsigned char> rowmat;
@@ -1274,15 +1291,11 @@ int batch_create(const std::vector<LeafTable>& tabs, bool is_float, const hmvm_p
   } catch (const std::bad_alloc&) {
     return set_error(HMVM_ENOMEM, "host allocation failed while merging the batch");
   }
-  hmvm_batch* b = new (std::nothrow) hmvm_batch();
-  if (!b) return set_error(HMVM_ENOMEM, "host allocation failed");
-  b->count = count;
-  b->ntot = ntot;
-  b->nmax = nmax;
   int64_t roff = 0, loff = 0;
-  for (const LeafTable& t : tabs) {
-    b->n.push_back(t.nd);
-    b->off.push_back(roff);
+  for (int32_t m : c.members) {
+    const LeafTable& t = tabs[m];
+    c.n.push_back(t.nd);
+    c.off.push_back(roff);
     for (int32_t i = 0; i < t.nlf; i++) {
       ltmtx.push_back(t.ltmtx[i]);
       kt.push_back(t.kt[i]);
@@ -1297,45 +1310,90 @@ int batch_create(const std::vector<LeafTable>& tabs, bool is_float, const hmvm_p
     roff += t.nd;
     loff += t.len;
   }
-  LeafTable m;
-  m.nd = (int32_t)ntot;
-  m.nlf = (int32_t)nlf;
-  m.ktmax = ktmax;
-  m.len = len;
-  m.ltmtx = ltmtx.data();
-  m.kt = kt.data();
-  m.ndl = ndl.data();
-  m.ndt = ndt.data();
-  m.nstrtl = sl.data();
-  m.nstrtt = st.data();
-  m.a1_64 = a1.data();
-  m.a2_64 = a2.data();
-  m.rowmat = rowmat.data();
-  m.rowmat_is_float = is_float;
-  int rc = create_plan(m, opts, &b->plan);
-  if (rc) {
-    delete b;
-    return rc;
-  }
-  hmvm_plan* p = b->plan;
+  c.ntot = ntot;
+  c.nmax = nmax;
+  LeafTable mt;
+  mt.nd = (int32_t)ntot;
+  mt.nlf = (int32_t)nlf;
+  mt.ktmax = ktmax;
+  mt.len = len;
+  mt.ltmtx = ltmtx.data();
+  mt.kt = kt.data();
+  mt.ndl = ndl.data();
+  mt.ndt = ndt.data();
+  mt.nstrtl = sl.data();
+  mt.nstrtt = st.data();
+  mt.a1_64 = a1.data();
+  mt.a2_64 = a2.data();
+  mt.rowmat = rowmat.data();
+  mt.rowmat_is_float = is_float;
+  o.nrhs_max = c.width;
+  int rc = create_plan(mt, &o, &c.plan);
+  if (rc) return rc;
+  hmvm_plan* p = c.plan;
   DeviceGuard g(p->device);
-  const size_t ncols = (size_t)std::max(1, p->nrhs_max);
-  cudaError_t e = cudaMalloc(&b->d_io, sizeof(BatchIO) * (size_t)count);
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_ycat, (size_t)(ntot + 16) * ncols * p->elem);
-  if (e == cudaSuccess && p->nrhs_max <= 1) {
-    e = cudaMalloc(&b->d_xcat, (size_t)(ntot + 16) * p->elem);
-    if (e == cudaSuccess) e = cudaMemset(b->d_xcat, 0, (size_t)(ntot + 16) * p->elem);
+  const size_t ncols = (size_t)c.width;
+  cudaError_t e = cudaMalloc(&c.d_io, sizeof(BatchIO) * c.members.size());
+  if (e == cudaSuccess) e = cudaMalloc(&c.d_ycat, (size_t)(ntot + 16) * ncols * p->elem);
+  if (e == cudaSuccess && c.width == 1) {
+    e = cudaMalloc(&c.d_xcat, (size_t)(ntot + 16) * p->elem);
+    if (e == cudaSuccess) e = cudaMemset(c.d_xcat, 0, (size_t)(ntot + 16) * p->elem);
   }
   // the packed multi-RHS inputs: the batch packing kernels never write the pad rows
   if (e == cudaSuccess && p->d_xm64) e = cudaMemset(p->d_xm64, 0, (size_t)(ntot + 16) * ncols * sizeof(double));
   if (e == cudaSuccess && p->d_xm32) e = cudaMemset(p->d_xm32, 0, (size_t)(ntot + 16) * ncols * sizeof(float));
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
-  if (e != cudaSuccess) {
-    rc = cuda_fail(e, "batch buffers");
-    free_batch(b);
-    delete b;
-    return rc;
+  if (e != cudaSuccess) return cuda_fail(e, "batch buffers");
+  return HMVM_OK;
+}
+
+int batch_create(const std::vector<LeafTable>& tabs, bool is_float, const hmvm_plan_opts* opts,
+                 const int32_t* nrhs, hmvm_batch** out) {
+  if (!out) return set_error(HMVM_EINVAL, "output handle is NULL");
+  *out = nullptr;
+  const int32_t count = (int32_t)tabs.size();
+  if (count <= 0) return set_error(HMVM_EINVAL, "a batch needs at least one matrix");
+  hmvm_plan_opts o;
+  hmvm_b200_default_opts(&o);
+  if (opts) o = *opts;
+  for (int32_t m = 0; m < count; m++) {
+    std::string msg;
+    int rc = validate_leaves(tabs[m], msg);
+    if (rc) return set_error(rc, "batch instance " + std::to_string(m) + ": " + msg);
+    if (nrhs && nrhs[m] < 0) return set_error(HMVM_EINVAL, "nrhs < 0");
   }
+  hmvm_batch* b = new (std::nothrow) hmvm_batch();
+  if (!b) return set_error(HMVM_ENOMEM, "host allocation failed");
+  b->count = count;
+  b->cls_of.assign(count, -1);
+  b->pos_of.assign(count, -1);
+  // classes in the order of their widths: 1, 2, 4, 8
+  const int default_w = batch_width(std::min(std::max(o.nrhs_max, 1), kMaxNrhsPass));
+  for (int w : {1, 2, 4, 8}) {
+    BatchClass c;
+    c.width = w;
+    for (int32_t m = 0; m < count; m++) {
+      const int wm = nrhs ? batch_width(nrhs[m]) : default_w;
+      if (wm == w) {
+        b->cls_of[m] = (int32_t)b->cls.size();
+        b->pos_of[m] = (int32_t)c.members.size();
+        c.members.push_back(m);
+      }
+    }
+    if (!c.members.empty()) b->cls.push_back(std::move(c));
+  }
+  for (BatchClass& c : b->cls) {
+    int rc = class_create(c, tabs, is_float, o);
+    if (rc) {
+      {
+        DeviceGuard g(b->cls.front().plan ? b->cls.front().plan->device : 0);
+        free_batch(b);
+      }
+      delete b;
+      return rc;
+    }
+  }
+  b->device = b->cls.front().plan->device;
   *out = b;
   return HMVM_OK;
 }
@@ -1344,73 +1402,84 @@ int batch_set_io(hmvm_batch* b, const void* const* X, const int64_t* ldx, void* 
                  const int32_t* nrhs) {
   if (!b) return set_error(HMVM_EINVAL, "batch is NULL");
   if (!X || !ldx || !Y || !ldy || !nrhs) return set_error(HMVM_EINVAL, "NULL argument array");
-  std::vector<BatchIO> io((size_t)b->count);
+  std::vector<std::vector<BatchIO>> io(b->cls.size());
+  for (size_t k = 0; k < b->cls.size(); k++) io[k].resize(b->cls[k].members.size());
   for (int32_t m = 0; m < b->count; m++) {
-    BatchIO& q = io[m];
+    const BatchClass& c = b->cls[b->cls_of[m]];
+    BatchIO& q = io[b->cls_of[m]][b->pos_of[m]];
     q.X = X[m];
     q.ldx = ldx[m];
     q.Y = Y[m];
     q.ldy = ldy[m];
-    q.off = b->off[m];
-    q.n = b->n[m];
+    q.off = c.off[b->pos_of[m]];
+    q.n = c.n[b->pos_of[m]];
     q.nrhs = nrhs[m];
     if (q.nrhs < 0) return set_error(HMVM_EINVAL, "instance " + std::to_string(m) + ": nrhs < 0");
     if (q.n == 0 || q.nrhs == 0) continue;
     if (!q.X || !q.Y) return set_error(HMVM_EINVAL, "instance " + std::to_string(m) + ": X or Y is NULL");
     if (q.ldx < q.n || q.ldy < q.n) return set_error(HMVM_EINVAL, "instance " + std::to_string(m) + ": ld < N");
   }
-  b->io.swap(io);
+  for (size_t k = 0; k < b->cls.size(); k++) b->cls[k].io.swap(io[k]);
   return HMVM_OK;
 }
 
-int batch_max_nrhs(const hmvm_batch* b) {
+int class_max_nrhs(const BatchClass& c) {
   int mx = 0;
-  for (const BatchIO& q : b->io) mx = std::max(mx, (int)q.nrhs);
+  for (const BatchIO& q : c.io) mx = std::max(mx, (int)q.nrhs);
   return mx;
 }
 
 template <typename T>
-int batch_run_t(hmvm_batch* b, cudaStream_t st) {
-  hmvm_plan* p = b->plan;
-  const int mx = batch_max_nrhs(b);
-  const unsigned cnt = (unsigned)b->count;
+int class_run_t(BatchClass& c, cudaStream_t st) {
+  hmvm_plan* p = c.plan;
+  const int mx = class_max_nrhs(c);
+  const unsigned cnt = (unsigned)c.members.size();
   auto blocks = [&](int64_t work) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 64)); };
   if (p->nrhs_max <= 1) {
-    for (int c = 0; c < mx; c++) {
-      hmvm_batch_pack1_kernel<T><<<dim3(blocks(b->nmax), cnt), 256, 0, st>>>(b->d_io, c, static_cast<T*>(b->d_xcat));
+    for (int col = 0; col < mx; col++) {
+      hmvm_batch_pack1_kernel<T><<<dim3(blocks(c.nmax), cnt), 256, 0, st>>>(c.d_io, col, static_cast<T*>(c.d_xcat));
       HMVM_CUDA_TRY(cudaGetLastError(), "batch packing launch");
-      int rc = apply_impl(p, b->d_xcat, b->d_ycat, st);
+      int rc = apply_impl(p, c.d_xcat, c.d_ycat, st);
       if (rc) return rc;
-      hmvm_batch_unpack_kernel<T><<<dim3(blocks(b->nmax), cnt), 256, 0, st>>>(
-          b->d_io, c, 1, static_cast<const T*>(b->d_ycat), b->ntot);
+      hmvm_batch_unpack_kernel<T><<<dim3(blocks(c.nmax), cnt), 256, 0, st>>>(
+          c.d_io, col, 1, static_cast<const T*>(c.d_ycat), c.ntot);
       HMVM_CUDA_TRY(cudaGetLastError(), "batch unpacking launch");
     }
     return HMVM_OK;
   }
-  for (int c0 = 0; c0 < mx;) {
-    const int w = multi_pass_width(p->nrhs_max, mx - c0);
-    const dim3 grid(blocks((int64_t)b->nmax * w), cnt);
+  const int w = c.width;  // every pass of a class has the class width
+  for (int c0 = 0; c0 < mx; c0 += w) {
+    const dim3 grid(blocks((int64_t)c.nmax * w), cnt);
     double* x64 = p->d_xm64;
     float* x32 = p->d_xm32;
     switch (w) {
-      case 2: hmvm_batch_packm_kernel<T, 2><<<grid, 256, 0, st>>>(b->d_io, c0, x64, x32); break;
-      case 4: hmvm_batch_packm_kernel<T, 4><<<grid, 256, 0, st>>>(b->d_io, c0, x64, x32); break;
-      default: hmvm_batch_packm_kernel<T, 8><<<grid, 256, 0, st>>>(b->d_io, c0, x64, x32); break;
+      case 2: hmvm_batch_packm_kernel<T, 2><<<grid, 256, 0, st>>>(c.d_io, c0, x64, x32); break;
+      case 4: hmvm_batch_packm_kernel<T, 4><<<grid, 256, 0, st>>>(c.d_io, c0, x64, x32); break;
+      default: hmvm_batch_packm_kernel<T, 8><<<grid, 256, 0, st>>>(c.d_io, c0, x64, x32); break;
     }
     HMVM_CUDA_TRY(cudaGetLastError(), "batch packing launch");
-    int rc = launch_multi_stages(p, b->d_ycat, b->ntot, w, w, st);
+    int rc = launch_multi_stages(p, c.d_ycat, c.ntot, w, w, st);
     if (rc) return rc;
-    hmvm_batch_unpack_kernel<T><<<grid, 256, 0, st>>>(b->d_io, c0, w, static_cast<const T*>(b->d_ycat), b->ntot);
+    hmvm_batch_unpack_kernel<T><<<grid, 256, 0, st>>>(c.d_io, c0, w, static_cast<const T*>(c.d_ycat), c.ntot);
     HMVM_CUDA_TRY(cudaGetLastError(), "batch unpacking launch");
-    c0 += w;
   }
   return HMVM_OK;
 }
 
 int batch_run(hmvm_batch* b, cudaStream_t st) {
-  HMVM_CUDA_TRY(cudaMemcpyAsync(b->d_io, b->io.data(), sizeof(BatchIO) * b->io.size(), cudaMemcpyHostToDevice, st),
-                "batch table upload");
-  return b->plan->precision == HMVM_FP32 ? batch_run_t<float>(b, st) : batch_run_t<double>(b, st);
+  for (BatchClass& c : b->cls) {
+    if (class_max_nrhs(c) == 0) continue;
+    HMVM_CUDA_TRY(cudaMemcpyAsync(c.d_io, c.io.data(), sizeof(BatchIO) * c.io.size(), cudaMemcpyHostToDevice, st),
+                  "batch table upload");
+    int rc = c.plan->precision == HMVM_FP32 ? class_run_t<float>(c, st) : class_run_t<double>(c, st);
+    if (rc) return rc;
+  }
+  return HMVM_OK;
+}
+
+int batch_create_tables(std::vector<LeafTable>& t, bool is_float, const hmvm_plan_opts* opts, const int32_t* nrhs,
+                        hmvm_batch** out) {
+  return batch_create(t, is_float, opts, nrhs, out);
 }
 
 }  // namespace
@@ -1418,15 +1487,15 @@ int batch_run(hmvm_batch* b, cudaStream_t st) {
 extern "C" {
 
 int hmvm_b200_batch_create64_d(const hmvm_leaves64* mats, int32_t count, const hmvm_plan_opts* opts,
-                               hmvm_batch** out) {
+                               const int32_t* nrhs, hmvm_batch** out) {
   if (!mats || count <= 0) return set_error(HMVM_EINVAL, "no matrices");
   std::vector<LeafTable> t((size_t)count);
   for (int32_t m = 0; m < count; m++) table_from_leaves64(&mats[m], false, t[m]);
-  return batch_create(t, false, opts, out);
+  return batch_create_tables(t, false, opts, nrhs, out);
 }
 
 int hmvm_b200_batch_create64_f(const hmvm_leaves64* mats, int32_t count, const hmvm_plan_opts* opts,
-                               hmvm_batch** out) {
+                               const int32_t* nrhs, hmvm_batch** out) {
   if (!mats || count <= 0) return set_error(HMVM_EINVAL, "no matrices");
   hmvm_plan_opts o;
   hmvm_b200_default_opts(&o);
@@ -1434,11 +1503,11 @@ int hmvm_b200_batch_create64_f(const hmvm_leaves64* mats, int32_t count, const h
   o.precision = HMVM_FP32;
   std::vector<LeafTable> t((size_t)count);
   for (int32_t m = 0; m < count; m++) table_from_leaves64(&mats[m], true, t[m]);
-  return batch_create(t, true, &o, out);
+  return batch_create_tables(t, true, &o, nrhs, out);
 }
 
 int hmvm_b200_batch_create_d(const hmvm_matrix2_d* mats, int32_t count, const hmvm_plan_opts* opts,
-                             hmvm_batch** out) {
+                             const int32_t* nrhs, hmvm_batch** out) {
   if (!mats || count <= 0) return set_error(HMVM_EINVAL, "no matrices");
   std::vector<LeafTable> t((size_t)count);
   for (int32_t m = 0; m < count; m++) {
@@ -1446,35 +1515,64 @@ int hmvm_b200_batch_create_d(const hmvm_matrix2_d* mats, int32_t count, const hm
     make_table_from_matrix2(q->nd, q->nlf, q->ktmax, q->len, q->ltmtx, q->kt, q->ndl, q->ndt, q->nstrtl, q->nstrtt,
                             q->a1, q->a2, q->rowmat, false, t[m]);
   }
-  return batch_create(t, false, opts, out);
+  return batch_create_tables(t, false, opts, nrhs, out);
 }
 
 void hmvm_b200_batch_destroy(hmvm_batch* b) {
   if (!b) return;
-  if (b->plan) {
-    DeviceGuard g(b->plan->device);
+  {
+    DeviceGuard g(b->device);
     free_batch(b);
   }
   delete b;
 }
 
 int hmvm_b200_batch_get_info(const hmvm_batch* b, hmvm_plan_info* info) {
-  if (!b) return set_error(HMVM_EINVAL, "batch is NULL");
-  return hmvm_b200_plan_get_info(b->plan, info);
-}
-
-int hmvm_b200_batch_instance(const hmvm_batch* b, int32_t m, int32_t* n, int64_t* offset) {
-  if (!b || m < 0 || m >= b->count) return set_error(HMVM_EINVAL, "no such instance");
-  if (n) *n = b->n[m];
-  if (offset) *offset = b->off[m];
+  if (!b || !info) return set_error(HMVM_EINVAL, "NULL argument");
+  int rc = hmvm_b200_plan_get_info(b->cls.front().plan, info);
+  if (rc) return rc;
+  // sums over the classes
+  for (size_t k = 1; k < b->cls.size(); k++) {
+    hmvm_plan_info q;
+    rc = hmvm_b200_plan_get_info(b->cls[k].plan, &q);
+    if (rc) return rc;
+    info->nd += q.nd;
+    info->nlf += q.nlf;
+    info->n_lowrank += q.n_lowrank;
+    info->n_dense += q.n_dense;
+    info->algorithmic_bytes += q.algorithmic_bytes;
+    info->device_bytes += q.device_bytes;
+    info->t_len += q.t_len;
+    info->stage1_tiles += q.stage1_tiles;
+    info->stage2_tiles += q.stage2_tiles;
+    info->split_rows += q.split_rows;
+    info->kernels_per_apply += q.kernels_per_apply;
+    info->flops += q.flops;
+    info->stage1_bytes += q.stage1_bytes;
+    info->stage2_bytes += q.stage2_bytes;
+    info->cols_fp32 += q.cols_fp32;
+    info->cols_lr16 += q.cols_lr16;
+    info->cols_fp8 += q.cols_fp8;
+  }
   return HMVM_OK;
 }
+
+int hmvm_b200_batch_instance(const hmvm_batch* b, int32_t m, int32_t* n, int32_t* cls, int64_t* offset) {
+  if (!b || m < 0 || m >= b->count) return set_error(HMVM_EINVAL, "no such instance");
+  const BatchClass& c = b->cls[b->cls_of[m]];
+  if (n) *n = c.n[b->pos_of[m]];
+  if (cls) *cls = b->cls_of[m];
+  if (offset) *offset = c.off[b->pos_of[m]];
+  return HMVM_OK;
+}
+
+int hmvm_b200_batch_class_count(const hmvm_batch* b) { return b ? (int)b->cls.size() : 0; }
 
 int hmvm_b200_batch_apply(hmvm_batch* b, const void* const* X, const int64_t* ldx, void* const* Y,
                           const int64_t* ldy, const int32_t* nrhs, void* stream) {
   int rc = batch_set_io(b, X, ldx, Y, ldy, nrhs);
   if (rc) return rc;
-  DeviceGuard g(b->plan->device);
+  DeviceGuard g(b->device);
   if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the batch's device");
   return batch_run(b, static_cast<cudaStream_t>(stream));
 }
@@ -1483,9 +1581,10 @@ int hmvm_b200_batch_capture(hmvm_batch* b, const void* const* X, const int64_t* 
                             const int64_t* ldy, const int32_t* nrhs) {
   int rc = batch_set_io(b, X, ldx, Y, ldy, nrhs);
   if (rc) return rc;
-  DeviceGuard g(b->plan->device);
+  DeviceGuard g(b->device);
   if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the batch's device");
-  if (b->plan->profiling) return set_error(HMVM_EINVAL, "profiling is on; a captured batch cannot record events");
+  for (const BatchClass& c : b->cls)
+    if (c.plan->profiling) return set_error(HMVM_EINVAL, "profiling is on; a captured batch cannot record events");
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
@@ -1518,7 +1617,7 @@ int hmvm_b200_batch_capture(hmvm_batch* b, const void* const* X, const int64_t* 
 int hmvm_b200_batch_launch(hmvm_batch* b, void* stream) {
   if (!b) return set_error(HMVM_EINVAL, "batch is NULL");
   if (!b->exec) return set_error(HMVM_EINVAL, "nothing captured: call hmvm_b200_batch_capture first");
-  DeviceGuard g(b->plan->device);
+  DeviceGuard g(b->device);
   if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the batch's device");
   HMVM_CUDA_TRY(cudaGraphLaunch(b->exec, static_cast<cudaStream_t>(stream)), "cudaGraphLaunch");
   return HMVM_OK;
@@ -1526,17 +1625,28 @@ int hmvm_b200_batch_launch(hmvm_batch* b, void* stream) {
 
 int hmvm_b200_batch_status(hmvm_batch* b) {
   if (!b) return set_error(HMVM_EINVAL, "batch is NULL");
-  return hmvm_b200_plan_status(b->plan);
+  for (BatchClass& c : b->cls) {
+    int rc = hmvm_b200_plan_status(c.plan);
+    if (rc) return rc;
+  }
+  return HMVM_OK;
 }
 
-int hmvm_b200_batch_kernel_count(const hmvm_batch* b, int32_t max_nrhs) {
-  if (!b || max_nrhs <= 0) return 0;
-  const hmvm_plan* p = b->plan;
-  if (p->nrhs_max <= 1) return max_nrhs * (2 + hmvm_b200_plan_kernel_count(p));  // pack, stages, unpack
-  int passes = 0;
-  for (int c0 = 0; c0 < max_nrhs; passes++) c0 += multi_pass_width(p->nrhs_max, max_nrhs - c0);
-  // per pass: pack, the stage kernels, unpack
-  return passes * (2 + (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1 + (p->n_red2 > 0));
+int hmvm_b200_batch_kernel_count(const hmvm_batch* b) {
+  if (!b) return 0;
+  int total = 0;
+  for (const BatchClass& c : b->cls) {
+    const int mx = class_max_nrhs(c);
+    if (mx == 0) continue;
+    const hmvm_plan* p = c.plan;
+    if (p->nrhs_max <= 1) {
+      total += mx * (2 + hmvm_b200_plan_kernel_count(p));  // pack, stages, unpack
+    } else {
+      const int passes = (mx + c.width - 1) / c.width;
+      total += passes * (2 + (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1 + (p->n_red2 > 0));
+    }
+  }
+  return total;
 }
 
 }  // extern "C"

@@ -203,25 +203,31 @@ int hmvm_b200_apply_multi_host(hmvm_plan *plan, const void *X_host, int64_t ldx,
 int hmvm_b200_plan_multi_kernel_count(const hmvm_plan *plan, int32_t nrhs);
 
 /* ---- batches of independent H-matrices -------------------------------------
- * Many H-matrices of uneven N planned together: the batch is one
- * block-diagonal plan (instance m owns rows/columns [offset_m, offset_m + N_m)
- * of the concatenated index space), so each stage is one persistent launch
- * over every instance's items.  The reference has no batched entry point.
- * Instances share the plan options (precision, nrhs_max, ...). */
+ * Many H-matrices of uneven N planned together.  Instances are grouped into
+ * classes by the right-hand sides they will be applied with (nrhs[m] at
+ * creation; NULL = opts->nrhs_max for all): pass width 1, 2, 4 or 8 (more than
+ * 8 columns run several 8-wide passes).  Each class is one block-diagonal plan
+ * (instance m owns rows/columns [offset, offset + N_m) of its class's
+ * concatenated index space), so each stage of a class is one persistent launch
+ * over all its instances' items.  The reference has no batched entry point.
+ * Instances share the plan options other than nrhs_max. */
 typedef struct hmvm_batch hmvm_batch;
 int hmvm_b200_batch_create64_d(const hmvm_leaves64 *mats, int32_t count, const hmvm_plan_opts *opts,
-                               hmvm_batch **batch);
+                               const int32_t *nrhs, hmvm_batch **batch);
 int hmvm_b200_batch_create64_f(const hmvm_leaves64 *mats, int32_t count, const hmvm_plan_opts *opts,
-                               hmvm_batch **batch);
+                               const int32_t *nrhs, hmvm_batch **batch);
 int hmvm_b200_batch_create_d(const hmvm_matrix2_d *mats, int32_t count, const hmvm_plan_opts *opts,
-                             hmvm_batch **batch);
+                             const int32_t *nrhs, hmvm_batch **batch);
 void hmvm_b200_batch_destroy(hmvm_batch *batch);
-int hmvm_b200_batch_get_info(const hmvm_batch *batch, hmvm_plan_info *info); /* of the block-diagonal plan */
-int hmvm_b200_batch_instance(const hmvm_batch *batch, int32_t m, int32_t *n, int64_t *offset);
+/* Sums over the classes' plans (nd, leaves, bytes, tiles, ...); the other
+ * fields are those of the first class. */
+int hmvm_b200_batch_get_info(const hmvm_batch *batch, hmvm_plan_info *info);
+int hmvm_b200_batch_instance(const hmvm_batch *batch, int32_t m, int32_t *n, int32_t *cls, int64_t *offset);
+int hmvm_b200_batch_class_count(const hmvm_batch *batch);
 /* Y_m = H_m X_m for every instance m < count: X[m], Y[m] device pointers to
  * column-major N_m x nrhs[m] blocks with leading dimensions ldx[m], ldy[m]
- * (arrays of `count` entries in host memory; nrhs[m] may differ, 0 skips the
- * instance).  Passes of up to nrhs_max columns cover the largest nrhs[m]. */
+ * (arrays of `count` entries in host memory; 0 columns skips the instance; an
+ * instance given more columns than its class width runs more passes). */
 int hmvm_b200_batch_apply(hmvm_batch *batch, const void *const *X, const int64_t *ldx, void *const *Y,
                           const int64_t *ldy, const int32_t *nrhs, void *stream);
 /* Record the launches of hmvm_b200_batch_apply for these buffers into a CUDA
@@ -231,8 +237,8 @@ int hmvm_b200_batch_capture(hmvm_batch *batch, const void *const *X, const int64
                             const int64_t *ldy, const int32_t *nrhs);
 int hmvm_b200_batch_launch(hmvm_batch *batch, void *stream);
 int hmvm_b200_batch_status(hmvm_batch *batch);
-/* Kernels one apply (or one graph replay) launches when the largest nrhs is max_nrhs. */
-int hmvm_b200_batch_kernel_count(const hmvm_batch *batch, int32_t max_nrhs);
+/* Kernels one apply (or one graph replay) launches for the columns last given. */
+int hmvm_b200_batch_kernel_count(const hmvm_batch *batch);
 
 /* Capacity of the scratch array used by hmvm_b200_apply_noalloc: 16 MiB. */
 #define HMVM_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
