@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--kernel", type=int, default=-1, help="0: register-streaming, 1: TMA-ring (default)")
     ap.add_argument("--nrhs", type=int, default=1, help="right-hand sides per step (multi-RHS HMVM when > 1)")
+    ap.add_argument("--x-dist", default="uniform", choices=["uniform", "normal"], help="entries of x / X")
     ap.add_argument("--lr-format", default="fp16", choices=["fp16", "bf16"], help="mixed plans: 16-bit factor format")
     ap.add_argument("--workload", default="single", choices=["single", "batch"],
                     help="batch: many independent H-matrices of uneven N in one CUDA-graph replay")
@@ -84,7 +85,8 @@ class CpuReference:
         self._i32 = [np.ascontiguousarray(getattr(hm, n), dtype=np.int32)
                      for n in ("ltmtx", "kt", "ndl", "ndt", "nstrtl", "nstrtt", "a1", "a2")]
         self._rm = hm.rowmat
-        if os.path.exists(REF_SO):
+        # the reference's matrix2 holds int offsets (hacapk.h:28,31): beyond 2^31 elements only the port runs
+        if os.path.exists(REF_SO) and hm.len <= np.iinfo(np.int32).max:
             self.kind = "reference"
             lib = C.CDLL(REF_SO)
             lib.ref_wrap2.restype = C.c_void_p
@@ -250,7 +252,8 @@ def run_reference(a, rank):
     if rank != 0:
         return
     hm = build_matrix(a)
-    x = np.random.default_rng(a.seed).uniform(-1.0, 1.0, hm.nd)
+    rng = np.random.default_rng(a.seed)
+    x = rng.uniform(-1.0, 1.0, hm.nd) if a.x_dist == "uniform" else rng.standard_normal(hm.nd)
     cpu = CpuReference(hm)
     y = np.empty(hm.nd)
     for _ in range(max(a.warmup, 1)):
@@ -270,7 +273,7 @@ def run_reference(a, rank):
         "impl": "reference", "metric": "HMVM/s", "value": value, "unit": "HMVM/s", "n_gpus": a.gpus,
         "steps": steps, "warmup": a.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded HACApK-rule H-matrix; x uniform[-1,1])",
+        "data": f"synthetic (seeded HACApK-rule H-matrix; x {'uniform[-1,1]' if a.x_dist == 'uniform' else 'standard normal'})",
         "config": workload_config(a, hm),
         "gbytes_per_s": hm.algorithmic_bytes(8) / (dt / steps) / 1e9,
         "cpu_baseline": {"value": value, "unit": "HMVM/s", "cores": cpu.threads, "kind": cpu.kind,
@@ -294,11 +297,13 @@ def run_b200(a, rank, world, local_rank):
         dist = dist_mod
     hm = build_matrix(a)
     rng = np.random.default_rng(a.seed)
-    X = rng.uniform(-1.0, 1.0, (a.nrhs, hm.nd))
+    X = rng.uniform(-1.0, 1.0, (a.nrhs, hm.nd)) if a.x_dist == "uniform" else rng.standard_normal((a.nrhs, hm.nd))
     x = X[0]
     t0 = time.perf_counter()
     plan = Plan(hm, a.precision, device=local_rank, stage1_cfg=a.stage1_cfg, stage2_cfg=a.stage2_cfg,
-                ctas_per_sm=a.ctas_per_sm, kernel=a.kernel, nrhs_max=min(a.nrhs, 8),
+                ctas_per_sm=a.ctas_per_sm, kernel=a.kernel,
+                # mixed plans take 16 right-hand sides per pass on the tensor cores
+                nrhs_max=16 if (a.precision == "mixed" and a.nrhs >= 16) else min(a.nrhs, 8),
                 mixed_lr_format=a.lr_format if a.precision == "mixed" else None)
     setup_s = time.perf_counter() - t0
     info = plan.info()
@@ -405,7 +410,7 @@ def run_b200(a, rank, world, local_rank):
     alg_bytes = info["algorithmic_bytes"] * passes + 2 * hm.nd * elem_xy * (a.nrhs - passes)
     kname = {0: "hmvm_tile_kernel", 1: "hmvm_stream_kernel", 2: "hmvm_mixed_kernel"}[info["kernel"]]
     if a.nrhs > 1:
-        kname = "hmvm_multi_kernel"
+        kname = "hmvm_tc_kernel" if (a.precision == "mixed" and a.nrhs >= 16) else "hmvm_multi_kernel"
     roof = {
         "bound": "hbm",
         "kernel": [f"{kname} (V stage)", "hmvm_reduce_kernel (V stage)", f"{kname} (row stage)",
@@ -432,7 +437,7 @@ def run_b200(a, rank, world, local_rank):
             "metric": unit, "value": value, "unit": unit, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": DTYPES[a.precision],
-            "data": "synthetic (seeded HACApK-rule H-matrix; x uniform[-1,1])",
+            "data": f"synthetic (seeded HACApK-rule H-matrix; x {'uniform[-1,1]' if a.x_dist == 'uniform' else 'standard normal'})",
             "config": cfg,
             "gbytes_per_s": alg_bytes / (ms_step * 1e-3) / 1e9,
             "algorithmic_bytes_per_step": alg_bytes,

@@ -56,7 +56,7 @@ def hmvm_sources() -> list[str]:
 
 
 def hmvm_deps() -> list[str]:
-    deps = hmvm_sources() + [os.path.join(CSRC, f) for f in ("kernels.cuh", "kernels_multi.cuh", "layout.hpp", "numfmt.hpp")]
+    deps = hmvm_sources() + [os.path.join(CSRC, f) for f in ("kernels.cuh", "kernels_multi.cuh", "kernels_tc.cuh", "layout.hpp", "numfmt.hpp")]
     deps.append(os.path.join(INCLUDE, "hmvm_b200.h"))
     return deps
 

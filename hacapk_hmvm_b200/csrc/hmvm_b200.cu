@@ -14,7 +14,7 @@
 #include <vector>
 
 #include "hmvm_b200.h"
-#include "kernels_multi.cuh"
+#include "kernels_tc.cuh"
 #include "layout.hpp"
 
 namespace hmvm {
@@ -155,6 +155,12 @@ struct hmvm_plan {
   float* d_xm32 = nullptr;
   void* d_tm = nullptr;
   void* d_pm = nullptr;
+  // tensor-core passes (mixed plans with nrhs_max = 16)
+  bool tc = false;
+  uint16_t* d_xplanes = nullptr;
+  uint16_t* d_tplanes = nullptr;
+  float* d_scal = nullptr;
+  unsigned* d_amax = nullptr;
   void* d_xh = nullptr;  // staging for apply_multi_host
   void* d_yh = nullptr;
   size_t xh_bytes = 0;
@@ -178,7 +184,8 @@ void free_plan_buffers(hmvm_plan* p) {
   p->prof_events.clear();
   void* bufs[] = {p->d_data, p->d_tiles, p->d_segs, p->d_tb1, p->d_tb2,  p->d_out_idx, p->d_red1,
                   p->d_red2, p->d_t,     p->d_p,    p->d_err, p->d_x,    p->d_y,       p->d_x32,
-                  p->d_scale, p->d_xm64, p->d_xm32, p->d_tm,  p->d_pm,   p->d_xh,      p->d_yh};
+                  p->d_scale, p->d_xm64, p->d_xm32, p->d_tm,  p->d_pm,   p->d_xh,      p->d_yh,
+                  p->d_xplanes, p->d_tplanes, p->d_scal, p->d_amax};
   for (void* b : bufs)
     if (b) cudaFree(b);
 }
@@ -218,11 +225,15 @@ int upload(Buf** dst, const void* src, size_t bytes, int64_t* total) {
 int plan_mode(const hmvm_plan* p);
 template <bool VST>
 MultiFn multi_kernel_for(int mode, int nr, int cfg);
+int tc_prepare(const hmvm_plan* p);
 
 // Dynamic shared memory beyond 48 KB must be enabled per kernel.
 template <typename T>
 int prepare_kernels(const hmvm_plan* p) {
-  if (p->nrhs_max > 1) {
+  if (p->tc) {
+    int rc = tc_prepare(p);
+    if (rc) return rc;
+  } else if (p->nrhs_max > 1) {
     const int smem = multi_smem_bytes(kMultiCfgs[kDefaultMultiCfg]);
     for (int nr : {2, 4, 8})
       for (MultiFn f : {multi_kernel_for<true>(plan_mode(p), nr, kDefaultMultiCfg),
@@ -323,6 +334,7 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   p->p_len = L->p_len;
   p->mixed = L->mixed;
   p->nrhs_max = L->nrhs_max;
+  p->tc = L->mixed && L->nrhs_max == kTcNrhs;
   p->mixed_kcode = opts.mixed_lr_format == HMVM_LR_BF16 ? 3 : 2;
   p->cols_fp32 = L->cols_fp32;
   p->cols_lr16 = L->cols_lr16;
@@ -383,6 +395,14 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
         e = cudaMalloc(&p->d_xm32, (size_t)(L->nd + 16) * nr * sizeof(float));
       if (e == cudaSuccess) e = cudaMalloc(&p->d_tm, (size_t)(L->t_len + 16) * nr * p->t_elem);
       if (e == cudaSuccess) e = cudaMalloc(&p->d_pm, (size_t)(L->p_len + 16) * nr * p->p_elem);
+      // t padding slots must read as zero (the tensor-core pass scales by max |t|)
+      if (e == cudaSuccess) e = cudaMemset(p->d_tm, 0, (size_t)(L->t_len + 16) * nr * p->t_elem);
+      if (e == cudaSuccess && p->tc) {
+        e = cudaMalloc(&p->d_xplanes, (size_t)4 * (L->nd + 16) * 16);
+        if (e == cudaSuccess) e = cudaMalloc(&p->d_tplanes, (size_t)4 * (L->t_len + 16) * 16);
+        if (e == cudaSuccess) e = cudaMalloc(&p->d_scal, 64 * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&p->d_amax, 32 * sizeof(unsigned));
+      }
       if (e != cudaSuccess) rc = cuda_fail(e, "multi-RHS buffers");
     }
     if (!rc) {
@@ -558,6 +578,7 @@ void launch_reduce_multi(int nr_inst, const int4* red, int n, const void* pbuf, 
   const TP* pp = static_cast<const TP*>(pbuf);
   TD* dd = static_cast<TD*>(dst);
   switch (nr_inst) {
+    case 16: hmvm_reduce_multi_kernel<TP, TD, 16, VST><<<blocks, 256, 0, st>>>(red, n, pp, dd, ldy, nr); break;
     case 2: hmvm_reduce_multi_kernel<TP, TD, 2, VST><<<blocks, 256, 0, st>>>(red, n, pp, dd, ldy, nr); break;
     case 4: hmvm_reduce_multi_kernel<TP, TD, 4, VST><<<blocks, 256, 0, st>>>(red, n, pp, dd, ldy, nr); break;
     default: hmvm_reduce_multi_kernel<TP, TD, 8, VST><<<blocks, 256, 0, st>>>(red, n, pp, dd, ldy, nr); break;
@@ -649,6 +670,91 @@ int launch_multi_stages(hmvm_plan* p, void* Y, int64_t ldy, int nr, int nr_inst,
   return HMVM_OK;
 }
 
+// ---- tensor-core passes ------------------------------------------------------------
+constexpr int kTcWpb = kTcWarpsPerSm;  // one CTA of 6 warps per SM
+using TcFn = void (*)(TcArgs);
+template <bool VST>
+TcFn tc_kernel_for(bool bf16) {
+  return bf16 ? hmvm_tc_kernel<kTcWpb, 4, 2048, kModeMixedBF16, VST> : hmvm_tc_kernel<kTcWpb, 4, 2048, kModeMixed16, VST>;
+}
+constexpr int tc_smem() { return tc_smem_bytes<kTcWpb, 4, 2048>(); }
+
+int tc_prepare(const hmvm_plan* p) {
+  const bool bf = p->mixed_kcode == 3;
+  for (TcFn f : {tc_kernel_for<true>(bf), tc_kernel_for<false>(bf)})
+    HMVM_CUDA_TRY(cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem()),
+                  "cudaFuncSetAttribute");
+  return HMVM_OK;
+}
+
+// One 16-column pass: pack X, scale and split it into 16-bit planes, V stage,
+// its reduction, t into planes, row stage, its reduction into Y.
+int launch_tc_pass(hmvm_plan* p, const void* X, int64_t ldx, void* Y, int64_t ldy, int nr, cudaStream_t st) {
+  const bool bf = p->mixed_kcode == 3;
+  const int gsm = p->num_sms * 8;  // grid stride (x 256 threads) is a multiple of 16, as the plane kernels need
+  HMVM_CUDA_TRY(cudaMemsetAsync(p->d_amax, 0, 32 * sizeof(unsigned), st), "scale reset");
+  launch_pack<kTcNrhs>(p, X, ldx, nr, st);
+  const int64_t nx = (int64_t)(p->nd + 16) * kTcNrhs, nt = (int64_t)(p->t_len + 16) * kTcNrhs;
+  hmvm_absmax_kernel<<<gsm, 256, 0, st>>>(p->d_xm32, nx, p->d_amax);
+  if (bf) hmvm_tc_planes_kernel<true><<<gsm, 256, 0, st>>>(p->d_xm32, p->nd, 16, p->d_amax, p->d_xplanes, p->d_scal);
+  else hmvm_tc_planes_kernel<false><<<gsm, 256, 0, st>>>(p->d_xm32, p->nd, 16, p->d_amax, p->d_xplanes, p->d_scal);
+  HMVM_CUDA_TRY(cudaGetLastError(), "input planes launch");
+  TcArgs ta;
+  MultiArgs& a = ta.m;
+  a.err = p->d_err;
+  a.tiles = p->d_tiles;
+  a.segs = p->d_segs;
+  a.data = p->d_data;
+  a.x64 = p->d_xm64;
+  a.x32 = p->d_xm32;
+  a.t = p->d_tm;
+  a.y = Y;
+  a.ldy = ldy;
+  a.nr = nr;
+  a.p = p->d_pm;
+  a.out_idx = p->d_out_idx;
+  a.scale = p->d_scale;
+  ta.xplanes = p->d_xplanes;
+  ta.tplanes = p->d_tplanes;
+  ta.xrows = p->nd + 16;
+  ta.trows = p->t_len + 16;
+  ta.scal = p->d_scal;
+  cudaEvent_t* ev = nullptr;
+  if (p->profiling && p->prof_count < kMaxProfiled) {
+    ev = &p->prof_events[kEventsPerApply * (size_t)p->prof_count];
+    p->prof_count++;
+  }
+  if (ev) cudaEventRecord(ev[0], st);
+  if (p->stage1_tiles > 0) {
+    a.team_begin = p->d_tb1;
+    a.nteams = p->stage1_teams;
+    tc_kernel_for<true>(bf)<<<(p->stage1_teams + kTcWpb - 1) / kTcWpb, 32 * kTcWpb, tc_smem(), st>>>(ta);
+    HMVM_CUDA_TRY(cudaGetLastError(), "tensor-core V-stage launch");
+  }
+  if (ev) cudaEventRecord(ev[1], st);
+  if (p->n_red1 > 0)
+    launch_reduce_multi<double, float, true>(kTcNrhs, p->d_red1, p->n_red1, p->d_pm, p->d_tm, 0, nr, st);
+  hmvm_absmax_kernel<<<gsm, 256, 0, st>>>(static_cast<const float*>(p->d_tm), nt, p->d_amax + 16);
+  if (bf)
+    hmvm_tc_planes_kernel<true><<<gsm, 256, 0, st>>>(static_cast<const float*>(p->d_tm), (int)p->t_len, 16,
+                                                    p->d_amax + 16, p->d_tplanes, p->d_scal + 32);
+  else
+    hmvm_tc_planes_kernel<false><<<gsm, 256, 0, st>>>(static_cast<const float*>(p->d_tm), (int)p->t_len, 16,
+                                                     p->d_amax + 16, p->d_tplanes, p->d_scal + 32);
+  HMVM_CUDA_TRY(cudaGetLastError(), "t planes launch");
+  if (ev) cudaEventRecord(ev[2], st);
+  a.team_begin = p->d_tb2;
+  a.nteams = p->stage2_teams;
+  tc_kernel_for<false>(bf)<<<(p->stage2_teams + kTcWpb - 1) / kTcWpb, 32 * kTcWpb, tc_smem(), st>>>(ta);
+  HMVM_CUDA_TRY(cudaGetLastError(), "tensor-core row-stage launch");
+  if (ev) cudaEventRecord(ev[3], st);
+  if (p->n_red2 > 0)
+    launch_reduce_multi<double, double, false>(kTcNrhs, p->d_red2, p->n_red2, p->d_pm, Y, ldy, nr, st);
+  HMVM_CUDA_TRY(cudaGetLastError(), "tensor-core reductions");
+  if (ev) cudaEventRecord(ev[4], st);
+  return HMVM_OK;
+}
+
 // Right-hand sides per pass: the largest of 8, 4, 2 that is <= nrhs_max and
 // not above what is left (a last single column runs in a 2-wide pass).
 int multi_pass_width(int nrhs_max, int left) {
@@ -665,6 +771,15 @@ int apply_multi_impl(hmvm_plan* p, const void* X, int64_t ldx, void* Y, int64_t 
     for (int r = 0; r < nrhs; r++) {
       int rc = apply_impl_fwd(p, static_cast<const char*>(X) + (size_t)r * ldx * ex,
                               static_cast<char*>(Y) + (size_t)r * ldy * ex, st);
+      if (rc) return rc;
+    }
+    return HMVM_OK;
+  }
+  if (p->tc) {
+    for (int r0 = 0; r0 < nrhs; r0 += kTcNrhs) {
+      const int nr = std::min(kTcNrhs, nrhs - r0);
+      int rc = launch_tc_pass(p, static_cast<const char*>(X) + (size_t)r0 * ldx * ex, ldx,
+                              static_cast<char*>(Y) + (size_t)r0 * ldy * ex, ldy, nr, st);
       if (rc) return rc;
     }
     return HMVM_OK;
@@ -974,6 +1089,8 @@ int hmvm_b200_apply_multi_host(hmvm_plan* p, const void* X_host, int64_t ldx, vo
 int hmvm_b200_plan_multi_kernel_count(const hmvm_plan* p, int32_t nrhs) {
   if (!p || p->nd == 0 || nrhs <= 0) return 0;
   if (p->nrhs_max <= 1) return nrhs * hmvm_b200_plan_kernel_count(p);
+  if (p->tc)  // per pass: pack, 2 x (max, planes), the stages and their reductions
+    return (nrhs + kTcNrhs - 1) / kTcNrhs * (5 + (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1 + (p->n_red2 > 0));
   int passes = 0;
   for (int r0 = 0; r0 < nrhs; passes++) r0 += std::min(multi_pass_width(p->nrhs_max, nrhs - r0), nrhs - r0);
   return passes * (1 + (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1 + (p->n_red2 > 0));

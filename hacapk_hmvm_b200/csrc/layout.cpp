@@ -154,7 +154,9 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     L.ctas_per_sm = opts.ctas_per_sm > 0 ? opts.ctas_per_sm
                     : (L.kernel == 0 ? kDefaultCtasPerSm : kDefaultStreamCtasPerSm);
     const int VEC = L.vec;  // plain plans: elements per vector
-    const int nrhs_max = std::min(std::max(opts.nrhs_max, 1), kMaxNrhsPass);
+    // 16 right-hand sides per pass run on the tensor cores (mixed plans only)
+    const int nrhs_max = (L.mixed && opts.nrhs_max >= kTcNrhs) ? kTcNrhs
+                                                               : std::min(std::max(opts.nrhs_max, 1), kMaxNrhsPass);
     L.nrhs_max = nrhs_max;
     const int RMAX = (opts.max_tile_rows >= 1 && opts.max_tile_rows <= kMaxRows) ? opts.max_tile_rows : kMaxRows;
     const int32_t nd = lt.nd, nlf = lt.nlf;
@@ -459,8 +461,9 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     if (nrhs_max > 1) {
       // teams for the multi-RHS kernel, all resident at once (and no more than
       // the single-vector kernels launch)
-      L.stage1_teams = std::min(L.stage1_teams, L.num_sms * kMultiWarpsPerSm);
-      L.stage2_teams = std::min(L.stage2_teams, L.num_sms * kMultiWarpsPerSm);
+      const int per_sm = nrhs_max == kTcNrhs ? kTcWarpsPerSm : kMultiWarpsPerSm;
+      L.stage1_teams = std::min(L.stage1_teams, L.num_sms * per_sm);
+      L.stage2_teams = std::min(L.stage2_teams, L.num_sms * per_sm);
     }
     int64_t stage_bytes[2] = {0, 0};
     for (int32_t k = 0; k < ntb; k++) stage_bytes[k < n1 ? 0 : 1] += (int64_t)tb[k].nvec * tb[k].nrows * 16;

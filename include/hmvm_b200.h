@@ -142,7 +142,9 @@ typedef struct hmvm_plan_opts {
                              factors, 0.05 for BF16, whose 8-bit significand needs more FP32 columns) */
   int32_t mixed_lr_format;/* enum hmvm_lr_format (default FP16) */
   int32_t nrhs_max;       /* right-hand sides per pass of hmvm_b200_apply_multi, 1..8 (default 1; items are
-                             sized so that nrhs_max inputs per column fit the multi-RHS kernel's buffer) */
+                             sized so that nrhs_max inputs per column fit the multi-RHS kernel's buffer);
+                             16 on HMVM_MIXED plans: 16-column passes with the 16-bit factor runs on the
+                             tensor cores (tcgen05) */
 } hmvm_plan_opts;
 
 typedef struct hmvm_plan_info {
