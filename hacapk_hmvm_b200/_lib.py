@@ -103,6 +103,19 @@ class PlanInfo(C.Structure):
                 ("cols_fp32", C.c_int64), ("cols_lr16", C.c_int64), ("cols_fp8", C.c_int64)]
 
 
+TUNE_MAX_ENTRIES = 64
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("kernel", C.c_int32), ("stage1_cfg", C.c_int32), ("stage2_cfg", C.c_int32),
+                ("max_tile_rows", C.c_int32), ("ctas_per_sm", C.c_int32), ("_pad0", C.c_int32),
+                ("stage1_ms", C.c_double), ("stage2_ms", C.c_double), ("total_ms", C.c_double)]
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("n_entries", C.c_int32), ("best_entry", C.c_int32), ("entries", TuneEntry * TUNE_MAX_ENTRIES)]
+
+
 class Stats(C.Structure):
     _fields_ = [("seconds_setup", C.c_double), ("seconds_apply", C.c_double),
                 ("algorithmic_bytes", C.c_int64), ("gbytes_per_s", C.c_double)]
@@ -182,6 +195,10 @@ HMVM_SIGNATURES = {
     "hmvm_b200_apply_multi_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32,
                                              C.c_void_p]),
     "hmvm_b200_plan_multi_kernel_count": (C.c_int, [C.c_void_p, C.c_int32]),
+    "hmvm_b200_bicgstab": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_double, C.c_void_p,
+                                     C.c_void_p, C.c_void_p]),
+    "hmvm_b200_autotune64": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "hmvm_b200_autotune_d": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "hmvm_b200_batch_create64_d": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hmvm_b200_batch_create64_f": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hmvm_b200_batch_create_d": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -52,7 +52,7 @@ def _stale(target: str, sources: list[str]) -> bool:
 
 
 def hmvm_sources() -> list[str]:
-    return [os.path.join(CSRC, f) for f in ("hmvm_b200.cu", "layout.cpp", "loader.cpp")]
+    return [os.path.join(CSRC, f) for f in ("hmvm_b200.cu", "layout.cpp", "loader.cpp", "tune.cpp", "solve.cu")]
 
 
 def hmvm_deps() -> list[str]:

@@ -12,6 +12,7 @@ converts it to the C structures the library takes.  Matrices come from
 from __future__ import annotations
 
 import ctypes as C
+import functools
 import weakref
 from dataclasses import dataclass, field
 
@@ -22,10 +23,18 @@ from . import _lib
 GEOMETRIES = {"sphere": 0, "cube": 1, "cube_surface": 1, "plate": 2, "plate_2x1": 2}
 
 
-def _np_from(ptr, n, dtype):
+def _np_from_owned(ptr, n, dtype, owner=None):
+    """An array over n elements of C memory at ptr.  With `owner` (the object
+    whose lifetime frees that memory), the array and every view of it keep the
+    owner alive."""
     if n == 0:
         return np.zeros(0, dtype)
-    return np.ctypeslib.as_array(ptr, shape=(n,)).view(dtype)
+    buf = (C.c_ubyte * (n * np.dtype(dtype).itemsize)).from_address(C.cast(ptr, C.c_void_p).value)
+    buf._owner = owner
+    return np.frombuffer(buf, dtype=dtype)
+
+
+_np_from = _np_from_owned
 
 
 def _ptr(a: np.ndarray, ctype):
@@ -104,6 +113,8 @@ class HMatrix:
             raise RuntimeError(f"hgen_build failed with status {rc}")
         m = mp.contents
         nlf = m.nlf
+        owner = _COwner(mp, lib.hgen_free)
+        _np_from = functools.partial(_np_from_owned, owner=owner)
         obj = cls(
             nd=m.nd, ktmax=m.ktmax,
             ltmtx=_np_from(m.ltmtx, nlf, np.int32), kt=_np_from(m.kt, nlf, np.int32),
@@ -118,7 +129,7 @@ class HMatrix:
         )
         obj.meta["lod"] = _np_from(m.lod, m.nd, np.int32)
         obj.meta["coords"] = _np_from(m.coords, 3 * m.nd, np.float64).reshape(-1, 3)
-        obj._keep.append(_COwner(mp, lib.hgen_free))
+        obj._keep.append(owner)
         obj._hgen_ptr = mp
         return obj
 

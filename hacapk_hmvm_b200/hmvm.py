@@ -161,6 +161,17 @@ class Plan:
         _lib.check(rc, "apply_multi_host")
         return Y
 
+    def bicgstab(self, b, u, eps: float = 1e-8, max_steps: int = 1000, stream=None) -> tuple[int, float]:
+        """Solve H u = b by BiCGSTAB (hmvm_b200_bicgstab): b, u CUDA tensors,
+        u holds the initial guess and receives the solution.  Returns (steps,
+        final relative residual)."""
+        steps = C.c_int32()
+        rel = C.c_double()
+        rc = _lib.hmvm_lib().hmvm_b200_bicgstab(self.handle, _dev_ptr(b), _dev_ptr(u), max_steps, eps,
+                                                C.byref(steps), C.byref(rel), _stream_handle(stream))
+        _lib.check(rc, "bicgstab")
+        return steps.value, rel.value
+
     def multi_kernel_count(self, nrhs: int) -> int:
         return int(_lib.hmvm_lib().hmvm_b200_plan_multi_kernel_count(self.handle, nrhs))
 
@@ -231,3 +242,26 @@ def hmvm_cuda(hm: HMatrix, b: np.ndarray, kernel: int = 0, dump_result: int = 0,
             t = np.array(times[5:])
             print(f"TIME {nbench} hmvm_cuda_{name} min {t.min():e} max {t.max():e} avg {t.mean():e}")
     return y
+
+
+def autotune(hm: HMatrix, precision: str = "fp64", reps: int = 5, device: int = -1, **base) -> tuple[dict, list]:
+    """Time candidate kernel configurations of this matrix's plan on the
+    current device (hmvm_b200_autotune64) and return (plan options of the
+    fastest measured plan, one dict per candidate timed).  Pass the options
+    to Plan(hm, precision, **options)."""
+    lib = _lib.hmvm_lib()
+    o = default_opts(precision=PRECISIONS[precision], device=device, **base)
+    best = _lib.PlanOpts()
+    rep = _lib.TuneReport()
+    lv = hm.as_leaves64()
+    _lib.check(lib.hmvm_b200_autotune64(C.byref(lv), 1 if hm.rowmat.dtype == np.float32 else 0, C.byref(o), reps,
+                                        C.byref(best), C.byref(rep)), "autotune")
+    keys = ("kernel", "stage1_cfg", "stage2_cfg", "max_tile_rows")
+    chosen = {k: getattr(best, k) for k in keys}
+    if precision == "mixed":
+        chosen.pop("kernel")
+    entries = [{f: getattr(rep.entries[i], f) for f, _ in _lib.TuneEntry._fields_ if not f.startswith("_")}
+               for i in range(rep.n_entries)]
+    for i, e in enumerate(entries):
+        e["best"] = i == rep.best_entry
+    return chosen, entries

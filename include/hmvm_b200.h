@@ -242,6 +242,45 @@ int hmvm_b200_batch_status(hmvm_batch *batch);
 /* Kernels one apply (or one graph replay) launches for the columns last given. */
 int hmvm_b200_batch_kernel_count(const hmvm_batch *batch);
 
+/* ---- Krylov solver on a resident plan ---------------------------------------
+ * Solves H u = b by BiCGSTAB, restating HACApK_bicgstab_lfmtx
+ * (src_lhdump/m_HACApK_solve.f90:977-1028): u_dev holds the initial guess and
+ * receives the solution; at most max_steps steps, stopping when
+ * ||b - H u|| / ||b|| < eps.  b and u are device vectors of the plan's x / y
+ * type; two HMVMs (hmvm_b200_apply) per step, inner products summed in a fixed
+ * order (repeatable).  *steps and *relres receive the steps taken and the
+ * final relative residual.  Returns HMVM_EINVAL on a breakdown (a vanishing
+ * BiCGSTAB scalar).  Allocates 7 work vectors for the call. */
+int hmvm_b200_bicgstab(hmvm_plan *plan, const void *b_dev, void *u_dev, int32_t max_steps, double eps,
+                       int32_t *steps, double *relres, void *stream);
+
+/* ---- autotuner ---------------------------------------------------------------
+ * Picks, per leaf shape class -- the V stage (stacked low-rank V factors) and
+ * the row stage (row tiles of dense leaves and U factors) -- the kernel
+ * configuration that runs fastest on the current device for this very matrix:
+ * one warp per team (stream kernel) or warp groups per tile item (tile kernel),
+ * their ring / buffer / group shapes, and the rows per row tile.  Every
+ * candidate plan is built and timed stage by stage (reps applies, CUDA events;
+ * building a plan costs about a second per million leaves); the best stage
+ * configurations are combined and timed as well.  `best` receives `base` with
+ * kernel, stage1_cfg, stage2_cfg and max_tile_rows of the fastest measured
+ * plan; pass it to hmvm_b200_plan_create*.  Replaces the hand-tuned warp/block
+ * thresholds of the reference's hmvm_cuda_hybrid kernels (hmvm_cuda1.cu). */
+#define HMVM_TUNE_MAX_ENTRIES 64
+typedef struct hmvm_tune_entry {
+  int32_t kernel, stage1_cfg, stage2_cfg, max_tile_rows;
+  int32_t ctas_per_sm, _pad0;
+  double stage1_ms, stage2_ms, total_ms; /* per apply; each stage with its reduction */
+} hmvm_tune_entry;
+typedef struct hmvm_tune_report {
+  int32_t n_entries, best_entry;
+  hmvm_tune_entry entries[HMVM_TUNE_MAX_ENTRIES];
+} hmvm_tune_report;
+int hmvm_b200_autotune64(const hmvm_leaves64 *lv, int32_t rowmat_is_float, const hmvm_plan_opts *base, int32_t reps,
+                         hmvm_plan_opts *best, hmvm_tune_report *report);
+int hmvm_b200_autotune_d(const hmvm_matrix2_d *mat2, const hmvm_plan_opts *base, int32_t reps,
+                         hmvm_plan_opts *best, hmvm_tune_report *report);
+
 /* Capacity of the scratch array used by hmvm_b200_apply_noalloc: 16 MiB. */
 #define HMVM_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
 

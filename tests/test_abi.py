@@ -40,7 +40,8 @@ STRUCTS = {
     "hmvm_matrix2_d": _lib.Matrix2_d, "hmvm_matrix2_f": _lib.Matrix2_f, "hmvm_matrix_d": _lib.Matrix_d,
     "hmvm_submatrix_d": _lib.Submatrix_d, "hmvm_leaves64": _lib.Leaves64, "hmvm_plan_opts": _lib.PlanOpts,
     "hmvm_plan_info": _lib.PlanInfo, "hmvm_stats": _lib.Stats, "hmvm_tile_desc": _lib.TileDesc,
-    "hmvm_seg_desc": _lib.SegDesc, "hmvm_layout_view": _lib.LayoutView,
+    "hmvm_seg_desc": _lib.SegDesc, "hmvm_layout_view": _lib.LayoutView, "hmvm_tune_entry": _lib.TuneEntry,
+    "hmvm_tune_report": _lib.TuneReport,
 }
 
 
