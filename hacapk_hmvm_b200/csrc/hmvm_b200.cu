@@ -77,7 +77,9 @@ KernelFn stream_kernel_for(int cfg) {
     case 2: return hmvm_stream_kernel<T, 8, 4, 2048, 256>;
     case 3: return hmvm_stream_kernel<T, 16, 4, 1024, 128>;
     case 4: return hmvm_stream_kernel<T, 4, 8, 1024, 512>;
-    default: return hmvm_stream_kernel<T, 8, 8, 512, 256>;
+    case 5: return hmvm_stream_kernel<T, 8, 8, 512, 256>;
+    case 6: return hmvm_stream_kernel<T, 8, 2, 4096, 256>;
+    default: return hmvm_stream_kernel<T, 4, 4, 4096, 512>;
   }
 }
 
@@ -90,7 +92,9 @@ KernelFn mixed_kernel_lr(int cfg) {
     case 2: return hmvm_mixed_kernel<8, 4, 2048, 4096, LR16, VST>;
     case 3: return hmvm_mixed_kernel<4, 4, 2048, 4096, LR16, VST>;
     case 4: return hmvm_mixed_kernel<6, 4, 2048, 4096, LR16, VST>;
-    default: return hmvm_mixed_kernel<16, 4, 1024, 2048, LR16, VST>;
+    case 5: return hmvm_mixed_kernel<16, 4, 1024, 2048, LR16, VST>;
+    case 6: return hmvm_mixed_kernel<8, 2, 4096, 2048, LR16, VST>;
+    default: return hmvm_mixed_kernel<4, 4, 4096, 2048, LR16, VST>;
   }
 }
 inline KernelFn mixed_kernel_for(int cfg, bool bf16, int stage) {
@@ -275,8 +279,8 @@ int resident_ctas(const hmvm_plan_opts& o, int dev, int* out) {
   const bool mixed = o.precision == HMVM_MIXED;
   const int kernel = mixed ? (o.mixed_lr_format == HMVM_LR_BF16 ? 3 : 2) : (o.kernel == 0 ? 0 : 1);
   const int ncfg = mixed ? kNumMixedCfgs : (kernel == 0 ? kNumCfgs : kNumStreamCfgs);
-  const int d1 = mixed ? kDefaultMixedCfg : (kernel == 0 ? kDefaultStage1Cfg : kDefaultStreamCfg);
-  const int d2 = mixed ? kDefaultMixedCfg : (kernel == 0 ? kDefaultStage2Cfg : kDefaultStreamCfg);
+  const int d1 = mixed ? kDefaultMixedCfg1 : (kernel == 0 ? kDefaultStage1Cfg : kDefaultStreamCfg);
+  const int d2 = mixed ? kDefaultMixedCfg2 : (kernel == 0 ? kDefaultStage2Cfg : kDefaultStreamCfg);
   const int c1 = (o.stage1_cfg >= 0 && o.stage1_cfg < ncfg) ? o.stage1_cfg : d1;
   const int c2 = (o.stage2_cfg >= 0 && o.stage2_cfg < ncfg) ? o.stage2_cfg : d2;
   return o.precision == HMVM_FP32 ? resident_ctas_t<float>(kernel, c1, c2, out)

@@ -146,11 +146,10 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     L.num_sms = num_sms > 0 ? num_sms : 148;
     L.kernel = (opts.kernel == 0 && !L.mixed) ? 0 : 1;
     const int ncfg = L.mixed ? kNumMixedCfgs : (L.kernel == 0 ? kNumCfgs : kNumStreamCfgs);
-    const int dcfg = L.mixed ? kDefaultMixedCfg : (L.kernel == 0 ? -1 : kDefaultStreamCfg);
-    L.stage1_cfg = (opts.stage1_cfg >= 0 && opts.stage1_cfg < ncfg) ? opts.stage1_cfg
-                   : (dcfg >= 0 ? dcfg : kDefaultStage1Cfg);
-    L.stage2_cfg = (opts.stage2_cfg >= 0 && opts.stage2_cfg < ncfg) ? opts.stage2_cfg
-                   : (dcfg >= 0 ? dcfg : kDefaultStage2Cfg);
+    const int d1 = L.mixed ? kDefaultMixedCfg1 : (L.kernel == 0 ? kDefaultStage1Cfg : kDefaultStreamCfg);
+    const int d2 = L.mixed ? kDefaultMixedCfg2 : (L.kernel == 0 ? kDefaultStage2Cfg : kDefaultStreamCfg);
+    L.stage1_cfg = (opts.stage1_cfg >= 0 && opts.stage1_cfg < ncfg) ? opts.stage1_cfg : d1;
+    L.stage2_cfg = (opts.stage2_cfg >= 0 && opts.stage2_cfg < ncfg) ? opts.stage2_cfg : d2;
     L.ctas_per_sm = opts.ctas_per_sm > 0 ? opts.ctas_per_sm
                     : (L.kernel == 0 ? kDefaultCtasPerSm : kDefaultStreamCtasPerSm);
     const int VEC = L.vec;  // plain plans: elements per vector

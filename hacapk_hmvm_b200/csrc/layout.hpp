@@ -73,9 +73,10 @@ constexpr KernelCfg kCfgs[kNumCfgs] = {{1, 8}, {2, 4}, {4, 2}, {8, 1}, {2, 8}, {
 struct StreamCfg {
   int wpb, slots, chunk, zcap;
 };
-constexpr int kNumStreamCfgs = 6;
+constexpr int kNumStreamCfgs = 8;
 constexpr StreamCfg kStreamCfgs[kNumStreamCfgs] = {{8, 4, 1024, 256}, {4, 4, 2048, 512}, {8, 4, 2048, 256},
-                                                   {16, 4, 1024, 128}, {4, 8, 1024, 512}, {8, 8, 512, 256}};
+                                                   {16, 4, 1024, 128}, {4, 8, 1024, 512}, {8, 8, 512, 256},
+                                                   {8, 2, 4096, 256},  {4, 4, 4096, 512}};
 inline int stream_smem_bytes(const StreamCfg& c, int elem) {
   return c.wpb * (c.slots * c.chunk + 2 * c.zcap * elem + c.slots * 8);
 }
@@ -84,7 +85,7 @@ constexpr int kDefaultKernel = 1;
 constexpr int kDefaultStage1Cfg = 4;  // variant 0 defaults
 constexpr int kDefaultStage2Cfg = 5;
 constexpr int kDefaultCtasPerSm = 2;
-constexpr int kDefaultStreamCfg = 2;  // variant 1 defaults
+constexpr int kDefaultStreamCfg = 7;  // variant 1 defaults
 constexpr int kDefaultStreamCtasPerSm = 2;  // plans use the occupancy the device reports
 constexpr int kMaxRows = 32;
 // Item split: a stage's tiles are cut so that no item exceeds
@@ -111,11 +112,15 @@ constexpr int kMixedMaxSegs = 32;
 struct MixedCfg {
   int wpb, slots, chunk, zbytes;
 };
-constexpr int kNumMixedCfgs = 6;
+constexpr int kNumMixedCfgs = 8;
 constexpr MixedCfg kMixedCfgs[kNumMixedCfgs] = {{8, 4, 2048, 2048}, {8, 4, 1024, 4096}, {8, 4, 2048, 4096},
-                                                {4, 4, 2048, 4096}, {6, 4, 2048, 4096}, {16, 4, 1024, 2048}};
+                                                {4, 4, 2048, 4096}, {6, 4, 2048, 4096}, {16, 4, 1024, 2048},
+                                                {8, 2, 4096, 2048}, {4, 4, 4096, 2048}};
 inline int mixed_smem_bytes(const MixedCfg& c) { return c.wpb * (c.slots * c.chunk + 2 * c.zbytes + c.slots * 8); }
-constexpr int kDefaultMixedCfg = 0;
+// defaults measured at N = 262,144: 4 warps x 16 KB rings for the V stage,
+// 8 warps x (2 slots of 4 KB) for the row stage
+constexpr int kDefaultMixedCfg1 = 7;
+constexpr int kDefaultMixedCfg2 = 6;
 
 // Multi-RHS kernel (hmvm_multi_kernel): rhs per pass and its input buffer.
 constexpr int kMaxNrhsPass = 8;   // CUDA-core multi-RHS passes

@@ -4,10 +4,10 @@
 //
 // Shape classes: the V stage (stacked low-rank V factors, one x segment per
 // panel) and the row stage (row tiles of dense leaves and U factors).  The
-// choices per class: one warp per team (the TMA-ring stream kernel, 6 ring /
+// choices per class: one warp per team (the TMA-ring stream kernel, 8 ring /
 // input-buffer shapes) or teams of 1..16 warps per tile item (the
 // register-streaming tile kernel, 8 warp-group shapes) -- the warp-versus-block
-// assignment -- for plain plans; the 6 ring / input-buffer shapes of the
+// assignment -- for plain plans; the 8 ring / input-buffer shapes of the
 // mixed-precision kernel for mixed plans; and the tile shape (rows per row
 // tile: 32 or 16).  Each candidate plan is timed stage by stage with CUDA
 // events (hmvm_b200_plan_profile); the best configuration of each stage is
@@ -95,9 +95,9 @@ extern "C" int hmvm_b200_autotune64(const hmvm_leaves64* lv, int32_t rowmat_is_f
   std::vector<Cand> cands;
   for (int rows : {32, 16}) {
     if (mixed) {
-      for (int c = 0; c < 6; c++) cands.push_back({-1, c, c, rows});
+      for (int c = 0; c < 8; c++) cands.push_back({-1, c, c, rows});  // the mixed kernel's shapes
     } else {
-      for (int c = 0; c < 6; c++) cands.push_back({1, c, c, rows});
+      for (int c = 0; c < 8; c++) cands.push_back({1, c, c, rows});  // the stream kernel's shapes
       for (int c = 0; c < 8; c++) cands.push_back({0, c, c, rows});
     }
   }

@@ -30,7 +30,7 @@ def test_layout_bounds_and_emulation(case):
             _lib.hmvm_lib().hmvm_b200_layout_destroy(h)
 
 
-MIXED_ZBYTES = {0: 2048, 1: 4096, 2: 4096, 3: 4096, 4: 4096, 5: 2048}  # kMixedCfgs (layout.hpp)
+MIXED_ZBYTES = {0: 2048, 1: 4096, 2: 4096, 3: 4096, 4: 4096, 5: 2048, 6: 2048, 7: 2048}  # kMixedCfgs (layout.hpp)
 MIXED_OPTS = [dict(), dict(mixed_lr_format="bf16"), dict(mixed_fp8_eps=0.0), dict(mixed_fp32_tau=2.0),
               dict(split_cols=8), dict(max_tile_rows=5), dict(stage1_cfg=5, stage2_cfg=1, ctas_per_sm=1)]
 
@@ -112,8 +112,8 @@ def test_stream_items_fit_input_buffer():
     from hacapk_hmvm_b200._lib import TileDesc
 
     hm = HMatrix.generate(3000, "sphere", seed=2)
-    zcap = {0: 256, 1: 512, 2: 256, 3: 128, 4: 512, 5: 256}  # kStreamCfgs (layout.hpp)
-    for cfg in range(6):
+    zcap = {0: 256, 1: 512, 2: 256, 3: 128, 4: 512, 5: 256, 6: 256, 7: 512}  # kStreamCfgs (layout.hpp)
+    for cfg in range(8):
         for prec, vec in ((0, 2), (1, 4)):
             h, v = layout_for(hm, precision=prec, stage1_cfg=cfg, stage2_cfg=cfg)
             tiles = np.ctypeslib.as_array((TileDesc * v.n_tiles).from_address(v.tiles))
