@@ -431,7 +431,7 @@ def run_b200(a, rank, world, local_rank):
         value = world * 1e3 / ms_step * a.nrhs
         cfg = workload_config(a, hm)
         cfg.update({"kernel": kname, "stage1_cfg": info["stage1_cfg"], "stage2_cfg": info["stage2_cfg"],
-                    "ctas_per_sm": info["ctas_per_sm"],
+                    "ctas_per_sm": [info["ctas_per_sm"], info["stage2_ctas_per_sm"]],
                     "device_bytes": info["device_bytes"], "plan_setup_s": setup_s})
         line = {
             "metric": unit, "value": value, "unit": unit, "n_gpus": world, "steps": a.steps,

@@ -100,7 +100,8 @@ class PlanInfo(C.Structure):
                 ("stage1_cfg", C.c_int32), ("stage2_cfg", C.c_int32), ("flops", C.c_int64),
                 ("stage1_bytes", C.c_int64), ("stage2_bytes", C.c_int64),
                 ("kernel", C.c_int32), ("ctas_per_sm", C.c_int32),
-                ("cols_fp32", C.c_int64), ("cols_lr16", C.c_int64), ("cols_fp8", C.c_int64)]
+                ("cols_fp32", C.c_int64), ("cols_lr16", C.c_int64), ("cols_fp8", C.c_int64),
+                ("stage2_ctas_per_sm", C.c_int32), ("_pad1", C.c_int32)]
 
 
 TUNE_MAX_ENTRIES = 64

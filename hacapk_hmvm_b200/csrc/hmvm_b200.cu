@@ -128,7 +128,7 @@ struct hmvm_plan {
   int precision = HMVM_FP64;
   int elem = 8;
   int32_t nd = 0, nlf = 0, n_lowrank = 0, n_dense = 0;
-  int num_sms = 0, kernel = 1, ctas_per_sm = 3, stage1_cfg = 0, stage2_cfg = 0;
+  int num_sms = 0, kernel = 1, ctas_per_sm = 3, ctas2_per_sm = 3, stage1_cfg = 0, stage2_cfg = 0;
   int32_t stage1_tiles = 0, stage2_tiles = 0, stage1_teams = 0, stage2_teams = 0, n_red1 = 0, n_red2 = 0;
   int64_t stored_elems = 0, device_bytes = 0, t_len = 0, p_len = 0;
   // device buffers
@@ -254,11 +254,11 @@ int prepare_kernels(const hmvm_plan* p) {
   return HMVM_OK;
 }
 
-// CTAs per SM that stay resident for both stage kernels of the configuration
-// `o` selects (its defaults resolved as the planner resolves them).
+// CTAs per SM that stay resident, per stage kernel of the configuration `o`
+// selects (its defaults resolved as the planner resolves them): out[0] the V
+// stage's, out[1] the row stage's.
 template <typename T>
 int resident_ctas_t(int kernel, int cfg1, int cfg2, int* out) {
-  int best = 64;
   for (int st = 1; st <= 2; st++) {
     const Launch l = stage_launch<T>(kernel, st == 1 ? cfg1 : cfg2, st);
     if (l.smem > 0)
@@ -267,9 +267,8 @@ int resident_ctas_t(int kernel, int cfg1, int cfg2, int* out) {
     int nb = 0;
     HMVM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)l.fn, l.threads, l.smem),
                   "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    best = std::min(best, std::max(nb, 1));
+    out[st - 1] = std::max(nb, 1);
   }
-  *out = best;
   return HMVM_OK;
 }
 
@@ -296,16 +295,20 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   int dev = 0, sms = 0;
   int rc = check_device(opts.device, &dev, &sms);
   if (rc) return rc;
+  int ctas2 = opts.ctas_per_sm;
   if (opts.ctas_per_sm <= 0) {
-    // Persistent grids: as many CTAs per SM as can be resident at once, so no
-    // CTA waits for another to finish.
-    rc = resident_ctas(opts, dev, &opts.ctas_per_sm);
+    // Persistent grids: per stage, as many CTAs per SM as can be resident at
+    // once, so no CTA waits for another to finish.
+    int r[2] = {1, 1};
+    rc = resident_ctas(opts, dev, r);
     if (rc) return rc;
+    opts.ctas_per_sm = r[0];
+    ctas2 = r[1];
   }
   HostLayout* L = new (std::nothrow) HostLayout();
   if (!L) return set_error(HMVM_ENOMEM, "host allocation failed");
   std::string msg;
-  rc = build_layout(lt, opts, sms, *L, msg);
+  rc = build_layout(lt, opts, sms, *L, msg, ctas2);
   if (rc) {
     delete L;
     return set_error(rc, msg);
@@ -325,6 +328,7 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   p->num_sms = sms;
   p->kernel = L->kernel;
   p->ctas_per_sm = L->ctas_per_sm;
+  p->ctas2_per_sm = L->ctas2_per_sm;
   p->stage1_cfg = L->stage1_cfg;
   p->stage2_cfg = L->stage2_cfg;
   p->stage1_tiles = L->stage1_tiles;
@@ -444,7 +448,7 @@ int launch_stages_mixed(hmvm_plan* p, const void* x, void* y, void* tbuf, void* 
   a.p = pbuf;
   a.out_idx = p->d_out_idx;
   a.x32 = x32;
-  const int ctas = p->num_sms * p->ctas_per_sm;
+  const int ctas = p->num_sms * p->ctas_per_sm, ctas2 = p->num_sms * p->ctas2_per_sm;
   cudaEvent_t* ev = nullptr;
   if (p->profiling && p->prof_count < kMaxProfiled) {
     ev = &p->prof_events[kEventsPerApply * (size_t)p->prof_count];
@@ -474,7 +478,7 @@ int launch_stages_mixed(hmvm_plan* p, const void* x, void* y, void* tbuf, void* 
     a.team_begin = p->d_tb2;
     a.nteams = p->stage2_teams;
     a.scale = nullptr;
-    l.fn<<<ctas, l.threads, l.smem, st>>>(a);
+    l.fn<<<ctas2, l.threads, l.smem, st>>>(a);
     HMVM_CUDA_TRY(cudaGetLastError(), "row-stage launch");
   }
   if (ev) cudaEventRecord(ev[3], st);
@@ -503,7 +507,7 @@ int launch_stages(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, 
   a.out_idx = p->d_out_idx;
   a.x32 = nullptr;
   a.scale = nullptr;
-  const int ctas = p->num_sms * p->ctas_per_sm;
+  const int ctas = p->num_sms * p->ctas_per_sm, ctas2 = p->num_sms * p->ctas2_per_sm;
   cudaEvent_t* ev = nullptr;
   if (p->profiling && p->prof_count < kMaxProfiled) {
     ev = &p->prof_events[kEventsPerApply * (size_t)p->prof_count];
@@ -528,7 +532,7 @@ int launch_stages(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, 
     const Launch l = stage_launch<T>(p->kernel, p->stage2_cfg, 2);
     a.team_begin = p->d_tb2;
     a.nteams = p->stage2_teams;
-    l.fn<<<ctas, l.threads, l.smem, st>>>(a);
+    l.fn<<<ctas2, l.threads, l.smem, st>>>(a);
     HMVM_CUDA_TRY(cudaGetLastError(), "row-stage launch");
   }
   if (ev) cudaEventRecord(ev[3], st);
@@ -959,6 +963,7 @@ int hmvm_b200_plan_get_info(const hmvm_plan* p, hmvm_plan_info* info) {
   info->stage2_bytes = p->stage2_bytes;
   info->kernel = p->mixed ? 2 : p->kernel;
   info->ctas_per_sm = p->ctas_per_sm;
+  info->stage2_ctas_per_sm = p->ctas2_per_sm;
   info->cols_fp32 = p->cols_fp32;
   info->cols_lr16 = p->cols_lr16;
   info->cols_fp8 = p->cols_fp8;

@@ -546,12 +546,13 @@ template <int TY>
 struct MixedZ {
   static constexpr int bytes = TY == kF64 ? 16 : TY == kF32 ? 16 : TY == kE4M3 ? 64 : 32;
 };
-// Vectors per batch: 4 (2 for FP8, whose vectors carry 16 products), fewer
+// Vectors per batch: 4 (2 for FP8, whose vectors carry 16 products), twice
+// that when the launch leaves at least 200 registers per thread (WIDE); fewer
 // when the ring cannot hold a batch of 32-row vectors beside the chunk being
 // refilled.
-template <int TY, int S, int CHUNK, bool VST>
+template <int TY, int S, int CHUNK, bool VST, bool WIDE>
 __host__ __device__ constexpr int mixed_batch() {
-  constexpr int want = TY == kE4M3 ? 2 : 4;
+  constexpr int want = TY == kE4M3 ? (WIDE ? 4 : 2) : (WIDE ? 8 : 4);
   constexpr int room = (S - 1) * CHUNK / (32 * 16);
   return want <= room ? want : (room >= 4 ? 4 : (room >= 2 ? 2 : 1));
 }
@@ -606,7 +607,7 @@ __device__ __forceinline__ void mixed_fma(const uint4 m, const unsigned char* z,
 // multiplies a row's total by its column scale before storing t (FP32); the
 // row-stage instance carries neither scales nor t slots.
 template <int WPB, int S, int CHUNK, int ZBYTES>
-constexpr int mixed_min_blocks() {
+__host__ __device__ constexpr int mixed_min_blocks() {
   constexpr int smem = WPB * (S * CHUNK + 2 * ZBYTES + S * 8);
   constexpr int by_smem = (227 * 1024) / smem;
   constexpr int by_warps = 24 / WPB;
@@ -620,7 +621,8 @@ __global__ void __launch_bounds__(32 * WPB, (mixed_min_blocks<WPB, S, CHUNK, ZBY
   constexpr uint32_t RING = (uint32_t)S * CHUNK;
   static_assert((RING & (RING - 1)) == 0, "ring size must be a power of two");
   static_assert(CHUNK % 16 == 0 && CHUNK >= 512, "bulk copies move multiples of 16 bytes");
-  static_assert(mixed_batch<kF32, S, CHUNK, VST>() * 32 * 16 <= (S - 1) * CHUNK, "ring too small for one batch");
+  constexpr bool WIDE = 65536 / (32 * WPB * mixed_min_blocks<WPB, S, CHUNK, ZBYTES>()) >= 200;
+  static_assert(mixed_batch<kF32, S, CHUNK, VST, WIDE>() * 32 * 16 <= (S - 1) * CHUNK, "ring too small for one batch");
   extern __shared__ __align__(128) unsigned char smem[];
 
   const int lane = threadIdx.x & 31;
@@ -713,7 +715,7 @@ __global__ void __launch_bounds__(32 * WPB, (mixed_min_blocks<WPB, S, CHUNK, ZBY
     // input loads are issued together; FP32 (FP64) partial sums per segment.
     auto run_seg = [&](auto tag, const unsigned char* zs, int nv) -> bool {
       constexpr int TY = decltype(tag)::value;
-      constexpr int B = mixed_batch<TY, S, CHUNK, VST>();
+      constexpr int B = mixed_batch<TY, S, CHUNK, VST, WIDE>();
       float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       double e[4] = {0.0, 0.0, 0.0, 0.0};
       for (int v = 0; v < nv; v += B) {

@@ -128,7 +128,7 @@ int validate_leaves(const LeafTable &lt, std::string &msg) {
 }
 
 int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, HostLayout &L,
-                 std::string &msg) {
+                 std::string &msg, int ctas2_per_sm) {
   int rc = validate_leaves(lt, msg);
   if (rc) return rc;
   if (opts.precision != HMVM_FP64 && opts.precision != HMVM_FP32 && opts.precision != HMVM_MIXED) {
@@ -152,6 +152,7 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     L.stage2_cfg = (opts.stage2_cfg >= 0 && opts.stage2_cfg < ncfg) ? opts.stage2_cfg : d2;
     L.ctas_per_sm = opts.ctas_per_sm > 0 ? opts.ctas_per_sm
                     : (L.kernel == 0 ? kDefaultCtasPerSm : kDefaultStreamCtasPerSm);
+    L.ctas2_per_sm = ctas2_per_sm > 0 ? ctas2_per_sm : L.ctas_per_sm;
     const int VEC = L.vec;  // plain plans: elements per vector
     // 16 right-hand sides per pass run on the tensor cores (mixed plans only)
     const int nrhs_max = (L.mixed && opts.nrhs_max >= kTcNrhs) ? kTcNrhs
@@ -454,9 +455,10 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     // A tile whose bytes exceed the stage's bound, or (stream kernels) whose
     // inputs exceed the kernel's input buffer, is cut into vector ranges that
     // write partial sums; the reduction lists add them in order.
-    const int32_t ctas = L.num_sms * L.ctas_per_sm;
-    L.stage1_teams = ctas * (L.mixed ? kMixedCfgs[L.stage1_cfg].wpb : teams_per_cta(L.kernel, L.stage1_cfg));
-    L.stage2_teams = ctas * (L.mixed ? kMixedCfgs[L.stage2_cfg].wpb : teams_per_cta(L.kernel, L.stage2_cfg));
+    L.stage1_teams = L.num_sms * L.ctas_per_sm *
+                     (L.mixed ? kMixedCfgs[L.stage1_cfg].wpb : teams_per_cta(L.kernel, L.stage1_cfg));
+    L.stage2_teams = L.num_sms * L.ctas2_per_sm *
+                     (L.mixed ? kMixedCfgs[L.stage2_cfg].wpb : teams_per_cta(L.kernel, L.stage2_cfg));
     if (nrhs_max > 1) {
       // teams for the multi-RHS kernel, all resident at once (and no more than
       // the single-vector kernels launch)

@@ -117,10 +117,11 @@ constexpr MixedCfg kMixedCfgs[kNumMixedCfgs] = {{8, 4, 2048, 2048}, {8, 4, 1024,
                                                 {4, 4, 2048, 4096}, {6, 4, 2048, 4096}, {16, 4, 1024, 2048},
                                                 {8, 2, 4096, 2048}, {4, 4, 4096, 2048}};
 inline int mixed_smem_bytes(const MixedCfg& c) { return c.wpb * (c.slots * c.chunk + 2 * c.zbytes + c.slots * 8); }
-// defaults measured at N = 262,144: 4 warps x 16 KB rings for the V stage,
-// 8 warps x (2 slots of 4 KB) for the row stage
+// defaults measured at N = 262,144 with each stage at its own resident CTAs
+// per SM: 4 warps x 16 KB rings for the V stage (2 CTAs per SM), 6 warps x
+// (4 slots of 2 KB) for the row stage (2 CTAs per SM)
 constexpr int kDefaultMixedCfg1 = 7;
-constexpr int kDefaultMixedCfg2 = 6;
+constexpr int kDefaultMixedCfg2 = 4;
 
 // Multi-RHS kernel (hmvm_multi_kernel): rhs per pass and its input buffer.
 constexpr int kMaxNrhsPass = 8;   // CUDA-core multi-RHS passes
@@ -143,6 +144,7 @@ struct HostLayout {
   int32_t nd = 0, nlf = 0, n_lowrank = 0, n_dense = 0;
   int kernel = kDefaultKernel;
   int stage1_cfg = kDefaultStreamCfg, stage2_cfg = kDefaultStreamCfg, ctas_per_sm = kDefaultStreamCtasPerSm;
+  int ctas2_per_sm = kDefaultStreamCtasPerSm;  // of the row stage (ctas_per_sm: the V stage)
   int num_sms = 148;
   std::vector<hmvm_tile_desc> tiles;  // [stage1 tiles][stage2 tiles], each in team order
   std::vector<hmvm_seg_desc> segs;
@@ -165,8 +167,10 @@ struct HostLayout {
 };
 
 // Returns HMVM_OK or a status; msg receives a description on failure.
+// ctas2_per_sm > 0 gives the row stage its own CTAs per SM (else both stages
+// use opts.ctas_per_sm, or the kernel's default).
 int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, HostLayout &out,
-                 std::string &msg);
+                 std::string &msg, int ctas2_per_sm = 0);
 
 int validate_leaves(const LeafTable &lt, std::string &msg);
 

@@ -158,8 +158,9 @@ typedef struct hmvm_plan_info {
   int64_t flops;             /* 2 * stored elements */
   int64_t stage1_bytes;      /* algorithmic bytes of the V stage: V elements + x */
   int64_t stage2_bytes;      /* algorithmic bytes of the row stage: U + dense elements + x + y */
-  int32_t kernel, ctas_per_sm;
+  int32_t kernel, ctas_per_sm;           /* ctas_per_sm: of the V stage */
   int64_t cols_fp32, cols_lr16, cols_fp8; /* HMVM_MIXED: low-rank columns per storage format */
+  int32_t stage2_ctas_per_sm, _pad1;      /* CTAs per SM of the row stage */
 } hmvm_plan_info;
 
 void hmvm_b200_default_opts(hmvm_plan_opts *opts);

@@ -31,6 +31,7 @@ def test_layout_bounds_and_emulation(case):
 
 
 MIXED_ZBYTES = {0: 2048, 1: 4096, 2: 4096, 3: 4096, 4: 4096, 5: 2048, 6: 2048, 7: 2048}  # kMixedCfgs (layout.hpp)
+MIXED_DEFAULT_CFGS = (7, 4)  # kDefaultMixedCfg1, kDefaultMixedCfg2 (layout.hpp)
 MIXED_OPTS = [dict(), dict(mixed_lr_format="bf16"), dict(mixed_fp8_eps=0.0), dict(mixed_fp32_tau=2.0),
               dict(split_cols=8), dict(max_tile_rows=5), dict(stage1_cfg=5, stage2_cfg=1, ctas_per_sm=1)]
 
@@ -45,7 +46,8 @@ def test_mixed_layout_bounds_and_emulation(case):
     yo = oracle_hmvm(hm, x)
     for opts in MIXED_OPTS:
         h, v = layout_for(hm, precision=2, **opts)
-        check_layout_bounds(v, zbytes=(MIXED_ZBYTES[opts.get("stage1_cfg", 0)], MIXED_ZBYTES[opts.get("stage2_cfg", 0)]))
+        check_layout_bounds(v, zbytes=(MIXED_ZBYTES[opts.get("stage1_cfg", MIXED_DEFAULT_CFGS[0])],
+                                       MIXED_ZBYTES[opts.get("stage2_cfg", MIXED_DEFAULT_CFGS[1])]))
         err = relerr(emulate_layout(v, x), yo)
         assert err < 1e-4, (opts, err)
         _lib.hmvm_lib().hmvm_b200_layout_destroy(h)
