@@ -163,6 +163,8 @@ class HgenMatrix(C.Structure):
 HMVM_SIGNATURES = {
     "hmvm_b200_load_hmatrix": (C.c_int, [C.c_char_p, C.POINTER(Matrix_d), C.POINTER(Matrix2_d)]),
     "hmvm_b200_load_hmatrix2": (C.c_int, [C.c_char_p, C.POINTER(Matrix2_d)]),
+    "hmvm_b200_load_leaves64": (C.c_int, [C.c_char_p, C.POINTER(Leaves64), C.POINTER(C.c_int32)]),
+    "hmvm_b200_free_leaves64": (None, [C.POINTER(Leaves64)]),
     "hmvm_b200_convert_d2f": (C.c_int, [C.POINTER(Matrix_f), C.POINTER(Matrix2_f), C.POINTER(Matrix_d),
                                         C.POINTER(Matrix2_d)]),
     "hmvm_b200_free_matrix_d": (None, [C.POINTER(Matrix_d)]),
@@ -198,6 +200,8 @@ HMVM_SIGNATURES = {
     "hmvm_b200_plan_multi_kernel_count": (C.c_int, [C.c_void_p, C.c_int32]),
     "hmvm_b200_bicgstab": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_double, C.c_void_p,
                                      C.c_void_p, C.c_void_p]),
+    "hmvm_b200_gcrm": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_void_p,
+                                 C.c_void_p, C.c_void_p]),
     "hmvm_b200_autotune64": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "hmvm_b200_autotune_d": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "hmvm_b200_batch_create64_d": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -225,6 +229,7 @@ HGEN_SIGNATURES = {
     "hgen_free": (None, [C.POINTER(HgenMatrix)]),
     "hgen_write_bin1": (C.c_int, [C.POINTER(HgenMatrix), C.c_char_p]),
     "hgen_write_bin2": (C.c_int, [C.POINTER(HgenMatrix), C.c_char_p]),
+    "hgen_write_bin64": (C.c_int, [C.POINTER(HgenMatrix), C.c_char_p]),
     "hgen_entry": (C.c_double, [C.POINTER(HgenMatrix), C.c_int32, C.c_int32]),
 }
 

@@ -548,17 +548,29 @@ int hgen_write_bin1(const hgen_hmatrix* m, const char* fname) {
   return rc;
 }
 
-int hgen_write_bin2(const hgen_hmatrix* m, const char* fname) {
+// bin2 and its 64-bit variant differ only in the width of the header's len.
+static int write_bin2_like(const hgen_hmatrix* m, const char* fname, bool len64) {
   FILE* f = fopen(fname, "wb");
   if (!f) return HGEN_EIO;
-  int32_t len32 = m->len > INT32_MAX ? INT32_MAX : (int32_t)m->len;
-  int32_t hdr[4] = {m->nd, m->nlf, m->ktmax, len32};
-  int rc = put_record(f, hdr, sizeof hdr);
+  unsigned char hdr[20];
+  const int32_t h3[3] = {m->nd, m->nlf, m->ktmax};
+  std::memcpy(hdr, h3, 12);
+  if (len64) {
+    const int64_t len = m->len;
+    std::memcpy(hdr + 12, &len, 8);
+  } else {
+    const int32_t len32 = m->len > INT32_MAX ? INT32_MAX : (int32_t)m->len;
+    std::memcpy(hdr + 12, &len32, 4);
+  }
+  int rc = put_record(f, hdr, len64 ? 20 : 16);
   const int32_t* cols[6] = {m->ltmtx, m->ndl, m->ndt, m->nstrtl, m->nstrtt, m->kt};
   for (int c = 0; rc == HGEN_OK && c < 6; c++) rc = put_record(f, cols[c], 4 * (int64_t)m->nlf);
   for (int32_t i = 0; rc == HGEN_OK && i < m->nlf; i++) rc = write_leaf_data(f, m, i);
   if (fclose(f) != 0 && rc == HGEN_OK) rc = HGEN_EIO;
   return rc;
 }
+
+int hgen_write_bin2(const hgen_hmatrix* m, const char* fname) { return write_bin2_like(m, fname, false); }
+int hgen_write_bin64(const hgen_hmatrix* m, const char* fname) { return write_bin2_like(m, fname, true); }
 
 }  // extern "C"

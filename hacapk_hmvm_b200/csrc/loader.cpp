@@ -87,9 +87,149 @@ void fill_rowmat_t(const int* ltmtx, const int* kt, const int* ndl, const int* n
   }
 }
 
+// The owned arrays of a 64-bit leaf table being loaded.
+struct Table64 {
+  int32_t *ltmtx = nullptr, *kt = nullptr, *ndl = nullptr, *ndt = nullptr, *nstrtl = nullptr, *nstrtt = nullptr;
+  int64_t *a1 = nullptr, *a2 = nullptr;
+  double* rowmat = nullptr;
+  ~Table64() {
+    free(ltmtx); free(kt); free(ndl); free(ndt); free(nstrtl); free(nstrtt); free(a1); free(a2); free(rowmat);
+  }
+  bool alloc(int32_t nlf) {
+    const size_t n = (size_t)(nlf > 0 ? nlf : 1);
+    ltmtx = (int32_t*)malloc(n * 4); kt = (int32_t*)malloc(n * 4); ndl = (int32_t*)malloc(n * 4);
+    ndt = (int32_t*)malloc(n * 4); nstrtl = (int32_t*)malloc(n * 4); nstrtt = (int32_t*)malloc(n * 4);
+    a1 = (int64_t*)malloc(n * 8); a2 = (int64_t*)malloc(n * 8);
+    return ltmtx && kt && ndl && ndt && nstrtl && nstrtt && a1 && a2;
+  }
+  // hands the arrays to `lv` (which then owns them)
+  void release_to(hmvm_leaves64* lv) {
+    lv->ltmtx = ltmtx; lv->kt = kt; lv->ndl = ndl; lv->ndt = ndt; lv->nstrtl = nstrtl; lv->nstrtt = nstrtt;
+    lv->a1 = a1; lv->a2 = a2; lv->rowmat = rowmat;
+    ltmtx = kt = ndl = ndt = nstrtl = nstrtt = nullptr;
+    a1 = a2 = nullptr;
+    rowmat = nullptr;
+  }
+};
+
+// Reads leaf i's data records at rowmat[off..] and sets a1/a2 (file order).
+int read_leaf_data64(FILE* f, Table64& T, int32_t i, int64_t& off) {
+  int rc;
+  if (T.ltmtx[i] == 1) {
+    const size_t n1 = (size_t)T.kt[i] * T.ndt[i], n2 = (size_t)T.kt[i] * T.ndl[i];
+    T.a1[i] = off;
+    if ((rc = read_record(f, T.rowmat + off, n1 * 8, "low-rank a1"))) return rc;
+    off += (int64_t)n1;
+    T.a2[i] = off;
+    if ((rc = read_record(f, T.rowmat + off, n2 * 8, "low-rank a2"))) return rc;
+    off += (int64_t)n2;
+  } else {
+    const size_t n1 = (size_t)T.ndl[i] * T.ndt[i];
+    T.a1[i] = off;
+    T.a2[i] = 0;
+    if ((rc = read_record(f, T.rowmat + off, n1 * 8, "dense a1"))) return rc;
+    off += (int64_t)n1;
+  }
+  return HMVM_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int hmvm_b200_load_leaves64(const char* fname, hmvm_leaves64* out, int32_t* format) {
+  if (!fname || !out) return set_error(HMVM_EINVAL, "NULL argument");
+  File F;
+  F.f = fopen(fname, "rb");
+  if (!F.f) return set_error(HMVM_EIO, std::string("cannot open ") + fname);
+  int32_t m0 = 0;
+  if (fread(&m0, 4, 1, F.f) != 1 || fseek(F.f, 0, SEEK_SET) != 0)
+    return set_error(HMVM_EFORMAT, "truncated before header");
+  const int fmt = m0 == 12 ? HMVM_BIN1 : m0 == 16 ? HMVM_BIN2 : m0 == 20 ? HMVM_BIN64 : 0;
+  if (!fmt)
+    return set_error(HMVM_EFORMAT, "header record of " + std::to_string(m0) + " bytes (12, 16 or 20 expected)");
+  unsigned char hdr[20];
+  int rc = read_record(F.f, hdr, (size_t)m0, "header");
+  if (rc) return rc;
+  int32_t h3[3];
+  std::memcpy(h3, hdr, 12);
+  const int32_t nd = h3[0], nlf = h3[1], ktmax = h3[2];
+  int64_t len = -1;  // bin1 carries none
+  if (fmt == HMVM_BIN2) {
+    int32_t l32;
+    std::memcpy(&l32, hdr + 12, 4);
+    len = l32;
+  } else if (fmt == HMVM_BIN64) {
+    std::memcpy(&len, hdr + 12, 8);
+  }
+  if (nd < 0 || nlf < 0 || ktmax < 0 || (fmt != HMVM_BIN1 && len < 0))
+    return set_error(HMVM_EFORMAT, "negative field in header");
+  Table64 T;
+  if (!T.alloc(nlf)) return set_error(HMVM_ENOMEM, "host allocation failed");
+  int64_t off = 0;
+  if (fmt == HMVM_BIN1) {
+    // per leaf: header record, then its data (loadmatrix.cpp:98-127); rowmat grows
+    size_t cap = 1 << 16;
+    T.rowmat = (double*)malloc(cap * sizeof(double));
+    if (!T.rowmat) return set_error(HMVM_ENOMEM, "host allocation failed");
+    for (int32_t i = 0; i < nlf; i++) {
+      int32_t h6[6];
+      if ((rc = read_record(F.f, h6, sizeof h6, "leaf header"))) return rc;
+      T.ltmtx[i] = h6[0]; T.ndl[i] = h6[1]; T.ndt[i] = h6[2]; T.nstrtl[i] = h6[3]; T.nstrtt[i] = h6[4];
+      T.kt[i] = h6[5];
+      if ((rc = check_leaf(nd, ktmax, i, T.ltmtx[i], T.ndl[i], T.ndt[i], T.nstrtl[i], T.nstrtt[i], T.kt[i])))
+        return rc;
+      const size_t need = (size_t)leaf_elems(T.ltmtx[i], T.kt[i], T.ndl[i], T.ndt[i]);
+      if ((size_t)off + need > cap) {
+        while ((size_t)off + need > cap) cap *= 2;
+        double* p = (double*)realloc(T.rowmat, cap * sizeof(double));
+        if (!p) return set_error(HMVM_ENOMEM, "host allocation failed");
+        T.rowmat = p;
+      }
+      if ((rc = read_leaf_data64(F.f, T, i, off))) return rc;
+    }
+    len = off;
+  } else {
+    // six int32[nlf] columns, then every leaf's data (loadmatrix.cpp:152-250)
+    int32_t* cols[6] = {T.ltmtx, T.ndl, T.ndt, T.nstrtl, T.nstrtt, T.kt};
+    const char* names[6] = {"ltmtx", "ndl", "ndt", "nstrtl", "nstrtt", "kt"};
+    for (int c = 0; c < 6; c++)
+      if ((rc = read_record(F.f, cols[c], (size_t)nlf * 4, names[c]))) return rc;
+    int64_t total = 0;
+    for (int32_t i = 0; i < nlf; i++) {
+      if ((rc = check_leaf(nd, ktmax, i, T.ltmtx[i], T.ndl[i], T.ndt[i], T.nstrtl[i], T.nstrtt[i], T.kt[i])))
+        return rc;
+      total += leaf_elems(T.ltmtx[i], T.kt[i], T.ndl[i], T.ndt[i]);
+    }
+    const bool saturated = fmt == HMVM_BIN2 && len == INT32_MAX && total >= INT32_MAX;
+    if (total != len && !saturated)
+      return set_error(HMVM_EFORMAT, "header len " + std::to_string(len) + " differs from the leaf sizes (" +
+                                         std::to_string(total) + ")");
+    len = total;
+    T.rowmat = (double*)malloc((size_t)(len > 0 ? len : 1) * sizeof(double));
+    if (!T.rowmat) return set_error(HMVM_ENOMEM, "host allocation failed");
+    for (int32_t i = 0; i < nlf; i++)
+      if ((rc = read_leaf_data64(F.f, T, i, off))) return rc;
+  }
+  std::memset(out, 0, sizeof(*out));
+  out->nd = nd;
+  out->nlf = nlf;
+  out->ktmax = ktmax;
+  out->len = len;
+  T.release_to(out);
+  if (format) *format = fmt;
+  return HMVM_OK;
+}
+
+void hmvm_b200_free_leaves64(hmvm_leaves64* lv) {
+  if (!lv) return;
+  free(const_cast<int32_t*>(lv->ltmtx)); free(const_cast<int32_t*>(lv->kt));
+  free(const_cast<int32_t*>(lv->ndl)); free(const_cast<int32_t*>(lv->ndt));
+  free(const_cast<int32_t*>(lv->nstrtl)); free(const_cast<int32_t*>(lv->nstrtt));
+  free(const_cast<int64_t*>(lv->a1)); free(const_cast<int64_t*>(lv->a2));
+  free(const_cast<void*>(lv->rowmat));
+  std::memset(lv, 0, sizeof(*lv));
+}
 
 void hmvm_b200_free_matrix2_d(hmvm_matrix2_d* m) {
   if (!m) return;

@@ -6,7 +6,8 @@ converts it to the C structures the library takes.  Matrices come from
 
 * ``HMatrix.load(path)``      hmatrix_1.bin / hmatrix_2.bin through the
                               library's loaders (replacing loadHmatrix /
-                              loadHmatrix2, src_hmvm/src_cpp/loadmatrix.cpp);
+                              loadHmatrix2, src_hmvm/src_cpp/loadmatrix.cpp),
+                              and the 64-bit variant of hmatrix_2.bin;
 * ``HMatrix.generate(...)``   the HACApK-rule generator (include/hacapk_hgen.h).
 """
 from __future__ import annotations
@@ -134,14 +135,19 @@ class HMatrix:
         return obj
 
     @classmethod
-    def load(cls, path: str, fmt: int | None = None) -> "HMatrix":
-        """Read hmatrix_1.bin (fmt=1) or hmatrix_2.bin (fmt=2); fmt=None guesses
-        from the header record length (12 bytes: format 1, 16 bytes: format 2)."""
+    def load(cls, path: str, fmt: int | None = None, wide: bool = False) -> "HMatrix":
+        """Read hmatrix_1.bin (fmt=1), hmatrix_2.bin (fmt=2) or its 64-bit variant
+        (fmt=3); fmt=None guesses from the header record length (12, 16 or 20
+        bytes).  Formats 1 and 2 go through the reference-signature loaders
+        (int offsets) unless `wide`; format 3, and `wide`, through
+        hmvm_b200_load_leaves64 (64-bit offsets, no element-count ceiling)."""
         if fmt is None:
             with open(path, "rb") as f:
                 head = np.frombuffer(f.read(4), dtype=np.int32)
-            fmt = 2 if head.size and head[0] == 16 else 1
+            fmt = {16: 2, 20: 3}.get(int(head[0]) if head.size else 12, 1)
         lib = _lib.hmvm_lib()
+        if fmt == 3 or wide:
+            return cls._load_wide(path)
         m2 = _lib.Matrix2_d()
         if fmt == 1:
             rc = lib.hmvm_b200_load_hmatrix(path.encode(), None, C.byref(m2))
@@ -159,6 +165,23 @@ class HMatrix:
         finally:
             lib.hmvm_b200_free_matrix2_d(C.byref(m2))
         return obj
+
+    @classmethod
+    def _load_wide(cls, path: str) -> "HMatrix":
+        lib = _lib.hmvm_lib()
+        lv = _lib.Leaves64()
+        fmt = C.c_int32(0)
+        _lib.check(lib.hmvm_b200_load_leaves64(path.encode(), C.byref(lv), C.byref(fmt)), f"load {path}")
+        keep = _lib.Leaves64()
+        C.memmove(C.byref(keep), C.byref(lv), C.sizeof(lv))
+        owner = _COwner(C.pointer(keep), lib.hmvm_b200_free_leaves64)
+        nlf = lv.nlf
+        arr = functools.partial(_np_from_owned, owner=owner)
+        return cls.from_arrays(
+            lv.nd, lv.ktmax, arr(lv.ltmtx, nlf, np.int32), arr(lv.kt, nlf, np.int32), arr(lv.ndl, nlf, np.int32),
+            arr(lv.ndt, nlf, np.int32), arr(lv.nstrtl, nlf, np.int32), arr(lv.nstrtt, nlf, np.int32),
+            arr(lv.a1, nlf, np.int64), arr(lv.a2, nlf, np.int64), arr(lv.rowmat, lv.len, np.float64),
+            meta=dict(source=path, format=int(fmt.value)))
 
     # ---- conversions -----------------------------------------------------
     def to_float(self) -> "HMatrix":
@@ -221,6 +244,12 @@ class HMatrix:
         rc = _lib.hgen_lib().hgen_write_bin2(C.byref(self._as_hgen()), path.encode())
         if rc != 0:
             raise OSError(f"hgen_write_bin2 failed with status {rc}")
+
+    def write_bin64(self, path: str) -> None:
+        """hmatrix_2.bin with a 64-bit len in the header (format 3)."""
+        rc = _lib.hgen_lib().hgen_write_bin64(C.byref(self._as_hgen()), path.encode())
+        if rc != 0:
+            raise OSError(f"hgen_write_bin64 failed with status {rc}")
 
     def entry(self, ill: int, itt: int) -> float:
         """Exact kernel entry at 1-based permuted positions (generated matrices only)."""

@@ -172,6 +172,16 @@ class Plan:
         _lib.check(rc, "bicgstab")
         return steps.value, rel.value
 
+    def gcrm(self, b, u, eps: float = 1e-8, max_steps: int = 1000, restart: int = 20,
+             stream=None) -> tuple[int, float]:
+        """Solve H u = b by GCR(restart) (hmvm_b200_gcrm); as bicgstab."""
+        steps = C.c_int32()
+        rel = C.c_double()
+        rc = _lib.hmvm_lib().hmvm_b200_gcrm(self.handle, _dev_ptr(b), _dev_ptr(u), max_steps, restart, eps,
+                                            C.byref(steps), C.byref(rel), _stream_handle(stream))
+        _lib.check(rc, "gcrm")
+        return steps.value, rel.value
+
     def multi_kernel_count(self, nrhs: int) -> int:
         return int(_lib.hmvm_lib().hmvm_b200_plan_multi_kernel_count(self.handle, nrhs))
 

@@ -75,6 +75,10 @@ void hgen_free(hgen_hmatrix* m);
  * when the element count does not fit. */
 int hgen_write_bin1(const hgen_hmatrix* m, const char* fname);
 int hgen_write_bin2(const hgen_hmatrix* m, const char* fname);
+/* The 64-bit variant of hmatrix_2.bin: the same records, but the header record
+ * holds len as int64 (nd, nlf, ktmax: int32; 20 bytes), as
+ * HACApK_hdump_dump_leafmtx2 writes it with `integer*8 :: len`. */
+int hgen_write_bin64(const hgen_hmatrix* m, const char* fname);
 
 /* Exact entry of the permuted matrix, row/col 1-based positions (for tests). */
 double hgen_entry(const hgen_hmatrix* m, int32_t ill, int32_t itt);

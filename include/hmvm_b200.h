@@ -106,6 +106,21 @@ int hmvm_b200_load_hmatrix2(const char *fname, hmvm_matrix2_d *mat2);
  * source may be NULL. */
 int hmvm_b200_convert_d2f(hmvm_matrix_f *matF, hmvm_matrix2_f *matF2, const hmvm_matrix_d *matD,
                           const hmvm_matrix2_d *matD2);
+/* File formats recognised by hmvm_b200_load_leaves64 (by the byte count of
+ * the first record: 12, 16 and 20). */
+#define HMVM_BIN1 1  /* hmatrix_1.bin: header nd, nlf, ktmax; per leaf a header record and its data */
+#define HMVM_BIN2 2  /* hmatrix_2.bin: header nd, nlf, ktmax, int32 len; six int32[nlf] columns; data */
+#define HMVM_BIN64 3 /* the bin2 layout with an int64 len (a 20-byte header record) */
+/* Reads any of the three formats into a 64-bit leaf table whose arrays the
+ * library allocates (rowmat: double); *format (may be NULL) receives the
+ * format found.  Lifts the int len / a1 / a2 ceiling of loadHmatrix /
+ * loadHmatrix2 (src_hmvm/src_cpp/hacapk.h:28,31; loadmatrix.cpp:13,38,70,100)
+ * for the HACApK dump formats (src_hdump/m_HACApK_hdump.f90:84-108,114-180),
+ * with the same validation as the loaders above.  A bin2 header whose len is
+ * INT32_MAX is taken as saturated (its leaves may hold more elements). */
+int hmvm_b200_load_leaves64(const char *fname, hmvm_leaves64 *out, int32_t *format);
+/* Release a table filled by hmvm_b200_load_leaves64 (and only such a table). */
+void hmvm_b200_free_leaves64(hmvm_leaves64 *lv);
 /* Release what the loaders / convert allocated (the reference never frees). */
 void hmvm_b200_free_matrix_d(hmvm_matrix_d *mat);
 void hmvm_b200_free_matrix_f(hmvm_matrix_f *mat);
@@ -254,6 +269,14 @@ int hmvm_b200_batch_kernel_count(const hmvm_batch *batch);
  * BiCGSTAB scalar).  Allocates 7 work vectors for the call. */
 int hmvm_b200_bicgstab(hmvm_plan *plan, const void *b_dev, void *u_dev, int32_t max_steps, double eps,
                        int32_t *steps, double *relres, void *stream);
+/* Solves H u = b by GCR(m), restating HACApK_gcrm_lfmtx
+ * (src_lhdump/m_HACApK_solve.f90:1277-1342; max_steps = param(83), restart =
+ * m = param(87) in 1..64, eps = param(91)): one HMVM per step, each new search
+ * direction A-orthogonalised against the last `restart` (stored cyclically).
+ * Same conventions as hmvm_b200_bicgstab; HMVM_EINVAL on a breakdown (A p = 0).
+ * Allocates 2 + 2 * restart work vectors for the call. */
+int hmvm_b200_gcrm(hmvm_plan *plan, const void *b_dev, void *u_dev, int32_t max_steps, int32_t restart, double eps,
+                   int32_t *steps, double *relres, void *stream);
 
 /* ---- autotuner ---------------------------------------------------------------
  * Picks, per leaf shape class -- the V stage (stacked low-rank V factors) and

@@ -92,3 +92,84 @@ def test_bicgstab_matches_numpy_iteration(gpu):
     assert abs(rel - rel_np) <= 1e-7 * rel_np
     u = ud.cpu().numpy()
     assert np.linalg.norm(u - u_np) <= 1e-7 * np.linalg.norm(u_np)
+
+
+# ---- GCR(m) -------------------------------------------------------------------
+
+def _numpy_gcrm(A_mv, b, steps, m):
+    """HACApK_gcrm_lfmtx (src_lhdump/m_HACApK_solve.f90:1277-1342), 0-based,
+    u0 = 0, exactly `steps` steps."""
+    u = np.zeros_like(b)
+    bnorm = np.linalg.norm(b)
+    zr = b - A_mv(u)
+    zp, zap, capap = [None] * m, [None] * m, [0.0] * m
+    zp[0] = zr.copy()
+    zap[0] = A_mv(zp[0])
+    for it in range(1, steps + 1):
+        ik = (it - 1) % m
+        zq = zap[ik]
+        znom = zq @ zr
+        capap[ik] = zq @ zq
+        alpha = znom / capap[ik]
+        u = u + alpha * zp[ik]
+        zr = zr - alpha * zq
+        if it == steps:
+            break
+        zar = A_mv(zr)
+        ikn = it % m
+        zp[ikn], zap[ikn] = zr.copy(), zar.copy()
+        for il in range(ik + 1):  # at a restart il == ikn is the slot being rebuilt
+            zq = zap[il]
+            beta = -(zq @ zar) / capap[il]
+            zp[ikn] = zp[ikn] + beta * zp[il]
+            zap[ikn] = zap[ikn] + beta * zq
+    return u, np.linalg.norm(zr) / bnorm
+
+
+@pytest.mark.parametrize("prec,eps,check", [("fp64", 1e-10, 1e-9), ("mixed", 1e-8, 2e-4), ("fp32", 1e-5, 1e-4)])
+def test_gcrm_converges(gpu, prec, eps, check):
+    import torch
+
+    hm = _mat(300.0)
+    u_true = np.random.default_rng(3).uniform(-1, 1, hm.nd)
+    b = oracle_hmvm(hm, u_true)
+    dt = torch.float32 if prec == "fp32" else torch.float64
+    with Plan(hm, prec) as plan:
+        bd = torch.from_numpy(b).to("cuda", dt)
+        ud = torch.zeros_like(bd)
+        steps, rel = plan.gcrm(bd, ud, eps=eps, max_steps=200, restart=4)
+        assert 4 < steps < 200 and rel < eps, (steps, rel)  # restarted at least once
+        ud2 = torch.zeros_like(bd)  # repeatable bit for bit
+        assert plan.gcrm(bd, ud2, eps=eps, max_steps=200, restart=4) == (steps, rel)
+        assert torch.equal(ud, ud2)
+        u = ud.cpu().numpy().astype(np.float64)
+    res = np.linalg.norm(b - oracle_hmvm(hm, u)) / np.linalg.norm(b)
+    assert res < check, res
+
+
+@pytest.mark.parametrize("m,steps", [(3, 7), (20, 5)])
+def test_gcrm_matches_numpy_iteration(gpu, m, steps):
+    import torch
+
+    hm = _mat(300.0)
+    b = np.random.default_rng(5).uniform(-1, 1, hm.nd)
+    u_np, rel_np = _numpy_gcrm(lambda v: oracle_hmvm(hm, v), b, steps, m)
+    with Plan(hm, "fp64") as plan:
+        bd = torch.from_numpy(b).cuda()
+        ud = torch.zeros_like(bd)
+        got_steps, rel = plan.gcrm(bd, ud, eps=0.0, max_steps=steps, restart=m)
+    assert got_steps == steps
+    assert abs(rel - rel_np) <= 1e-7 * rel_np
+    u = ud.cpu().numpy()
+    assert np.linalg.norm(u - u_np) <= 1e-7 * np.linalg.norm(u_np)
+
+
+def test_gcrm_rejects_bad_restart(gpu):
+    import torch
+
+    hm = _mat(300.0)
+    with Plan(hm, "fp64") as plan:
+        bd = torch.ones(hm.nd, dtype=torch.float64, device="cuda")
+        for m in (0, 65):
+            with pytest.raises(RuntimeError):
+                plan.gcrm(bd, torch.zeros_like(bd), restart=m)
