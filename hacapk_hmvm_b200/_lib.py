@@ -159,6 +159,11 @@ class HgenMatrix(C.Structure):
                 ("n_lowrank", C.c_int64), ("n_dense", C.c_int64), ("aca_incomplete", C.c_int64)]
 
 
+class AcaReport(C.Structure):
+    _fields_ = [("rounds", C.c_int32), ("ktmax", C.c_int32), ("scratch_bytes", C.c_int64),
+                ("ms_aca", C.c_double), ("ms_dense", C.c_double), ("ms_gather_copy", C.c_double)]
+
+
 # Every C symbol declared in include/hmvm_b200.h, with (restype, argtypes).
 HMVM_SIGNATURES = {
     "hmvm_b200_load_hmatrix": (C.c_int, [C.c_char_p, C.POINTER(Matrix_d), C.POINTER(Matrix2_d)]),
@@ -221,11 +226,15 @@ HMVM_SIGNATURES = {
     "hmvm_b200_plan_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "hmvm_b200_plan_profile_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "hmvm_b200_plan_status": (C.c_int, [C.c_void_p]),
+    "hmvm_b200_aca_fill": (C.c_int, [C.POINTER(HgenMatrix), C.POINTER(HgenParams), C.c_int32,
+                                     C.POINTER(AcaReport)]),
 }
 
 HGEN_SIGNATURES = {
     "hgen_default_params": (None, [C.POINTER(HgenParams)]),
     "hgen_build": (C.c_int, [C.POINTER(HgenParams), C.POINTER(C.POINTER(HgenMatrix))]),
+    "hgen_build_tree": (C.c_int, [C.POINTER(HgenParams), C.POINTER(C.POINTER(HgenMatrix))]),
+    "hgen_fill_leaves": (C.c_int, [C.POINTER(HgenMatrix), C.POINTER(HgenParams)]),
     "hgen_free": (None, [C.POINTER(HgenMatrix)]),
     "hgen_write_bin1": (C.c_int, [C.POINTER(HgenMatrix), C.c_char_p]),
     "hgen_write_bin2": (C.c_int, [C.POINTER(HgenMatrix), C.c_char_p]),

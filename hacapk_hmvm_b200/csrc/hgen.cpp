@@ -374,7 +374,7 @@ void hgen_free(hgen_hmatrix* m) {
   free(m);
 }
 
-int hgen_build(const hgen_params* p, hgen_hmatrix** out) {
+int hgen_build_tree(const hgen_params* p, hgen_hmatrix** out) {
   *out = nullptr;
   if (!p || p->n < 1 || p->n > INT32_MAX || p->leaf_size < 1 || !(p->eta >= 0.0) ||
       !(p->eps > 0.0) || p->kmax < 1 || p->geometry < 0 || p->geometry > 2)
@@ -424,6 +424,37 @@ int hgen_build(const hgen_params* p, hgen_hmatrix** out) {
     }
   }
 
+  // Structural arrays in file order; no leaf data yet.
+  m->nlf = nlf;
+  size_t nb = (size_t)(nlf > 0 ? nlf : 1);
+  m->ltmtx = (int32_t*)malloc(nb * 4); m->kt = (int32_t*)calloc(nb, 4);
+  m->ndl = (int32_t*)malloc(nb * 4); m->ndt = (int32_t*)malloc(nb * 4);
+  m->nstrtl = (int32_t*)malloc(nb * 4); m->nstrtt = (int32_t*)malloc(nb * 4);
+  m->a1 = (int64_t*)calloc(nb, 8); m->a2 = (int64_t*)calloc(nb, 8);
+  if (!m->ltmtx || !m->kt || !m->ndl || !m->ndt || !m->nstrtl || !m->nstrtt || !m->a1 || !m->a2) {
+    hgen_free(m);
+    return HGEN_ENOMEM;
+  }
+  for (int32_t i = 0; i < nlf; i++) {
+    const Leaf& lf = leaves[i];
+    m->ltmtx[i] = lf.ltmtx; m->ndl[i] = lf.ndl; m->ndt[i] = lf.ndt;
+    m->nstrtl[i] = lf.nstrtl; m->nstrtt[i] = lf.nstrtt;
+    if (lf.ltmtx == 1) m->n_lowrank++;
+    else m->n_dense++;
+  }
+  *out = m;
+  return HGEN_OK;
+}
+
+int hgen_fill_leaves(hgen_hmatrix* m, const hgen_params* p) {
+  if (!m || !p || m->rowmat || !(p->eps > 0.0) || p->kmax < 1) return HGEN_EINVAL;
+#ifdef _OPENMP
+  if (p->nthreads > 0) omp_set_num_threads(p->nthreads);
+#endif
+  const int32_t nlf = m->nlf;
+  std::vector<Leaf> leaves((size_t)nlf);
+  for (int32_t i = 0; i < nlf; i++)
+    leaves[i] = Leaf{m->ltmtx[i], m->ndl[i], m->ndt[i], m->nstrtl[i], m->nstrtt[i], 0};
   // ACA for every low-rank leaf (independent per leaf; results do not depend on
   // the thread count).
   std::vector<AcaOut> fac(nlf);
@@ -449,44 +480,31 @@ int hgen_build(const hgen_params* p, hgen_hmatrix** out) {
     leaves[i].kt = fac[i].kt;
     if (fac[i].incomplete) incomplete++;
   }
-  if (oom) { hgen_free(m); return HGEN_ENOMEM; }
+  if (oom) return HGEN_ENOMEM;
 
   // Offsets in file order, then the single packed array.
-  m->nlf = nlf;
-  size_t nb = (size_t)(nlf > 0 ? nlf : 1);
-  m->ltmtx = (int32_t*)malloc(nb * 4); m->kt = (int32_t*)malloc(nb * 4);
-  m->ndl = (int32_t*)malloc(nb * 4); m->ndt = (int32_t*)malloc(nb * 4);
-  m->nstrtl = (int32_t*)malloc(nb * 4); m->nstrtt = (int32_t*)malloc(nb * 4);
-  m->a1 = (int64_t*)malloc(nb * 8); m->a2 = (int64_t*)malloc(nb * 8);
-  if (!m->ltmtx || !m->kt || !m->ndl || !m->ndt || !m->nstrtl || !m->nstrtt || !m->a1 || !m->a2) {
-    hgen_free(m);
-    return HGEN_ENOMEM;
-  }
   int64_t off = 0;
   int32_t ktmax = 0;
   for (int32_t i = 0; i < nlf; i++) {
     const Leaf& lf = leaves[i];
-    m->ltmtx[i] = lf.ltmtx; m->kt[i] = lf.kt; m->ndl[i] = lf.ndl; m->ndt[i] = lf.ndt;
-    m->nstrtl[i] = lf.nstrtl; m->nstrtt[i] = lf.nstrtt;
+    m->kt[i] = lf.kt;
     if (lf.ltmtx == 1) {
       m->a1[i] = off;
       off += (int64_t)lf.kt * lf.ndt;
       m->a2[i] = off;
       off += (int64_t)lf.kt * lf.ndl;
       if (lf.kt > ktmax) ktmax = lf.kt;
-      m->n_lowrank++;
     } else {
       m->a1[i] = off;
       m->a2[i] = 0;
       off += (int64_t)lf.ndl * lf.ndt;
-      m->n_dense++;
     }
   }
   m->len = off;
   m->ktmax = ktmax;
   m->aca_incomplete = incomplete;
   m->rowmat = (double*)malloc(sizeof(double) * (size_t)(off > 0 ? off : 1));
-  if (!m->rowmat) { hgen_free(m); return HGEN_ENOMEM; }
+  if (!m->rowmat) return HGEN_ENOMEM;
 #pragma omp parallel for schedule(dynamic, 16)
   for (int32_t i = 0; i < nlf; i++) {
     const Leaf& lf = leaves[i];
@@ -505,6 +523,20 @@ int hgen_build(const hgen_params* p, hgen_hmatrix** out) {
           a[it + (int64_t)il * lf.ndt] = kernel_entry(m->coords, pi, m->lod[it + lf.nstrtt - 1] - 1);
       }
     }
+  }
+  return HGEN_OK;
+}
+
+int hgen_build(const hgen_params* p, hgen_hmatrix** out) {
+  if (!out) return HGEN_EINVAL;
+  *out = nullptr;
+  hgen_hmatrix* m = nullptr;
+  int rc = hgen_build_tree(p, &m);
+  if (rc) return rc;
+  rc = hgen_fill_leaves(m, p);
+  if (rc) {
+    hgen_free(m);
+    return rc;
   }
   *out = m;
   return HGEN_OK;

@@ -95,7 +95,13 @@ class HMatrix:
     @classmethod
     def generate(cls, n: int, geometry: str | int = "sphere", leaf_size: int = 32, eta: float = 2.0,
                  eps: float = 1e-4, seed: int = 1, kmax: int = 1000, aca_eps_factor: float = 1e-3,
-                 nthreads: int = 0) -> "HMatrix":
+                 nthreads: int = 0, fill: str = "cpu", device: int = 0) -> "HMatrix":
+        """An H-matrix of the point kernel built with HACApK's rules.  `fill`:
+        "cpu" fills the leaves on the host (hgen_fill_leaves, OpenMP); "gpu" on
+        `device` (hmvm_b200_aca_fill; bit-identical leaf data, report in
+        meta["aca_report"])."""
+        if fill not in ("cpu", "gpu"):
+            raise ValueError("fill must be 'cpu' or 'gpu'")
         lib = _lib.hgen_lib()
         p = _lib.HgenParams()
         lib.hgen_default_params(C.byref(p))
@@ -109,9 +115,22 @@ class HMatrix:
         p.aca_eps_factor = float(aca_eps_factor)
         p.nthreads = int(nthreads)
         mp = C.POINTER(_lib.HgenMatrix)()
-        rc = lib.hgen_build(C.byref(p), C.byref(mp))
+        rc = lib.hgen_build_tree(C.byref(p), C.byref(mp))
         if rc != 0:
-            raise RuntimeError(f"hgen_build failed with status {rc}")
+            raise RuntimeError(f"hgen_build_tree failed with status {rc}")
+        report = None
+        if fill == "cpu":
+            rc = lib.hgen_fill_leaves(mp, C.byref(p))
+            where = "hgen_fill_leaves"
+        else:
+            report = _lib.AcaReport()
+            rc = _lib.hmvm_lib().hmvm_b200_aca_fill(mp, C.byref(p), int(device), C.byref(report))
+            where = "hmvm_b200_aca_fill"
+        if rc != 0:
+            lib.hgen_free(mp)
+            if fill == "gpu":
+                _lib.check(rc, where)
+            raise RuntimeError(f"{where} failed with status {rc}")
         m = mp.contents
         nlf = m.nlf
         owner = _COwner(mp, lib.hgen_free)
@@ -128,6 +147,8 @@ class HMatrix:
                       n_lowrank=int(m.n_lowrank), n_dense=int(m.n_dense),
                       aca_incomplete=int(m.aca_incomplete)),
         )
+        if report is not None:
+            obj.meta["aca_report"] = {f: getattr(report, f) for f, _ in _lib.AcaReport._fields_}
         obj.meta["lod"] = _np_from(m.lod, m.nd, np.int32)
         obj.meta["coords"] = _np_from(m.coords, 3 * m.nd, np.float64).reshape(-1, 3)
         obj._keep.append(owner)

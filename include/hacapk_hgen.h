@@ -68,7 +68,16 @@ typedef struct hgen_hmatrix {
 } hgen_hmatrix;
 
 void hgen_default_params(hgen_params* p);
+/* hgen_build = hgen_build_tree + hgen_fill_leaves. */
 int hgen_build(const hgen_params* p, hgen_hmatrix** out);
+/* Points, cluster tree, block tree and leaf order only: the leaf arrays are
+ * set, kt / a1 / a2 are 0, rowmat is NULL and len 0.  Fill it with
+ * hgen_fill_leaves (host, OpenMP) or hmvm_b200_aca_fill (GPU, libhmvm_b200). */
+int hgen_build_tree(const hgen_params* p, hgen_hmatrix** out);
+/* ACA for the low-rank leaves and kernel entries for the dense ones
+ * (HACApK_fill_leafmtx_hyp, src_hdump/m_HACApK_base.f90:580-662); sets kt,
+ * a1, a2, len, ktmax, aca_incomplete and allocates rowmat. */
+int hgen_fill_leaves(hgen_hmatrix* m, const hgen_params* p);
 void hgen_free(hgen_hmatrix* m);
 
 /* Writers.  bin2's int32 `len` header field is written saturated at INT32_MAX

@@ -278,6 +278,26 @@ int hmvm_b200_bicgstab(hmvm_plan *plan, const void *b_dev, void *u_dev, int32_t 
 int hmvm_b200_gcrm(hmvm_plan *plan, const void *b_dev, void *u_dev, int32_t max_steps, int32_t restart, double eps,
                    int32_t *steps, double *relres, void *stream);
 
+/* ---- leaf fill on the GPU ------------------------------------------------------
+ * Fills a matrix from hgen_build_tree (include/hacapk_hgen.h) on `device`: ACA
+ * for its low-rank leaves (HACApK_aca, src_hdump/m_HACApK_base.f90:494-577)
+ * and kernel entries for its dense leaves (HACApK_fill_leafmtx_hyp, :580-662),
+ * with results bit-identical to hgen_fill_leaves.  Sets kt, a1, a2, len, ktmax
+ * and aca_incomplete and allocates rowmat (malloc; hgen_free releases it).
+ * The matrix is left unchanged on failure. */
+struct hgen_hmatrix;
+struct hgen_params;
+typedef struct hmvm_aca_report {
+  int32_t rounds;        /* capacity rounds (32, 128, 512, ... terms per leaf) */
+  int32_t ktmax;
+  int64_t scratch_bytes; /* device factor scratch over all rounds */
+  double ms_aca;         /* device time of the ACA rounds */
+  double ms_dense;       /* ... of the dense-leaf fill */
+  double ms_gather_copy; /* ... of packing the factors and copying rowmat to the host */
+} hmvm_aca_report;
+int hmvm_b200_aca_fill(struct hgen_hmatrix *m, const struct hgen_params *p, int32_t device,
+                       hmvm_aca_report *report);
+
 /* ---- autotuner ---------------------------------------------------------------
  * Picks, per leaf shape class -- the V stage (stacked low-rank V factors) and
  * the row stage (row tiles of dense leaves and U factors) -- the kernel

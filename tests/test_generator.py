@@ -99,3 +99,60 @@ def test_write_rejects_range(tmp_path):
     hm = HMatrix.from_arrays(1, 1, [2], [0], [1], [1], [1], [1], [0], [0], np.array([1.0]))
     hm.write_bin1(str(tmp_path / "ok.bin"))
     assert HMatrix.load(str(tmp_path / "ok.bin")).rowmat[0] == 1.0
+
+
+def test_tree_then_fill_equals_build():
+    """hgen_build == hgen_build_tree + hgen_fill_leaves, and the tree alone
+    carries no leaf data."""
+    import ctypes as C
+
+    from hacapk_hmvm_b200 import _lib
+
+    lib = _lib.hgen_lib()
+    p = _lib.HgenParams()
+    lib.hgen_default_params(C.byref(p))
+    p.n, p.geometry, p.eps, p.seed = 1500, 1, 1e-5, 11
+    whole, tree = C.POINTER(_lib.HgenMatrix)(), C.POINTER(_lib.HgenMatrix)()
+    assert lib.hgen_build(C.byref(p), C.byref(whole)) == 0
+    assert lib.hgen_build_tree(C.byref(p), C.byref(tree)) == 0
+    try:
+        t = tree.contents
+        assert not t.rowmat and t.len == 0 and t.nlf == whole.contents.nlf
+        assert lib.hgen_fill_leaves(tree, C.byref(p)) == 0
+        assert lib.hgen_fill_leaves(tree, C.byref(p)) != 0  # already filled
+        w = whole.contents
+        assert (t.len, t.ktmax, t.aca_incomplete) == (w.len, w.ktmax, w.aca_incomplete)
+        n = w.nlf
+        for f in ("ltmtx", "kt", "ndl", "ndt", "nstrtl", "nstrtt", "a1", "a2"):
+            dt = np.int64 if f in ("a1", "a2") else np.int32
+            assert np.array_equal(np.ctypeslib.as_array(getattr(t, f), (n,)).view(dt),
+                                  np.ctypeslib.as_array(getattr(w, f), (n,)).view(dt)), f
+        assert np.array_equal(np.ctypeslib.as_array(t.rowmat, (t.len,)), np.ctypeslib.as_array(w.rowmat, (w.len,)))
+    finally:
+        lib.hgen_free(whole)
+        lib.hgen_free(tree)
+
+
+def test_gpu_fill_refuses_without_device():
+    """hmvm_b200_aca_fill returns a status (no crash) where no sm_100 device is
+    usable, and leaves the matrix unfilled."""
+    import ctypes as C
+
+    import torch
+
+    from hacapk_hmvm_b200 import _lib
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    lib = _lib.hgen_lib()
+    p = _lib.HgenParams()
+    lib.hgen_default_params(C.byref(p))
+    p.n = 600
+    tree = C.POINTER(_lib.HgenMatrix)()
+    assert lib.hgen_build_tree(C.byref(p), C.byref(tree)) == 0
+    try:
+        rep = _lib.AcaReport()
+        rc = _lib.hmvm_lib().hmvm_b200_aca_fill(tree, C.byref(p), 0, C.byref(rep))
+        assert rc == _lib.HMVM_ENODEV and not tree.contents.rowmat
+    finally:
+        lib.hgen_free(tree)
