@@ -561,9 +561,12 @@ __host__ __device__ constexpr int mixed_batch() {
 // inputs at z.  Each of a vector's products goes to its own accumulator of
 // acc[8] (FP32 vectors use half of them: the caller passes acc or acc + 4 by
 // vector parity); FP64 vectors add to e[2].
+// Two independent FP32 FMAs as one packed sm_100 instruction (fma.rn.f32x2):
+// each lane rounds exactly as fmaf.
 __device__ __forceinline__ void fma2(float& a0, float& a1, const float2 m, const float2 z) {
-  a0 = fmaf(m.x, z.x, a0);
-  a1 = fmaf(m.y, z.y, a1);
+  const float2 r = __ffma2_rn(m, z, make_float2(a0, a1));
+  a0 = r.x;
+  a1 = r.y;
 }
 template <int TY>
 __device__ __forceinline__ void mixed_fma(const uint4 m, const unsigned char* z, float* acc, double* e) {
@@ -573,10 +576,8 @@ __device__ __forceinline__ void mixed_fma(const uint4 m, const unsigned char* z,
     e[1] = fma(__hiloint2double(m.w, m.z), zz.y, e[1]);
   } else if constexpr (TY == kF32) {
     const float4 zz = *reinterpret_cast<const float4*>(z);
-    acc[0] = fmaf(__uint_as_float(m.x), zz.x, acc[0]);
-    acc[1] = fmaf(__uint_as_float(m.y), zz.y, acc[1]);
-    acc[2] = fmaf(__uint_as_float(m.z), zz.z, acc[2]);
-    acc[3] = fmaf(__uint_as_float(m.w), zz.w, acc[3]);
+    fma2(acc[0], acc[1], make_float2(__uint_as_float(m.x), __uint_as_float(m.y)), make_float2(zz.x, zz.y));
+    fma2(acc[2], acc[3], make_float2(__uint_as_float(m.z), __uint_as_float(m.w)), make_float2(zz.z, zz.w));
   } else if constexpr (TY == kE4M3) {
     const float4* zz = reinterpret_cast<const float4*>(z);
     const uint32_t w[4] = {m.x, m.y, m.z, m.w};

@@ -146,22 +146,21 @@ __device__ __forceinline__ void gather_multi(const hmvm_tile_desc& d, const hmvm
   }
 }
 
-// acc[r] += a * z[r] for the NR inputs of one column (FP32 z).
+// acc[r] += a * z[r] for the NR inputs of one column (FP32 z); pairs of
+// right-hand sides as packed FP32 FMAs (fma2).
 template <int NR>
 __device__ __forceinline__ void axpy_f(float* acc, float a, const float* z) {
+  const float2 aa = make_float2(a, a);
   if constexpr (NR >= 4) {
 #pragma unroll
     for (int q = 0; q < NR / 4; q++) {
       const float4 zz = reinterpret_cast<const float4*>(z)[q];
-      acc[4 * q + 0] = fmaf(a, zz.x, acc[4 * q + 0]);
-      acc[4 * q + 1] = fmaf(a, zz.y, acc[4 * q + 1]);
-      acc[4 * q + 2] = fmaf(a, zz.z, acc[4 * q + 2]);
-      acc[4 * q + 3] = fmaf(a, zz.w, acc[4 * q + 3]);
+      fma2(acc[4 * q + 0], acc[4 * q + 1], aa, make_float2(zz.x, zz.y));
+      fma2(acc[4 * q + 2], acc[4 * q + 3], aa, make_float2(zz.z, zz.w));
     }
   } else if constexpr (NR == 2) {
     const float2 zz = *reinterpret_cast<const float2*>(z);
-    acc[0] = fmaf(a, zz.x, acc[0]);
-    acc[1] = fmaf(a, zz.y, acc[1]);
+    fma2(acc[0], acc[1], aa, zz);
   } else {
     acc[0] = fmaf(a, z[0], acc[0]);
   }
