@@ -158,7 +158,7 @@ __device__ __forceinline__ int tc_seg_type(int enc) { return enc >> 28; }
 
 template <int WPB, int S, int CHUNK>
 constexpr int tc_smem_bytes() {
-  return WPB * (S * CHUNK + 2 * kTcZBytes + kTcStageBytes) + kTcPad + 2048 + WPB * (S + 1) * 8 + 16;
+  return WPB * (S * CHUNK + 2 * kTcZBytes + kTcStageBytes) + kTcPad + 2048 + WPB * (S + 3) * 8 + 16;
 }
 
 template <int WPB, int S, int CHUNK, int MODE, bool VST>
@@ -187,9 +187,10 @@ __global__ void __launch_bounds__(32 * WPB, 1) hmvm_tc_kernel(TcArgs ta) {
   unsigned char* zbase = smem + kTcPad + (size_t)WPB * (kTcStageBytes + RING) + (size_t)warp * 2 * kTcZBytes;
   uint64_t* bars_all =
       reinterpret_cast<uint64_t*>(smem + kTcPad + (size_t)WPB * (kTcStageBytes + RING + 2 * kTcZBytes) + 2048);
-  uint64_t* bars = bars_all + warp * (S + 1);
-  uint64_t* mbar = bars + S;  // MMA completion
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars_all + WPB * (S + 1));
+  uint64_t* bars = bars_all + warp * (S + 3);
+  uint64_t* mbar = bars + S;      // MMA completion
+  uint64_t* zbars = bars + S + 1;  // input buffers 0 and 1 (bulk-copy completion)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars_all + WPB * (S + 3));
 
   // TMEM: warp 0 allocates for the CTA
   if (warp == 0) {
@@ -233,7 +234,7 @@ __global__ void __launch_bounds__(32 * WPB, 1) hmvm_tc_kernel(TcArgs ta) {
     nchunks = failed ? 0 : (total + CHUNK - 1) / CHUNK;
     if (lane == 0) {
 #pragma unroll
-      for (int s = 0; s <= S; s++) mbar_init(&bars[s], 1);
+      for (int s = 0; s < S + 3; s++) mbar_init(&bars[s], 1);
       fence_mbar_init();
     }
     __syncwarp();
@@ -249,50 +250,59 @@ __global__ void __launch_bounds__(32 * WPB, 1) hmvm_tc_kernel(TcArgs ta) {
 
     // inputs of one item: 16-bit segments go to the front of the buffer as
     // four planes of K16 rows (K16 = the run's columns, rounded up to 16);
-    // the other segments follow, in order, as ncp columns x 16 values.
-    auto gather = [&](const hmvm_tile_desc& d, const hmvm_seg_desc& sreg, unsigned char* zb, int* k16_out) {
-      int k16 = 0;
-      for (int j = 0; j < d.nseg; j++) {
-        const int enc = __shfl_sync(0xffffffffu, sreg.ncols, j);
-        if (tc_seg_type(enc) == LR) k16 += ((enc & 0x0fffffff) + 7) / 8 * 8;
+    // the other segments follow, in order, as ncp columns x 16 values.  Lane j
+    // takes segment j: its rows (plane slices, or input rows of 16 values) are
+    // contiguous in global memory, so each is one TMA bulk copy completing on
+    // the buffer's mbarrier (lane 0 posts the item's byte count); the padding
+    // is written with plain stores.
+    auto gather = [&](const hmvm_tile_desc& d, const hmvm_seg_desc& sreg, unsigned char* zb, uint64_t* zbar,
+                      int* k16_out) {
+      const bool has = lane < d.nseg;
+      const int type = has ? tc_seg_type(sreg.ncols) : -1;
+      const int nc = has ? (sreg.ncols & 0x0fffffff) : 0;
+      const int vs = has ? mixed_vec(type) : 1;
+      const int ncp = (nc + vs - 1) / vs * vs;
+      const bool lr = has && type == LR;
+      const int es = type == kF64 ? 8 : 4;
+      const int lr_rows = lr ? ncp : 0;
+      const int zb_bytes = (has && !lr) ? ncp * NR * es : 0;
+      int koff = lr_rows, zo = zb_bytes;  // inclusive scans, then made exclusive
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int k2 = __shfl_up_sync(0xffffffffu, koff, o), z2 = __shfl_up_sync(0xffffffffu, zo, o);
+        if (lane >= o) {
+          koff += k2;
+          zo += z2;
+        }
       }
+      const int k16 = __shfl_sync(0xffffffffu, koff, 31);
+      koff -= lr_rows;
+      zo -= zb_bytes;
       const int k16p = (k16 + 15) / 16 * 16;
       *k16_out = k16p;
-      int koff = 0;
-      int zoff = 4 * k16p * 16;
-      for (int j = 0; j < d.nseg; j++) {
-        const int src = __shfl_sync(0xffffffffu, sreg.src, j);
-        const int enc = __shfl_sync(0xffffffffu, sreg.ncols, j);
-        const int type = tc_seg_type(enc), nc = enc & 0x0fffffff;
-        const int vs = mixed_vec(type);
-        const int ncp = (nc + vs - 1) / vs * vs;
-        const int64_t row0 = src < 0 ? (src & 0x7fffffff) : src;
-        if (type == LR) {
-          // 4 planes x ncp rows of 16 bytes -> plane g at zb + g * k16p * 16, rows koff..
-          for (int c = lane; c < 4 * ncp; c += 32) {
-            const int g = c / ncp, r = c % ncp;
-            unsigned char* dst = zb + ((size_t)g * k16p + koff + r) * 16;
-            if (r < nc) cp_async<16>(dst, planes + ((int64_t)g * prows + row0 + r) * 8);
-            else *reinterpret_cast<uint4*>(dst) = make_uint4(0, 0, 0, 0);
-          }
-          koff += ncp;
-        } else if (type == kF64) {
-          const double* s = a.x64 + row0 * NR;
-          double* z = reinterpret_cast<double*>(zb + zoff);
-          for (int c = lane; c < ncp * NR / 2; c += 32) {
-            if (c < nc * NR / 2) cp_async<16>(z + 2 * c, s + 2 * c);
-            else *reinterpret_cast<double2*>(z + 2 * c) = make_double2(0.0, 0.0);
-          }
-          zoff += ncp * NR * 8;
-        } else {
-          const float* s = (src < 0 ? static_cast<const float*>(a.t) : a.x32) + row0 * NR;
-          float* z = reinterpret_cast<float*>(zb + zoff);
-          for (int c = lane; c < ncp * NR / 4; c += 32) {
-            if (c < nc * NR / 4) cp_async<16>(z + 4 * c, s + 4 * c);
-            else *reinterpret_cast<float4*>(z + 4 * c) = make_float4(0.f, 0.f, 0.f, 0.f);
-          }
-          zoff += ncp * NR * 4;
+      const int zoff = 4 * k16p * 16 + zo;
+      const uint32_t tx = lr ? 4u * nc * 16 : (has ? (uint32_t)nc * NR * es : 0u);
+      uint32_t tx_all = tx;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) tx_all += __shfl_xor_sync(0xffffffffu, tx_all, o);
+      fence_proxy_async();  // this buffer's earlier generic reads and stores before the async writes
+      __syncwarp();
+      if (lane == 0) mbar_expect_tx(zbar, tx_all);
+      __syncwarp();
+      const int64_t row0 = sreg.src < 0 ? (sreg.src & 0x7fffffff) : sreg.src;
+      if (lr) {
+        for (int g = 0; g < 4; g++) {
+          unsigned char* dst = zb + ((size_t)g * k16p + koff) * 16;
+          if (nc > 0) bulk_g2s(dst, planes + ((int64_t)g * prows + row0) * 8, (uint32_t)nc * 16, zbar);
+          for (int r = nc; r < ncp; r++) *reinterpret_cast<uint4*>(dst + (size_t)r * 16) = make_uint4(0, 0, 0, 0);
         }
+      } else if (has) {
+        const void* src = type == kF64 ? static_cast<const void*>(a.x64 + row0 * NR)
+                                       : static_cast<const void*>((sreg.src < 0 ? static_cast<const float*>(a.t)
+                                                                                : a.x32) + row0 * NR);
+        if (nc > 0) bulk_g2s(zb + zoff, src, (uint32_t)nc * NR * es, zbar);
+        for (int b = nc * NR * es; b < zb_bytes; b += 16)
+          *reinterpret_cast<uint4*>(zb + zoff + b) = make_uint4(0, 0, 0, 0);
       }
       // zero rows [k16, k16p) of the 16-bit planes
       for (int c = lane; c < 4 * (k16p - k16); c += 32) {
@@ -311,8 +321,12 @@ __global__ void __launch_bounds__(32 * WPB, 1) hmvm_tc_kernel(TcArgs ta) {
     };
     hmvm_seg_desc cur_seg = (!failed && lane < cur.nseg) ? segs[cur.seg_begin + lane] : szero;
     int cur_k16 = 0, nxt_k16 = 0;
-    if (!failed) gather(cur, cur_seg, zbase, &cur_k16);
-    cp_async_commit();
+    uint32_t zpar[2] = {0, 0};
+    bool zpend[2] = {false, false};
+    if (!failed) {
+      gather(cur, cur_seg, zbase, &zbars[0], &cur_k16);
+      zpend[0] = true;
+    }
     int cur_oidx = out_slot(cur);
     double cur_scale = row_scale(cur);
     hmvm_tile_desc nxt = tb + 1 < te ? tiles[tb + 1] : dzero;
@@ -321,14 +335,20 @@ __global__ void __launch_bounds__(32 * WPB, 1) hmvm_tc_kernel(TcArgs ta) {
     for (int ti = tb, k = 0; ti < te && !failed; ++ti, ++k) {
       unsigned char* zcur = zbase + (k & 1) * kTcZBytes;
       __syncwarp();
-      if (ti + 1 < te) gather(nxt, nxt_seg, zbase + ((k + 1) & 1) * kTcZBytes, &nxt_k16);
-      cp_async_commit();
+      if (ti + 1 < te) {
+        gather(nxt, nxt_seg, zbase + ((k + 1) & 1) * kTcZBytes, &zbars[(k + 1) & 1], &nxt_k16);
+        zpend[(k + 1) & 1] = true;
+      }
       const bool has_nn = ti + 2 < te;
       const hmvm_tile_desc nn = has_nn ? tiles[ti + 2] : dzero;
       const int nxt_oidx = ti + 1 < te ? out_slot(nxt) : 0;
       const double nxt_scale = ti + 1 < te ? row_scale(nxt) : 1.0;
-      cp_async_wait<1>();
-      __syncwarp();
+      if (!warp_wait(&zbars[k & 1], zpar[k & 1])) {
+        failed = true;
+        break;
+      }
+      zpar[k & 1] ^= 1;
+      zpend[k & 1] = false;
 
       const int R = cur.nrows;
       const uint32_t rstride = (uint32_t)R * 16;
@@ -519,12 +539,13 @@ __global__ void __launch_bounds__(32 * WPB, 1) hmvm_tc_kernel(TcArgs ta) {
       nxt = nn;
       nxt_seg = (has_nn && lane < nn.nseg) ? segs[nn.seg_begin + lane] : szero;
     }
-    cp_async_wait<0>();
     if (failed) {
       // let the copies and MMAs in flight finish (bounded) before the shared
       // memory and TMEM go away
       const uint32_t issued = min(nchunks, q_rel + (uint32_t)S);
       for (uint32_t q = q_ready; q < issued; q++) warp_wait(&bars[q % S], (q / S) & 1);
+      for (int b = 0; b < 2; b++)
+        if (zpend[b]) warp_wait(&zbars[b], zpar[b]);
       if (mma_open) warp_wait(mbar, mma_phase);
       if (lane == 0) atomicExch(a.err, 1);
     }
