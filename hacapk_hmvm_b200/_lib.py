@@ -149,6 +149,13 @@ class HgenParams(C.Structure):
                 ("nthreads", C.c_int32), ("seed", C.c_uint64)]
 
 
+class HgenMesh(C.Structure):
+    _fields_ = [("nond", C.c_int32), ("nofc", C.c_int32), ("nond_on_face", C.c_int32), ("nint_para_fc", C.c_int32),
+                ("ndble_para_fc", C.c_int32), ("_pad0", C.c_int32), ("nodes", C.POINTER(C.c_double)),
+                ("face2node", C.POINTER(C.c_int32)), ("int_para_fc", C.POINTER(C.c_int32)),
+                ("dble_para_fc", C.POINTER(C.c_double))]
+
+
 class HgenMatrix(C.Structure):
     _fields_ = [("nd", C.c_int32), ("nlf", C.c_int32), ("ktmax", C.c_int32), ("_pad0", C.c_int32),
                 ("len", C.c_int64),
@@ -156,7 +163,8 @@ class HgenMatrix(C.Structure):
                 ("ndt", C.POINTER(C.c_int32)), ("nstrtl", C.POINTER(C.c_int32)), ("nstrtt", C.POINTER(C.c_int32)),
                 ("a1", C.POINTER(C.c_int64)), ("a2", C.POINTER(C.c_int64)), ("rowmat", C.POINTER(C.c_double)),
                 ("lod", C.POINTER(C.c_int32)), ("coords", C.POINTER(C.c_double)),
-                ("n_lowrank", C.c_int64), ("n_dense", C.c_int64), ("aca_incomplete", C.c_int64)]
+                ("n_lowrank", C.c_int64), ("n_dense", C.c_int64), ("aca_incomplete", C.c_int64),
+                ("mesh", C.POINTER(HgenMesh))]
 
 
 class AcaReport(C.Structure):
@@ -234,6 +242,9 @@ HGEN_SIGNATURES = {
     "hgen_default_params": (None, [C.POINTER(HgenParams)]),
     "hgen_build": (C.c_int, [C.POINTER(HgenParams), C.POINTER(C.POINTER(HgenMatrix))]),
     "hgen_build_tree": (C.c_int, [C.POINTER(HgenParams), C.POINTER(C.POINTER(HgenMatrix))]),
+    "hgen_build_tree_mesh": (C.c_int, [C.POINTER(HgenParams), C.POINTER(HgenMesh), C.POINTER(C.POINTER(HgenMatrix))]),
+    "hgen_read_pbf": (C.c_int, [C.c_char_p, C.POINTER(C.POINTER(HgenMesh))]),
+    "hgen_free_mesh": (None, [C.POINTER(HgenMesh)]),
     "hgen_fill_leaves": (C.c_int, [C.POINTER(HgenMatrix), C.POINTER(HgenParams)]),
     "hgen_free": (None, [C.POINTER(HgenMatrix)]),
     "hgen_write_bin1": (C.c_int, [C.POINTER(HgenMatrix), C.c_char_p]),

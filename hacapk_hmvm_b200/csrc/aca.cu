@@ -527,6 +527,7 @@ int aca_fill(hgen_hmatrix* m, const hgen_params* p, cudaStream_t st, hmvm_aca_re
 extern "C" int hmvm_b200_aca_fill(hgen_hmatrix* m, const hgen_params* p, int32_t device, hmvm_aca_report* report) {
   if (!m || !p) return set_error(HMVM_EINVAL, "NULL argument");
   if (m->rowmat) return set_error(HMVM_EINVAL, "aca fill: the matrix already holds leaf data");
+  if (m->mesh) return set_error(HMVM_EINVAL, "aca fill: the GPU fill evaluates the point kernel only (not a mesh)");
   if (!(p->eps > 0.0) || p->kmax < 1) return set_error(HMVM_EINVAL, "aca fill: eps must be > 0 and kmax >= 1");
   if (m->nlf > 0 && (!m->ltmtx || !m->ndl || !m->ndt || !m->nstrtl || !m->nstrtt || !m->kt || !m->a1 || !m->a2))
     return set_error(HMVM_EINVAL, "aca fill: missing leaf array");

@@ -74,6 +74,81 @@ inline double kernel_entry(const double* xyz, int32_t i, int32_t j) {
   return 1.0 / (4.0 * kPi * std::sqrt(dx * dx + dy * dy + dz * dz));
 }
 
+// ppohBEM's collocation kernel (face_integral, src_hdump/m_ppohBEM_user_func.f90:
+// 49-100): the potential at (x, y, z) of a uniform unit charge density on the
+// triangle (xs, ys, zs), from the closed-form edge terms.  The module's PI and
+// EPSILON_0 are default-kind (single precision) Fortran literals promoted to
+// double; they are reproduced as such.  Operation order follows the source.
+inline void cross3(const double* u, const double* v, double* w) {
+  w[0] = u[1] * v[2] - u[2] * v[1];
+  w[1] = u[2] * v[0] - u[0] * v[2];
+  w[2] = u[0] * v[1] - u[1] * v[0];
+}
+double face_integral(const double* xs, const double* ys, const double* zs, double x, double y, double z) {
+  const double pi_f = (double)3.141592653589793f;
+  const double eps0 = (double)8.854187818f * 1e-12;
+  double r[3];
+  for (int k = 0; k < 3; k++)
+    r[k] = std::sqrt((xs[k] - x) * (xs[k] - x) + (ys[k] - y) * (ys[k] - y) + (zs[k] - z) * (zs[k] - z));
+  double u[3] = {xs[1] - xs[0], ys[1] - ys[0], zs[1] - zs[0]};
+  double v[3] = {xs[2] - xs[1], ys[2] - ys[1], zs[2] - zs[1]};
+  double w[3];
+  cross3(u, v, w);
+  const double wn = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+  for (int k = 0; k < 3; k++) w[k] = w[k] / wn;
+  u[0] = x - xs[0];
+  u[1] = y - ys[0];
+  u[2] = z - zs[0];
+  const double zp = u[0] * w[0] + u[1] * w[1] + u[2] * w[2];
+  const double ox = x - zp * w[0], oy = y - zp * w[1], oz = z - zp * w[2];
+  const double zpabs = std::fabs(zp);
+  double sum = 0.0;
+  for (int i = 0; i < 3; i++) {
+    const int j = (i + 1) % 3;
+    u[0] = xs[j] - ox;
+    u[1] = ys[j] - oy;
+    u[2] = zs[j] - oz;
+    const double xj = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    for (int k = 0; k < 3; k++) u[k] = u[k] / xj;
+    cross3(w, u, v);
+    const double xi = (xs[i] - ox) * u[0] + (ys[i] - oy) * u[1] + (zs[i] - oz) * u[2];
+    const double yi = (xs[i] - ox) * v[0] + (ys[i] - oy) * v[1] + (zs[i] - oz) * v[2];
+    const double dx = xj - xi, dy = -yi;  // yj = 0
+    const double t = std::sqrt(dx * dx + dy * dy);
+    const double l = dx / t, mm = dy / t;
+    const double d = l * yi - mm * xi;
+    const double ti = l * xi + mm * yi, tj = l * xj;
+    const double theta = std::atan2(yi, xi);
+    const double omega = theta - std::atan2(r[i] * d, zpabs * ti) + std::atan2(r[j] * d, zpabs * tj);
+    const double q = std::log((r[j] + tj) / (r[i] + ti));
+    const double g = d * q - zpabs * omega;
+    sum = sum + g;
+  }
+  return std::fabs(sum) / (4.0 * pi_f * eps0);
+}
+
+// The matrix entry between original points (or faces) i and j, 0-based: the
+// point kernel, or for a mesh ppohBEM_matrix_element_ij
+// (src_hdump/m_ppohBEM_matrix_element_ij.f90): face j's integral at the
+// centroid of face i.
+struct Kernel {
+  const double* xyz;
+  const hgen_mesh* mesh;
+  double operator()(int32_t i, int32_t j) const {
+    if (!mesh) return kernel_entry(xyz, i, j);
+    const int32_t* fi = mesh->face2node + (int64_t)i * mesh->nond_on_face;
+    const int32_t* fj = mesh->face2node + (int64_t)j * mesh->nond_on_face;
+    const double* np = mesh->nodes;
+    const double xp = (np[3 * fi[0]] + np[3 * fi[1]] + np[3 * fi[2]]) / 3.0;
+    const double yp = (np[3 * fi[0] + 1] + np[3 * fi[1] + 1] + np[3 * fi[2] + 1]) / 3.0;
+    const double zp = (np[3 * fi[0] + 2] + np[3 * fi[1] + 2] + np[3 * fi[2] + 2]) / 3.0;
+    const double xf[3] = {np[3 * fj[0]], np[3 * fj[1]], np[3 * fj[2]]};
+    const double yf[3] = {np[3 * fj[0] + 1], np[3 * fj[1] + 1], np[3 * fj[2] + 1]};
+    const double zf[3] = {np[3 * fj[0] + 2], np[3 * fj[1] + 2], np[3 * fj[2] + 2]};
+    return face_integral(xf, yf, zf, xp, yp, zp);
+  }
+};
+
 // ---------------------------------------------------------------------------
 // Cluster tree (HACApK_generate_cbitree, m_HACApK_base.f90:994-1054) with
 // bounding boxes (HACApK_bndbox, :953-991).
@@ -265,8 +340,8 @@ struct AcaOut {
 
 // Partially pivoted ACA (HACApK_aca, m_HACApK_base.f90:494-577) with
 // param(61)=1 (the k=1 term's norm is the block norm), param(64)=1.
-void aca(const double* xyz, const int32_t* lod, const Leaf& lf, int32_t kmax, double eps,
-         double aca_eps, AcaOut& o) {
+void aca(const Kernel& K, const int32_t* lod, const Leaf& lf, int32_t kmax, double eps, double aca_eps,
+         AcaOut& o) {
   const int32_t ndl = lf.ndl, ndt = lf.ndt, nstrtl = lf.nstrtl, nstrtt = lf.nstrtt;
   const int32_t krank = std::min(ndl, ndt);
   const int32_t kstop = std::min(kmax, krank);
@@ -280,7 +355,7 @@ void aca(const double* xyz, const int32_t* lod, const Leaf& lf, int32_t kmax, do
   double znrm = 0.0, zeps = 0.0;
   std::vector<double> zau;
   // Entry of the permuted matrix at 1-based positions (lod holds 1-based point ids).
-  auto ent = [&](int32_t ill, int32_t itt) { return kernel_entry(xyz, lod[ill - 1] - 1, lod[itt - 1] - 1); };
+  auto ent = [&](int32_t ill, int32_t itt) { return K(lod[ill - 1] - 1, lod[itt - 1] - 1); };
   for (;;) {
     V.resize((size_t)ndt * k);
     U.resize((size_t)ndl * k);
@@ -374,23 +449,10 @@ void hgen_free(hgen_hmatrix* m) {
   free(m);
 }
 
-int hgen_build_tree(const hgen_params* p, hgen_hmatrix** out) {
-  *out = nullptr;
-  if (!p || p->n < 1 || p->n > INT32_MAX || p->leaf_size < 1 || !(p->eta >= 0.0) ||
-      !(p->eps > 0.0) || p->kmax < 1 || p->geometry < 0 || p->geometry > 2)
-    return HGEN_EINVAL;
-#ifdef _OPENMP
-  if (p->nthreads > 0) omp_set_num_threads(p->nthreads);
-#endif
-  const int32_t n = (int32_t)p->n;
-  hgen_hmatrix* m = (hgen_hmatrix*)calloc(1, sizeof(hgen_hmatrix));
-  if (!m) return HGEN_ENOMEM;
-  m->nd = n;
-  m->coords = (double*)malloc(sizeof(double) * 3 * (size_t)n);
-  m->lod = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
-  if (!m->coords || !m->lod) { hgen_free(m); return HGEN_ENOMEM; }
-  make_points(n, p->geometry, p->seed, m->coords);
-
+// Cluster tree, block tree and leaf order over m->coords (m->nd points);
+// frees m on failure.
+static int build_tree_points(const hgen_params* p, hgen_hmatrix* m, hgen_hmatrix** out) {
+  const int32_t n = m->nd;
   std::vector<Leaf> leaves;
   try {
     Tree t;
@@ -446,6 +508,57 @@ int hgen_build_tree(const hgen_params* p, hgen_hmatrix** out) {
   return HGEN_OK;
 }
 
+static bool tree_params_ok(const hgen_params* p) {
+  return p && p->leaf_size >= 1 && p->eta >= 0.0 && p->eps > 0.0 && p->kmax >= 1;
+}
+
+int hgen_build_tree(const hgen_params* p, hgen_hmatrix** out) {
+  if (!out) return HGEN_EINVAL;
+  *out = nullptr;
+  if (!tree_params_ok(p) || p->n < 1 || p->n > INT32_MAX || p->geometry < 0 || p->geometry > 2)
+    return HGEN_EINVAL;
+#ifdef _OPENMP
+  if (p->nthreads > 0) omp_set_num_threads(p->nthreads);
+#endif
+  const int32_t n = (int32_t)p->n;
+  hgen_hmatrix* m = (hgen_hmatrix*)calloc(1, sizeof(hgen_hmatrix));
+  if (!m) return HGEN_ENOMEM;
+  m->nd = n;
+  m->coords = (double*)malloc(sizeof(double) * 3 * (size_t)n);
+  m->lod = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+  if (!m->coords || !m->lod) { hgen_free(m); return HGEN_ENOMEM; }
+  make_points(n, p->geometry, p->seed, m->coords);
+  return build_tree_points(p, m, out);
+}
+
+int hgen_build_tree_mesh(const hgen_params* p, const hgen_mesh* mesh, hgen_hmatrix** out) {
+  if (!out) return HGEN_EINVAL;
+  *out = nullptr;
+  if (!tree_params_ok(p) || !mesh || mesh->nofc < 1 || mesh->nond_on_face != 3 || !mesh->nodes ||
+      !mesh->face2node)
+    return HGEN_EINVAL;
+  for (int64_t k = 0; k < (int64_t)mesh->nofc * 3; k++)
+    if (mesh->face2node[k] < 0 || mesh->face2node[k] >= mesh->nond) return HGEN_EINVAL;
+#ifdef _OPENMP
+  if (p->nthreads > 0) omp_set_num_threads(p->nthreads);
+#endif
+  const int32_t n = mesh->nofc;
+  hgen_hmatrix* m = (hgen_hmatrix*)calloc(1, sizeof(hgen_hmatrix));
+  if (!m) return HGEN_ENOMEM;
+  m->nd = n;
+  m->mesh = mesh;
+  m->coords = (double*)malloc(sizeof(double) * 3 * (size_t)n);
+  m->lod = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+  if (!m->coords || !m->lod) { hgen_free(m); return HGEN_ENOMEM; }
+  // cluster points: face centroids (m_ppohBEM_bembb2hacapk.f90, "center of balance")
+  const double* np = mesh->nodes;
+  for (int32_t f = 0; f < n; f++) {
+    const int32_t* fn = mesh->face2node + 3 * (int64_t)f;
+    for (int d = 0; d < 3; d++) m->coords[3 * f + d] = (np[3 * fn[0] + d] + np[3 * fn[1] + d] + np[3 * fn[2] + d]) / 3.0;
+  }
+  return build_tree_points(p, m, out);
+}
+
 int hgen_fill_leaves(hgen_hmatrix* m, const hgen_params* p) {
   if (!m || !p || m->rowmat || !(p->eps > 0.0) || p->kmax < 1) return HGEN_EINVAL;
 #ifdef _OPENMP
@@ -472,7 +585,7 @@ int hgen_fill_leaves(hgen_hmatrix* m, const hgen_params* p) {
   for (size_t oi = 0; oi < order.size(); oi++) {
     int32_t i = order[oi];
     try {
-      aca(m->coords, m->lod, leaves[i], p->kmax, p->eps, aca_eps, fac[i]);
+      aca(Kernel{m->coords, m->mesh}, m->lod, leaves[i], p->kmax, p->eps, aca_eps, fac[i]);
     } catch (const std::bad_alloc&) {
 #pragma omp critical
       oom = true;
@@ -505,6 +618,7 @@ int hgen_fill_leaves(hgen_hmatrix* m, const hgen_params* p) {
   m->aca_incomplete = incomplete;
   m->rowmat = (double*)malloc(sizeof(double) * (size_t)(off > 0 ? off : 1));
   if (!m->rowmat) return HGEN_ENOMEM;
+  const Kernel K{m->coords, m->mesh};
 #pragma omp parallel for schedule(dynamic, 16)
   for (int32_t i = 0; i < nlf; i++) {
     const Leaf& lf = leaves[i];
@@ -520,7 +634,7 @@ int hgen_fill_leaves(hgen_hmatrix* m, const hgen_params* p) {
       for (int32_t il = 0; il < lf.ndl; il++) {
         int32_t pi = m->lod[il + lf.nstrtl - 1] - 1;
         for (int32_t it = 0; it < lf.ndt; it++)
-          a[it + (int64_t)il * lf.ndt] = kernel_entry(m->coords, pi, m->lod[it + lf.nstrtt - 1] - 1);
+          a[it + (int64_t)il * lf.ndt] = K(pi, m->lod[it + lf.nstrtt - 1] - 1);
       }
     }
   }
@@ -542,8 +656,91 @@ int hgen_build(const hgen_params* p, hgen_hmatrix** out) {
   return HGEN_OK;
 }
 
+// ---- .pbf meshes --------------------------------------------------------------
+namespace {
+// Whitespace-separated tokens of a list-directed Fortran text file (numbers
+// may use d / D exponents).
+struct Tokens {
+  FILE* f;
+  bool next(char* buf, size_t cap) {
+    int c;
+    do c = fgetc(f);
+    while (c != EOF && (c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == ','));
+    if (c == EOF) return false;
+    size_t n = 0;
+    while (c != EOF && c != ' ' && c != '\t' && c != '\n' && c != '\r' && c != ',') {
+      if (n + 1 < cap) buf[n++] = (c == 'd' || c == 'D') ? 'e' : (char)c;
+      c = fgetc(f);
+    }
+    buf[n] = 0;
+    return true;
+  }
+  bool real(double* v) {
+    char b[128], *end;
+    if (!next(b, sizeof b)) return false;
+    *v = std::strtod(b, &end);
+    return end != b && *end == 0;
+  }
+  bool integer(int32_t* v) {
+    char b[64], *end;
+    if (!next(b, sizeof b)) return false;
+    const long x = std::strtol(b, &end, 10);
+    if (end == b || *end != 0 || x < INT32_MIN || x > INT32_MAX) return false;
+    *v = (int32_t)x;
+    return true;
+  }
+};
+}  // namespace
+
+void hgen_free_mesh(hgen_mesh* mesh) {
+  if (!mesh) return;
+  free(mesh->nodes);
+  free(mesh->face2node);
+  free(mesh->int_para_fc);
+  free(mesh->dble_para_fc);
+  free(mesh);
+}
+
+int hgen_read_pbf(const char* fname, hgen_mesh** out) {
+  if (!fname || !out) return HGEN_EINVAL;
+  *out = nullptr;
+  FILE* f = fopen(fname, "r");
+  if (!f) return HGEN_EIO;
+  Tokens T{f};
+  hgen_mesh* m = (hgen_mesh*)calloc(1, sizeof(hgen_mesh));
+  int rc = m ? HGEN_OK : HGEN_ENOMEM;
+  auto bad = [&]() { rc = HGEN_EIO; };
+  if (!rc && (!T.integer(&m->nond) || m->nond < 1)) bad();
+  if (!rc && !(m->nodes = (double*)malloc(sizeof(double) * 3 * (size_t)m->nond))) rc = HGEN_ENOMEM;
+  for (int64_t k = 0; !rc && k < 3 * (int64_t)m->nond; k++)
+    if (!T.real(&m->nodes[k])) bad();
+  if (!rc && (!T.integer(&m->nofc) || m->nofc < 1 || !T.integer(&m->nond_on_face) || m->nond_on_face < 1 ||
+              !T.integer(&m->nint_para_fc) || m->nint_para_fc < 0 || !T.integer(&m->ndble_para_fc) ||
+              m->ndble_para_fc < 0))
+    bad();
+  const int64_t nfn = rc ? 0 : (int64_t)m->nofc * m->nond_on_face;
+  if (!rc && !(m->face2node = (int32_t*)malloc(sizeof(int32_t) * (size_t)nfn))) rc = HGEN_ENOMEM;
+  for (int64_t k = 0; !rc && k < nfn; k++)
+    if (!T.integer(&m->face2node[k]) || m->face2node[k] < 0 || m->face2node[k] >= m->nond) bad();
+  const int64_t ni = rc ? 0 : (int64_t)m->nofc * m->nint_para_fc;
+  if (!rc && ni && !(m->int_para_fc = (int32_t*)malloc(sizeof(int32_t) * (size_t)ni))) rc = HGEN_ENOMEM;
+  for (int64_t k = 0; !rc && k < ni; k++)
+    if (!T.integer(&m->int_para_fc[k])) bad();
+  const int64_t nr = rc ? 0 : (int64_t)m->nofc * m->ndble_para_fc;
+  if (!rc && nr && !(m->dble_para_fc = (double*)malloc(sizeof(double) * (size_t)nr))) rc = HGEN_ENOMEM;
+  for (int64_t k = 0; !rc && k < nr; k++)
+    if (!T.real(&m->dble_para_fc[k])) bad();
+  fclose(f);
+  if (rc) {
+    hgen_free_mesh(m);
+    return rc;
+  }
+  *out = m;
+  return HGEN_OK;
+}
+
 double hgen_entry(const hgen_hmatrix* m, int32_t ill, int32_t itt) {
-  return kernel_entry(m->coords, m->lod[ill - 1] - 1, m->lod[itt - 1] - 1);
+  return Kernel{m->coords, m->mesh}(m->lod[ill - 1] - 1, m->lod[itt - 1] - 1);
 }
 
 // Fortran unformatted sequential records: int32 byte count, payload, byte count.

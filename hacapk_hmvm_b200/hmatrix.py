@@ -131,6 +131,45 @@ class HMatrix:
             if fill == "gpu":
                 _lib.check(rc, where)
             raise RuntimeError(f"{where} failed with status {rc}")
+        obj = cls._wrap_hgen(mp, dict(n=int(n), geometry=geometry, leaf_size=leaf_size, eta=eta, eps=eps,
+                                      seed=seed, kmax=kmax, aca_eps_factor=aca_eps_factor))
+        if report is not None:
+            obj.meta["aca_report"] = {f: getattr(report, f) for f, _ in _lib.AcaReport._fields_}
+        return obj
+
+    @classmethod
+    def from_mesh(cls, path: str, eps: float = 1e-6, leaf_size: int = 15, eta: float = 2.0, kmax: int = 1000,
+                  aca_eps_factor: float = 1e-3, nthreads: int = 0) -> "HMatrix":
+        """The ppohBEM collocation H-matrix of a .pbf triangle mesh
+        (hgen_read_pbf + hgen_build_tree_mesh + hgen_fill_leaves); the defaults
+        are HACApK's with the reference driver's tolerance 1e-6."""
+        lib = _lib.hgen_lib()
+        mesh = C.POINTER(_lib.HgenMesh)()
+        rc = lib.hgen_read_pbf(path.encode(), C.byref(mesh))
+        if rc != 0:
+            raise OSError(f"hgen_read_pbf({path}) failed with status {rc}")
+        mesh_owner = _COwner(mesh, lib.hgen_free_mesh)
+        p = _lib.HgenParams()
+        lib.hgen_default_params(C.byref(p))
+        p.leaf_size, p.eta, p.eps, p.kmax = int(leaf_size), float(eta), float(eps), int(kmax)
+        p.aca_eps_factor, p.nthreads = float(aca_eps_factor), int(nthreads)
+        mp = C.POINTER(_lib.HgenMatrix)()
+        rc = lib.hgen_build_tree_mesh(C.byref(p), mesh, C.byref(mp))
+        if rc != 0:
+            raise RuntimeError(f"hgen_build_tree_mesh failed with status {rc}")
+        rc = lib.hgen_fill_leaves(mp, C.byref(p))
+        if rc != 0:
+            lib.hgen_free(mp)
+            raise RuntimeError(f"hgen_fill_leaves failed with status {rc}")
+        obj = cls._wrap_hgen(mp, dict(mesh=path, leaf_size=leaf_size, eta=eta, eps=eps, kmax=kmax,
+                                      aca_eps_factor=aca_eps_factor))
+        obj._keep.append(mesh_owner)  # entry() evaluates the mesh kernel
+        return obj
+
+    @classmethod
+    def _wrap_hgen(cls, mp, gen_meta) -> "HMatrix":
+        """An HMatrix over a filled hgen_hmatrix (arrays owned by it)."""
+        lib = _lib.hgen_lib()
         m = mp.contents
         nlf = m.nlf
         owner = _COwner(mp, lib.hgen_free)
@@ -142,13 +181,9 @@ class HMatrix:
             nstrtl=_np_from(m.nstrtl, nlf, np.int32), nstrtt=_np_from(m.nstrtt, nlf, np.int32),
             a1=_np_from(m.a1, nlf, np.int64), a2=_np_from(m.a2, nlf, np.int64),
             rowmat=_np_from(m.rowmat, m.len, np.float64),
-            meta=dict(generator=dict(n=int(n), geometry=geometry, leaf_size=leaf_size, eta=eta, eps=eps,
-                                     seed=seed, kmax=kmax, aca_eps_factor=aca_eps_factor),
-                      n_lowrank=int(m.n_lowrank), n_dense=int(m.n_dense),
+            meta=dict(generator=gen_meta, n_lowrank=int(m.n_lowrank), n_dense=int(m.n_dense),
                       aca_incomplete=int(m.aca_incomplete)),
         )
-        if report is not None:
-            obj.meta["aca_report"] = {f: getattr(report, f) for f, _ in _lib.AcaReport._fields_}
         obj.meta["lod"] = _np_from(m.lod, m.nd, np.int32)
         obj.meta["coords"] = _np_from(m.coords, 3 * m.nd, np.float64).reshape(-1, 3)
         obj._keep.append(owner)

@@ -53,6 +53,18 @@ typedef struct hgen_params {
   uint64_t seed;          /* point-cloud seed */
 } hgen_params;
 
+/* A triangle mesh in ppohBEM's .pbf text format (read by the reference driver,
+ * src_hdump/bem-bb-fw-HACApK-0.5.0.f90:396-500): node count, node xyz lines,
+ * face count, nodes per face (3), integer and real parameter counts per face,
+ * the faces' 0-based node indices, then the per-face parameters. */
+typedef struct hgen_mesh {
+  int32_t nond, nofc, nond_on_face, nint_para_fc, ndble_para_fc, _pad0;
+  double *nodes;        /* [nond * 3] xyz */
+  int32_t *face2node;   /* [nofc * nond_on_face], 0-based */
+  int32_t *int_para_fc; /* [nofc * nint_para_fc] (NULL if none) */
+  double *dble_para_fc; /* [nofc * ndble_para_fc] (NULL if none) */
+} hgen_mesh;
+
 /* The generated matrix: the SoA view of src_hmvm/src_cpp/hacapk.h:23-36 with
  * 64-bit element offsets (a1/a2/len), plus the construction by-products. */
 typedef struct hgen_hmatrix {
@@ -65,6 +77,7 @@ typedef struct hgen_hmatrix {
   double *coords;     /* [nd*3] original points, xyz interleaved */
   int64_t n_lowrank, n_dense;
   int64_t aca_incomplete; /* leaves where HACApK would have stopped (m_HACApK_base.f90:565-575) */
+  const hgen_mesh* mesh;  /* hgen_build_tree_mesh: the mesh (borrowed; keep it until the fill); else NULL */
 } hgen_hmatrix;
 
 void hgen_default_params(hgen_params* p);
@@ -74,6 +87,16 @@ int hgen_build(const hgen_params* p, hgen_hmatrix** out);
  * set, kt / a1 / a2 are 0, rowmat is NULL and len 0.  Fill it with
  * hgen_fill_leaves (host, OpenMP) or hmvm_b200_aca_fill (GPU, libhmvm_b200). */
 int hgen_build_tree(const hgen_params* p, hgen_hmatrix** out);
+/* The same for the ppohBEM collocation matrix of a triangle mesh: points are
+ * the face centroids (src_hdump/m_ppohBEM_bembb2hacapk.f90), entry (i, j) is
+ * face j's integral at face i's centroid (m_ppohBEM_matrix_element_ij.f90,
+ * face_integral in m_ppohBEM_user_func.f90:49-100); nd = the face count and
+ * p->n / p->geometry / p->seed are ignored.  The matrix keeps a pointer to the
+ * mesh for its fill.  HACApK's own settings are leaf_size 15, eta 2, kmax 1000,
+ * aca_eps_factor 1e-3 and eps = the driver's tolerance. */
+int hgen_build_tree_mesh(const hgen_params* p, const hgen_mesh* mesh, hgen_hmatrix** out);
+int hgen_read_pbf(const char* fname, hgen_mesh** out);
+void hgen_free_mesh(hgen_mesh* mesh);
 /* ACA for the low-rank leaves and kernel entries for the dense ones
  * (HACApK_fill_leafmtx_hyp, src_hdump/m_HACApK_base.f90:580-662); sets kt,
  * a1, a2, len, ktmax, aca_incomplete and allocates rowmat. */

@@ -282,7 +282,8 @@ int hmvm_b200_gcrm(hmvm_plan *plan, const void *b_dev, void *u_dev, int32_t max_
  * Fills a matrix from hgen_build_tree (include/hacapk_hgen.h) on `device`: ACA
  * for its low-rank leaves (HACApK_aca, src_hdump/m_HACApK_base.f90:494-577)
  * and kernel entries for its dense leaves (HACApK_fill_leafmtx_hyp, :580-662),
- * with results bit-identical to hgen_fill_leaves.  Sets kt, a1, a2, len, ktmax
+ * with results bit-identical to hgen_fill_leaves (point-kernel matrices only;
+ * a matrix from hgen_build_tree_mesh is refused).  Sets kt, a1, a2, len, ktmax
  * and aca_incomplete and allocates rowmat (malloc; hgen_free releases it).
  * The matrix is left unchanged on failure. */
 struct hgen_hmatrix;

@@ -1,10 +1,13 @@
 """The H-matrix generator (include/hacapk_hgen.h): HACApK's construction rules
-hold on its output, and the reference's own loaders read its files."""
+hold on its output, the reference's own loaders read its files, and from the
+reference's sample mesh it rebuilds the reference's sample matrix."""
+import os
+
 import numpy as np
 import pytest
 
 from hacapk_hmvm_b200 import HMatrix
-from helpers import RefMatrix, ref_available, relerr
+from helpers import SAMPLE_BIN, RefMatrix, ref_available, relerr
 
 
 def _boxes(hm, r0, n):
@@ -156,3 +159,60 @@ def test_gpu_fill_refuses_without_device():
         assert rc == _lib.HMVM_ENODEV and not tree.contents.rowmat
     finally:
         lib.hgen_free(tree)
+
+
+# ---- ppohBEM meshes: the reference's own sample matrix --------------------------
+SAMPLE_PBF = "/root/reference/src_hdump/input_sample.pbf"
+
+
+@pytest.mark.skipif(not (os.path.exists(SAMPLE_PBF) and os.path.exists(SAMPLE_BIN)),
+                    reason="the reference's sample mesh and matrix are not present")
+def test_mesh_reproduces_reference_sample():
+    """HACApK built src_hdump/hmatrix_sample.bin from input_sample.pbf with the
+    ppohBEM collocation kernel (leaf 15, eta 2, tolerance 1e-6 from
+    bem-bb-config.txt).  The generator, given the same mesh, rebuilds the same
+    leaf list -- every leaf's position, size, type and ACA rank -- and the same
+    values up to the last bits of libm's atan2/log (dense entries within 1e-12
+    relative; the HMVM within 1e-13)."""
+    ref = HMatrix.load(SAMPLE_BIN)
+    ours = HMatrix.from_mesh(SAMPLE_PBF)
+    assert (ours.nd, ours.nlf, ours.ktmax, ours.len) == (ref.nd, ref.nlf, ref.ktmax, ref.len) == (600, 1426, 31, 248662)
+    for f in ("ltmtx", "ndl", "ndt", "nstrtl", "nstrtt", "kt", "a1", "a2"):
+        assert np.array_equal(getattr(ours, f), getattr(ref, f)), f
+    dense = np.nonzero(ref.ltmtx == 2)[0]
+    for i in dense:
+        n = int(ref.ndl[i]) * int(ref.ndt[i])
+        a, b = ref.rowmat[ref.a1[i]:ref.a1[i] + n], ours.rowmat[ours.a1[i]:ours.a1[i] + n]
+        assert np.all(np.abs(a - b) <= 1e-12 * np.abs(a)), i
+    x = np.sin(np.arange(1, ref.nd + 1, dtype=np.float64))  # the reference harness's b[i] = sin(i+1)
+    from helpers import oracle_hmvm
+
+    y_ref, y = oracle_hmvm(ref, x), oracle_hmvm(ours, x)
+    assert relerr(y, y_ref) < 1e-13
+    # the entries are the kernel's: a dense leaf's values equal entry(i, j)
+    i = int(dense[0])
+    r, c = int(ours.nstrtl[i]), int(ours.nstrtt[i])
+    assert ours.entry(r, c) == ours.rowmat[ours.a1[i]]
+
+
+@pytest.mark.parametrize("fault", ["missing", "truncated", "node_index", "not_a_number"])
+def test_pbf_reader_faults(tmp_path, fault):
+    import ctypes as C
+
+    from hacapk_hmvm_b200 import _lib
+
+    good = "4\n0 0 0\n1 0 0\n0 1 0\n0 0 1\n2\n3\n0\n1\n0 1 2\n0 1 3\n-1.0\n-1.0\n"
+    text = {"truncated": good[:40], "node_index": good.replace("0 1 3", "0 1 4"),
+            "not_a_number": good.replace("1 0 0", "1 x 0"), "missing": None}[fault]
+    p = str(tmp_path / "m.pbf")
+    if text is not None:
+        open(p, "w").write(text)
+    lib = _lib.hgen_lib()
+    mesh = C.POINTER(_lib.HgenMesh)()
+    assert lib.hgen_read_pbf(p.encode(), C.byref(mesh)) == -3 and not mesh  # HGEN_EIO
+    open(p, "w").write(good)
+    assert lib.hgen_read_pbf(p.encode(), C.byref(mesh)) == 0
+    m = mesh.contents
+    assert (m.nond, m.nofc, m.nond_on_face, m.nint_para_fc, m.ndble_para_fc) == (4, 2, 3, 0, 1)
+    assert [m.face2node[k] for k in range(6)] == [0, 1, 2, 0, 1, 3] and m.dble_para_fc[1] == -1.0
+    lib.hgen_free_mesh(mesh)
