@@ -278,8 +278,8 @@ int resident_ctas(const hmvm_plan_opts& o, int dev, int* out) {
   const bool mixed = o.precision == HMVM_MIXED;
   const int kernel = mixed ? (o.mixed_lr_format == HMVM_LR_BF16 ? 3 : 2) : (o.kernel == 0 ? 0 : 1);
   const int ncfg = mixed ? kNumMixedCfgs : (kernel == 0 ? kNumCfgs : kNumStreamCfgs);
-  const int d1 = mixed ? kDefaultMixedCfg1 : (kernel == 0 ? kDefaultStage1Cfg : kDefaultStreamCfg);
-  const int d2 = mixed ? kDefaultMixedCfg2 : (kernel == 0 ? kDefaultStage2Cfg : kDefaultStreamCfg);
+  const int d1 = default_stage_cfg(o.precision, mixed ? 1 : kernel, 1);
+  const int d2 = default_stage_cfg(o.precision, mixed ? 1 : kernel, 2);
   const int c1 = (o.stage1_cfg >= 0 && o.stage1_cfg < ncfg) ? o.stage1_cfg : d1;
   const int c2 = (o.stage2_cfg >= 0 && o.stage2_cfg < ncfg) ? o.stage2_cfg : d2;
   return o.precision == HMVM_FP32 ? resident_ctas_t<float>(kernel, c1, c2, out)

@@ -127,6 +127,12 @@ int validate_leaves(const LeafTable &lt, std::string &msg) {
   return HMVM_OK;
 }
 
+int default_stage_cfg(int precision, int kernel, int stage) {
+  if (precision == HMVM_MIXED) return stage == 1 ? kDefaultMixedCfg1 : kDefaultMixedCfg2;
+  if (kernel == 0) return stage == 1 ? kDefaultStage1Cfg : kDefaultStage2Cfg;
+  return (precision == HMVM_FP32 && stage == 2) ? 1 : kDefaultStreamCfg;
+}
+
 int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, HostLayout &L,
                  std::string &msg, int ctas2_per_sm) {
   int rc = validate_leaves(lt, msg);
@@ -146,8 +152,8 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     L.num_sms = num_sms > 0 ? num_sms : 148;
     L.kernel = (opts.kernel == 0 && !L.mixed) ? 0 : 1;
     const int ncfg = L.mixed ? kNumMixedCfgs : (L.kernel == 0 ? kNumCfgs : kNumStreamCfgs);
-    const int d1 = L.mixed ? kDefaultMixedCfg1 : (L.kernel == 0 ? kDefaultStage1Cfg : kDefaultStreamCfg);
-    const int d2 = L.mixed ? kDefaultMixedCfg2 : (L.kernel == 0 ? kDefaultStage2Cfg : kDefaultStreamCfg);
+    const int d1 = default_stage_cfg(opts.precision, L.kernel, 1);
+    const int d2 = default_stage_cfg(opts.precision, L.kernel, 2);
     L.stage1_cfg = (opts.stage1_cfg >= 0 && opts.stage1_cfg < ncfg) ? opts.stage1_cfg : d1;
     L.stage2_cfg = (opts.stage2_cfg >= 0 && opts.stage2_cfg < ncfg) ? opts.stage2_cfg : d2;
     L.ctas_per_sm = opts.ctas_per_sm > 0 ? opts.ctas_per_sm
