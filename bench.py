@@ -65,6 +65,11 @@ def parse():
     ap.add_argument("--nrhs", type=int, default=1, help="right-hand sides per step (multi-RHS HMVM when > 1)")
     ap.add_argument("--x-dist", default="uniform", choices=["uniform", "normal"], help="entries of x / X")
     ap.add_argument("--lr-format", default="fp16", choices=["fp16", "bf16"], help="mixed plans: 16-bit factor format")
+    ap.add_argument("--mesh", default=None,
+                    help="single workload: the ppohBEM collocation matrix of this .pbf mesh instead of a generated one")
+    ap.add_argument("--mesh-eps", type=float, default=1e-6, help="--mesh: ACA tolerance (the reference driver's 1e-6)")
+    ap.add_argument("--graph", action="store_true",
+                    help="nrhs 1: time CUDA-graph replays of one captured apply (stage times from a profiled pass after)")
     ap.add_argument("--workload", default="single", choices=["single", "batch"],
                     help="batch: many independent H-matrices of uneven N in one CUDA-graph replay")
     ap.add_argument("--batch-count", type=int, default=64)
@@ -231,10 +236,39 @@ def measured_peak_gbs():
 def build_matrix(a):
     from hacapk_hmvm_b200 import HMatrix
 
+    if a.mesh:
+        return HMatrix.from_mesh(a.mesh, eps=a.mesh_eps)
     return HMatrix.generate(a.n, a.geometry, eta=a.eta, eps=a.eps, leaf_size=a.leaf, seed=a.seed)
 
 
+# The reference's published best CUDA times (hybrid2, src_hmvm/src_cpp/result/time_<matrix>_<d|f>.csv,
+# hardware not stated) for the matrices whose meshes it ships: (faces, seconds per HMVM).
+PUBLISHED = {"216h": (21600, {"fp64": 1.002e-3, "fp32": 6.638e-4}),
+             "sample": (600, {"fp64": 1.920e-5, "fp32": 1.674e-5})}
+
+
+def published_hmvm_per_s(a, hm):
+    if not a.mesh or a.nrhs != 1:
+        return None
+    for key, (faces, t) in PUBLISHED.items():
+        if key in os.path.basename(a.mesh) and hm.nd == faces and a.precision in t:
+            return 1.0 / t[a.precision]
+    return None
+
+
 def workload_config(a, hm):
+    if a.mesh:
+        mb = hm.stored_elements() * (4 if a.precision == "fp32" else 8) / 1e6
+        return {
+            "workload": f"ppohBEM collocation matrix of {os.path.basename(a.mesh)} (N={hm.nd}, HACApK leaf 15, "
+                        f"eta 2, ACA eps {a.mesh_eps:g}), single-vector HMVM, {a.precision.upper()}",
+            "nrhs": a.nrhs, "n": hm.nd, "mesh": os.path.basename(a.mesh), "aca_eps": a.mesh_eps,
+            "nlf": hm.nlf, "n_lowrank": int((hm.ltmtx == 1).sum()), "n_dense": int((hm.ltmtx == 2).sum()),
+            "stored_elements": hm.stored_elements(), "precision": a.precision,
+            "l2": (f"matrix {mb:.0f} MB, above the 126 MB L2" if mb > 126 else
+                   f"matrix {mb:.1f} MB fits the 126 MB L2 (not an HBM figure)"),
+            "parallelism": f"replicas x{a.gpus}",
+        }
     return {
         "workload": f"{a.geometry} N={a.n} leaf={a.leaf} eta={a.eta} ACA eps={a.eps:g}, "
                     + ("single-vector HMVM, " if a.nrhs == 1 else f"multi-RHS HMVM nrhs={a.nrhs}, ")
@@ -273,7 +307,8 @@ def run_reference(a, rank):
         "impl": "reference", "metric": "HMVM/s", "value": value, "unit": "HMVM/s", "n_gpus": a.gpus,
         "steps": steps, "warmup": a.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": f"synthetic (seeded HACApK-rule H-matrix; x {'uniform[-1,1]' if a.x_dist == 'uniform' else 'standard normal'})",
+        "data": (f"the ppohBEM mesh {os.path.basename(a.mesh)}" if a.mesh else "synthetic (seeded HACApK-rule H-matrix")
+                + f"; x {'uniform[-1,1]' if a.x_dist == 'uniform' else 'standard normal'}" + ("" if a.mesh else ")"),
         "config": workload_config(a, hm),
         "gbytes_per_s": hm.algorithmic_bytes(8) / (dt / steps) / 1e9,
         "cpu_baseline": {"value": value, "unit": "HMVM/s", "cores": cpu.threads, "kind": cpu.kind,
@@ -320,6 +355,13 @@ def run_b200(a, rank, world, local_rank):
     else:
         def step():
             plan.apply_multi(xd, yd, stream)
+    use_graph = a.graph and a.nrhs == 1
+    direct_step = step
+    if use_graph:
+        plan.capture(xd[0], yd[0])
+
+        def step():
+            plan.replay(stream)
 
     for _ in range(a.warmup):
         step()
@@ -330,7 +372,8 @@ def run_b200(a, rank, world, local_rank):
     clocks = ClockSampler(vis.split(",")[local_rank].strip() if vis else str(local_rank))
     clocks.start()
     time.sleep(0.3)
-    plan.profile(True)
+    if not use_graph:
+        plan.profile(True)
     if dist:
         dist.barrier()
     torch.cuda.synchronize(dev)
@@ -344,6 +387,11 @@ def run_b200(a, rank, world, local_rank):
     if dist:
         dist.barrier()
     ms_total = e0.elapsed_time(e1)
+    if use_graph:  # stage times: a profiled pass of direct applies (a replayed graph records no events)
+        plan.profile(True)
+        for _ in range(min(a.steps, 200)):
+            direct_step()
+        torch.cuda.synchronize(dev)
     stage_ms, napplies = plan.profile_read()
     plan.profile(False)
     clk = clocks.stop()
@@ -430,14 +478,20 @@ def run_b200(a, rank, world, local_rank):
     if rank == 0:
         value = world * 1e3 / ms_step * a.nrhs
         cfg = workload_config(a, hm)
+        if use_graph:
+            cfg["timing"] = ("CUDA-graph replays of one captured apply (hmvm_b200_plan_replay); stage times "
+                             "from a profiled pass of direct applies after the timed region")
         cfg.update({"kernel": kname, "stage1_cfg": info["stage1_cfg"], "stage2_cfg": info["stage2_cfg"],
                     "ctas_per_sm": [info["ctas_per_sm"], info["stage2_ctas_per_sm"]],
                     "device_bytes": info["device_bytes"], "plan_setup_s": setup_s})
         line = {
             "metric": unit, "value": value, "unit": unit, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": DTYPES[a.precision],
-            "data": f"synthetic (seeded HACApK-rule H-matrix; x {'uniform[-1,1]' if a.x_dist == 'uniform' else 'standard normal'})",
+            "vs_baseline": (value / published_hmvm_per_s(a, hm)) if published_hmvm_per_s(a, hm) else None,
+            "dtype": DTYPES[a.precision],
+            "data": (f"the ppohBEM mesh {os.path.basename(a.mesh)}" if a.mesh else
+                     "synthetic (seeded HACApK-rule H-matrix") +
+                    f"; x {'uniform[-1,1]' if a.x_dist == 'uniform' else 'standard normal'}" + ("" if a.mesh else ")"),
             "config": cfg,
             "gbytes_per_s": alg_bytes / (ms_step * 1e-3) / 1e9,
             "algorithmic_bytes_per_step": alg_bytes,

@@ -211,6 +211,8 @@ HMVM_SIGNATURES = {
     "hmvm_b200_apply_multi_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32,
                                              C.c_void_p]),
     "hmvm_b200_plan_multi_kernel_count": (C.c_int, [C.c_void_p, C.c_int32]),
+    "hmvm_b200_plan_capture": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "hmvm_b200_plan_replay": (C.c_int, [C.c_void_p, C.c_void_p]),
     "hmvm_b200_bicgstab": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_double, C.c_void_p,
                                      C.c_void_p, C.c_void_p]),
     "hmvm_b200_gcrm": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_void_p,

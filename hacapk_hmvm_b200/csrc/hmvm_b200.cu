@@ -170,6 +170,8 @@ struct hmvm_plan {
   size_t xh_bytes = 0;
   // profiling: kEventsPerApply events per recorded apply
   bool profiling = false;
+  cudaGraph_t graph = nullptr;       // hmvm_b200_plan_capture: one apply
+  cudaGraphExec_t graph_exec = nullptr;
   std::vector<cudaEvent_t> prof_events;
   int prof_count = 0;
 };
@@ -184,6 +186,10 @@ constexpr int kMaxProfiled = 4096;
 constexpr int kEventsPerApply = 5;
 
 void free_plan_buffers(hmvm_plan* p) {
+  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  p->graph_exec = nullptr;
+  p->graph = nullptr;
   for (cudaEvent_t e : p->prof_events) cudaEventDestroy(e);
   p->prof_events.clear();
   void* bufs[] = {p->d_data, p->d_tiles, p->d_segs, p->d_tb1, p->d_tb2,  p->d_out_idx, p->d_red1,
@@ -1027,6 +1033,51 @@ int hmvm_b200_apply(hmvm_plan* p, const void* x, void* y, void* stream) {
   DeviceGuard g(p->device);
   if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
   return apply_impl(p, x, y, static_cast<cudaStream_t>(stream));
+}
+
+int hmvm_b200_plan_capture(hmvm_plan* p, const void* x, void* y) {
+  int rc = check_xy(p, x, y);
+  if (rc) return rc;
+  if (p->profiling) return set_error(HMVM_EINVAL, "profiling is on; a captured apply cannot record events");
+  DeviceGuard g(p->device);
+  if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
+  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  p->graph_exec = nullptr;
+  p->graph = nullptr;
+  cudaStream_t cs;
+  HMVM_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "cudaStreamCreate");
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(cs);
+    return cuda_fail(e, "cudaStreamBeginCapture");
+  }
+  rc = apply_impl(p, x, y, cs);
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(cs, &graph);  // always end the capture
+  cudaStreamDestroy(cs);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&p->graph_exec, graph, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return cuda_fail(e, "cudaGraphInstantiate");
+  }
+  p->graph = graph;
+  return HMVM_OK;
+}
+
+int hmvm_b200_plan_replay(hmvm_plan* p, void* stream) {
+  if (!p) return set_error(HMVM_EINVAL, "plan is NULL");
+  if (p->nd == 0) return HMVM_OK;
+  if (!p->graph_exec) return set_error(HMVM_EINVAL, "nothing captured: call hmvm_b200_plan_capture first");
+  DeviceGuard g(p->device);
+  if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the plan's device");
+  HMVM_CUDA_TRY(cudaGraphLaunch(p->graph_exec, static_cast<cudaStream_t>(stream)), "cudaGraphLaunch");
+  return HMVM_OK;
 }
 
 int hmvm_b200_apply_host(hmvm_plan* p, const void* x_host, void* y_host, void* stream) {

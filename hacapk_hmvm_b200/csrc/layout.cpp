@@ -477,7 +477,9 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     int64_t max_item[2];
     for (int st = 0; st < 2; st++) {
       int32_t nteams = st == 0 ? L.stage1_teams : L.stage2_teams;
-      max_item[st] = std::max<int64_t>(kMinItemBytes, stage_bytes[st] / std::max<int64_t>(1, (int64_t)nteams * kItemsPerTeam));
+      max_item[st] = stage_bytes[st] < kSmallStageBytes
+                         ? std::max<int64_t>(kSmallItemBytes, stage_bytes[st] / std::max<int64_t>(1, (int64_t)nteams))
+                         : std::max<int64_t>(kMinItemBytes, stage_bytes[st] / std::max<int64_t>(1, (int64_t)nteams * kItemsPerTeam));
     }
     struct Item {
       int32_t tile, va, vb, mode, out_base;

@@ -91,6 +91,11 @@ constexpr int kMaxRows = 32;
 // Item split: a stage's tiles are cut so that no item exceeds
 // max(kMinItemBytes, stage bytes / (teams * kItemsPerTeam)).
 constexpr int64_t kMinItemBytes = 32 * 1024;
+// A stage below this many bytes is cut finer (items of at least
+// kSmallItemBytes, about one per team): there every team holds at most an item
+// or two and the stage takes as long as its longest item.
+constexpr int64_t kSmallStageBytes = 8 << 20;
+constexpr int64_t kSmallItemBytes = 4 * 1024;
 constexpr int64_t kItemsPerTeam = 6;
 constexpr int64_t kItemOverheadBytes = 1024;
 

@@ -161,6 +161,16 @@ class Plan:
         _lib.check(rc, "apply_multi_host")
         return Y
 
+    def capture(self, x, y) -> None:
+        """Record y = H x for these CUDA tensors into the plan's CUDA graph
+        (hmvm_b200_plan_capture); replay() then runs it with one graph launch."""
+        if x.shape != (self.nd,) or y.shape != (self.nd,):
+            raise ValueError(f"x and y must have shape ({self.nd},)")
+        _lib.check(_lib.hmvm_lib().hmvm_b200_plan_capture(self.handle, _dev_ptr(x), _dev_ptr(y)), "plan_capture")
+
+    def replay(self, stream=None) -> None:
+        _lib.check(_lib.hmvm_lib().hmvm_b200_plan_replay(self.handle, _stream_handle(stream)), "plan_replay")
+
     def bicgstab(self, b, u, eps: float = 1e-8, max_steps: int = 1000, stream=None) -> tuple[int, float]:
         """Solve H u = b by BiCGSTAB (hmvm_b200_bicgstab): b, u CUDA tensors,
         u holds the initial guess and receives the solution.  Returns (steps,

@@ -202,6 +202,15 @@ int hmvm_b200_apply(hmvm_plan *plan, const void *x_dev, void *y_dev, void *strea
 /* The same with host buffers: copies x in, runs, copies y out, and waits for
  * the stream. */
 int hmvm_b200_apply_host(hmvm_plan *plan, const void *x_host, void *y_host, void *stream);
+/* Records one apply (y = H x for these device buffers) into a CUDA graph the
+ * plan keeps (a new capture replaces the previous one; the buffers must stay
+ * valid while it is replayed; profiling must be off), and launches it with one
+ * cudaGraphLaunch.  For small matrices an apply is 2-5 kernels whose host
+ * launch cost exceeds their device time; a solver loop replays instead.  The
+ * reference launches its kernel per call (hmvm_cuda2.cu:262-306) and has no
+ * counterpart. */
+int hmvm_b200_plan_capture(hmvm_plan *plan, const void *x_dev, void *y_dev);
+int hmvm_b200_plan_replay(hmvm_plan *plan, void *stream);
 
 /* Y = H X for nrhs right-hand sides: X and Y column-major in device memory
  * (column r at X + r * ldx, ldx >= N; same for Y), element type as for

@@ -296,3 +296,42 @@ def test_golden_fixtures(gpu):
                 yf = _run(plan, x)
             assert relerr(yf, Y[f"{name}/y_seq2_f_{xn}"]) <= TOL32, (name, xn)
             assert relerr(yf, Y[f"{name}/y_seq2_d_{xn}"]) <= TOL32
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "mixed"])
+def test_capture_replay(gpu, prec):
+    """hmvm_b200_plan_capture + hmvm_b200_plan_replay: a replayed graph of one
+    apply gives y bit for bit equal to the direct apply, follows new contents
+    of x, and a new capture replaces the old one."""
+    import torch
+
+    from hacapk_hmvm_b200 import _lib
+
+    hm = HMatrix.generate(3000, "sphere", eta=2.0, eps=1e-5, leaf_size=24, seed=6)
+    dt = torch.float32 if prec == "fp32" else torch.float64
+    with Plan(hm, prec) as plan:
+        with pytest.raises(_lib.HMVMError):
+            plan.replay()  # nothing captured yet
+        x = torch.rand(hm.nd, dtype=dt, device="cuda") - 0.5
+        y_ref, y = torch.empty_like(x), torch.full_like(x, float("nan"))
+        plan.apply(x, y_ref)
+        plan.capture(x, y)
+        for _ in range(2):
+            plan.replay()
+            torch.cuda.synchronize()
+            assert torch.equal(y, y_ref)
+        x.mul_(-2.0)  # the graph reads the buffer's current contents
+        plan.apply(x, y_ref)
+        plan.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(y, y_ref)
+        x2, y2 = torch.rand_like(x), torch.empty_like(x)
+        plan.capture(x2, y2)
+        plan.replay()
+        plan.apply(x2, y_ref)
+        torch.cuda.synchronize()
+        assert torch.equal(y2, y_ref)
+        plan.profile(True)
+        with pytest.raises(_lib.HMVMError):
+            plan.capture(x, y)
+        plan.profile(False)
