@@ -52,6 +52,27 @@ struct DeviceGuard {
 };
 
 using KernelFn = void (*)(TileArgs);
+
+// Launches a kernel of an apply; every kernel after the apply's first one is a
+// programmatic dependent of its predecessor (it may start, and prefetch plan
+// data, while the predecessor drains; it waits for it before reading its
+// outputs -- griddep_wait in the kernels).
+template <typename... P, typename... A>
+cudaError_t launch_in_apply(bool& first, void (*fn)(P...), unsigned grid, unsigned block, size_t smem,
+                            cudaStream_t st, A... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = first ? nullptr : attr;
+  cfg.numAttrs = first ? 0 : 1;
+  first = false;
+  return cudaLaunchKernelEx(&cfg, fn, args...);
+}
 using MultiFn = void (*)(MultiArgs);
 
 template <typename T>
@@ -461,22 +482,23 @@ int launch_stages_mixed(hmvm_plan* p, const void* x, void* y, void* tbuf, void* 
     p->prof_count++;
   }
   if (ev) cudaEventRecord(ev[0], st);
-  hmvm_round_f32_kernel<<<std::min((p->nd + 255) / 256, p->num_sms * 8), 256, 0, st>>>(
-      static_cast<const double*>(x), x32, p->nd);
-  HMVM_CUDA_TRY(cudaGetLastError(), "x rounding launch");
+  bool first = true;
+  HMVM_CUDA_TRY(launch_in_apply(first, hmvm_round_f32_kernel, (unsigned)std::min((p->nd + 255) / 256, p->num_sms * 8),
+                                256, 0, st, static_cast<const double*>(x), x32, p->nd),
+                "x rounding launch");
   if (p->stage1_tiles > 0) {
     const Launch l = stage_launch<double>(p->mixed_kcode, p->stage1_cfg, 1);
     a.team_begin = p->d_tb1;
     a.nteams = p->stage1_teams;
     a.scale = p->d_scale;
-    l.fn<<<ctas, l.threads, l.smem, st>>>(a);
-    HMVM_CUDA_TRY(cudaGetLastError(), "V-stage launch");
+    HMVM_CUDA_TRY(launch_in_apply(first, l.fn, ctas, l.threads, l.smem, st, a), "V-stage launch");
   }
   if (ev) cudaEventRecord(ev[1], st);
   if (p->n_red1 > 0) {
-    hmvm_reduce_kernel<double, float><<<(p->n_red1 + 255) / 256, 256, 0, st>>>(
-        p->d_red1, p->n_red1, static_cast<const double*>(pbuf), static_cast<float*>(tbuf));
-    HMVM_CUDA_TRY(cudaGetLastError(), "V-stage reduction launch");
+    HMVM_CUDA_TRY(launch_in_apply(first, hmvm_reduce_kernel<double, float>, (unsigned)((p->n_red1 + 255) / 256), 256,
+                                  0, st, (const int4*)p->d_red1, p->n_red1, static_cast<const double*>(pbuf),
+                                  static_cast<float*>(tbuf)),
+                  "V-stage reduction launch");
   }
   if (ev) cudaEventRecord(ev[2], st);
   {
@@ -484,14 +506,14 @@ int launch_stages_mixed(hmvm_plan* p, const void* x, void* y, void* tbuf, void* 
     a.team_begin = p->d_tb2;
     a.nteams = p->stage2_teams;
     a.scale = nullptr;
-    l.fn<<<ctas2, l.threads, l.smem, st>>>(a);
-    HMVM_CUDA_TRY(cudaGetLastError(), "row-stage launch");
+    HMVM_CUDA_TRY(launch_in_apply(first, l.fn, ctas2, l.threads, l.smem, st, a), "row-stage launch");
   }
   if (ev) cudaEventRecord(ev[3], st);
   if (p->n_red2 > 0) {
-    hmvm_reduce_kernel<double, double><<<(p->n_red2 + 255) / 256, 256, 0, st>>>(
-        p->d_red2, p->n_red2, static_cast<const double*>(pbuf), static_cast<double*>(y));
-    HMVM_CUDA_TRY(cudaGetLastError(), "row-stage reduction launch");
+    HMVM_CUDA_TRY(launch_in_apply(first, hmvm_reduce_kernel<double, double>, (unsigned)((p->n_red2 + 255) / 256), 256,
+                                  0, st, (const int4*)p->d_red2, p->n_red2, static_cast<const double*>(pbuf),
+                                  static_cast<double*>(y)),
+                  "row-stage reduction launch");
   }
   if (ev) cudaEventRecord(ev[4], st);
   return HMVM_OK;
@@ -519,33 +541,33 @@ int launch_stages(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, 
     ev = &p->prof_events[kEventsPerApply * (size_t)p->prof_count];
     p->prof_count++;
   }
+  bool first = true;
   if (ev) cudaEventRecord(ev[0], st);
   if (p->stage1_tiles > 0) {
     const Launch l = stage_launch<T>(p->kernel, p->stage1_cfg, 1);
     a.team_begin = p->d_tb1;
     a.nteams = p->stage1_teams;
-    l.fn<<<ctas, l.threads, l.smem, st>>>(a);
-    HMVM_CUDA_TRY(cudaGetLastError(), "V-stage launch");
+    HMVM_CUDA_TRY(launch_in_apply(first, l.fn, ctas, l.threads, l.smem, st, a), "V-stage launch");
   }
   if (ev) cudaEventRecord(ev[1], st);
   if (p->n_red1 > 0) {
-    hmvm_reduce_kernel<T, T><<<(p->n_red1 + 255) / 256, 256, 0, st>>>(p->d_red1, p->n_red1,
-                                                                      static_cast<const T*>(pbuf), static_cast<T*>(tbuf));
-    HMVM_CUDA_TRY(cudaGetLastError(), "V-stage reduction launch");
+    HMVM_CUDA_TRY(launch_in_apply(first, hmvm_reduce_kernel<T, T>, (unsigned)((p->n_red1 + 255) / 256), 256, 0, st,
+                                  (const int4*)p->d_red1, p->n_red1, static_cast<const T*>(pbuf),
+                                  static_cast<T*>(tbuf)),
+                  "V-stage reduction launch");
   }
   if (ev) cudaEventRecord(ev[2], st);
   {
     const Launch l = stage_launch<T>(p->kernel, p->stage2_cfg, 2);
     a.team_begin = p->d_tb2;
     a.nteams = p->stage2_teams;
-    l.fn<<<ctas2, l.threads, l.smem, st>>>(a);
-    HMVM_CUDA_TRY(cudaGetLastError(), "row-stage launch");
+    HMVM_CUDA_TRY(launch_in_apply(first, l.fn, ctas2, l.threads, l.smem, st, a), "row-stage launch");
   }
   if (ev) cudaEventRecord(ev[3], st);
   if (p->n_red2 > 0) {
-    hmvm_reduce_kernel<T, T><<<(p->n_red2 + 255) / 256, 256, 0, st>>>(p->d_red2, p->n_red2,
-                                                                      static_cast<const T*>(pbuf), static_cast<T*>(y));
-    HMVM_CUDA_TRY(cudaGetLastError(), "row-stage reduction launch");
+    HMVM_CUDA_TRY(launch_in_apply(first, hmvm_reduce_kernel<T, T>, (unsigned)((p->n_red2 + 255) / 256), 256, 0, st,
+                                  (const int4*)p->d_red2, p->n_red2, static_cast<const T*>(pbuf), static_cast<T*>(y)),
+                  "row-stage reduction launch");
   }
   if (ev) cudaEventRecord(ev[4], st);
   return HMVM_OK;

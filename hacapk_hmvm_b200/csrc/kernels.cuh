@@ -82,6 +82,16 @@ __device__ __forceinline__ void fma_vec(float& a0, float& a1, const float4& m, c
   a1 = fmaf(m.w, z.w, a1);
 }
 
+// Programmatic dependent launch (sm_90+): a kernel lets the next kernel of the
+// apply be scheduled as soon as every CTA has started (launch_dependents), and
+// a kernel launched as a dependent waits for its predecessors' completion and
+// memory (wait) before it reads their outputs; launched normally, wait returns
+// at once.
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 template <typename T>
 __device__ __forceinline__ typename VecT<T>::V zero_vec() {
   typename VecT<T>::V v;
@@ -113,6 +123,8 @@ __global__ void __launch_bounds__(32 * WG * TPC) hmvm_tile_kernel(TileArgs a) {
   using V = typename VecT<T>::V;
   constexpr int VN = VecT<T>::N;
   __shared__ T red[TPC][2][WG > 1 ? WG : 1][32];
+  griddep_launch_dependents();
+  griddep_wait();
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -319,6 +331,7 @@ __global__ void __launch_bounds__(32 * WPB, (stream_min_blocks<T, WPB, S, CHUNK,
   static_assert(B * 32 * 16 <= (S - 1) * CHUNK, "ring too small for one batch");
   static_assert(ZCAP % 4 == 0, "input buffers hold whole vectors");
   extern __shared__ __align__(128) unsigned char smem[];
+  griddep_launch_dependents();
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -369,6 +382,9 @@ __global__ void __launch_bounds__(32 * WPB, (stream_min_blocks<T, WPB, S, CHUNK,
 
   // ---- descriptor pipeline: item i+1's inputs are gathered during item i ----
   hmvm_seg_desc cur_seg = lane < cur.nseg ? segs[cur.seg_begin + lane] : szero;
+  // the ring's first chunks (plan data) are in flight; x / t and the outputs
+  // wait for the preceding kernels of the apply
+  griddep_wait();
   gather_inputs<T>(cur, cur_seg, segs, x, tv, zbase, lane);
   cp_async_commit();
   hmvm_tile_desc nxt = tb + 1 < te ? tiles[tb + 1] : dzero;
@@ -473,6 +489,8 @@ __global__ void __launch_bounds__(32 * WPB, (stream_min_blocks<T, WPB, S, CHUNK,
 template <typename TP, typename TD>
 __global__ void hmvm_reduce_kernel(const int4* __restrict__ red, int n, const TP* __restrict__ p,
                                    TD* __restrict__ dst) {
+  griddep_launch_dependents();
+  griddep_wait();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int4 e = red[i];  // destination, first partial, parts, stride
     TP s = p[e.y];
@@ -483,6 +501,8 @@ __global__ void hmvm_reduce_kernel(const int4* __restrict__ red, int n, const TP
 
 // x rounded to FP32 once per HMVM (the inputs of the FP32 / FP16 / FP8 segments).
 __global__ void hmvm_round_f32_kernel(const double* __restrict__ x, float* __restrict__ x32, int n) {
+  griddep_launch_dependents();
+  griddep_wait();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x32[i] = (float)x[i];
 }
 
@@ -625,6 +645,7 @@ __global__ void __launch_bounds__(32 * WPB, (mixed_min_blocks<WPB, S, CHUNK, ZBY
   constexpr bool WIDE = 65536 / (32 * WPB * mixed_min_blocks<WPB, S, CHUNK, ZBYTES>()) >= 200;
   static_assert(mixed_batch<kF32, S, CHUNK, VST, WIDE>() * 32 * 16 <= (S - 1) * CHUNK, "ring too small for one batch");
   extern __shared__ __align__(128) unsigned char smem[];
+  griddep_launch_dependents();
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -681,6 +702,7 @@ __global__ void __launch_bounds__(32 * WPB, (mixed_min_blocks<WPB, S, CHUNK, ZBY
     else return 0;
   };
   hmvm_seg_desc cur_seg = lane < cur.nseg ? segs[cur.seg_begin + lane] : szero;
+  griddep_wait();  // as in hmvm_stream_kernel
   gather_inputs_mixed(cur, cur_seg, x, x32, tv, zbase, lane);
   cp_async_commit();
   int cur_oidx = out_slot(cur);
