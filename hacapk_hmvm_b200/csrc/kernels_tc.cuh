@@ -32,11 +32,11 @@ namespace hmvm {
 
 constexpr int kTcNr = 16;             // right-hand sides per tensor-core pass
 constexpr int kTcN = 2 * kTcNr;       // MMA N: hi and lo parts
-constexpr int kTcPiece = 16;          // 16-byte column chunks staged per MMA batch (8 K-steps)
+constexpr int kTcPiece = 8;           // 16-byte column chunks staged per MMA batch (4 K-steps)
 // input buffer per item (x2, double-buffered): the planner's budget for 16
 // right-hand sides (8 KiB) plus the 16-bit planes' padding to 16 rows (< 1 KiB)
 constexpr int kTcZBytes = 9216;
-constexpr int kTcStageBytes = kTcPiece * 32 * 16;  // 8 KiB A staging per warp
+constexpr int kTcStageBytes = kTcPiece * 32 * 16;  // 4 KiB A staging per warp
 constexpr int kTcPad = 2048;          // slack before the staging tiles (M rows below 32q)
 
 // ---- global inputs as 16-bit hi/lo planes -----------------------------------

@@ -136,7 +136,7 @@ constexpr int kDefaultMixedCfg2 = 4;
 // Multi-RHS kernel (hmvm_multi_kernel): rhs per pass and its input buffer.
 constexpr int kMaxNrhsPass = 8;   // CUDA-core multi-RHS passes
 constexpr int kTcNrhs = 16;        // tensor-core passes (mixed plans with nrhs_max = 16)
-constexpr int kTcWarpsPerSm = 6;   // resident warps (teams) per SM of the tensor-core kernel
+constexpr int kTcWarpsPerSm = 7;   // resident warps (teams) per SM of the tensor-core kernel
 constexpr int kMultiZBytes = 8192;
 struct MultiCfg {
   int wpb, slots, chunk;
