@@ -189,6 +189,8 @@ struct hmvm_plan {
   void* d_xh = nullptr;  // staging for apply_multi_host
   void* d_yh = nullptr;
   size_t xh_bytes = 0;
+  cudaStream_t cs_in = nullptr, cs_out = nullptr;  // apply_multi_host: copy streams
+  std::vector<cudaEvent_t> pass_events;            // apply_multi_host: per-pass ordering
   // profiling: kEventsPerApply events per recorded apply
   bool profiling = false;
   cudaGraph_t graph = nullptr;       // hmvm_b200_plan_capture: one apply
@@ -212,6 +214,11 @@ void free_plan_buffers(hmvm_plan* p) {
   p->graph_exec = nullptr;
   p->graph = nullptr;
   for (cudaEvent_t e : p->prof_events) cudaEventDestroy(e);
+  for (cudaEvent_t e : p->pass_events) cudaEventDestroy(e);
+  p->pass_events.clear();
+  if (p->cs_in) cudaStreamDestroy(p->cs_in);
+  if (p->cs_out) cudaStreamDestroy(p->cs_out);
+  p->cs_in = p->cs_out = nullptr;
   p->prof_events.clear();
   void* bufs[] = {p->d_data, p->d_tiles, p->d_segs, p->d_tb1, p->d_tb2,  p->d_out_idx, p->d_red1,
                   p->d_red2, p->d_t,     p->d_p,    p->d_err, p->d_x,    p->d_y,       p->d_x32,
@@ -799,34 +806,34 @@ int multi_pass_width(int nrhs_max, int left) {
   return 2;
 }
 
+// The passes of a multi-RHS apply: {first column, columns, pass width}.
+struct Pass {
+  int r0, nr, w;
+};
+std::vector<Pass> multi_passes(const hmvm_plan* p, int nrhs) {
+  std::vector<Pass> v;
+  for (int r0 = 0; r0 < nrhs;) {
+    const int w = p->nrhs_max <= 1 ? 1 : p->tc ? kTcNrhs : multi_pass_width(p->nrhs_max, nrhs - r0);
+    const int nr = std::min(w, nrhs - r0);
+    v.push_back(Pass{r0, nr, w});
+    r0 += nr;
+  }
+  return v;
+}
+// One pass; X and Y point at the pass's first column.
+int run_pass(hmvm_plan* p, const Pass& q, const void* X, int64_t ldx, void* Y, int64_t ldy, cudaStream_t st) {
+  if (p->nrhs_max <= 1) return apply_impl_fwd(p, X, Y, st);  // single-vector passes
+  if (p->tc) return launch_tc_pass(p, X, ldx, Y, ldy, q.nr, st);
+  return launch_multi_pass(p, X, ldx, Y, ldy, q.nr, q.w, st);
+}
+
 int apply_multi_impl(hmvm_plan* p, const void* X, int64_t ldx, void* Y, int64_t ldy, int nrhs, cudaStream_t st) {
   if (p->nd == 0 || nrhs == 0) return HMVM_OK;
   const size_t ex = (size_t)p->elem;
-  if (p->nrhs_max <= 1) {
-    // single-vector passes
-    for (int r = 0; r < nrhs; r++) {
-      int rc = apply_impl_fwd(p, static_cast<const char*>(X) + (size_t)r * ldx * ex,
-                              static_cast<char*>(Y) + (size_t)r * ldy * ex, st);
-      if (rc) return rc;
-    }
-    return HMVM_OK;
-  }
-  if (p->tc) {
-    for (int r0 = 0; r0 < nrhs; r0 += kTcNrhs) {
-      const int nr = std::min(kTcNrhs, nrhs - r0);
-      int rc = launch_tc_pass(p, static_cast<const char*>(X) + (size_t)r0 * ldx * ex, ldx,
-                              static_cast<char*>(Y) + (size_t)r0 * ldy * ex, ldy, nr, st);
-      if (rc) return rc;
-    }
-    return HMVM_OK;
-  }
-  for (int r0 = 0; r0 < nrhs;) {
-    const int w = multi_pass_width(p->nrhs_max, nrhs - r0);
-    const int nr = std::min(w, nrhs - r0);
-    int rc = launch_multi_pass(p, static_cast<const char*>(X) + (size_t)r0 * ldx * ex, ldx,
-                               static_cast<char*>(Y) + (size_t)r0 * ldy * ex, ldy, nr, w, st);
+  for (const Pass& q : multi_passes(p, nrhs)) {
+    int rc = run_pass(p, q, static_cast<const char*>(X) + (size_t)q.r0 * ldx * ex, ldx,
+                      static_cast<char*>(Y) + (size_t)q.r0 * ldy * ex, ldy, st);
     if (rc) return rc;
-    r0 += nr;
   }
   return HMVM_OK;
 }
@@ -1148,23 +1155,51 @@ int hmvm_b200_apply_multi_host(hmvm_plan* p, const void* X_host, int64_t ldx, vo
     p->xh_bytes = nb;
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (ldx == p->nd) {
-    HMVM_CUDA_TRY(cudaMemcpyAsync(p->d_xh, X_host, nb, cudaMemcpyHostToDevice, st), "copy X to device");
-  } else {
-    HMVM_CUDA_TRY(cudaMemcpy2DAsync(p->d_xh, col, X_host, (size_t)ldx * p->elem, col, (size_t)nrhs,
-                                    cudaMemcpyHostToDevice, st),
-                  "copy X to device");
+  // Pass by pass: X columns in on cs_in, the pass on st, its Y columns out on
+  // cs_out, ordered by events, so a pass's compute overlaps the next pass's
+  // upload and the previous pass's download (each pass has its own slice of
+  // the staging buffers).
+  const std::vector<Pass> passes = multi_passes(p, nrhs);
+  if (!p->cs_in) HMVM_CUDA_TRY(cudaStreamCreateWithFlags(&p->cs_in, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (!p->cs_out) HMVM_CUDA_TRY(cudaStreamCreateWithFlags(&p->cs_out, cudaStreamNonBlocking), "cudaStreamCreate");
+  while (p->pass_events.size() < 2 * passes.size() + 1) {
+    cudaEvent_t e;
+    HMVM_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    p->pass_events.push_back(e);
   }
-  rc = apply_multi_impl(p, p->d_xh, p->nd, p->d_yh, p->nd, nrhs, st);
+  cudaEvent_t* ev = p->pass_events.data();
+  cudaError_t e = cudaEventRecord(ev[0], st);  // after the caller's earlier work on st
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(p->cs_in, ev[0], 0);
+  const size_t ex = (size_t)p->elem;
+  for (size_t k = 0; k < passes.size() && e == cudaSuccess && !rc; k++) {
+    const Pass& q = passes[k];
+    char* dx = static_cast<char*>(p->d_xh) + (size_t)q.r0 * col;
+    char* dy = static_cast<char*>(p->d_yh) + (size_t)q.r0 * col;
+    const char* hx = static_cast<const char*>(X_host) + (size_t)q.r0 * ldx * ex;
+    char* hy = static_cast<char*>(Y_host) + (size_t)q.r0 * ldy * ex;
+    e = ldx == p->nd ? cudaMemcpyAsync(dx, hx, col * q.nr, cudaMemcpyHostToDevice, p->cs_in)
+                     : cudaMemcpy2DAsync(dx, col, hx, (size_t)ldx * ex, col, (size_t)q.nr, cudaMemcpyHostToDevice,
+                                         p->cs_in);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[1 + 2 * k], p->cs_in);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ev[1 + 2 * k], 0);
+    if (e != cudaSuccess) break;
+    rc = run_pass(p, q, dx, p->nd, dy, p->nd, st);
+    if (rc) break;
+    e = cudaEventRecord(ev[2 + 2 * k], st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(p->cs_out, ev[2 + 2 * k], 0);
+    if (e == cudaSuccess)
+      e = ldy == p->nd ? cudaMemcpyAsync(hy, dy, col * q.nr, cudaMemcpyDeviceToHost, p->cs_out)
+                       : cudaMemcpy2DAsync(hy, (size_t)ldy * ex, dy, col, col, (size_t)q.nr, cudaMemcpyDeviceToHost,
+                                           p->cs_out);
+  }
+  // drain every stream before returning (the staging buffers may be in use)
+  const cudaError_t e1 = cudaStreamSynchronize(p->cs_in);
+  const cudaError_t e2 = cudaStreamSynchronize(st);
+  const cudaError_t e3 = cudaStreamSynchronize(p->cs_out);
   if (rc) return rc;
-  if (ldy == p->nd) {
-    HMVM_CUDA_TRY(cudaMemcpyAsync(Y_host, p->d_yh, nb, cudaMemcpyDeviceToHost, st), "copy Y to host");
-  } else {
-    HMVM_CUDA_TRY(cudaMemcpy2DAsync(Y_host, (size_t)ldy * p->elem, p->d_yh, col, col, (size_t)nrhs,
-                                    cudaMemcpyDeviceToHost, st),
-                  "copy Y to host");
-  }
-  HMVM_CUDA_TRY(cudaStreamSynchronize(st), "stream synchronize");
+  if (e != cudaSuccess) return cuda_fail(e, "apply_multi_host: copies");
+  if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+    return cuda_fail(e1 != cudaSuccess ? e1 : e2 != cudaSuccess ? e2 : e3, "stream synchronize");
   return HMVM_OK;
 }
 
