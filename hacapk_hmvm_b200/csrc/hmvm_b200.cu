@@ -718,9 +718,9 @@ constexpr int kTcWpb = kTcWarpsPerSm;  // one CTA of 6 warps per SM
 using TcFn = void (*)(TcArgs);
 template <bool VST>
 TcFn tc_kernel_for(bool bf16) {
-  return bf16 ? hmvm_tc_kernel<kTcWpb, 4, 2048, kModeMixedBF16, VST> : hmvm_tc_kernel<kTcWpb, 4, 2048, kModeMixed16, VST>;
+  return bf16 ? hmvm_tc_kernel<kTcWpb, 2, 4096, kModeMixedBF16, VST> : hmvm_tc_kernel<kTcWpb, 2, 4096, kModeMixed16, VST>;
 }
-constexpr int tc_smem() { return tc_smem_bytes<kTcWpb, 4, 2048>(); }
+constexpr int tc_smem() { return tc_smem_bytes<kTcWpb, 2, 4096>(); }
 
 int tc_prepare(const hmvm_plan* p) {
   const bool bf = p->mixed_kcode == 3;
