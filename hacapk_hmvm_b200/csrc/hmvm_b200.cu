@@ -588,7 +588,7 @@ inline int apply_impl_fwd(hmvm_plan* p, const void* x, void* y, cudaStream_t st)
 template <int NR, int MODE, bool VST>
 MultiFn multi_kernel_cfg(int cfg) {
   switch (cfg) {
-    default: return hmvm_multi_kernel<4, 4, 2048, NR, MODE, VST>;
+    default: return hmvm_multi_kernel<4, 2, 4096, NR, MODE, VST>;
   }
 }
 template <int MODE, bool VST>

@@ -142,7 +142,7 @@ struct MultiCfg {
   int wpb, slots, chunk;
 };
 constexpr int kNumMultiCfgs = 3;
-constexpr MultiCfg kMultiCfgs[kNumMultiCfgs] = {{4, 4, 2048}, {8, 4, 2048}, {4, 8, 1024}};
+constexpr MultiCfg kMultiCfgs[kNumMultiCfgs] = {{4, 2, 4096}, {8, 4, 2048}, {4, 8, 1024}};
 inline int multi_smem_bytes(const MultiCfg& c) { return c.wpb * (c.slots * c.chunk + 2 * kMultiZBytes + c.slots * 8); }
 constexpr int kDefaultMultiCfg = 0;
 constexpr int kMultiWarpsPerSm = 8;  // resident warps (teams) per SM of the multi-RHS kernel
