@@ -509,8 +509,11 @@ __global__ void hmvm_round_f32_kernel(const double* __restrict__ x, float* __res
 // ---- mixed precision ---------------------------------------------------------
 // Segment element types (the top 4 bits of hmvm_seg_desc.ncols in mixed plans).
 enum : int { kF64 = 0, kF32 = 1, kF16 = 2, kE4M3 = 3, kBF16 = 4 };
-__device__ __forceinline__ int mixed_vec(int type) {
-  return type == kF64 ? 2 : type == kF32 ? 4 : type == kE4M3 ? 16 : 8;
+// log2 of a type's elements per 16-byte vector (2 FP64, 4 FP32, 8 FP16/BF16,
+// 16 E4M3): whole vectors of a segment by shifts, not a division by a value
+// the compiler cannot see is a power of two
+__device__ __forceinline__ int mixed_vec_log2(int type) {
+  return type == kF64 ? 1 : type == kF32 ? 2 : type == kE4M3 ? 4 : 3;
 }
 
 // Copy the inputs item `d` reads into zb: FP64 segments take x (8-byte
@@ -524,8 +527,8 @@ __device__ __forceinline__ void gather_inputs_mixed(const hmvm_tile_desc& d, con
     const int src = __shfl_sync(0xffffffffu, sreg.src, j);
     const int enc = __shfl_sync(0xffffffffu, sreg.ncols, j);
     const int type = enc >> 28, nc = enc & 0x0fffffff;
-    const int vs = mixed_vec(type);
-    const int ncp = (nc + vs - 1) / vs * vs;
+    const int lg = mixed_vec_log2(type);
+    const int ncp = ((nc + (1 << lg) - 1) >> lg) << lg;
     if (type == kF64) {
       double* z = reinterpret_cast<double*>(zb + zoff);
       for (int c = lane; c < ncp; c += 32) {
@@ -786,7 +789,7 @@ __global__ void __launch_bounds__(32 * WPB, (mixed_min_blocks<WPB, S, CHUNK, ZBY
     int j = 0;
     while (j < (VST ? 1 : cur.nseg)) {
       const int type = __shfl_sync(0xffffffffu, cur_seg.ncols, j) >> 28;
-      const int vs = mixed_vec(type);
+      const int lg = mixed_vec_log2(type);
       const unsigned char* zs = zcur + zoff;
       int nv = 0;
       if constexpr (VST) {
@@ -796,10 +799,10 @@ __global__ void __launch_bounds__(32 * WPB, (mixed_min_blocks<WPB, S, CHUNK, ZBY
         for (; j < cur.nseg; j++) {
           const int enc = __shfl_sync(0xffffffffu, cur_seg.ncols, j);
           if ((enc >> 28) != type) break;
-          nv += ((enc & 0x0fffffff) + vs - 1) / vs;
+          nv += ((enc & 0x0fffffff) + (1 << lg) - 1) >> lg;
         }
       }
-      zoff += nv * vs * (type == kF64 ? 8 : 4);
+      zoff += (nv << lg) * (type == kF64 ? 8 : 4);
       bool ok;
       switch (type) {
         case kF64: ok = run_seg(TypeTag<kF64>{}, zs, nv); break;

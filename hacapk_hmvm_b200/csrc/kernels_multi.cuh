@@ -103,8 +103,8 @@ __device__ __forceinline__ void gather_multi(const hmvm_tile_desc& d, const hmvm
     const int enc = __shfl_sync(0xffffffffu, sreg.ncols, j);
     const int type = MultiMode<MODE>::mixed ? (enc >> 28) : (MODE == kModePlain64 ? kF64 : kF32);
     const int nc = MultiMode<MODE>::mixed ? (enc & 0x0fffffff) : enc;
-    const int vs = mixed_vec(type);
-    const int ncp = (nc + vs - 1) / vs * vs;
+    const int lg = mixed_vec_log2(type);
+    const int ncp = ((nc + (1 << lg) - 1) >> lg) << lg;
     const bool from_t = src < 0;
     const int64_t base = (int64_t)(from_t ? (src & 0x7fffffff) : src) * NR;
     if (type == kF64) {
@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(32 * WPB, (multi_min_blocks<WPB, S, CHUNK>()))
     while (j < (VST ? 1 : cur.nseg)) {
       const int enc0 = __shfl_sync(0xffffffffu, cur_seg.ncols, j);
       const int type = MM::mixed ? (enc0 >> 28) : (MODE == kModePlain64 ? kF64 : kF32);
-      const int vs = mixed_vec(type);
+      const int lg = mixed_vec_log2(type);
       const unsigned char* zs = zcur + zoff;
       int nv = 0;
       if (VST) {
@@ -377,10 +377,10 @@ __global__ void __launch_bounds__(32 * WPB, (multi_min_blocks<WPB, S, CHUNK>()))
         for (; j < cur.nseg; j++) {
           const int enc = __shfl_sync(0xffffffffu, cur_seg.ncols, j);
           if (MM::mixed && (enc >> 28) != type) break;
-          nv += ((MM::mixed ? (enc & 0x0fffffff) : enc) + vs - 1) / vs;
+          nv += ((MM::mixed ? (enc & 0x0fffffff) : enc) + (1 << lg) - 1) >> lg;
         }
       }
-      zoff += nv * vs * NR * (type == kF64 ? 8 : 4);
+      zoff += (nv << lg) * NR * (type == kF64 ? 8 : 4);
       bool ok;
       if constexpr (MODE == kModePlain64) {
         ok = run_seg(TypeTag<kF64>{}, zs, nv);

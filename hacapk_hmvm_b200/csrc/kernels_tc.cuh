@@ -260,8 +260,8 @@ __global__ void __launch_bounds__(32 * WPB, 1) hmvm_tc_kernel(TcArgs ta) {
       const bool has = lane < d.nseg;
       const int type = has ? tc_seg_type(sreg.ncols) : -1;
       const int nc = has ? (sreg.ncols & 0x0fffffff) : 0;
-      const int vs = has ? mixed_vec(type) : 1;
-      const int ncp = (nc + vs - 1) / vs * vs;
+      const int lg = has ? mixed_vec_log2(type) : 0;
+      const int ncp = ((nc + (1 << lg) - 1) >> lg) << lg;
       const bool lr = has && type == LR;
       const int es = type == kF64 ? 8 : 4;
       const int lr_rows = lr ? ncp : 0;
@@ -465,7 +465,7 @@ __global__ void __launch_bounds__(32 * WPB, 1) hmvm_tc_kernel(TcArgs ta) {
       int j = 0;
       while (j < (VST ? 1 : cur.nseg)) {
         const int type = tc_seg_type(__shfl_sync(0xffffffffu, cur_seg.ncols, j));
-        const int vs = mixed_vec(type);
+        const int lg = mixed_vec_log2(type);
         int nv = 0;
         if (VST) {
           nv = cur.nvec;
@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(32 * WPB, 1) hmvm_tc_kernel(TcArgs ta) {
           for (; j < cur.nseg; j++) {
             const int enc = __shfl_sync(0xffffffffu, cur_seg.ncols, j);
             if (tc_seg_type(enc) != type) break;
-            nv += ((enc & 0x0fffffff) + vs - 1) / vs;
+            nv += ((enc & 0x0fffffff) + (1 << lg) - 1) >> lg;
           }
         }
         bool ok;
@@ -482,7 +482,7 @@ __global__ void __launch_bounds__(32 * WPB, 1) hmvm_tc_kernel(TcArgs ta) {
           ok = run_tc(nv);
         } else {
           const unsigned char* zs = zcur + zoff;
-          zoff += nv * vs * NR * (type == kF64 ? 8 : 4);
+          zoff += (nv << lg) * NR * (type == kF64 ? 8 : 4);
           switch (type) {
             case kF64: ok = run_cc(TypeTag<kF64>{}, zs, nv); break;
             case kF32: ok = run_cc(TypeTag<kF32>{}, zs, nv); break;

@@ -102,7 +102,8 @@ def test_bitwise_repeatable(gpu):
         assert np.array_equal(y.view(np.uint64), ys[0].view(np.uint64))
 
 
-KCFGS = [(0, c) for c in range(8)] + [(1, c) for c in range(8)]
+NCFGS = {0: 8, 1: 8}  # kNumCfgs, kNumStreamCfgs (layout.hpp)
+KCFGS = [(k, c) for k in (0, 1) for c in range(NCFGS[k])]
 
 
 @pytest.mark.parametrize("kernel,cfg1", KCFGS, ids=[f"k{k}c{c}" for k, c in KCFGS])
@@ -112,7 +113,7 @@ def test_kernel_configs(gpu, kernel, cfg1):
     hm = _mat(CASES[1])
     x = _x(hm.nd)
     yo = oracle_hmvm(hm, x)
-    ncfg = 8
+    ncfg = NCFGS[kernel]
     for prec, tol in (("fp64", TOL64), ("fp32", TOL32)):
         with Plan(hm, prec, kernel=kernel, stage1_cfg=cfg1, stage2_cfg=ncfg - 1 - cfg1,
                   ctas_per_sm=1 + cfg1 % 2) as plan:
