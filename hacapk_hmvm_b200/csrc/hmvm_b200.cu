@@ -117,7 +117,8 @@ KernelFn mixed_kernel_lr(int cfg) {
     case 6: return hmvm_mixed_kernel<8, 2, 4096, 2048, LR16, VST>;
     case 7: return hmvm_mixed_kernel<4, 4, 4096, 2048, LR16, VST>;
     case 8: return hmvm_mixed_kernel<6, 2, 4096, 4096, LR16, VST>;
-    default: return hmvm_mixed_kernel<4, 2, 8192, 2048, LR16, VST>;
+    case 9: return hmvm_mixed_kernel<4, 2, 8192, 2048, LR16, VST>;
+    default: return hmvm_mixed_kernel<5, 2, 8192, 2048, LR16, VST>;
   }
 }
 inline KernelFn mixed_kernel_for(int cfg, bool bf16, int stage) {

@@ -570,7 +570,8 @@ struct MixedZ {
   static constexpr int bytes = TY == kF64 ? 16 : TY == kF32 ? 16 : TY == kE4M3 ? 64 : 32;
 };
 // Vectors per batch: 4 (2 for FP8, whose vectors carry 16 products), twice
-// that when the launch leaves at least 200 registers per thread (WIDE); fewer
+// that when the launch leaves at least 216 registers per thread (WIDE: the
+// 8-vector instances use up to 211); fewer
 // when the ring cannot hold a batch of 32-row vectors beside the chunk being
 // refilled.
 template <int TY, int S, int CHUNK, bool VST, bool WIDE>
@@ -645,7 +646,7 @@ __global__ void __launch_bounds__(32 * WPB, (mixed_min_blocks<WPB, S, CHUNK, ZBY
   constexpr uint32_t RING = (uint32_t)S * CHUNK;
   static_assert((RING & (RING - 1)) == 0, "ring size must be a power of two");
   static_assert(CHUNK % 16 == 0 && CHUNK >= 512, "bulk copies move multiples of 16 bytes");
-  constexpr bool WIDE = 65536 / (32 * WPB * mixed_min_blocks<WPB, S, CHUNK, ZBYTES>()) >= 200;
+  constexpr bool WIDE = 65536 / (32 * WPB * mixed_min_blocks<WPB, S, CHUNK, ZBYTES>()) >= 216;
   static_assert(mixed_batch<kF32, S, CHUNK, VST, WIDE>() * 32 * 16 <= (S - 1) * CHUNK, "ring too small for one batch");
   extern __shared__ __align__(128) unsigned char smem[];
   griddep_launch_dependents();

@@ -117,11 +117,11 @@ constexpr int kMixedMaxSegs = 32;
 struct MixedCfg {
   int wpb, slots, chunk, zbytes;
 };
-constexpr int kNumMixedCfgs = 10;
+constexpr int kNumMixedCfgs = 11;
 constexpr MixedCfg kMixedCfgs[kNumMixedCfgs] = {{8, 4, 2048, 2048}, {8, 4, 1024, 4096}, {8, 4, 2048, 4096},
                                                 {4, 4, 2048, 4096}, {6, 4, 2048, 4096}, {16, 4, 1024, 2048},
                                                 {8, 2, 4096, 2048}, {4, 4, 4096, 2048}, {6, 2, 4096, 4096},
-                                                {4, 2, 8192, 2048}};
+                                                {4, 2, 8192, 2048}, {5, 2, 8192, 2048}};
 inline int mixed_smem_bytes(const MixedCfg& c) { return c.wpb * (c.slots * c.chunk + 2 * c.zbytes + c.slots * 8); }
 // Default configuration of a stage (1: V stage, 2: row stage) for a plan's
 // precision and kernel variant.  Stream kernel: 4 warps x 16 KB rings for FP64
@@ -129,10 +129,11 @@ inline int mixed_smem_bytes(const MixedCfg& c) { return c.wpb * (c.slots * c.chu
 // 4 x 2 KB (cfg 1: 0.445 against 0.454 ms at N = 262,144).
 int default_stage_cfg(int precision, int kernel, int stage);
 // defaults measured at N = 262,144 with each stage at its own resident CTAs
-// per SM: 4 warps x (2 slots of 8 KB) for the V stage, 6 warps x (2 slots of
-// 4 KB) for the row stage, 2 CTAs per SM each (0.480 ms against 0.518 ms
-// with 4 slots of 4 KB and 4 slots of 2 KB: half the bulk-copy issues)
-constexpr int kDefaultMixedCfg1 = 9;
+// per SM: 5 warps x (2 slots of 8 KB) for the V stage, 6 warps x (2 slots of
+// 4 KB) for the row stage, 2 CTAs per SM each (0.473 ms against 0.518 ms
+// with 4 x (4 slots of 4 KB) and 6 x (4 slots of 2 KB): half the bulk-copy
+// issues per byte, and one more warp per CTA in the V stage)
+constexpr int kDefaultMixedCfg1 = 10;
 constexpr int kDefaultMixedCfg2 = 8;
 
 // Multi-RHS kernel (hmvm_multi_kernel): rhs per pass and its input buffer.

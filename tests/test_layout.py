@@ -30,11 +30,11 @@ def test_layout_bounds_and_emulation(case):
             _lib.hmvm_lib().hmvm_b200_layout_destroy(h)
 
 
-MIXED_ZBYTES = {0: 2048, 1: 4096, 2: 4096, 3: 4096, 4: 4096, 5: 2048, 6: 2048, 7: 2048, 8: 4096, 9: 2048}  # kMixedCfgs (layout.hpp)
-MIXED_DEFAULT_CFGS = (9, 8)  # kDefaultMixedCfg1, kDefaultMixedCfg2 (layout.hpp)
+MIXED_ZBYTES = {0: 2048, 1: 4096, 2: 4096, 3: 4096, 4: 4096, 5: 2048, 6: 2048, 7: 2048, 8: 4096, 9: 2048, 10: 2048}  # kMixedCfgs (layout.hpp)
+MIXED_DEFAULT_CFGS = (10, 8)  # kDefaultMixedCfg1, kDefaultMixedCfg2 (layout.hpp)
 MIXED_OPTS = [dict(), dict(mixed_lr_format="bf16"), dict(mixed_fp8_eps=0.0), dict(mixed_fp32_tau=2.0),
               dict(split_cols=8), dict(max_tile_rows=5), dict(stage1_cfg=5, stage2_cfg=1, ctas_per_sm=1),
-              dict(stage1_cfg=7, stage2_cfg=4)]
+              dict(stage1_cfg=7, stage2_cfg=4), dict(stage1_cfg=9, stage2_cfg=10)]
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[1]}{c[0]}")

@@ -94,11 +94,11 @@ def test_mixed_formats(gpu, opts):
     assert relerr(y, oracle_hmvm(hm, x)) <= (2e-4 if opts.get("mixed_fp8_eps") == 1e-3 else TOL_ORACLE)
 
 
-@pytest.mark.parametrize("cfg", range(10))
+@pytest.mark.parametrize("cfg", range(11))
 def test_mixed_kernel_configs(gpu, cfg):
     hm = _mat(CASES[1])
     x = _x(hm.nd, 1)
-    opts = dict(stage1_cfg=cfg, stage2_cfg=9 - cfg, ctas_per_sm=1 + cfg % 2)
+    opts = dict(stage1_cfg=cfg, stage2_cfg=10 - cfg, ctas_per_sm=1 + cfg % 2)
     with Plan(hm, "mixed", **opts) as plan:
         y = _run(plan, x)
     assert relerr(y, _walk(hm, x, **opts)) <= TOL_WALK
