@@ -11,6 +11,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "hmvm_b200.h"
@@ -75,51 +76,51 @@ cudaError_t launch_in_apply(bool& first, void (*fn)(P...), unsigned grid, unsign
 }
 using MultiFn = void (*)(MultiArgs);
 
+// The kernel instance of configuration `cfg` of a table in layout.hpp: the
+// template arguments are read from the table itself, so the launch shape the
+// host sizes shared memory for (stream_smem_bytes, mixed_smem_bytes) and the
+// kernel's own layout cannot disagree.  An index outside the table picks its
+// last entry.
+template <typename T, int... I>
+KernelFn tile_kernel_pick(int cfg, std::integer_sequence<int, I...>) {
+  KernelFn fn = nullptr;
+  ((fn = (cfg == I ? hmvm_tile_kernel<T, kCfgs[I].wg, kCfgs[I].tpc> : fn)), ...);
+  return fn;
+}
 template <typename T>
 KernelFn tile_kernel_for(int cfg) {
-  switch (cfg) {
-    case 0: return hmvm_tile_kernel<T, 1, 8>;
-    case 1: return hmvm_tile_kernel<T, 2, 4>;
-    case 2: return hmvm_tile_kernel<T, 4, 2>;
-    case 3: return hmvm_tile_kernel<T, 8, 1>;
-    case 4: return hmvm_tile_kernel<T, 2, 8>;
-    case 5: return hmvm_tile_kernel<T, 4, 4>;
-    case 6: return hmvm_tile_kernel<T, 8, 2>;
-    default: return hmvm_tile_kernel<T, 16, 1>;
-  }
+  if (cfg < 0 || cfg >= kNumCfgs) cfg = kNumCfgs - 1;
+  return tile_kernel_pick<T>(cfg, std::make_integer_sequence<int, kNumCfgs>{});
 }
 
-// Must list kStreamCfgs (layout.hpp) in order.
+template <typename T, int... I>
+KernelFn stream_kernel_pick(int cfg, std::integer_sequence<int, I...>) {
+  KernelFn fn = nullptr;
+  ((fn = (cfg == I ? hmvm_stream_kernel<T, kStreamCfgs[I].wpb, kStreamCfgs[I].slots, kStreamCfgs[I].chunk,
+                                        kStreamCfgs[I].zcap>
+                   : fn)),
+   ...);
+  return fn;
+}
 template <typename T>
 KernelFn stream_kernel_for(int cfg) {
-  switch (cfg) {
-    case 0: return hmvm_stream_kernel<T, 8, 4, 1024, 256>;
-    case 1: return hmvm_stream_kernel<T, 4, 4, 2048, 512>;
-    case 2: return hmvm_stream_kernel<T, 8, 4, 2048, 256>;
-    case 3: return hmvm_stream_kernel<T, 16, 4, 1024, 128>;
-    case 4: return hmvm_stream_kernel<T, 4, 8, 1024, 512>;
-    case 5: return hmvm_stream_kernel<T, 8, 8, 512, 256>;
-    case 6: return hmvm_stream_kernel<T, 8, 2, 4096, 256>;
-    default: return hmvm_stream_kernel<T, 4, 4, 4096, 512>;
-  }
+  if (cfg < 0 || cfg >= kNumStreamCfgs) cfg = kNumStreamCfgs - 1;
+  return stream_kernel_pick<T>(cfg, std::make_integer_sequence<int, kNumStreamCfgs>{});
 }
 
-// Must list kMixedCfgs (layout.hpp) in order.
+template <int LR16, bool VST, int... I>
+KernelFn mixed_kernel_pick(int cfg, std::integer_sequence<int, I...>) {
+  KernelFn fn = nullptr;
+  ((fn = (cfg == I ? hmvm_mixed_kernel<kMixedCfgs[I].wpb, kMixedCfgs[I].slots, kMixedCfgs[I].chunk,
+                                       kMixedCfgs[I].zbytes, LR16, VST>
+                   : fn)),
+   ...);
+  return fn;
+}
 template <int LR16, bool VST>
 KernelFn mixed_kernel_lr(int cfg) {
-  switch (cfg) {
-    case 0: return hmvm_mixed_kernel<8, 4, 2048, 2048, LR16, VST>;
-    case 1: return hmvm_mixed_kernel<8, 4, 1024, 4096, LR16, VST>;
-    case 2: return hmvm_mixed_kernel<8, 4, 2048, 4096, LR16, VST>;
-    case 3: return hmvm_mixed_kernel<4, 4, 2048, 4096, LR16, VST>;
-    case 4: return hmvm_mixed_kernel<6, 4, 2048, 4096, LR16, VST>;
-    case 5: return hmvm_mixed_kernel<16, 4, 1024, 2048, LR16, VST>;
-    case 6: return hmvm_mixed_kernel<8, 2, 4096, 2048, LR16, VST>;
-    case 7: return hmvm_mixed_kernel<4, 4, 4096, 2048, LR16, VST>;
-    case 8: return hmvm_mixed_kernel<6, 2, 4096, 4096, LR16, VST>;
-    case 9: return hmvm_mixed_kernel<4, 2, 8192, 2048, LR16, VST>;
-    default: return hmvm_mixed_kernel<5, 2, 8192, 2048, LR16, VST>;
-  }
+  if (cfg < 0 || cfg >= kNumMixedCfgs) cfg = kNumMixedCfgs - 1;
+  return mixed_kernel_pick<LR16, VST>(cfg, std::make_integer_sequence<int, kNumMixedCfgs>{});
 }
 inline KernelFn mixed_kernel_for(int cfg, bool bf16, int stage) {
   if (stage == 1) return bf16 ? mixed_kernel_lr<kBF16, true>(cfg) : mixed_kernel_lr<kF16, true>(cfg);
