@@ -588,12 +588,14 @@ int apply_impl(hmvm_plan* p, const void* x, void* y, cudaStream_t st);
 inline int apply_impl_fwd(hmvm_plan* p, const void* x, void* y, cudaStream_t st) { return apply_impl(p, x, y, st); }
 
 // ---- multi-RHS ---------------------------------------------------------------
-// Must list kMultiCfgs (layout.hpp) in order.
+// The multi-RHS kernel's launch shape is read from kMultiCfgs (layout.hpp),
+// like the single-vector kernels' (see tile_kernel_pick).
 template <int NR, int MODE, bool VST>
 MultiFn multi_kernel_cfg(int cfg) {
-  switch (cfg) {
-    default: return hmvm_multi_kernel<4, 2, 4096, NR, MODE, VST>;
-  }
+  static_assert(kNumMultiCfgs == 1 && kDefaultMultiCfg == 0, "one multi-RHS shape is instantiated");
+  (void)cfg;
+  constexpr MultiCfg c = kMultiCfgs[kDefaultMultiCfg];
+  return hmvm_multi_kernel<c.wpb, c.slots, c.chunk, NR, MODE, VST>;
 }
 template <int MODE, bool VST>
 MultiFn multi_kernel_nr(int nr, int cfg) {

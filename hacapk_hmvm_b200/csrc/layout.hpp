@@ -144,8 +144,10 @@ constexpr int kMultiZBytes = 8192;
 struct MultiCfg {
   int wpb, slots, chunk;
 };
-constexpr int kNumMultiCfgs = 3;
-constexpr MultiCfg kMultiCfgs[kNumMultiCfgs] = {{4, 2, 4096}, {8, 4, 2048}, {4, 8, 1024}};
+// one shape: 4 warps per CTA, a ring of 2 x 4 KiB per warp (faster than the
+// 4 x 2 KiB and 8 x 1 KiB rings it replaced)
+constexpr int kNumMultiCfgs = 1;
+constexpr MultiCfg kMultiCfgs[kNumMultiCfgs] = {{4, 2, 4096}};
 inline int multi_smem_bytes(const MultiCfg& c) { return c.wpb * (c.slots * c.chunk + 2 * kMultiZBytes + c.slots * 8); }
 constexpr int kDefaultMultiCfg = 0;
 constexpr int kMultiWarpsPerSm = 8;  // resident warps (teams) per SM of the multi-RHS kernel
