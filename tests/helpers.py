@@ -332,11 +332,13 @@ def layout_for(hm, **opts):
     from hacapk_hmvm_b200.hmvm import default_opts
 
     lib = _lib.hmvm_lib()
+    opts = dict(opts)
+    num_sms = int(opts.pop("num_sms", 148))  # the SM count the plan is laid out for
     o = default_opts(**opts)
     h = C.c_void_p()
     lv = hm.as_leaves64()
     rc = lib.hmvm_b200_layout_build64(C.byref(lv), 1 if hm.rowmat.dtype == np.float32 else 0, C.byref(o),
-                                      int(opts.get("num_sms", 148)) if "num_sms" in opts else 148, C.byref(h))
+                                      num_sms, C.byref(h))
     _lib.check(rc, "layout build")
     v = _lib.LayoutView()
     _lib.check(lib.hmvm_b200_layout_view(h, C.byref(v)), "layout view")
