@@ -209,14 +209,20 @@ def max_over_ranks(value: float, dist, device) -> float:
 DTYPES = {"fp64": "f64", "fp32": "f32",
           "mixed": "mixed: f32/f16/e4m3 low-rank, f32/f64 dense storage; f32 segment sums, f64 rows and x, y"}
 
-TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "stream_kernel_fp64_sphere65536.md")
+# ncu summaries that carry traffic_per_algorithmic_byte lines, by the single-vector
+# kernel they captured: FP64 stream kernel, mixed kernel (FP16 factors)
+TRAFFIC_PROFILES = {"fp64": os.path.join(ROOT, "profiles", "stream_kernel_fp64_sphere65536.md"),
+                    "mixed": os.path.join(ROOT, "profiles", "mixed_kernel_fp16_sphere65536.md")}
 
 
-def traffic_ratio(stage: int):
+def traffic_ratio(stage: int, precision: str = "fp64"):
     """DRAM bytes per algorithmic byte of a stage kernel, from the committed ncu
     summary (a capture of a smaller case of the same kernel), or None."""
+    path = TRAFFIC_PROFILES.get(precision)
+    if path is None:
+        return None
     try:
-        for line in open(TRAFFIC_PROFILE):
+        for line in open(path):
             parts = line.split()
             if len(parts) == 3 and parts[0] == "traffic_per_algorithmic_byte" and parts[1] == f"stage{stage}":
                 return float(parts[2])
@@ -464,11 +470,13 @@ def run_b200(a, rank, world, local_rank):
         "kernel": [f"{kname} (V stage)", "hmvm_reduce_kernel (V stage)", f"{kname} (row stage)",
                    "hmvm_reduce_kernel (row stage)"][dom],
         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-        "traffic": (stage_bytes[dom] * traffic_ratio(1 if dom == 0 else 2)
-                    if dom in (0, 2) and info["kernel"] == 1 and a.precision == "fp64"
-                    and traffic_ratio(1 if dom == 0 else 2) else None),
-        "traffic_source": "ncu capture of the same kernel at N=65536, scaled by algorithmic bytes "
-                          "(profiles/stream_kernel_fp64_sphere65536.md)",
+        "traffic": (stage_bytes[dom] * traffic_ratio(1 if dom == 0 else 2, a.precision)
+                    if dom in (0, 2) and a.nrhs == 1 and a.lr_format == "fp16"
+                    and ((info["kernel"] == 1 and a.precision == "fp64") or a.precision == "mixed")
+                    and traffic_ratio(1 if dom == 0 else 2, a.precision) else None),
+        "traffic_source": "ncu capture of the same kernel at N=65536, scaled by algorithmic bytes ("
+                          + os.path.relpath(TRAFFIC_PROFILES.get(a.precision, TRAFFIC_PROFILES["fp64"]), ROOT)
+                          + ")",
         "whole_hmvm_gbs": alg_bytes / (ms_step * 1e-3) / 1e9,
         "whole_hmvm_frac": alg_bytes / (ms_step * 1e-3) / 1e9 / peak,
         "stage_ms_avg": [s / max(napplies, 1) for s in stage_ms],
