@@ -42,3 +42,16 @@ def test_published_lookup():
     big = SimpleNamespace(mesh="input_216h.pbf", nrhs=1, precision="fp64")
     assert bench.published_hmvm_per_s(big, SimpleNamespace(nd=21600)) == pytest.approx(1 / 1.002e-3)
     assert bench.published_hmvm_per_s(SimpleNamespace(mesh=None, nrhs=1, precision="fp64"), hm) is None
+
+
+def test_traffic_ratios_from_committed_profiles():
+    """The roofline's traffic field scales the DRAM-bytes ratios that the
+    committed ncu summaries carry; both single-vector kernels have them."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    for prec in ("fp64", "mixed"):
+        for stage in (1, 2):
+            r = bench.traffic_ratio(stage, prec)
+            assert r is not None and 1.0 <= r < 1.2, (prec, stage, r)
+    assert bench.traffic_ratio(2, "fp32") is None
