@@ -474,14 +474,15 @@ def run_b200(a, rank, world, local_rank):
                     if dom in (0, 2) and a.nrhs == 1 and a.lr_format == "fp16"
                     and ((info["kernel"] == 1 and a.precision == "fp64") or a.precision == "mixed")
                     and traffic_ratio(1 if dom == 0 else 2, a.precision) else None),
-        "traffic_source": "ncu capture of the same kernel at N=65536, scaled by algorithmic bytes ("
-                          + os.path.relpath(TRAFFIC_PROFILES.get(a.precision, TRAFFIC_PROFILES["fp64"]), ROOT)
-                          + ")",
+        "traffic_source": None,
         "whole_hmvm_gbs": alg_bytes / (ms_step * 1e-3) / 1e9,
         "whole_hmvm_frac": alg_bytes / (ms_step * 1e-3) / 1e9 / peak,
         "stage_ms_avg": [s / max(napplies, 1) for s in stage_ms],
         "stage_bytes": stage_bytes,
     }
+    if roof["traffic"] is not None:
+        roof["traffic_source"] = ("ncu capture of the same kernel at N=65536, scaled by algorithmic bytes ("
+                                  + os.path.relpath(TRAFFIC_PROFILES[a.precision], ROOT) + ")")
 
     if rank == 0:
         value = world * 1e3 / ms_step * a.nrhs
