@@ -657,6 +657,8 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
       item_off[order[k]] = off;
       off += (int64_t)d.nvec * t.nrows;
     }
+    // Not zeroed (UninitAlloc): the items partition [0, off) and the pack
+    // below copies every item's whole range from a zero-padded tile buffer.
     L.data.resize((size_t)off);
 
     // ---- pack: each tile into a scratch buffer, then its items' ranges -----
