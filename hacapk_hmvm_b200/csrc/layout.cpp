@@ -676,8 +676,9 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
         for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) {
           const SegBuild &sg = sb[s];
           const int type = sg.type, vs = seg_vec(type), eb = elem_bytes(type);
+          const int lg = vs == 2 ? 1 : vs == 4 ? 2 : vs == 8 ? 3 : 4;  // vs is 2, 4, 8 or 16
           auto put = [&](int64_t c, int32_t r, double v) {
-            store_elem(base, ((vs0 + c / vs) * R + r) * 16 + (c % vs) * eb, type, v);
+            store_elem(base, ((vs0 + (c >> lg)) * R + r) * 16 + (c & (vs - 1)) * eb, type, v);
           };
           if (t.stage == 1) {
             for (int32_t r = 0; r < R; r++) {
