@@ -76,6 +76,11 @@ def parse():
     ap.add_argument("--batch-nmin", type=int, default=4096)
     ap.add_argument("--batch-nmax", type=int, default=131072)
     ap.add_argument("--batch-rhs-max", type=int, default=16)
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the secondary workloads (FP32, mixed, multi-RHS) timed after the headline")
+    ap.add_argument("--secondary-steps", type=int, default=40, help="timed steps of each single-vector secondary leg")
+    ap.add_argument("--no-cpu-variants", action="store_true",
+                    help="skip the reference's full OpenMP variant sweep and its one-core hmvm_seq_2")
     return ap.parse_args()
 
 
@@ -97,6 +102,9 @@ class CpuReference:
             lib.ref_wrap2.restype = C.c_void_p
             lib.ref_wrap2.argtypes = [C.c_int] * 4 + [P] * 9
             lib.ref_omp2_d.argtypes = [C.c_void_p, P, P, C.c_int]
+            lib.ref_seq2_d.argtypes = [C.c_void_p, P, P, C.c_int]
+            lib.ref_omp_bench_d.argtypes = [C.c_void_p, P, C.c_char_p, C.c_int]
+            lib.ref_omp_bench_d.restype = C.c_int
             lib.ref_max_threads.restype = C.c_int
             self.lib = lib
             self.h = lib.ref_wrap2(hm.nd, hm.nlf, hm.ktmax, hm.len,
@@ -324,10 +332,230 @@ def run_reference(a, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_b200(a, rank, world, local_rank):
+def make_plan(hm, precision, nrhs, lr_format, device, a=None):
+    """The plan a workload runs on: single-vector plans for nrhs 1, multi-RHS
+    plans sized for the pass width otherwise (tensor-core passes for mixed
+    plans from 16 right-hand sides)."""
+    from hacapk_hmvm_b200 import Plan
+
+    kw = {}
+    if a is not None:
+        kw = dict(stage1_cfg=a.stage1_cfg, stage2_cfg=a.stage2_cfg, ctas_per_sm=a.ctas_per_sm, kernel=a.kernel)
+    nrhs_max = 16 if (precision == "mixed" and nrhs >= 16) else min(nrhs, 8)
+    return Plan(hm, precision, device=device, nrhs_max=nrhs_max,
+                mixed_lr_format=lr_format if precision == "mixed" else None, **kw)
+
+
+def kernel_name(plan, info, nrhs):
+    if nrhs > 1:
+        return "hmvm_tc_kernel" if (plan.precision == "mixed" and info["nrhs_max"] >= 16) else "hmvm_multi_kernel"
+    return {0: "hmvm_tile_kernel", 1: "hmvm_stream_kernel", 2: "hmvm_mixed_kernel"}[info["kernel"]]
+
+
+def passes_of(plan, nrhs):
+    """Matrix streams per multi-RHS apply (one per pass)."""
+    if nrhs <= 1:
+        return 1
+    per_pass = max(plan.multi_kernel_count(min(nrhs, 2)), 1)
+    return max(1, plan.multi_kernel_count(nrhs) // per_pass)
+
+
+def roofline_of(plan, info, nrhs, stage_ms, napplies, ms_step, precision, lr_format="fp16"):
+    """Dominant kernel's achieved bandwidth (its algorithmic bytes per launch /
+    its average CUDA-event duration) and the whole step's, against the
+    measured HBM peak."""
+    peak, peak_kind = measured_peak_gbs()
+    stage_bytes = [info["stage1_bytes"], 0, info["stage2_bytes"], 0]
+    dom = int(np.argmax(stage_ms))
+    dom_avg_s = stage_ms[dom] / max(napplies, 1) * 1e-3
+    achieved = stage_bytes[dom] / dom_avg_s / 1e9 if dom_avg_s > 0 else 0.0
+    passes = passes_of(plan, nrhs)
+    elem_xy = 4 if precision == "fp32" else 8
+    # a multi-RHS step streams the matrix once per pass and reads/writes every column once
+    alg_bytes = info["algorithmic_bytes"] * passes + 2 * plan.nd * elem_xy * (nrhs - passes)
+    kname = kernel_name(plan, info, nrhs)
+    ratio = None
+    if dom in (0, 2) and nrhs == 1 and lr_format == "fp16" and (
+            (info["kernel"] == 1 and precision == "fp64") or precision == "mixed"):
+        ratio = traffic_ratio(1 if dom == 0 else 2, precision)
+    roof = {
+        "bound": "hbm",
+        "kernel": [f"{kname} (V stage)", "hmvm_reduce_kernel (V stage)", f"{kname} (row stage)",
+                   "hmvm_reduce_kernel (row stage)"][dom],
+        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+        "traffic": stage_bytes[dom] * ratio if ratio else None,
+        "traffic_source": None,
+        "whole_step_gbs": alg_bytes / (ms_step * 1e-3) / 1e9,
+        "whole_step_frac": alg_bytes / (ms_step * 1e-3) / 1e9 / peak,
+        "stage_ms_avg": [s / max(napplies, 1) for s in stage_ms],
+        "stage_bytes": stage_bytes,
+        "passes_per_step": passes,
+    }
+    if ratio:
+        roof["traffic_source"] = ("ncu capture of the same kernel at N=65536, scaled by algorithmic bytes ("
+                                  + os.path.relpath(TRAFFIC_PROFILES[precision], ROOT) + ")")
+    return roof, alg_bytes
+
+
+def time_steps(step, steps, warmup, stream, dev, dist=None):
+    """ms per step over `steps` timed steps after `warmup` untimed ones (CUDA
+    events on the launching stream, max over ranks)."""
     import torch
 
-    from hacapk_hmvm_b200 import Plan
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    return max_over_ranks(e0.elapsed_time(e1), dist, dev) / steps
+
+
+class CpuColumns:
+    """The reference CPU HMVM (hmvm_omp_2<double,0>) of columns of X, each
+    computed once."""
+
+    def __init__(self, cpu, X):
+        self.cpu, self.X, self.y = cpu, X, {}
+
+    def __call__(self, c):
+        if c not in self.y:
+            yc = np.empty(self.cpu.nd)
+            self.cpu.run(self.X[c], yc)
+            self.y[c] = yc
+        return self.y[c]
+
+
+def checked_columns(nrhs):
+    """Every column up to 16 right-hand sides, else a fixed sample of 8."""
+    if nrhs <= 16:
+        return list(range(nrhs))
+    return sorted(set(int(round(v)) for v in np.linspace(0, nrhs - 1, 8)))
+
+
+def cpu_bench_variants(cpu, x, seq_seconds):
+    """The reference's own timed sweep of its SoA OpenMP variants
+    (hmvm_omp_bench, L=10 with the first 5 discarded) and hmvm_seq_2 on one
+    core (the reference proxy's loop shape, bounded to about seq_seconds)."""
+    out = {}
+    if cpu.kind != "reference":
+        return out
+    import tempfile
+
+    with tempfile.NamedTemporaryFile("r", suffix=".txt") as f:
+        rc = cpu.lib.ref_omp_bench_d(cpu.h, x.ctypes.data_as(C.c_void_p), f.name.encode(), 0)
+        if rc == 0:
+            rows = {}
+            for line in open(f.name):
+                p = line.split()
+                if len(p) == 9 and p[0] == "TIME":
+                    rows[p[2]] = {"min_s": float(p[4]), "max_s": float(p[6]), "avg_s": float(p[8])}
+            if rows:
+                best = min(rows, key=lambda k: rows[k]["min_s"])
+                out["omp_variants"] = rows
+                out["best_omp_variant"] = {"name": best, "value": 1.0 / rows[best]["min_s"], "unit": "HMVM/s",
+                                           "cores": cpu.threads}
+    y = np.empty(cpu.nd)
+    t0 = time.perf_counter()
+    cpu.lib.ref_seq2_d(cpu.h, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p), 0)
+    one = max(time.perf_counter() - t0, 1e-6)
+    runs = int(min(10, max(6, seq_seconds / one)))
+    ts = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        cpu.lib.ref_seq2_d(cpu.h, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p), 0)
+        ts.append(time.perf_counter() - t0)
+    kept = ts[5:]
+    out["seq_2_one_core"] = {"value": 1.0 / min(kept), "unit": "HMVM/s", "cores": 1,
+                             "sample": f"hmvm_seq_2<double,0>, {runs} runs, first 5 discarded, min of {len(kept)}"}
+    return out
+
+
+# Secondary workloads timed after the headline on the same matrix: (label,
+# precision, right-hand sides, 16-bit factor format).  Plans are built once per
+# (precision, factor format, pass kind) and reused by the legs that share them.
+SECONDARY = [
+    ("fp32 single-vector", "fp32", 1, None),
+    ("mixed single-vector, FP16 factors", "mixed", 1, "fp16"),
+    ("mixed single-vector, BF16 factors", "mixed", 1, "bf16"),
+    ("mixed multi-RHS nrhs=16, FP16 factors", "mixed", 16, "fp16"),
+    ("mixed multi-RHS nrhs=128, FP16 factors", "mixed", 128, "fp16"),
+    ("mixed multi-RHS nrhs=16, BF16 factors", "mixed", 16, "bf16"),
+    ("mixed multi-RHS nrhs=128, BF16 factors", "mixed", 128, "bf16"),
+    ("fp32 multi-RHS nrhs=8", "fp32", 8, None),
+    ("fp32 multi-RHS nrhs=128", "fp32", 128, None),
+]
+
+
+def run_secondary(a, hm, X, cpucols, fp64_rate, local_rank, stream, dev):
+    import torch
+
+    legs = []
+    key_of = lambda prec, nrhs, fmt: (prec, fmt, "single" if nrhs == 1 else
+                                      ("tc" if prec == "mixed" and nrhs >= 16 else "multi"))
+    plans = {}
+    for i, (label, prec, nrhs, fmt) in enumerate(SECONDARY):
+        key = key_of(prec, nrhs, fmt)
+        if key not in plans:
+            t0 = time.perf_counter()
+            plans[key] = (make_plan(hm, prec, nrhs, fmt, local_rank), time.perf_counter() - t0)
+        plan, setup_s = plans[key]
+        info = plan.info()
+        ndt = np.float32 if prec == "fp32" else np.float64
+        tdt = torch.float32 if prec == "fp32" else torch.float64
+        xd = torch.from_numpy(X[:nrhs].astype(ndt)).to(dev)
+        yd = torch.full((nrhs, hm.nd), float("nan"), dtype=tdt, device=dev)
+        if nrhs == 1:
+            step = lambda: plan.apply(xd[0], yd[0], stream)
+        else:
+            step = lambda: plan.apply_multi(xd, yd, stream)
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize(dev)
+        plan.profile(True)
+        steps = max(3, a.secondary_steps if nrhs == 1 else a.secondary_steps // 4)
+        ms = time_steps(step, steps, a.warmup, stream, dev)
+        stage_ms, napplies = plan.profile_read()
+        plan.profile(False)
+        plan.status()
+        roof, alg = roofline_of(plan, info, nrhs, stage_ms, napplies, ms, prec, fmt or "fp16")
+        Y = yd.cpu().numpy().astype(np.float64)
+        errs = {}
+        for c in checked_columns(nrhs):
+            yc = cpucols(c)
+            errs[c] = float(np.linalg.norm(Y[c] - yc) / np.linalg.norm(yc))
+        rate = 1e3 / ms * nrhs
+        legs.append({
+            "workload": label, "precision": prec, "lr_format": fmt, "nrhs": nrhs,
+            "unit": "HMVM/s" if nrhs == 1 else "vectors/s", "value": rate, "ms_per_step": ms, "steps": steps,
+            "ratio_vs_fp64_vectors": rate / fp64_rate,
+            "relerr_vs_fp64_cpu_reference": max(errs.values()),
+            "relerr_columns_checked": len(errs), "aca_eps": a.eps,
+            "roofline": roof, "algorithmic_bytes_per_step": alg,
+            "kernel": kernel_name(plan, info, nrhs), "plan_setup_s": setup_s,
+            "device_bytes": info["device_bytes"],
+            "gpu_launches": steps * (plan.kernel_count() if nrhs == 1 else plan.multi_kernel_count(nrhs)),
+        })
+        del xd, yd
+        # close a plan after the last leg that uses it
+        if all(key_of(p2, n2, f2) != key for (_, p2, n2, f2) in SECONDARY[i + 1:]):
+            plan.close()
+            del plans[key]
+            torch.cuda.empty_cache()
+    return legs
+
+
+def run_b200(a, rank, world, local_rank):
+    import torch
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
@@ -337,22 +565,21 @@ def run_b200(a, rank, world, local_rank):
 
         dist = dist_mod
     hm = build_matrix(a)
+    secondary = (not a.no_secondary and a.nrhs == 1 and a.precision == "fp64" and not a.mesh and rank == 0
+                 and world == 1 and not a.graph)
     rng = np.random.default_rng(a.seed)
-    X = rng.uniform(-1.0, 1.0, (a.nrhs, hm.nd)) if a.x_dist == "uniform" else rng.standard_normal((a.nrhs, hm.nd))
+    ncols = max(a.nrhs, 128 if secondary else 1)
+    X = rng.uniform(-1.0, 1.0, (ncols, hm.nd)) if a.x_dist == "uniform" else rng.standard_normal((ncols, hm.nd))
     x = X[0]
     t0 = time.perf_counter()
-    plan = Plan(hm, a.precision, device=local_rank, stage1_cfg=a.stage1_cfg, stage2_cfg=a.stage2_cfg,
-                ctas_per_sm=a.ctas_per_sm, kernel=a.kernel,
-                # mixed plans take 16 right-hand sides per pass on the tensor cores
-                nrhs_max=16 if (a.precision == "mixed" and a.nrhs >= 16) else min(a.nrhs, 8),
-                mixed_lr_format=a.lr_format if a.precision == "mixed" else None)
+    plan = make_plan(hm, a.precision, a.nrhs, a.lr_format, local_rank, a)
     setup_s = time.perf_counter() - t0
     info = plan.info()
     # x and y: FP64 for FP64 and mixed plans, FP32 for FP32 plans
     tdt = torch.float32 if a.precision == "fp32" else torch.float64
     ndt = np.float32 if a.precision == "fp32" else np.float64
     elem = 4 if a.precision == "fp32" else 8
-    xd = torch.from_numpy(X.astype(ndt)).to(dev)
+    xd = torch.from_numpy(X[:a.nrhs].astype(ndt)).to(dev)
     yd = torch.empty((a.nrhs, hm.nd), dtype=tdt, device=dev)
     stream = torch.cuda.current_stream(dev)
     if a.nrhs == 1:
@@ -380,19 +607,7 @@ def run_b200(a, rank, world, local_rank):
     time.sleep(0.3)
     if not use_graph:
         plan.profile(True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(a.steps):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    if dist:
-        dist.barrier()
-    ms_total = e0.elapsed_time(e1)
+    ms_step = time_steps(step, a.steps, 0, stream, dev, dist)
     if use_graph:  # stage times: a profiled pass of direct applies (a replayed graph records no events)
         plan.profile(True)
         for _ in range(min(a.steps, 200)):
@@ -401,13 +616,11 @@ def run_b200(a, rank, world, local_rank):
     stage_ms, napplies = plan.profile_read()
     plan.profile(False)
     clk = clocks.stop()
-    ms_total = max_over_ranks(ms_total, dist, dev)
-    ms_step = ms_total / a.steps
     Y_gpu = yd.cpu().numpy().astype(np.float64)
     y_gpu = Y_gpu[0]
 
     # ---- e2e: the C-ABI host-buffer call, pinned buffers, copies inside ----
-    xh = torch.from_numpy(X.astype(ndt)).pin_memory()
+    xh = torch.from_numpy(X[:a.nrhs].astype(ndt)).pin_memory()
     yh = torch.empty((a.nrhs, hm.nd), dtype=tdt).pin_memory()
     xh_np, yh_np = xh.numpy(), yh.numpy()
     if a.nrhs == 1:
@@ -416,83 +629,45 @@ def run_b200(a, rank, world, local_rank):
     else:
         def host_step():
             plan.apply_multi_host(xh_np, yh_np, stream)
-    for _ in range(3):
-        host_step()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(a.e2e_steps):
-        host_step()
-    f1.record(stream)
-    torch.cuda.synchronize(dev)
-    e2e_ms = f0.elapsed_time(f1)
-    e2e_ms = max_over_ranks(e2e_ms, dist, dev)
-    e2e_step = e2e_ms / a.e2e_steps
+    e2e_step = time_steps(host_step, a.e2e_steps, 3, stream, dev, dist)
 
     unit = "HMVM/s" if a.nrhs == 1 else "vectors/s"
+    roof, alg_bytes = roofline_of(plan, info, a.nrhs, stage_ms, napplies, ms_step, a.precision, a.lr_format)
+    kname = kernel_name(plan, info, a.nrhs)
+    plan_keys = {"kernel": kname, "stage1_cfg": info["stage1_cfg"], "stage2_cfg": info["stage2_cfg"],
+                 "ctas_per_sm": [info["ctas_per_sm"], info["stage2_ctas_per_sm"]],
+                 "device_bytes": info["device_bytes"], "plan_setup_s": setup_s}
+    launches = a.steps * (plan.kernel_count() if a.nrhs == 1 else plan.multi_kernel_count(a.nrhs))
+    plan.close()
+    del xd, yd
+    torch.cuda.empty_cache()
+
     # ---- CPU baseline (rank 0, N=1 only) and parity of this run ----
     cpu_line = None
     rel = None
+    legs = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = CpuReference(hm)
+        cpucols = CpuColumns(cpu, X)
         y_cpu, st = cpu.time_sample(x, a.cpu_seconds)
+        cpucols.y[0] = y_cpu
         rel = float(np.linalg.norm(y_gpu - y_cpu) / np.linalg.norm(y_cpu))
-        for r in range(1, min(a.nrhs, 4)):  # a few more columns of a multi-RHS step
-            yc = np.empty(hm.nd)
-            cpu.run(X[r], yc)
-            rel = max(rel, float(np.linalg.norm(Y_gpu[r] - yc) / np.linalg.norm(yc)))
-        cpu_line = {"value": 1.0 / st["min"], "unit": unit, "cores": cpu.threads, "kind": cpu.kind,
+        for r in checked_columns(a.nrhs)[1:]:
+            rel = max(rel, float(np.linalg.norm(Y_gpu[r] - cpucols(r)) / np.linalg.norm(cpucols(r))))
+        cpu_line = {"value": 1.0 / st["min"], "unit": "HMVM/s", "cores": cpu.threads, "kind": cpu.kind,
                     "sample": f"hmvm_omp_2<double,0> on the full matrix (one vector per call), {st['runs']} runs, "
                               f"first 5 discarded, min of {st['kept']} (avg {st['avg'] * 1e3:.2f} ms)",
                     "relerr_gpu_vs_cpu": rel}
+        if not a.no_cpu_variants:
+            cpu_line.update(cpu_bench_variants(cpu, x, a.cpu_seconds))
+        if secondary:
+            legs = run_secondary(a, hm, X, cpucols, 1e3 / ms_step, local_rank, stream, dev)
     if dist:
         dist.barrier()
-
-    # ---- roofline of the dominant kernel ----
-    peak, peak_kind = measured_peak_gbs()
-    stage_bytes = [info["stage1_bytes"], 0, info["stage2_bytes"], 0]
-    dom = int(np.argmax(stage_ms))
-    dom_avg_s = stage_ms[dom] / max(napplies, 1) * 1e-3
-    achieved = stage_bytes[dom] / dom_avg_s / 1e9 if dom_avg_s > 0 else 0.0
-    # a multi-RHS step streams the matrix once per pass and reads/writes every column once
-    elem_xy = 4 if a.precision == "fp32" else 8
-    passes = max(1, plan.multi_kernel_count(a.nrhs) // max(plan.multi_kernel_count(min(a.nrhs, 8)), 1)) \
-        if a.nrhs > 1 else 1
-    alg_bytes = info["algorithmic_bytes"] * passes + 2 * hm.nd * elem_xy * (a.nrhs - passes)
-    kname = {0: "hmvm_tile_kernel", 1: "hmvm_stream_kernel", 2: "hmvm_mixed_kernel"}[info["kernel"]]
-    if a.nrhs > 1:
-        kname = "hmvm_tc_kernel" if (a.precision == "mixed" and a.nrhs >= 16) else "hmvm_multi_kernel"
-    roof = {
-        "bound": "hbm",
-        "kernel": [f"{kname} (V stage)", "hmvm_reduce_kernel (V stage)", f"{kname} (row stage)",
-                   "hmvm_reduce_kernel (row stage)"][dom],
-        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-        "traffic": (stage_bytes[dom] * traffic_ratio(1 if dom == 0 else 2, a.precision)
-                    if dom in (0, 2) and a.nrhs == 1 and a.lr_format == "fp16"
-                    and ((info["kernel"] == 1 and a.precision == "fp64") or a.precision == "mixed")
-                    and traffic_ratio(1 if dom == 0 else 2, a.precision) else None),
-        "traffic_source": None,
-        "whole_hmvm_gbs": alg_bytes / (ms_step * 1e-3) / 1e9,
-        "whole_hmvm_frac": alg_bytes / (ms_step * 1e-3) / 1e9 / peak,
-        "stage_ms_avg": [s / max(napplies, 1) for s in stage_ms],
-        "stage_bytes": stage_bytes,
-    }
-    if roof["traffic"] is not None:
-        roof["traffic_source"] = ("ncu capture of the same kernel at N=65536, scaled by algorithmic bytes ("
-                                  + os.path.relpath(TRAFFIC_PROFILES[a.precision], ROOT) + ")")
 
     if rank == 0:
         value = world * 1e3 / ms_step * a.nrhs
         cfg = workload_config(a, hm)
-        if use_graph:
-            cfg["timing"] = ("CUDA-graph replays of one captured apply (hmvm_b200_plan_replay); stage times "
-                             "from a profiled pass of direct applies after the timed region")
-        cfg.update({"kernel": kname, "stage1_cfg": info["stage1_cfg"], "stage2_cfg": info["stage2_cfg"],
-                    "ctas_per_sm": [info["ctas_per_sm"], info["stage2_ctas_per_sm"]],
-                    "device_bytes": info["device_bytes"], "plan_setup_s": setup_s})
         line = {
             "metric": unit, "value": value, "unit": unit, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -502,6 +677,7 @@ def run_b200(a, rank, world, local_rank):
                      "synthetic (seeded HACApK-rule H-matrix") +
                     f"; x {'uniform[-1,1]' if a.x_dist == 'uniform' else 'standard normal'}" + ("" if a.mesh else ")"),
             "config": cfg,
+            "plan": plan_keys,
             "gbytes_per_s": alg_bytes / (ms_step * 1e-3) / 1e9,
             "algorithmic_bytes_per_step": alg_bytes,
             "relerr_vs_fp64_cpu_reference": rel, "aca_eps": a.eps,
@@ -511,10 +687,14 @@ def run_b200(a, rank, world, local_rank):
                     "h2d_bytes_per_step": hm.nd * elem * a.nrhs, "d2h_bytes_per_step": hm.nd * elem * a.nrhs,
                     "ms_per_step": e2e_step},
             "clocks": clk,
-            "gpu_launches": a.steps * (plan.kernel_count() if a.nrhs == 1 else plan.multi_kernel_count(a.nrhs)),
+            "gpu_launches": launches,
         }
+        if use_graph:
+            line["timing"] = ("CUDA-graph replays of one captured apply (hmvm_b200_plan_replay); stage times "
+                              "from a profiled pass of direct applies after the timed region")
+        if legs is not None:
+            line["secondary"] = legs
         print(json.dumps(line), flush=True)
-    plan.close()
 
 
 def batch_specs(a):

@@ -2,6 +2,7 @@
 // kernel dispatch, host-buffer apply, the one-shot reference-shaped call, and
 // the allocation-free apply.
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -51,6 +52,26 @@ struct DeviceGuard {
     if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
   }
 };
+
+// A CUDA driver-API function by name, through the runtime (so the library
+// needs no link-time dependency on libcuda), or nullptr.
+void* driver_fn(const char* name) {
+  void* f = nullptr;
+  cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+  if (cudaGetDriverEntryPointByVersion(name, &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess)
+    return nullptr;
+  return f;
+}
+
+// The calling thread's current CUDA context (nullptr if none or unknown).
+CUcontext current_context() {
+  using Fn = CUresult (*)(CUcontext*);
+  static Fn fn = reinterpret_cast<Fn>(driver_fn("cuCtxGetCurrent"));
+  CUcontext c = nullptr;
+  if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+  return c;
+}
 
 using KernelFn = void (*)(TileArgs);
 
@@ -1300,17 +1321,22 @@ namespace {
 constexpr int kNoallocMaxDevices = 64;
 std::mutex g_noalloc_mu;
 void* g_noalloc_addr[kNoallocMaxDevices] = {};
+CUcontext g_noalloc_ctx[kNoallocMaxDevices] = {};
 
 // Device address of the scratch array on `dev`, which must be the current
-// device; looked up once per device and cached.
+// device; looked up once per device and context and cached.  A new context on
+// the device (after cudaDeviceReset, say) holds a new copy of the array, so a
+// change of context makes the lookup run again.
 int noalloc_scratch(int dev, void** out) {
   if (dev < 0 || dev >= kNoallocMaxDevices) return set_error(HMVM_EINVAL, "device ordinal beyond the scratch table");
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  const CUcontext ctx = current_context();
+  if (!g_noalloc_addr[dev] || !ctx || ctx != g_noalloc_ctx[dev]) {
     void* addr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress of the no-alloc scratch");
     g_noalloc_addr[dev] = addr;
+    g_noalloc_ctx[dev] = ctx;
   }
   *out = g_noalloc_addr[dev];
   return HMVM_OK;

@@ -345,11 +345,16 @@ int hmvm_b200_autotune_d(const hmvm_matrix2_d *mat2, const hmvm_plan_opts *base,
  * This call allocates nothing.  Its scratch -- the intermediate V x vector and
  * the partial sums of split panels -- lives in one library-wide array of
  * HMVM_NOALLOC_SCRATCH_BYTES in device memory, which every GPU that loads the
- * library holds until the process exits.  A plan whose scratch (t_len + 16 and
+ * library holds until the process exits.  The array is reserved on a device
+ * when the library's kernels are loaded there: under CUDA's default lazy module
+ * loading that happens during the first plan creation on that device, not when
+ * the library is loaded, so a caller with a fixed memory budget should create its
+ * plans before it hands the remaining memory to its own pool.  A plan whose scratch (t_len + 16 and
  * p_len + 16 elements, each rounded up to 256 bytes; see hmvm_plan_info.t_len)
  * does not fit is rejected with HMVM_ERANGE.  The first call on each device
- * looks up that array's device address (once per device, with that device
- * current); make that first call before any stream capture.  All calls share
+ * looks up that array's device address (once per device and context, with
+ * that device current; a new context after cudaDeviceReset looks it up again);
+ * make that first call before any stream capture.  All calls share
  * the array and it keeps the last call's contents: the call clears, on
  * `stream` and before its kernels, the part that has to start at zero.  Calls
  * whose work overlaps on the GPU (other streams, threads or plans running at

@@ -207,6 +207,27 @@ void ref_omp2_f(void* hv, const float* x, float* y, int nthreads) {
 
 int ref_max_threads(void) { return omp_get_max_threads(); }
 
+// The reference's own timed sweep of its SoA OpenMP variants,
+// hmvm_omp_bench<double>(NULL, mat2, x, 0) (src_hmvm/src_cpp/hmvm_omp.cpp:992-1347;
+// with mat == NULL it skips the AoS variants).  It prints "TIME <L> <name> min
+// max avg" lines on stdout; they are written to out_path instead, for the
+// caller to parse.  Returns 0, or -1 if out_path cannot be opened.
+int ref_omp_bench_d(void* hv, const double* x, const char* out_path, int nthreads) {
+  RefHandle* h = static_cast<RefHandle*>(hv);
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  FILE* f = fopen(out_path, "w");
+  if (!f) return -1;
+  fflush(stdout);
+  int saved = dup(1);
+  dup2(fileno(f), 1);
+  hmvm_omp_bench<double>(NULL, h->matD2, x, 0);
+  fflush(stdout);
+  dup2(saved, 1);
+  close(saved);
+  fclose(f);
+  return 0;
+}
+
 void ref_free(void* hv) {
   RefHandle* h = static_cast<RefHandle*>(hv);
   if (!h) return;

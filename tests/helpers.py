@@ -17,7 +17,13 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libhmvm_ref.so")
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-SAMPLE_BIN = "/root/reference/src_hdump/hmatrix_sample.bin"
+# Where the reference's source tree lies (its sample mesh and matrix and its
+# headers are read from there; tests that need them are skipped when it is
+# absent).  Override with the HACAPK_REFERENCE environment variable.
+REFERENCE = os.environ.get("HACAPK_REFERENCE", "/root/reference")
+SAMPLE_BIN = os.path.join(REFERENCE, "src_hdump", "hmatrix_sample.bin")
+SAMPLE_PBF = os.path.join(REFERENCE, "src_hdump", "input_sample.pbf")
+REF_INC = os.path.join(REFERENCE, "src_hmvm", "src_cpp")
 
 _P = C.c_void_p
 

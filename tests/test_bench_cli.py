@@ -9,9 +9,7 @@ from types import SimpleNamespace
 
 import pytest
 
-from helpers import ROOT
-
-SAMPLE_PBF = "/root/reference/src_hdump/input_sample.pbf"
+from helpers import ROOT, SAMPLE_PBF
 
 
 @pytest.mark.skipif(not os.path.exists(SAMPLE_PBF), reason="the reference's sample mesh is not present")

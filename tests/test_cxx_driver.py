@@ -8,10 +8,9 @@ import numpy as np
 import pytest
 
 from hacapk_hmvm_b200 import HMatrix
-from helpers import ROOT, oracle_hmvm, relerr
+from helpers import REF_INC, ROOT, oracle_hmvm, relerr
 
 DRIVER = os.path.join(ROOT, "tests", "cxx", "hmvm1_b200.cpp")
-REF_INC = "/root/reference/src_hmvm/src_cpp"
 CUDA = "/usr/local/cuda"
 
 

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from hacapk_hmvm_b200 import HMatrix
-from helpers import SAMPLE_BIN, RefMatrix, ref_available, relerr
+from helpers import SAMPLE_BIN, SAMPLE_PBF, RefMatrix, ref_available, relerr
 
 
 def _boxes(hm, r0, n):
@@ -162,7 +162,6 @@ def test_gpu_fill_refuses_without_device():
 
 
 # ---- ppohBEM meshes: the reference's own sample matrix --------------------------
-SAMPLE_PBF = "/root/reference/src_hdump/input_sample.pbf"
 
 
 @pytest.mark.skipif(not (os.path.exists(SAMPLE_PBF) and os.path.exists(SAMPLE_BIN)),

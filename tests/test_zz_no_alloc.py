@@ -7,8 +7,9 @@ keeps its HMVM scratch (the V x vector and split-panel partial sums) in one
 fixed 16 MiB device array instead of per-plan buffers.  These tests call that
 entry point through the C ABI and compare it with hmvm_b200_apply on the same
 inputs, on consecutive calls that share (and inherit the contents of) the
-array.  Tolerance: relative 2-norm difference <= 1e-12 for FP64 plans and
-<= 1e-5 for FP32 plans, the bars the other GPU tests use.
+array.  Both entry points run the same kernels in the same fixed order, so the
+results must agree bit for bit (the tolerance the other GPU tests use for a
+path against itself); the device's free memory must not move across the calls.
 """
 import numpy as np
 import pytest
@@ -18,7 +19,9 @@ from helpers import relerr
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"fp64": 1e-12, "fp32": 1e-5}
+
+def _bits(a):
+    return a.view(np.uint64 if a.dtype == np.float64 else np.uint32)
 
 
 def _dev(a, dtype):
@@ -28,7 +31,8 @@ def _dev(a, dtype):
 
 
 def _both(plan, x):
-    """(hmvm_b200_apply result, hmvm_b200_apply_noalloc result) for one x."""
+    """(hmvm_b200_apply result, hmvm_b200_apply_noalloc result, free device
+    bytes before and after the no-alloc call) for one x."""
     import torch
 
     tdt = torch.float64 if plan.dtype == np.float64 else torch.float32
@@ -36,9 +40,12 @@ def _both(plan, x):
     y_ref = torch.full((plan.nd,), float("nan"), dtype=tdt, device="cuda")
     y_new = torch.full((plan.nd,), float("nan"), dtype=tdt, device="cuda")
     plan.apply(xd, y_ref)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
     plan.apply_noalloc(xd, y_new)
     torch.cuda.synchronize()
-    return y_ref.cpu().numpy(), y_new.cpu().numpy()
+    free1 = torch.cuda.mem_get_info()[0]
+    return y_ref.cpu().numpy(), y_new.cpu().numpy(), free0, free1
 
 
 def test_noalloc_matches_apply_on_consecutive_calls(gpu):
@@ -53,9 +60,12 @@ def test_noalloc_matches_apply_on_consecutive_calls(gpu):
             with Plan(hm, prec, split_cols=64 if k == 0 else 0) as plan:
                 for _ in range(2):
                     x = rng.uniform(-1.0, 1.0, hm.nd)
-                    y_ref, y_new = _both(plan, x)
+                    y_ref, y_new, free0, free1 = _both(plan, x)
                     assert np.all(np.isfinite(y_new))
-                    assert relerr(y_new, y_ref) <= TOL[prec], (prec, k, relerr(y_new, y_ref))
+                    assert np.array_equal(_bits(y_new), _bits(y_ref)), (prec, k, relerr(y_new, y_ref))
+                    # the first call on the device may look the array up; later calls allocate nothing
+                    if calls > 0:
+                        assert free1 == free0, (prec, k, free0 - free1)
                     calls += 1
     assert calls == 8
 
