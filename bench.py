@@ -332,6 +332,10 @@ def run_reference(a, rank):
     print(json.dumps(line), flush=True)
 
 
+# Right-hand sides from which FP32 and mixed workloads run on the wide tensor-core form.
+TC_WIDE_MIN = 16
+
+
 def make_plan(hm, precision, nrhs, lr_format, device, a=None):
     """The plan a workload runs on: single-vector plans for nrhs 1, multi-RHS
     plans sized for the pass width otherwise (tensor-core passes for mixed
@@ -341,12 +345,17 @@ def make_plan(hm, precision, nrhs, lr_format, device, a=None):
     kw = {}
     if a is not None:
         kw = dict(stage1_cfg=a.stage1_cfg, stage2_cfg=a.stage2_cfg, ctas_per_sm=a.ctas_per_sm, kernel=a.kernel)
-    nrhs_max = 16 if (precision == "mixed" and nrhs >= 16) else min(nrhs, 8)
+    if precision in ("fp32", "mixed") and nrhs >= TC_WIDE_MIN:
+        nrhs_max = 128  # the wide tensor-core form: 128 right-hand sides per pass on tcgen05
+    else:
+        nrhs_max = min(nrhs, 8)
     return Plan(hm, precision, device=device, nrhs_max=nrhs_max,
                 mixed_lr_format=lr_format if precision == "mixed" else None, **kw)
 
 
 def kernel_name(plan, info, nrhs):
+    if info["kernel"] == 4:
+        return "hmvm_tcw_kernel"
     if nrhs > 1:
         return "hmvm_tc_kernel" if (plan.precision == "mixed" and info["nrhs_max"] >= 16) else "hmvm_multi_kernel"
     return {0: "hmvm_tile_kernel", 1: "hmvm_stream_kernel", 2: "hmvm_mixed_kernel"}[info["kernel"]]
@@ -501,57 +510,69 @@ def run_secondary(a, hm, X, cpucols, fp64_rate, local_rank, stream, dev):
 
     legs = []
     key_of = lambda prec, nrhs, fmt: (prec, fmt, "single" if nrhs == 1 else
-                                      ("tc" if prec == "mixed" and nrhs >= 16 else "multi"))
+                                      ("tc" if prec in ("fp32", "mixed") and nrhs >= TC_WIDE_MIN else "multi"))
     plans = {}
     for i, (label, prec, nrhs, fmt) in enumerate(SECONDARY):
         key = key_of(prec, nrhs, fmt)
-        if key not in plans:
-            t0 = time.perf_counter()
-            plans[key] = (make_plan(hm, prec, nrhs, fmt, local_rank), time.perf_counter() - t0)
-        plan, setup_s = plans[key]
-        info = plan.info()
-        ndt = np.float32 if prec == "fp32" else np.float64
-        tdt = torch.float32 if prec == "fp32" else torch.float64
-        xd = torch.from_numpy(X[:nrhs].astype(ndt)).to(dev)
-        yd = torch.full((nrhs, hm.nd), float("nan"), dtype=tdt, device=dev)
-        if nrhs == 1:
-            step = lambda: plan.apply(xd[0], yd[0], stream)
-        else:
-            step = lambda: plan.apply_multi(xd, yd, stream)
-        for _ in range(2):
-            step()
-        torch.cuda.synchronize(dev)
-        plan.profile(True)
-        steps = max(3, a.secondary_steps if nrhs == 1 else a.secondary_steps // 4)
-        ms = time_steps(step, steps, a.warmup, stream, dev)
-        stage_ms, napplies = plan.profile_read()
-        plan.profile(False)
-        plan.status()
-        roof, alg = roofline_of(plan, info, nrhs, stage_ms, napplies, ms, prec, fmt or "fp16")
-        Y = yd.cpu().numpy().astype(np.float64)
-        errs = {}
-        for c in checked_columns(nrhs):
-            yc = cpucols(c)
-            errs[c] = float(np.linalg.norm(Y[c] - yc) / np.linalg.norm(yc))
-        rate = 1e3 / ms * nrhs
-        legs.append({
-            "workload": label, "precision": prec, "lr_format": fmt, "nrhs": nrhs,
-            "unit": "HMVM/s" if nrhs == 1 else "vectors/s", "value": rate, "ms_per_step": ms, "steps": steps,
-            "ratio_vs_fp64_vectors": rate / fp64_rate,
-            "relerr_vs_fp64_cpu_reference": max(errs.values()),
-            "relerr_columns_checked": len(errs), "aca_eps": a.eps,
-            "roofline": roof, "algorithmic_bytes_per_step": alg,
-            "kernel": kernel_name(plan, info, nrhs), "plan_setup_s": setup_s,
-            "device_bytes": info["device_bytes"],
-            "gpu_launches": steps * (plan.kernel_count() if nrhs == 1 else plan.multi_kernel_count(nrhs)),
-        })
-        del xd, yd
+        try:
+            legs.append(secondary_leg(a, hm, X, cpucols, fp64_rate, local_rank, stream, dev, plans, key,
+                                      label, prec, nrhs, fmt))
+        except Exception as e:  # one leg's failure is reported in its place; the others still run
+            legs.append({"workload": label, "precision": prec, "lr_format": fmt, "nrhs": nrhs,
+                         "error": f"{type(e).__name__}: {e}"})
         # close a plan after the last leg that uses it
-        if all(key_of(p2, n2, f2) != key for (_, p2, n2, f2) in SECONDARY[i + 1:]):
-            plan.close()
+        if key in plans and all(key_of(p2, n2, f2) != key for (_, p2, n2, f2) in SECONDARY[i + 1:]):
+            plans[key][0].close()
             del plans[key]
             torch.cuda.empty_cache()
     return legs
+
+
+def secondary_leg(a, hm, X, cpucols, fp64_rate, local_rank, stream, dev, plans, key, label, prec, nrhs, fmt):
+    import torch
+
+    if key not in plans:
+        t0 = time.perf_counter()
+        plans[key] = (make_plan(hm, prec, nrhs, fmt, local_rank), time.perf_counter() - t0)
+    plan, setup_s = plans[key]
+    info = plan.info()
+    ndt = np.float32 if prec == "fp32" else np.float64
+    tdt = torch.float32 if prec == "fp32" else torch.float64
+    xd = torch.from_numpy(X[:nrhs].astype(ndt)).to(dev)
+    yd = torch.full((nrhs, hm.nd), float("nan"), dtype=tdt, device=dev)
+    if nrhs == 1:
+        step = lambda: plan.apply(xd[0], yd[0], stream)
+    else:
+        step = lambda: plan.apply_multi(xd, yd, stream)
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize(dev)
+    plan.profile(True)
+    steps = max(3, a.secondary_steps if nrhs == 1 else a.secondary_steps // 4)
+    ms = time_steps(step, steps, a.warmup, stream, dev)
+    stage_ms, napplies = plan.profile_read()
+    plan.profile(False)
+    plan.status()
+    roof, alg = roofline_of(plan, info, nrhs, stage_ms, napplies, ms, prec, fmt or "fp16")
+    Y = yd.cpu().numpy().astype(np.float64)
+    errs = {}
+    for c in checked_columns(nrhs):
+        yc = cpucols(c)
+        errs[c] = float(np.linalg.norm(Y[c] - yc) / np.linalg.norm(yc))
+    rate = 1e3 / ms * nrhs
+    leg = {
+        "workload": label, "precision": prec, "lr_format": fmt, "nrhs": nrhs,
+        "unit": "HMVM/s" if nrhs == 1 else "vectors/s", "value": rate, "ms_per_step": ms, "steps": steps,
+        "ratio_vs_fp64_vectors": rate / fp64_rate,
+        "relerr_vs_fp64_cpu_reference": max(errs.values()),
+        "relerr_columns_checked": len(errs), "aca_eps": a.eps,
+        "roofline": roof, "algorithmic_bytes_per_step": alg,
+        "kernel": kernel_name(plan, info, nrhs), "plan_setup_s": setup_s,
+        "device_bytes": info["device_bytes"],
+        "gpu_launches": steps * (plan.kernel_count() if nrhs == 1 else plan.multi_kernel_count(nrhs)),
+    }
+    del xd, yd
+    return leg
 
 
 def run_b200(a, rank, world, local_rank):

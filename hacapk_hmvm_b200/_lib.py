@@ -101,7 +101,7 @@ class PlanInfo(C.Structure):
                 ("stage1_bytes", C.c_int64), ("stage2_bytes", C.c_int64),
                 ("kernel", C.c_int32), ("ctas_per_sm", C.c_int32),
                 ("cols_fp32", C.c_int64), ("cols_lr16", C.c_int64), ("cols_fp8", C.c_int64),
-                ("stage2_ctas_per_sm", C.c_int32), ("_pad1", C.c_int32)]
+                ("stage2_ctas_per_sm", C.c_int32), ("nrhs_max", C.c_int32)]
 
 
 TUNE_MAX_ENTRIES = 64
@@ -140,7 +140,9 @@ class LayoutView(C.Structure):
                 ("tiles", C.c_void_p), ("segs", C.c_void_p), ("team_begin1", C.POINTER(C.c_int32)),
                 ("team_begin2", C.POINTER(C.c_int32)), ("out_idx", C.POINTER(C.c_int32)),
                 ("red1", C.POINTER(C.c_int32)), ("red2", C.POINTER(C.c_int32)), ("data", C.c_void_p),
-                ("rowscale", C.POINTER(C.c_double)), ("n_rowscale", C.c_int64)]
+                ("rowscale", C.POINTER(C.c_double)), ("n_rowscale", C.c_int64),
+                ("tcw", C.c_int32), ("tcw_bf16", C.c_int32), ("tscale", C.POINTER(C.c_float)),
+                ("n_tscale", C.c_int64), ("tscale_rows0", C.c_int32), ("_pad_view", C.c_int32)]
 
 
 class HgenParams(C.Structure):

@@ -52,11 +52,11 @@ def _stale(target: str, sources: list[str]) -> bool:
 
 
 def hmvm_sources() -> list[str]:
-    return [os.path.join(CSRC, f) for f in ("hmvm_b200.cu", "layout.cpp", "loader.cpp", "tune.cpp", "solve.cu", "aca.cu")]
+    return [os.path.join(CSRC, f) for f in ("hmvm_b200.cu", "layout.cpp", "layout_tc.cpp", "loader.cpp", "tune.cpp", "solve.cu", "aca.cu")]
 
 
 def hmvm_deps() -> list[str]:
-    deps = hmvm_sources() + [os.path.join(CSRC, f) for f in ("kernels.cuh", "kernels_multi.cuh", "kernels_tc.cuh", "layout.hpp", "numfmt.hpp")]
+    deps = hmvm_sources() + [os.path.join(CSRC, f) for f in ("kernels.cuh", "kernels_multi.cuh", "kernels_tc.cuh", "kernels_tcw.cuh", "layout.hpp", "numfmt.hpp")]
     deps += [os.path.join(INCLUDE, "hmvm_b200.h"), os.path.join(INCLUDE, "hacapk_hgen.h")]
     return deps
 

@@ -17,6 +17,7 @@
 
 #include "hmvm_b200.h"
 #include "kernels_tc.cuh"
+#include "kernels_tcw.cuh"
 #include "layout.hpp"
 
 namespace hmvm {
@@ -211,6 +212,17 @@ struct hmvm_plan {
   uint16_t* d_tplanes = nullptr;
   float* d_scal = nullptr;
   unsigned* d_amax = nullptr;
+  // wide tensor-core passes (FP32 and mixed plans made with nrhs_max >= 32):
+  // 128 right-hand sides per pass, hmvm_tcw_kernel
+  bool tcw = false, tcw_bf = false;
+  uint16_t* d_xpl = nullptr;  // x planes [32][nd][8]
+  uint16_t* d_tpl = nullptr;  // t planes [32][tpl_rows][8]
+  int64_t tpl_rows = 0;
+  float* d_tscale = nullptr;  // V-stage 2^-c per panel row, then the row scale s_i per y row
+  float* d_xscale = nullptr;  // sigma_x per right-hand side of the current pass
+  unsigned* d_amax128 = nullptr;
+  float* d_part = nullptr;    // split V-stage panels' partial sums [p_len][128]
+  CUtensorMap xmap, tmap;     // the planes as 3-D tensors {8, rows, 32}
   void* d_xh = nullptr;  // staging for apply_multi_host
   void* d_yh = nullptr;
   size_t xh_bytes = 0;
@@ -248,7 +260,8 @@ void free_plan_buffers(hmvm_plan* p) {
   void* bufs[] = {p->d_data, p->d_tiles, p->d_segs, p->d_tb1, p->d_tb2,  p->d_out_idx, p->d_red1,
                   p->d_red2, p->d_t,     p->d_p,    p->d_err, p->d_x,    p->d_y,       p->d_x32,
                   p->d_scale, p->d_xm64, p->d_xm32, p->d_tm,  p->d_pm,   p->d_xh,      p->d_yh,
-                  p->d_xplanes, p->d_tplanes, p->d_scal, p->d_amax};
+                  p->d_xplanes, p->d_tplanes, p->d_scal, p->d_amax, p->d_xpl, p->d_tpl,
+                  p->d_tscale, p->d_xscale, p->d_amax128, p->d_part};
   for (void* b : bufs)
     if (b) cudaFree(b);
 }
@@ -291,8 +304,11 @@ MultiFn multi_kernel_for(int mode, int nr, int cfg);
 int tc_prepare(const hmvm_plan* p);
 
 // Dynamic shared memory beyond 48 KB must be enabled per kernel.
+int tcw_prepare(const hmvm_plan* p);
+
 template <typename T>
 int prepare_kernels(const hmvm_plan* p) {
+  if (p->tcw) return tcw_prepare(p);
   if (p->tc) {
     int rc = tc_prepare(p);
     if (rc) return rc;
@@ -345,6 +361,48 @@ int resident_ctas(const hmvm_plan_opts& o, int dev, int* out) {
                                   : resident_ctas_t<double>(kernel, c1, c2, out);
 }
 
+// Plans of FP32 or mixed storage made for 32 or more right-hand sides take the
+// wide tensor-core form.
+bool tcw_wanted(const hmvm_plan_opts& o) {
+  return (o.precision == HMVM_FP32 || o.precision == HMVM_MIXED) && o.nrhs_max >= kTcwMinNrhs;
+}
+
+// A planes buffer [32][rows][8] of 16-bit values as a 3-D tensor {8, rows, 32}
+// with boxes {8, 16, 32}: one K step of the 128 right-hand sides' hi and lo
+// parts per TMA copy.  Rows past the end read as zero.
+int encode_planes_map(CUtensorMap* map, void* base, int64_t rows) {
+  using Fn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                          const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                          CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static Fn fn = reinterpret_cast<Fn>(driver_fn("cuTensorMapEncodeTiled"));
+  if (!fn) return set_error(HMVM_ECUDA, "cuTensorMapEncodeTiled is not available");
+  const cuuint64_t dims[3] = {8, (cuuint64_t)rows, 32};
+  const cuuint64_t strides[2] = {16, (cuuint64_t)rows * 16};
+  const cuuint32_t box[3] = {8, 16, 32};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, base, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(HMVM_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return HMVM_OK;
+}
+
+// Device buffers and tensor maps of a wide tensor-core plan.
+int tcw_buffers(hmvm_plan* p, const HostLayout& L) {
+  p->tpl_rows = std::max<int64_t>(L.t_len, 1);
+  const int64_t xrows = std::max<int32_t>(L.nd, 1);
+  HMVM_CUDA_TRY(cudaMalloc(&p->d_xpl, (size_t)xrows * 512), "x planes");
+  HMVM_CUDA_TRY(cudaMalloc(&p->d_tpl, (size_t)p->tpl_rows * 512), "t planes");
+  HMVM_CUDA_TRY(cudaMemset(p->d_tpl, 0, (size_t)p->tpl_rows * 512), "t planes");
+  HMVM_CUDA_TRY(cudaMalloc(&p->d_xscale, kTcwRhs * sizeof(float)), "x scales");
+  HMVM_CUDA_TRY(cudaMalloc(&p->d_amax128, kTcwRhs * sizeof(unsigned)), "x maxima");
+  HMVM_CUDA_TRY(cudaMalloc(&p->d_part, (size_t)(L.p_len + 1) * kTcwRhs * sizeof(float)), "partial sums");
+  int rc = upload(&p->d_tscale, L.tscale.data(), L.tscale.size() * sizeof(float), nullptr);
+  if (!rc) rc = encode_planes_map(&p->xmap, p->d_xpl, xrows);
+  if (!rc) rc = encode_planes_map(&p->tmap, p->d_tpl, p->tpl_rows);
+  return rc;
+}
+
 int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** out) {
   if (!out) return set_error(HMVM_EINVAL, "plan output pointer is NULL");
   *out = nullptr;
@@ -355,7 +413,8 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   int rc = check_device(opts.device, &dev, &sms);
   if (rc) return rc;
   int ctas2 = opts.ctas_per_sm;
-  if (opts.ctas_per_sm <= 0) {
+  const bool want_tcw = tcw_wanted(opts);
+  if (opts.ctas_per_sm <= 0 && !want_tcw) {
     // Persistent grids: per stage, as many CTAs per SM as can be resident at
     // once, so no CTA waits for another to finish.
     int r[2] = {1, 1};
@@ -367,7 +426,7 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   HostLayout* L = new (std::nothrow) HostLayout();
   if (!L) return set_error(HMVM_ENOMEM, "host allocation failed");
   std::string msg;
-  rc = build_layout(lt, opts, sms, *L, msg, ctas2);
+  rc = want_tcw ? build_tc_layout(lt, opts, sms, *L, msg) : build_layout(lt, opts, sms, *L, msg, ctas2);
   if (rc) {
     delete L;
     return set_error(rc, msg);
@@ -401,14 +460,25 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   p->p_len = L->p_len;
   p->mixed = L->mixed;
   p->nrhs_max = L->nrhs_max;
-  p->tc = L->mixed && L->nrhs_max == kTcNrhs;
+  p->tc = !L->tcw && L->mixed && L->nrhs_max == kTcNrhs;
+  p->tcw = L->tcw;
+  p->tcw_bf = L->tcw_bf16;
   p->mixed_kcode = opts.mixed_lr_format == HMVM_LR_BF16 ? 3 : 2;
   p->cols_fp32 = L->cols_fp32;
   p->cols_lr16 = L->cols_lr16;
   p->cols_fp8 = L->cols_fp8;
   p->t_elem = L->mixed ? 4 : L->elem_size;
   p->p_elem = L->elem_size;
-  if (L->mixed) {
+  if (L->tcw) {
+    // Algorithmic bytes per pass: the stored elements in their storage formats
+    // (pairs count 4 bytes) and scales; per stage kernel also the 16-bit planes
+    // it reads and writes and, for the row stage, Y (128 columns).
+    const int64_t planes = 512 * ((int64_t)lt.nd + L->t_len);
+    p->stored_bytes = L->stored_bytes + 4 * (int64_t)L->tscale.size();
+    p->stage1_bytes = L->stored_bytes1 + 4 * (int64_t)L->tscale_rows0 + planes;
+    p->stage2_bytes = L->stored_bytes - L->stored_bytes1 + 4 * (int64_t)lt.nd + planes +
+                      (int64_t)lt.nd * kTcwRhs * L->elem_size;
+  } else if (L->mixed) {
     // Algorithmic bytes: the stored elements in their storage formats, the
     // per-column scales, x and y once.
     p->stored_bytes = L->stored_bytes + 8 * (int64_t)L->rowscale.size();
@@ -454,7 +524,8 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
       if (e != cudaSuccess) rc = cuda_fail(e, "x32 buffer");
       if (!rc) rc = upload(&p->d_scale, L->rowscale.data(), L->rowscale.size() * sizeof(double), nullptr);
     }
-    if (!rc && p->nrhs_max > 1) {
+    if (!rc && p->tcw) rc = tcw_buffers(p, *L);
+    if (!rc && p->nrhs_max > 1 && !p->tcw) {
       const size_t nr = (size_t)p->nrhs_max;
       cudaError_t e = cudaSuccess;
       if (p->precision != HMVM_FP32) e = cudaMalloc(&p->d_xm64, (size_t)(L->nd + 16) * nr * sizeof(double));
@@ -825,6 +896,95 @@ int launch_tc_pass(hmvm_plan* p, const void* X, int64_t ldx, void* Y, int64_t ld
   return HMVM_OK;
 }
 
+// ---- wide tensor-core passes ---------------------------------------------------------
+template <bool VST, bool BF>
+void tcw_fn_attr(int* rc) {
+  if (*rc) return;
+  const cudaError_t e = cudaFuncSetAttribute((const void*)hmvm_tcw_kernel<VST, BF>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, kTcwSmem);
+  if (e != cudaSuccess) *rc = cuda_fail(e, "cudaFuncSetAttribute");
+}
+int tcw_prepare(const hmvm_plan* p) {
+  int rc = HMVM_OK;
+  if (p->tcw_bf) {
+    tcw_fn_attr<true, true>(&rc);
+    tcw_fn_attr<false, true>(&rc);
+  } else {
+    tcw_fn_attr<true, false>(&rc);
+    tcw_fn_attr<false, false>(&rc);
+  }
+  return rc;
+}
+
+// One pass of up to 128 right-hand sides: (FP16) per-column maxima, the x
+// planes, V stage into the t planes, the split panels' reduction, row stage
+// into Y.
+int launch_tcw_pass(hmvm_plan* p, const void* X, int64_t ldx, void* Y, int64_t ldy, int nr, cudaStream_t st) {
+  const bool f32 = p->precision == HMVM_FP32;
+  const int gx = p->num_sms * 4;
+  if (!p->tcw_bf) {
+    HMVM_CUDA_TRY(cudaMemsetAsync(p->d_amax128, 0, kTcwRhs * sizeof(unsigned), st), "scale reset");
+    const dim3 g((unsigned)std::max(1, std::min(p->num_sms, (p->nd + 255) / 256)), (unsigned)nr);
+    if (f32) hmvm_tcw_absmax_kernel<float><<<g, 256, 0, st>>>(static_cast<const float*>(X), ldx, p->nd, p->d_amax128);
+    else hmvm_tcw_absmax_kernel<double><<<g, 256, 0, st>>>(static_cast<const double*>(X), ldx, p->nd, p->d_amax128);
+  }
+  if (f32) {
+    if (p->tcw_bf) hmvm_tcw_xplanes_kernel<float, true><<<gx, 256, 0, st>>>(static_cast<const float*>(X), ldx, p->nd, nr, p->d_amax128, p->d_xscale, p->d_xpl);
+    else hmvm_tcw_xplanes_kernel<float, false><<<gx, 256, 0, st>>>(static_cast<const float*>(X), ldx, p->nd, nr, p->d_amax128, p->d_xscale, p->d_xpl);
+  } else {
+    if (p->tcw_bf) hmvm_tcw_xplanes_kernel<double, true><<<gx, 256, 0, st>>>(static_cast<const double*>(X), ldx, p->nd, nr, p->d_amax128, p->d_xscale, p->d_xpl);
+    else hmvm_tcw_xplanes_kernel<double, false><<<gx, 256, 0, st>>>(static_cast<const double*>(X), ldx, p->nd, nr, p->d_amax128, p->d_xscale, p->d_xpl);
+  }
+  HMVM_CUDA_TRY(cudaGetLastError(), "input planes launch");
+  TcwArgs a;
+  a.tiles = p->d_tiles;
+  a.segs = p->d_segs;
+  a.data = static_cast<const char*>(p->d_data);
+  a.out_idx = p->d_out_idx;
+  a.tscale = p->d_tscale;
+  a.xscale = p->d_xscale;
+  a.tplanes = p->d_tpl;
+  a.trows = p->tpl_rows;
+  a.part = p->d_part;
+  a.y = Y;
+  a.ldy = ldy;
+  a.nr = nr;
+  a.y32 = f32 ? 1 : 0;
+  a.err = p->d_err;
+  cudaEvent_t* ev = nullptr;
+  if (p->profiling && p->prof_count < kMaxProfiled) {
+    ev = &p->prof_events[kEventsPerApply * (size_t)p->prof_count];
+    p->prof_count++;
+  }
+  if (ev) cudaEventRecord(ev[0], st);
+  if (p->stage1_tiles > 0) {
+    a.team_begin = p->d_tb1;
+    a.nteams = p->stage1_teams;
+    if (p->tcw_bf) hmvm_tcw_kernel<true, true><<<p->stage1_teams, kTcwThreads, kTcwSmem, st>>>(p->xmap, p->tmap, a);
+    else hmvm_tcw_kernel<true, false><<<p->stage1_teams, kTcwThreads, kTcwSmem, st>>>(p->xmap, p->tmap, a);
+    HMVM_CUDA_TRY(cudaGetLastError(), "tensor-core V-stage launch");
+  }
+  if (ev) cudaEventRecord(ev[1], st);
+  if (p->n_red1 > 0) {
+    const int blocks = (int)std::min<int64_t>(((int64_t)p->n_red1 * kTcwRhs + 255) / 256, (int64_t)p->num_sms * 8);
+    if (p->tcw_bf) hmvm_tcw_reduce_kernel<true><<<blocks, 256, 0, st>>>(p->d_red1, p->n_red1, p->d_part, p->d_tpl, p->tpl_rows);
+    else hmvm_tcw_reduce_kernel<false><<<blocks, 256, 0, st>>>(p->d_red1, p->n_red1, p->d_part, p->d_tpl, p->tpl_rows);
+    HMVM_CUDA_TRY(cudaGetLastError(), "tensor-core V-stage reduction launch");
+  }
+  if (ev) cudaEventRecord(ev[2], st);
+  a.team_begin = p->d_tb2;
+  a.nteams = p->stage2_teams;
+  if (p->tcw_bf) hmvm_tcw_kernel<false, true><<<p->stage2_teams, kTcwThreads, kTcwSmem, st>>>(p->xmap, p->tmap, a);
+  else hmvm_tcw_kernel<false, false><<<p->stage2_teams, kTcwThreads, kTcwSmem, st>>>(p->xmap, p->tmap, a);
+  HMVM_CUDA_TRY(cudaGetLastError(), "tensor-core row-stage launch");
+  if (ev) cudaEventRecord(ev[3], st);
+  if (ev) cudaEventRecord(ev[4], st);
+  return HMVM_OK;
+}
+int tcw_kernels_per_pass(const hmvm_plan* p) {
+  return (p->tcw_bf ? 1 : 2) + (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1;
+}
+
 // Right-hand sides per pass: the largest of 8, 4, 2 that is <= nrhs_max and
 // not above what is left (a last single column runs in a 2-wide pass).
 int multi_pass_width(int nrhs_max, int left) {
@@ -840,7 +1000,7 @@ struct Pass {
 std::vector<Pass> multi_passes(const hmvm_plan* p, int nrhs) {
   std::vector<Pass> v;
   for (int r0 = 0; r0 < nrhs;) {
-    const int w = p->nrhs_max <= 1 ? 1 : p->tc ? kTcNrhs : multi_pass_width(p->nrhs_max, nrhs - r0);
+    const int w = p->tcw ? kTcwRhs : p->nrhs_max <= 1 ? 1 : p->tc ? kTcNrhs : multi_pass_width(p->nrhs_max, nrhs - r0);
     const int nr = std::min(w, nrhs - r0);
     v.push_back(Pass{r0, nr, w});
     r0 += nr;
@@ -849,6 +1009,7 @@ std::vector<Pass> multi_passes(const hmvm_plan* p, int nrhs) {
 }
 // One pass; X and Y point at the pass's first column.
 int run_pass(hmvm_plan* p, const Pass& q, const void* X, int64_t ldx, void* Y, int64_t ldy, cudaStream_t st) {
+  if (p->tcw) return launch_tcw_pass(p, X, ldx, Y, ldy, q.nr, st);
   if (p->nrhs_max <= 1) return apply_impl_fwd(p, X, Y, st);  // single-vector passes
   if (p->tc) return launch_tc_pass(p, X, ldx, Y, ldy, q.nr, st);
   return launch_multi_pass(p, X, ldx, Y, ldy, q.nr, q.w, st);
@@ -880,6 +1041,7 @@ int check_multi(const hmvm_plan* p, const void* X, int64_t ldx, const void* Y, i
 
 int apply_impl(hmvm_plan* p, const void* x, void* y, cudaStream_t st) {
   if (p->nd == 0) return HMVM_OK;
+  if (p->tcw) return launch_tcw_pass(p, x, p->nd, y, p->nd, 1, st);  // one right-hand side in a pass
   if (p->mixed) return launch_stages_mixed(p, x, y, p->d_t, p->d_p, p->d_x32, st);
   if (p->precision == HMVM_FP64) return launch_stages<double>(p, x, y, p->d_t, p->d_p, st);
   return launch_stages<float>(p, x, y, p->d_t, p->d_p, st);
@@ -1023,12 +1185,13 @@ int hmvm_b200_plan_get_info(const hmvm_plan* p, hmvm_plan_info* info) {
   info->flops = 2 * p->stored_elems;
   info->stage1_bytes = p->stage1_bytes;
   info->stage2_bytes = p->stage2_bytes;
-  info->kernel = p->mixed ? 2 : p->kernel;
+  info->kernel = p->tcw ? 4 : p->mixed ? 2 : p->kernel;
   info->ctas_per_sm = p->ctas_per_sm;
   info->stage2_ctas_per_sm = p->ctas2_per_sm;
   info->cols_fp32 = p->cols_fp32;
   info->cols_lr16 = p->cols_lr16;
   info->cols_fp8 = p->cols_fp8;
+  info->nrhs_max = p->tcw ? kTcwRhs : p->nrhs_max;
   return HMVM_OK;
 }
 
@@ -1080,6 +1243,7 @@ int hmvm_b200_plan_status(hmvm_plan* p) {
 
 int hmvm_b200_plan_kernel_count(const hmvm_plan* p) {
   if (!p || p->nd == 0) return 0;
+  if (p->tcw) return tcw_kernels_per_pass(p);
   return (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1 + (p->n_red2 > 0) + (p->mixed ? 1 : 0);
 }
 
@@ -1232,6 +1396,7 @@ int hmvm_b200_apply_multi_host(hmvm_plan* p, const void* X_host, int64_t ldx, vo
 
 int hmvm_b200_plan_multi_kernel_count(const hmvm_plan* p, int32_t nrhs) {
   if (!p || p->nd == 0 || nrhs <= 0) return 0;
+  if (p->tcw) return (nrhs + kTcwRhs - 1) / kTcwRhs * tcw_kernels_per_pass(p);
   if (p->nrhs_max <= 1) return nrhs * hmvm_b200_plan_kernel_count(p);
   if (p->tc)  // per pass: pack, 2 x (max, planes), the stages and their reductions
     return (nrhs + kTcNrhs - 1) / kTcNrhs * (5 + (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1 + (p->n_red2 > 0));
@@ -1349,6 +1514,7 @@ extern "C" {
 int hmvm_b200_apply_noalloc(hmvm_plan* p, const void* x, void* y, void* stream) {
   int rc = check_xy(p, x, y);
   if (rc) return rc;
+  if (p->tcw) return set_error(HMVM_EINVAL, "tensor-core multi-RHS plans keep their scratch in the plan; use hmvm_b200_apply");
   auto round256 = [](size_t b) { return (b + 255) / 256 * 256; };
   const size_t tbytes = round256((size_t)(p->t_len + 16) * p->t_elem);
   const size_t pbytes = round256((size_t)(p->p_len + 16) * p->p_elem);
@@ -1389,7 +1555,7 @@ int hmvm_b200_layout_build_d(const hmvm_matrix2_d* m, const hmvm_plan_opts* opts
   hmvm_layout* h = new (std::nothrow) hmvm_layout();
   if (!h) return set_error(HMVM_ENOMEM, "host allocation failed");
   std::string msg;
-  int rc = build_layout(lt, o, num_sms, h->L, msg);
+  int rc = tcw_wanted(o) ? build_tc_layout(lt, o, num_sms, h->L, msg) : build_layout(lt, o, num_sms, h->L, msg);
   if (rc) {
     delete h;
     return set_error(rc, msg);
@@ -1410,7 +1576,7 @@ int hmvm_b200_layout_build64(const hmvm_leaves64* lv, int32_t rowmat_is_float, c
   hmvm_layout* h = new (std::nothrow) hmvm_layout();
   if (!h) return set_error(HMVM_ENOMEM, "host allocation failed");
   std::string msg;
-  int rc = build_layout(lt, o, num_sms, h->L, msg);
+  int rc = tcw_wanted(o) ? build_tc_layout(lt, o, num_sms, h->L, msg) : build_layout(lt, o, num_sms, h->L, msg);
   if (rc) {
     delete h;
     return set_error(rc, msg);
@@ -1448,6 +1614,11 @@ int hmvm_b200_layout_view(const hmvm_layout* h, hmvm_layout_view* v) {
   v->red1 = L.red1.data();
   v->red2 = L.red2.data();
   v->data = L.data.data();
+  v->tcw = L.tcw ? 1 : 0;
+  v->tcw_bf16 = L.tcw_bf16 ? 1 : 0;
+  v->tscale = L.tscale.empty() ? nullptr : L.tscale.data();
+  v->n_tscale = (int64_t)L.tscale.size();
+  v->tscale_rows0 = L.tscale_rows0;
   return HMVM_OK;
 }
 

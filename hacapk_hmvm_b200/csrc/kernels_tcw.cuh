@@ -1,0 +1,466 @@
+// Wide tensor-core multi-RHS HMVM: 128 right-hand sides per pass, every
+// product on the 5th-generation tensor cores (tcgen05, FP32 accumulation in
+// TMEM), the matrix streamed from HBM once per pass.  The layout it walks is
+// built by build_tc_layout (layout_tc.cpp).
+//
+// GEMM orientation: Y^T = X^T H^T, so the MMA (kind::f16, cta_group::1) has
+//   M = 128 right-hand sides (TMEM lanes),
+//   N = the item's rows rounded up to 16 (<= 32 row-stage, <= 128 V-stage),
+//   K = 16 matrix columns,
+//   A = the inputs: 16 planes of x_hi (or t_hi) and 16 of x_lo, 8 right-hand
+//       sides x 16 rows each, MN-major without swizzle, one TMA tensor copy per
+//       K step (a 3-D box {8, 16, 32} of the planes tensor [32][rows][8]);
+//   B = the matrix, K-major without swizzle, read by the MMA straight from the
+//       ring the bulk copies fill (8-row core matrices 128 B apart, the second
+//       8 columns R*16 B on; the missing half of an odd last step points at a
+//       zero block);
+//   D = FP32 in one of four 128-column accumulator buffers.
+// Per K step: hi x x_hi and hi x x_lo, plus lo x x_hi for pair-stored segments.
+//
+// One CTA of 6 warps per SM, warp-specialised:
+//   warp 0 (one thread)  producer: bulk copies of the matrix stream into an
+//                        8 x 8 KiB ring (chunks never split a K step) and TMA
+//                        tensor copies of each K step's inputs into a
+//                        10 x 8 KiB ring;
+//   warp 1 (one thread)  allocates TMEM, issues the MMAs, commits each input
+//                        slot, matrix slot and finished accumulator to its
+//                        mbarrier;
+//   warps 2..5           epilogue: tcgen05.ld the accumulator (warp w reads
+//                        lanes 32 (w % 4) ..), scale, and write t (as 16-bit
+//                        hi/lo planes) or y (through a shared-memory transpose
+//                        so each store covers 32 consecutive rows).
+// Every mbarrier wait is bounded (kWaitLimitNs); a role that gives up records
+// the error and stops; before the CTA exits, the copies still in flight and
+// the MMAs issued are waited for (bounded) and the TMEM is freed.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "kernels_tc.cuh"
+
+namespace hmvm {
+
+constexpr int kTcwSlotM = 8192;   // matrix ring slot (a K step of a 128-row pair panel is 8 KiB)
+constexpr int kTcwSlotsM = 8;
+constexpr int kTcwSlotA = 8192;   // one K step of inputs: 32 planes x 16 rows x 16 B
+constexpr int kTcwSlotsA = 10;
+constexpr int kTcwAccBufs = 4;
+constexpr int kTcwAccCols = 128;  // TMEM columns of an accumulator buffer
+constexpr int kTcwThreads = 192;
+constexpr int kTcwStageBytes = 32 * 33 * 8;  // per epilogue warp: 32 rhs x 32 rows of FP64 (+1 column)
+constexpr int kTcwZeroBytes = 2048;          // 128 rows x 16 B of zeros
+constexpr int kTcwOffA = kTcwSlotsM * kTcwSlotM;
+constexpr int kTcwOffStage = kTcwOffA + kTcwSlotsA * kTcwSlotA;
+constexpr int kTcwOffZero = kTcwOffStage + 4 * kTcwStageBytes;
+constexpr int kTcwOffBar = kTcwOffZero + kTcwZeroBytes;
+constexpr int kTcwNumBars = 2 * kTcwSlotsM + 2 * kTcwSlotsA + 2 * kTcwAccBufs + 1;
+constexpr int kTcwOffMisc = kTcwOffBar + kTcwNumBars * 8;
+constexpr int kTcwSmem = kTcwOffMisc + 32;
+static_assert(kTcwSmem <= 227 * 1024, "shared memory");
+static_assert(kTcwAccBufs * kTcwAccCols == 512, "the CTA owns the SM's 512 TMEM columns");
+
+struct TcwArgs {
+  const hmvm_tile_desc* tiles;
+  const hmvm_seg_desc* segs;
+  const int32_t* team_begin;  // [nteams + 1]
+  int nteams;
+  const char* data;           // the 16-byte vectors of the stream
+  const int32_t* out_idx;     // V stage: t slot per panel row
+  const float* tscale;        // V stage: 2^-c per panel row; row stage: s_i per row (tile _pad indexes it)
+  const float* xscale;        // sigma_x per right-hand side [128]
+  uint16_t* tplanes;          // V stage output: 32 planes x trows x 8
+  int64_t trows;
+  float* part;                // V-stage split panels: FP32 partial sums [row][128]
+  void* y;                    // row-stage output, column-major, leading dimension ldy
+  int64_t ldy;
+  int nr;                     // right-hand sides of this pass (<= 128)
+  int y32;                    // y is FP32 (FP32 plans), else FP64
+  int* err;
+};
+
+// Instruction descriptor, kind::f16: D FP32, A and B FP16 (bf = 0) or BF16
+// (bf = 1), A MN-major, B K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t tcw_idesc(int bf, int n) {
+  return (1u << 4) | ((uint32_t)bf << 7) | ((uint32_t)bf << 10) | (1u << 15) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// Single-thread bounded wait for the phase with parity `parity`.
+__device__ __forceinline__ bool thread_wait(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (global_ns() - t0 > kWaitLimitNs) return false;
+  return true;
+}
+
+template <bool BF>
+__device__ __forceinline__ void tcw_split(float v, uint16_t& hi, uint16_t& lo) {
+  if (BF) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+    hi = __bfloat16_as_ushort(h);
+    lo = __bfloat16_as_ushort(l);
+  } else {
+    const __half h = __float2half_rn(v);
+    const __half l = __float2half_rn(v - __half2float(h));
+    hi = __half_as_ushort(h);
+    lo = __half_as_ushort(l);
+  }
+}
+
+// A segment's K-step geometry: format, columns, bytes per 8-column vector
+// (hi, or hi + lo), vectors, K steps and K steps per ring chunk.
+struct TcwSeg {
+  int fmt, ncols, nv, nks, per;
+  uint32_t vb;
+  int row0;
+  bool tsrc;
+};
+__device__ __forceinline__ TcwSeg tcw_seg(const hmvm_seg_desc& s, int R) {
+  TcwSeg g;
+  g.fmt = (s.ncols >> 28) & 1;
+  g.ncols = s.ncols & 0x0fffffff;
+  g.vb = (uint32_t)R * 16u * (g.fmt ? 2u : 1u);
+  g.nv = (g.ncols + 7) >> 3;
+  g.nks = (g.nv + 1) >> 1;
+  g.per = max(1, kTcwSlotM / (int)(2 * g.vb));
+  g.tsrc = s.src < 0;
+  g.row0 = s.src & 0x7fffffff;
+  return g;
+}
+
+template <bool VST, bool BF>
+__global__ void __launch_bounds__(kTcwThreads, 1)
+    hmvm_tcw_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap tmap,
+                    const TcwArgs a) {
+  extern __shared__ __align__(1024) unsigned char tcw_smem[];
+  unsigned char* ringM = tcw_smem;
+  unsigned char* ringA = tcw_smem + kTcwOffA;
+  unsigned char* zero = tcw_smem + kTcwOffZero;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tcw_smem + kTcwOffBar);
+  uint64_t* mfull = bars;
+  uint64_t* mempty = mfull + kTcwSlotsM;
+  uint64_t* afull = mempty + kTcwSlotsM;
+  uint64_t* aempty = afull + kTcwSlotsA;
+  uint64_t* accfull = aempty + kTcwSlotsA;
+  uint64_t* accempty = accfull + kTcwAccBufs;
+  uint64_t* done = accempty + kTcwAccBufs;
+  uint32_t* misc = reinterpret_cast<uint32_t*>(tcw_smem + kTcwOffMisc);
+  // misc: [0] TMEM base, [1] matrix chunks issued, [2] input steps issued,
+  //       [3] matrix chunks consumed, [4] input steps consumed
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    for (int s = 0; s < kTcwSlotsM; s++) {
+      mbar_init(&mfull[s], 1);
+      mbar_init(&mempty[s], 1);
+    }
+    for (int s = 0; s < kTcwSlotsA; s++) {
+      mbar_init(&afull[s], 1);
+      mbar_init(&aempty[s], 1);
+    }
+    for (int s = 0; s < kTcwAccBufs; s++) {
+      mbar_init(&accfull[s], 1);
+      mbar_init(&accempty[s], 4);
+    }
+    mbar_init(done, 1);
+    for (int k = 1; k < 5; k++) misc[k] = 0;
+    fence_mbar_init();
+  }
+  for (int k = tid; k < kTcwZeroBytes / 16; k += kTcwThreads)
+    reinterpret_cast<uint4*>(zero)[k] = make_uint4(0, 0, 0, 0);
+  fence_proxy_async();  // the zeros, before the tensor cores read them
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(misc))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = misc[0];
+  const int team = blockIdx.x;
+  const int tb = team < a.nteams ? a.team_begin[team] : 0;
+  const int te = team < a.nteams ? a.team_begin[team + 1] : 0;
+
+  if (warp == 0) {
+    // ---- producer ----
+    if (lane == 0) {
+      uint32_t mI = 0, aI = 0;
+      bool ok = true;
+      for (int it = tb; it < te && ok; it++) {
+        const hmvm_tile_desc d = a.tiles[it];
+        const int R = d.nrows;
+        const char* g = a.data + d.data_off * 16;
+        for (int s = 0; s < d.nseg && ok; s++) {
+          const TcwSeg sg = tcw_seg(a.segs[d.seg_begin + s], R);
+          const CUtensorMap* map = sg.tsrc ? &tmap : &xmap;
+          for (int j = 0; j < sg.nks && ok;) {
+            const int j2 = min(sg.nks, j + sg.per);
+            const uint32_t bytes = (uint32_t)(j2 == sg.nks ? sg.nv - 2 * j : 2 * (j2 - j)) * sg.vb;
+            const int ms = mI % kTcwSlotsM;
+            if (mI >= kTcwSlotsM && !thread_wait(&mempty[ms], ((mI / kTcwSlotsM) - 1) & 1)) {
+              ok = false;
+              break;
+            }
+            mbar_expect_tx(&mfull[ms], bytes);
+            bulk_g2s(ringM + ms * kTcwSlotM, g, bytes, &mfull[ms]);
+            g += bytes;
+            mI++;
+            for (int jj = j; jj < j2; jj++) {
+              const int as = aI % kTcwSlotsA;
+              if (aI >= kTcwSlotsA && !thread_wait(&aempty[as], ((aI / kTcwSlotsA) - 1) & 1)) {
+                ok = false;
+                break;
+              }
+              mbar_expect_tx(&afull[as], kTcwSlotA);
+              tma_load_3d(ringA + as * kTcwSlotA, map, 0, sg.row0 + 16 * jj, 0, &afull[as]);
+              aI++;
+            }
+            j = j2;
+          }
+        }
+      }
+      misc[1] = mI;
+      misc[2] = aI;
+      if (!ok) atomicExch(a.err, 1);
+    }
+  } else if (warp == 1) {
+    // ---- MMA issue ----
+    if (lane == 0) {
+      uint32_t mC = 0, aC = 0, ic = 0;
+      bool ok = true;
+      const uint32_t zaddr = smem_u32(zero);
+      for (int it = tb; it < te && ok; it++, ic++) {
+        const hmvm_tile_desc d = a.tiles[it];
+        const int R = d.nrows;
+        const uint32_t idesc = tcw_idesc(BF ? 1 : 0, max(16, (R + 15) & ~15));
+        const int buf = ic % kTcwAccBufs;
+        if (ic >= kTcwAccBufs && !thread_wait(&accempty[buf], ((ic / kTcwAccBufs) - 1) & 1)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t dcol = tmem_base + (uint32_t)(buf * kTcwAccCols);
+        int accum = 0;
+        for (int s = 0; s < d.nseg && ok; s++) {
+          const TcwSeg sg = tcw_seg(a.segs[d.seg_begin + s], R);
+          for (int j = 0; j < sg.nks && ok;) {
+            const int j2 = min(sg.nks, j + sg.per);
+            const int ms = mC % kTcwSlotsM;
+            if (!thread_wait(&mfull[ms], (mC / kTcwSlotsM) & 1)) {
+              ok = false;
+              break;
+            }
+            mC++;
+            const uint32_t cbase = smem_u32(ringM + ms * kTcwSlotM);
+            for (int jj = j; jj < j2; jj++) {
+              const int as = aC % kTcwSlotsA;
+              if (!thread_wait(&afull[as], (aC / kTcwSlotsA) & 1)) {
+                ok = false;
+                break;
+              }
+              aC++;
+              tc_fence_after();
+              const uint32_t abase = smem_u32(ringA + as * kTcwSlotA);
+              const int nvj = min(2, sg.nv - 2 * jj);
+              const uint32_t bhi = cbase + (uint32_t)(jj - j) * 2u * sg.vb;
+              const uint32_t blo = bhi + (uint32_t)nvj * (uint32_t)R * 16u;
+              // A: planes 0..15 (hi) and 16..31 (lo); K 8-row groups 128 B apart, planes 256 B apart
+              const uint64_t ah = tc_desc(abase, 128, 256), al = tc_desc(abase + 4096, 128, 256);
+              const uint64_t bh = tc_desc(bhi, nvj == 2 ? (uint32_t)R * 16u : zaddr - bhi, 128);
+              tc_mma(dcol, ah, bh, idesc, accum);
+              tc_mma(dcol, al, bh, idesc, 1);
+              if (sg.fmt) {
+                const uint64_t bl = tc_desc(blo, nvj == 2 ? (uint32_t)R * 16u : zaddr - blo, 128);
+                tc_mma(dcol, ah, bl, idesc, 1);
+              }
+              accum = 1;
+              tc_commit(&aempty[as]);
+            }
+            if (!ok) break;
+            tc_commit(&mempty[ms]);
+            j = j2;
+          }
+        }
+        if (ok) tc_commit(&accfull[buf]);
+      }
+      misc[3] = mC;
+      misc[4] = aC;
+      // every MMA issued has completed before the CTA goes on (bounded)
+      tc_commit(done);
+      if (!thread_wait(done, 0)) ok = false;
+      if (!ok) atomicExch(a.err, 1);
+    }
+  } else {
+    // ---- epilogue ----
+    const int e = warp - 2, q = warp & 3;
+    const int r = 32 * q + lane;  // this thread's right-hand side
+    double* stg = reinterpret_cast<double*>(tcw_smem + kTcwOffStage + e * kTcwStageBytes);
+    const float sx = a.xscale[r];
+    uint32_t ic = 0;
+    for (int it = tb; it < te; it++, ic++) {
+      const hmvm_tile_desc d = a.tiles[it];
+      const int buf = ic % kTcwAccBufs;
+      if (!warp_wait(&accfull[buf], (ic / kTcwAccBufs) & 1)) {
+        if (lane == 0) atomicExch(a.err, 1);
+        break;
+      }
+      tc_fence_after();
+      const int R = d.nrows;
+      const uint32_t tbase = tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * kTcwAccCols);
+      for (int c0 = 0; c0 < R; c0 += 32) {
+        float v[32];
+        if (d.nseg > 0) {
+          tc_ld32(tbase + (uint32_t)c0, v);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 32; i++) v[i] = 0.f;
+        }
+        const int nrow = min(32, R - c0);
+        if constexpr (VST) {
+#pragma unroll
+          for (int i = 0; i < 32; i++) {
+            if (i < nrow) {
+              const float tv = v[i] * a.tscale[d._pad + c0 + i];
+              if (d.mode == 1) {
+                const int64_t slot = a.out_idx[d.out_base + c0 + i];
+                uint16_t hi, lo;
+                tcw_split<BF>(tv, hi, lo);
+                a.tplanes[((int64_t)(r >> 3) * a.trows + slot) * 8 + (r & 7)] = hi;
+                a.tplanes[((int64_t)(16 + (r >> 3)) * a.trows + slot) * 8 + (r & 7)] = lo;
+              } else {
+                a.part[(int64_t)(d.out_base + c0 + i) * 128 + r] = tv;
+              }
+            }
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < 32; i++)
+            stg[lane * 33 + i] = i < nrow ? (double)v[i] * (double)a.tscale[d._pad + c0 + i] * (double)sx : 0.0;
+          __syncwarp();
+          for (int c = 0; c < 32; c++) {
+            const int rr = 32 * q + c;
+            if (rr < a.nr && lane < nrow) {
+              const double val = stg[c * 33 + lane];
+              const int64_t o = (int64_t)d.out_base + c0 + lane + (int64_t)rr * a.ldy;
+              if (a.y32) static_cast<float*>(a.y)[o] = (float)val;
+              else static_cast<double*>(a.y)[o] = val;
+            }
+          }
+          __syncwarp();
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&accempty[buf]);
+    }
+  }
+
+  __syncthreads();
+  if (tid == 0) {
+    // copies issued but never consumed (a role gave up): let them land (bounded)
+    // before the shared memory is released
+    for (uint32_t c = misc[3]; c < misc[1]; c++) thread_wait(&mfull[c % kTcwSlotsM], (c / kTcwSlotsM) & 1);
+    for (uint32_t c = misc[4]; c < misc[2]; c++) thread_wait(&afull[c % kTcwSlotsA], (c / kTcwSlotsA) & 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem_base) : "memory");
+  }
+}
+
+// ---- per-pass input planes -------------------------------------------------------
+// amax[r] = max |X[:, r]| as float bits (FP16 plans scale each right-hand side).
+template <typename TX>
+__global__ void hmvm_tcw_absmax_kernel(const TX* __restrict__ X, int64_t ldx, int n, unsigned* __restrict__ amax) {
+  const int r = blockIdx.y;
+  float m = 0.f;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    m = fmaxf(m, fabsf((float)X[i + r * ldx]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(amax + r, __float_as_uint(m));
+}
+
+// sigma = 2^(ceil(log2 m) - 15), so |x| / sigma <= 2^15; 1 for m = 0, not finite, or BF16.
+template <bool BF>
+__device__ __forceinline__ float tcw_sigma(unsigned amax_bits) {
+  if (BF) return 1.f;
+  const float m = __uint_as_float(amax_bits);
+  if (!(m > 0.f) || !isfinite(m)) return 1.f;
+  int e;
+  const float f = frexpf(m, &e);
+  return ldexpf(1.f, (f == 0.5f ? e - 1 : e) - 15);
+}
+
+// X (column-major, nr <= 128 columns) -> planes[32][n][8]: plane p < 16 holds
+// the hi parts of right-hand sides 8p..8p+7 (scaled by 1 / sigma_r), plane
+// 16 + p their lo parts; columns nr..127 are zero.  xscale[r] = sigma_r.
+template <typename TX, bool BF>
+__global__ void hmvm_tcw_xplanes_kernel(const TX* __restrict__ X, int64_t ldx, int n, int nr,
+                                        const unsigned* __restrict__ amax, float* __restrict__ xscale,
+                                        uint16_t* __restrict__ planes) {
+  if (blockIdx.x == 0 && threadIdx.x < 128)
+    xscale[threadIdx.x] = threadIdx.x < nr ? tcw_sigma<BF>(amax[threadIdx.x]) : 1.f;
+  const int64_t total = (int64_t)n * 16;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+    const int p = (int)(k / n);
+    const int64_t i = k - (int64_t)p * n;
+    uint16_t hi[8], lo[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      const int r = 8 * p + e;
+      float v = 0.f;
+      if (r < nr) v = (float)X[i + r * ldx] / tcw_sigma<BF>(amax[r]);
+      tcw_split<BF>(v, hi[e], lo[e]);
+    }
+    uint4 h, l;
+    h.x = hi[0] | ((uint32_t)hi[1] << 16);
+    h.y = hi[2] | ((uint32_t)hi[3] << 16);
+    h.z = hi[4] | ((uint32_t)hi[5] << 16);
+    h.w = hi[6] | ((uint32_t)hi[7] << 16);
+    l.x = lo[0] | ((uint32_t)lo[1] << 16);
+    l.y = lo[2] | ((uint32_t)lo[3] << 16);
+    l.z = lo[4] | ((uint32_t)lo[5] << 16);
+    l.w = lo[6] | ((uint32_t)lo[7] << 16);
+    reinterpret_cast<uint4*>(planes)[(int64_t)p * n + i] = h;
+    reinterpret_cast<uint4*>(planes)[(int64_t)(16 + p) * n + i] = l;
+  }
+}
+
+// V-stage panels cut into parts: add each t slot's parts in part order and
+// write the sum as hi/lo planes.  red[e] = {slot, first partial row, parts, stride}.
+template <bool BF>
+__global__ void hmvm_tcw_reduce_kernel(const int4* __restrict__ red, int n, const float* __restrict__ part,
+                                       uint16_t* __restrict__ tplanes, int64_t trows) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)n * 128;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(k >> 7), r = (int)(k & 127);
+    const int4 rd = red[e];
+    float s = 0.f;
+    for (int q = 0; q < rd.z; q++) s += part[(int64_t)(rd.y + q * rd.w) * 128 + r];
+    uint16_t hi, lo;
+    tcw_split<BF>(s, hi, lo);
+    tplanes[((int64_t)(r >> 3) * trows + rd.x) * 8 + (r & 7)] = hi;
+    tplanes[((int64_t)(16 + (r >> 3)) * trows + rd.x) * 8 + (r & 7)] = lo;
+  }
+}
+
+}  // namespace hmvm

@@ -176,6 +176,15 @@ inline int multi_smem_bytes(const MultiCfg& c) { return c.wpb * (c.slots * c.chu
 constexpr int kDefaultMultiCfg = 0;
 constexpr int kMultiWarpsPerSm = 8;  // resident warps (teams) per SM of the multi-RHS kernel
 
+// Wide tensor-core passes (plans with nrhs_max >= kTcwMinNrhs, FP32 or mixed
+// storage): 128 right-hand sides per pass, every product on tcgen05.
+constexpr int kTcwRhs = 128;        // right-hand sides per pass: the MMA's M
+constexpr int kTcwMinNrhs = 32;     // nrhs_max from which a plan takes this form
+constexpr int kTcwPanelRows = 128;  // V-stage panel rows: the MMA's N, at most
+constexpr int kTcwTileRows = 32;    // row-stage tile rows
+// Segment formats of the wide tensor-core layout (top bits of ncols).
+enum TcwFmt : int32_t { TF_HI = 0, TF_HILO = 1 };
+
 struct HostLayout {
   int precision = HMVM_FP64;
   int vec = 2;
@@ -203,6 +212,11 @@ struct HostLayout {
   int64_t stored_bytes = 0;      // bytes of the stored elements in their storage formats
   int64_t stored_bytes1 = 0;     // ... of the V stage
   int nrhs_max = 1;              // items fit the multi-RHS input buffer for this many rhs
+  // wide tensor-core layout
+  bool tcw = false;
+  bool tcw_bf16 = false;          // 16-bit format of the stored pairs and the input planes
+  std::vector<float> tscale;      // per V-stage panel row 2^-c, then per y row the row scale s_i
+  int32_t tscale_rows0 = 0;       // index of y row 0 in tscale
 };
 
 // Returns HMVM_OK or a status; msg receives a description on failure.
@@ -212,5 +226,9 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
                  std::string &msg, int ctas2_per_sm = 0);
 
 int validate_leaves(const LeafTable &lt, std::string &msg);
+
+// The wide tensor-core layout (see layout_tc.cpp).
+int build_tc_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, HostLayout &out,
+                    std::string &msg);
 
 }  // namespace hmvm

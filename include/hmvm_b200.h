@@ -159,7 +159,10 @@ typedef struct hmvm_plan_opts {
   int32_t nrhs_max;       /* right-hand sides per pass of hmvm_b200_apply_multi, 1..8 (default 1; items are
                              sized so that nrhs_max inputs per column fit the multi-RHS kernel's buffer);
                              16 on HMVM_MIXED plans: 16-column passes with the 16-bit factor runs on the
-                             tensor cores (tcgen05) */
+                             tensor cores (tcgen05); 32 or more on HMVM_FP32 and HMVM_MIXED plans: the wide
+                             tensor-core form, 128 right-hand sides per pass with every product on tcgen05
+                             (the matrix stored as FP16 -- BF16 for BF16-factor plans -- values and hi/lo
+                             pairs) */
 } hmvm_plan_opts;
 
 typedef struct hmvm_plan_info {
@@ -175,7 +178,8 @@ typedef struct hmvm_plan_info {
   int64_t stage2_bytes;      /* algorithmic bytes of the row stage: U + dense elements + x + y */
   int32_t kernel, ctas_per_sm;           /* ctas_per_sm: of the V stage */
   int64_t cols_fp32, cols_lr16, cols_fp8; /* HMVM_MIXED: low-rank columns per storage format */
-  int32_t stage2_ctas_per_sm, _pad1;      /* CTAs per SM of the row stage */
+  int32_t stage2_ctas_per_sm;             /* CTAs per SM of the row stage */
+  int32_t nrhs_max;                       /* right-hand sides per multi-RHS pass (1: single-vector plan) */
 } hmvm_plan_info;
 
 void hmvm_b200_default_opts(hmvm_plan_opts *opts);
@@ -413,6 +417,13 @@ typedef struct hmvm_layout_view {
   const double *rowscale;            /* HMVM_MIXED: [n_rowscale] s_u * s_v per V-stage output row, in
                                         stage-1 item order (tile _pad = first index of the tile) */
   int64_t n_rowscale;
+  /* wide tensor-core layout (FP32 / mixed plans with nrhs_max >= 32); segment formats in the top bits of
+     ncols: 0 one 16-bit value per element, 1 a 16-bit hi/lo pair, stored K-step-major */
+  int32_t tcw, tcw_bf16;             /* 16-bit format: FP16 (0) or BF16 (1) */
+  const float *tscale;               /* [n_tscale]: per V-stage panel row 2^-c (tile _pad = first index of the
+                                        tile), from tscale_rows0 on the row scale s_i of every y row */
+  int64_t n_tscale;
+  int32_t tscale_rows0, _pad_view;
 } hmvm_layout_view;
 
 /* Tile and segment records as stored in the data structures above. */

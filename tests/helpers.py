@@ -332,6 +332,121 @@ def emulate_mixed(view, x: np.ndarray) -> np.ndarray:
     return y
 
 
+def _round16(v, bf16: bool):
+    """float32 array -> the nearest FP16 (or BF16) values, ties to even, as float64."""
+    v = np.asarray(v, dtype=np.float32)
+    if not bf16:
+        return v.astype(np.float16).astype(np.float64)
+    b = v.view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) & 0xFFFF0000
+    return b.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def _split16(v, bf16: bool):
+    """(hi, lo) of float32 values as the kernels split them: hi = fmt(v),
+    lo = fmt(v - hi) with the difference in float32."""
+    v = np.asarray(v, dtype=np.float32)
+    hi = _round16(v, bf16)
+    lo = _round16((v - hi.astype(np.float32)).astype(np.float32), bf16)
+    return hi, lo
+
+
+def _tcw_decode(raw16, nc, fmt, R):
+    """The stored matrix of one K-step-major segment: (hi, lo) as float64
+    [R, nc] (lo is None for one-value segments)."""
+    nv = -(-nc // 8)
+    h = 2 if fmt else 1
+    hi_idx, lo_idx = [], []
+    for j in range(-(-nv // 2)):
+        nvj = min(2, nv - 2 * j)
+        base = j * 2 * h
+        hi_idx += [base + u for u in range(nvj)]
+        lo_idx += [base + nvj + u for u in range(nvj)]
+    vec = raw16.reshape(-1, R, 8)
+
+    def mat(idx):
+        m = vec[idx].transpose(1, 0, 2).reshape(R, len(idx) * 8)[:, :nc]
+        return m
+
+    return mat(hi_idx), (mat(lo_idx) if fmt else None)
+
+
+def emulate_tcw(view, X: np.ndarray) -> np.ndarray:
+    """Y = H X (X: [nrhs, N], nrhs <= 128) for a wide tensor-core layout,
+    walking it as hmvm_tcw_kernel does: the inputs as scaled 16-bit hi/lo
+    planes, per K step hi*x_hi + hi*x_lo (+ lo*x_hi for pair segments), the
+    V-stage output scaled by 2^-c and split into planes, the row stage scaled
+    by s_i and sigma_x.  Products are summed in FP64 here (FP32 on the GPU)."""
+    from hacapk_hmvm_b200 import _lib
+
+    bf = bool(view.tcw_bf16)
+    tiles = np.ctypeslib.as_array((_lib.TileDesc * view.n_tiles).from_address(view.tiles)) if view.n_tiles else []
+    segs = np.ctypeslib.as_array((_lib.SegDesc * view.n_segs).from_address(view.segs)) if view.n_segs else []
+    raw = (np.ctypeslib.as_array((C.c_uint8 * (16 * view.data_vectors)).from_address(view.data))
+           if view.data_vectors else np.zeros(0, np.uint8))
+    vals = raw.view("<f2").astype(np.float64) if not bf else \
+        (raw.view("<u2").astype(np.uint32) << 16).view("<f4").astype(np.float64)
+    tscale = np.ctypeslib.as_array(view.tscale, (view.n_tscale,)).astype(np.float64) if view.n_tscale else np.zeros(0)
+    n_out = max([int(tiles[k]["out_base"]) + int(tiles[k]["nrows"]) for k in range(view.stage1_tiles)
+                 if tiles[k]["mode"] == 1] or [0])
+    out_idx = np.ctypeslib.as_array(view.out_idx, (n_out,)) if n_out else np.zeros(0, np.int32)
+    X = np.asarray(X, dtype=np.float64)
+    nr, nd = X.shape
+    if bf:
+        sig = np.ones(nr)
+    else:
+        am = np.abs(X.astype(np.float32)).max(axis=1).astype(np.float64)
+        sig = np.array([2.0 ** (int(np.ceil(np.log2(m))) - 15) if m > 0 else 1.0 for m in am])
+    xi = (X.astype(np.float32) / sig[:, None].astype(np.float32)).astype(np.float32)
+    xh, xl = _split16(xi.T, bf)  # [nd, nr]
+    th = np.zeros((view.t_len + 1, nr))
+    tl = np.zeros((view.t_len + 1, nr))
+    part = np.zeros((view.p_len + 1, nr))
+    Y = np.full((nr, nd), np.nan)
+
+    def run_item(td):
+        R = int(td["nrows"])
+        v0 = int(td["data_off"]) * 8
+        acc = np.zeros((R, nr))
+        for s in range(int(td["seg_begin"]), int(td["seg_begin"]) + int(td["nseg"])):
+            src, enc = int(segs[s]["src"]), int(segs[s]["ncols"])
+            fmt, nc = (enc >> 28) & 1, enc & 0x0FFFFFFF
+            nvec = -(-nc // 8) * (2 if fmt else 1)
+            bh, bl = _tcw_decode(vals[v0:v0 + nvec * R * 8], nc, fmt, R)
+            v0 += nvec * R * 8
+            if src < 0:
+                r0 = src & 0x7FFFFFFF
+                ah, al = th[r0:r0 + nc], tl[r0:r0 + nc]
+            else:
+                ah, al = xh[src:src + nc], xl[src:src + nc]
+            acc += bh @ ah + bh @ al
+            if fmt:
+                acc += bl @ ah
+        return acc
+
+    for k in range(view.stage1_tiles):
+        td = tiles[k]
+        R, ob, sb = int(td["nrows"]), int(td["out_base"]), int(td["_pad"])
+        tv = (run_item(td) * tscale[sb:sb + R, None]).astype(np.float32)
+        if td["mode"] == 1:
+            h, l = _split16(tv, bf)
+            th[out_idx[ob:ob + R]] = h
+            tl[out_idx[ob:ob + R]] = l
+        else:
+            part[ob:ob + R] = tv
+    if view.n_red1:
+        red = np.ctypeslib.as_array(view.red1, (view.n_red1 * 4,)).reshape(-1, 4)
+        for slot, pb, nch, stride in red:
+            sm = sum(part[pb + c * stride] for c in range(nch)).astype(np.float32)
+            th[slot], tl[slot] = _split16(sm, bf)
+    for k in range(view.stage1_tiles, view.n_tiles):
+        td = tiles[k]
+        R, ob, sb = int(td["nrows"]), int(td["out_base"]), int(td["_pad"])
+        acc = run_item(td)
+        Y[:, ob:ob + R] = (acc * tscale[sb:sb + R, None] * sig[None, :]).T
+    return Y
+
+
 def layout_for(hm, **opts):
     """Build the host layout of a plan without a GPU; returns (handle, view)."""
     from hacapk_hmvm_b200 import _lib

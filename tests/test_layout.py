@@ -141,3 +141,90 @@ def test_invalid_leaf_tables_rejected():
         with pytest.raises(_lib.HMVMError) as e:
             layout_for(bad)
         assert e.value.status == _lib.HMVM_EINVAL, name
+
+
+# ---- the wide tensor-core layout (FP32 / mixed plans with nrhs_max >= 32) -------------
+def _tcw_bounds(view):
+    """Every address hmvm_tcw_kernel and its helpers form stays inside its buffer."""
+    from hacapk_hmvm_b200 import _lib
+
+    tiles = np.ctypeslib.as_array((_lib.TileDesc * view.n_tiles).from_address(view.tiles))
+    segs = np.ctypeslib.as_array((_lib.SegDesc * view.n_segs).from_address(view.segs))
+    covered = np.zeros(view.data_vectors, np.int32)
+    for k in range(view.n_tiles):
+        td = tiles[k]
+        R, nv = int(td["nrows"]), int(td["nvec"])
+        assert 1 <= R <= (128 if k < view.stage1_tiles else 32)
+        off = int(td["data_off"])
+        assert 0 <= off and off + nv * R <= view.data_vectors
+        covered[off:off + nv * R] += 1
+        tot = 0
+        for s in range(int(td["seg_begin"]), int(td["seg_begin"]) + int(td["nseg"])):
+            src, enc = int(segs[s]["src"]), int(segs[s]["ncols"])
+            fmt, nc = (enc >> 28) & 1, enc & 0x0FFFFFFF
+            assert nc >= 1 and (enc >> 28) in (0, 1)
+            # a K step (<= 4 vectors of R rows) fits one 8 KiB ring chunk
+            assert 2 * R * 16 * (2 if fmt else 1) <= 8192
+            tot += -(-nc // 8) * (2 if fmt else 1)
+            if src < 0:
+                assert k >= view.stage1_tiles and (src & 0x7FFFFFFF) + nc <= view.t_len
+            else:
+                assert src + nc <= view.nd
+        assert tot == nv
+        pad = int(td["_pad"])
+        if k < view.stage1_tiles:
+            assert td["mode"] in (1, 2) and pad + R <= view.tscale_rows0
+            if td["mode"] == 1:
+                assert int(td["out_base"]) + R <= view.tscale_rows0
+            else:
+                assert int(td["out_base"]) + R <= view.p_len
+        else:
+            assert td["mode"] == 0 and view.tscale_rows0 <= pad and pad + R <= view.n_tscale
+            assert int(td["out_base"]) + R <= view.nd
+    assert np.all(covered == 1)  # the items partition the stream
+    n1 = view.tscale_rows0
+    out_idx = np.ctypeslib.as_array(view.out_idx, (n1,)) if n1 else np.zeros(0, np.int32)
+    assert np.all((out_idx >= 0) & (out_idx < max(view.t_len, 1)))
+    if view.n_red1:
+        red = np.ctypeslib.as_array(view.red1, (view.n_red1 * 4,)).reshape(-1, 4)
+        assert np.all(red[:, 0] < view.t_len)
+        assert np.all(red[:, 1] + (red[:, 2] - 1) * red[:, 3] < view.p_len)
+    sc = np.ctypeslib.as_array(view.tscale, (view.n_tscale,))
+    assert np.all(np.isfinite(sc)) and np.all(sc > 0)
+    assert np.all(np.log2(sc) == np.round(np.log2(sc)))  # powers of two: exact scaling
+
+
+@pytest.mark.parametrize("prec,fmt,tol", [(2, "fp16", 1e-4), (2, "bf16", 1e-4), (1, None, 1e-5)])
+@pytest.mark.parametrize("case", [(3000, "sphere", 3), (2500, "plate", 4), (2200, "cube", 6)],
+                         ids=lambda c: f"{c[1]}{c[0]}")
+def test_tcw_layout_against_oracle(prec, fmt, tol, case):
+    from helpers import emulate_tcw
+
+    n, geo, seed = case
+    hm = HMatrix.generate(n, geo, eta=2.0, eps=1e-4, leaf_size=32, seed=seed)
+    kw = dict(precision=prec, nrhs_max=128, num_sms=16)
+    if fmt:
+        kw["mixed_lr_format"] = fmt
+    h, view = layout_for(hm, **kw)
+    assert view.tcw == 1 and view.tcw_bf16 == (fmt == "bf16")
+    _tcw_bounds(view)
+    rng = np.random.default_rng(seed)
+    X = rng.uniform(-1, 1, (3, hm.nd)) * np.array([1.0, 1e-9, 1e7])[:, None]
+    Y = emulate_tcw(view, X)
+    for r in range(3):
+        assert relerr(Y[r], oracle_hmvm(hm, X[r])) <= tol, (r, relerr(Y[r], oracle_hmvm(hm, X[r])))
+
+
+def test_tcw_layout_split_panels():
+    """Large V-stage panels are cut into K-step ranges whose partial sums the
+    reduction adds; the result is unchanged."""
+    from helpers import emulate_tcw
+
+    hm = HMatrix.generate(12000, "sphere", eta=2.0, eps=1e-4, leaf_size=32, seed=8)
+    h, view = layout_for(hm, precision=1, nrhs_max=128, num_sms=148)
+    assert view.n_red1 > 0
+    _tcw_bounds(view)
+    X = np.random.default_rng(3).standard_normal((2, hm.nd))
+    Y = emulate_tcw(view, X)
+    for r in range(2):
+        assert relerr(Y[r], oracle_hmvm(hm, X[r])) <= 1e-5
