@@ -38,6 +38,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libhmvm_ref.so")
+REF_CUDA_SO = os.path.join(ROOT, "oracle", "_ref", "libhmvm_ref_cuda.so")
 ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
@@ -79,6 +80,9 @@ def parse():
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the secondary workloads (FP32, mixed, multi-RHS) timed after the headline")
     ap.add_argument("--secondary-steps", type=int, default=40, help="timed steps of each single-vector secondary leg")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own hybrid2 CUDA kernels on this GPU")
+    ap.add_argument("--reference-gpu-runs", type=int, default=20, help="timed runs of the reference's GPU kernel")
     ap.add_argument("--no-cpu-variants", action="store_true",
                     help="skip the reference's full OpenMP variant sweep and its one-core hmvm_seq_2")
     return ap.parse_args()
@@ -489,6 +493,60 @@ def cpu_bench_variants(cpu, x, seq_seconds):
     return out
 
 
+# The reference's fastest published GPU variants (hybrid2; src_hmvm/src_cpp/result/
+# time_216h_d.csv:469 and time_216h_f.csv:379) as (kernel index, div, mul, a2t, a2i,
+# aa, da); the index encodes the knobs as hmvm_cuda2.cu:395-404 decodes them.
+REF_GPU_VARIANTS = {"fp64": (356, 4, 12, 1, 1, 0, 0), "fp32": (266, 4, 13, 0, 1, 0, 0)}
+
+
+def reference_gpu(cpu, x, ours, nbench):
+    """The reference's own hybrid2 CUDA kernels (hmvm_cuda2.cu, built unchanged
+    for sm_100a into oracle/_ref) on this GPU: their TIME line from the
+    reference's own wrapper, and the relative error of one launch's y against
+    the reference CPU HMVM in FP64.  ours: {"fp64": HMVM/s, "fp32": HMVM/s}."""
+    import tempfile
+
+    if cpu.kind != "reference" or not os.path.exists(REF_CUDA_SO):
+        return None
+    P = C.c_void_p
+    lib = C.CDLL(REF_CUDA_SO)
+    lib.refgpu_cuda2_bench.argtypes = [P, C.c_int, P, C.c_int, C.c_int, C.c_char_p]
+    lib.refgpu_hybrid2_y.argtypes = [P, C.c_int, P] + [C.c_int] * 6 + [P]
+    cpu.lib.ref_matrix2_d.restype = P
+    cpu.lib.ref_matrix2_f.restype = P
+    cpu.lib.ref_make_float.argtypes = [P]
+    y_ref = np.empty(cpu.nd)
+    cpu.run(x, y_ref)
+    out = {}
+    for prec in ("fp64", "fp32"):
+        kidx, div, mul, a2t, a2i, aa, da = REF_GPU_VARIANTS[prec]
+        f32 = prec == "fp32"
+        if f32 and cpu.lib.ref_make_float(cpu.h) != 0:
+            continue
+        m2 = cpu.lib.ref_matrix2_f(cpu.h) if f32 else cpu.lib.ref_matrix2_d(cpu.h)
+        xv = np.ascontiguousarray(x, dtype=np.float32 if f32 else np.float64)
+        with tempfile.NamedTemporaryFile("r", suffix=".txt") as f:
+            if lib.refgpu_cuda2_bench(m2, int(f32), xv.ctypes.data_as(P), kidx, nbench, f.name.encode()) != 0:
+                continue
+            line = [ln.split() for ln in open(f.name) if ln.startswith("TIME")]
+        if not line or len(line[0]) != 9:
+            continue
+        t = line[0]
+        y = np.empty(cpu.nd, dtype=xv.dtype)
+        rc = lib.refgpu_hybrid2_y(m2, int(f32), xv.ctypes.data_as(P), div, mul, a2t, a2i, aa, da, y.ctypes.data_as(P))
+        rate = 1.0 / float(t[4])
+        out[prec] = {
+            "kernel": t[2] + " (src_hmvm/src_cpp/hmvm_cuda2.cu, built unchanged for sm_100a)",
+            "value": rate, "unit": "HMVM/s", "time_s": {"min": float(t[4]), "max": float(t[6]), "avg": float(t[8])},
+            "timing": f"the reference's own TIME line: kernel launch + cudaDeviceSynchronize timed with omp_get_wtime, "
+                      f"{5 + nbench} runs with the first 5 discarded, min (hmvm_cuda2.cu:236-302)",
+            "relerr_vs_fp64_cpu_reference": (float(np.linalg.norm(y.astype(np.float64) - y_ref) /
+                                                   np.linalg.norm(y_ref)) if rc == 0 else None),
+            "ratio_vs_reference_gpu": (ours.get(prec) / rate) if ours.get(prec) else None,
+        }
+    return out or None
+
+
 # Secondary workloads timed after the headline on the same matrix: (label,
 # precision, right-hand sides, 16-bit factor format).  Plans are built once per
 # (precision, factor format, pass kind) and reused by the legs that share them.
@@ -667,6 +725,7 @@ def run_b200(a, rank, world, local_rank):
     cpu_line = None
     rel = None
     legs = None
+    ref_gpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = CpuReference(hm)
         cpucols = CpuColumns(cpu, X)
@@ -683,6 +742,15 @@ def run_b200(a, rank, world, local_rank):
             cpu_line.update(cpu_bench_variants(cpu, x, a.cpu_seconds))
         if secondary:
             legs = run_secondary(a, hm, X, cpucols, 1e3 / ms_step, local_rank, stream, dev)
+        if secondary and not a.no_reference_gpu:
+            ours = {"fp64": 1e3 / ms_step}
+            for leg in legs or []:
+                if leg.get("workload") == "fp32 single-vector" and "value" in leg:
+                    ours["fp32"] = leg["value"]
+            try:
+                ref_gpu = reference_gpu(cpu, x, ours, a.reference_gpu_runs)
+            except Exception as e:
+                ref_gpu = {"error": f"{type(e).__name__}: {e}"}
     if dist:
         dist.barrier()
 
@@ -715,6 +783,8 @@ def run_b200(a, rank, world, local_rank):
                               "from a profiled pass of direct applies after the timed region")
         if legs is not None:
             line["secondary"] = legs
+        if ref_gpu is not None:
+            line["reference_gpu"] = ref_gpu
         print(json.dumps(line), flush=True)
 
 

@@ -207,6 +207,11 @@ void ref_omp2_f(void* hv, const float* x, float* y, int nthreads) {
 
 int ref_max_threads(void) { return omp_get_max_threads(); }
 
+// The handle's matrix2<double> / matrix2<float> (after ref_make_float), for the
+// reference's CUDA code in the companion library (ref_cuda_harness.cu).
+void* ref_matrix2_d(void* hv) { return static_cast<RefHandle*>(hv)->matD2; }
+void* ref_matrix2_f(void* hv) { return static_cast<RefHandle*>(hv)->matF2; }
+
 // The reference's own timed sweep of its SoA OpenMP variants,
 // hmvm_omp_bench<double>(NULL, mat2, x, 0) (src_hmvm/src_cpp/hmvm_omp.cpp:992-1347;
 // with mat == NULL it skips the AoS variants).  It prints "TIME <L> <name> min

@@ -41,3 +41,20 @@ def gpu():
     import torch
 
     return torch.device("cuda:0")
+
+
+_REPORT = []
+
+
+@pytest.fixture(scope="session")
+def report():
+    """Lines shown in the terminal summary: the measured relative errors of
+    the parity tests at configuration size, beside their bounds."""
+    return _REPORT
+
+
+def pytest_terminal_summary(terminalreporter):
+    if _REPORT:
+        terminalreporter.write_sep("-", "parity at configuration size (relative 2-norm error)")
+        for line in _REPORT:
+            terminalreporter.write_line(line)
