@@ -215,8 +215,8 @@ struct hmvm_plan {
   // wide tensor-core passes (FP32 and mixed plans made with nrhs_max >= 32):
   // 128 right-hand sides per pass, hmvm_tcw_kernel
   bool tcw = false, tcw_bf = false;
-  uint16_t* d_xpl = nullptr;  // x planes [32][nd][8]
-  uint16_t* d_tpl = nullptr;  // t planes [32][tpl_rows][8]
+  uint16_t* d_xpl = nullptr;  // x input chunks [4][nd][64]
+  uint16_t* d_tpl = nullptr;  // t input chunks [4][tpl_rows][64]
   int64_t tpl_rows = 0;
   float* d_tscale = nullptr;  // V-stage 2^-c per panel row, then the row scale s_i per y row
   float* d_xscale = nullptr;  // sigma_x per right-hand side of the current pass
@@ -367,21 +367,23 @@ bool tcw_wanted(const hmvm_plan_opts& o) {
   return (o.precision == HMVM_FP32 || o.precision == HMVM_MIXED) && o.nrhs_max >= kTcwMinNrhs;
 }
 
-// A planes buffer [32][rows][8] of 16-bit values as a 3-D tensor {8, rows, 32}
-// with boxes {8, 16, 32}: one K step of the 128 right-hand sides' hi and lo
-// parts per TMA copy.  Rows past the end read as zero.
+// An input buffer [4][rows][64] of 16-bit values (four chunks: hi and lo parts
+// of right-hand sides 0..63 and 64..127) as a 3-D tensor {64, rows, 4} with
+// boxes {64, 16, 4} and 128-byte swizzle: one K step of the 128 right-hand
+// sides' hi and lo parts per TMA copy, in the MMA's swizzled MN-major layout.
+// Rows past the end read as zero.
 int encode_planes_map(CUtensorMap* map, void* base, int64_t rows) {
   using Fn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
                           const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
                           CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
   static Fn fn = reinterpret_cast<Fn>(driver_fn("cuTensorMapEncodeTiled"));
   if (!fn) return set_error(HMVM_ECUDA, "cuTensorMapEncodeTiled is not available");
-  const cuuint64_t dims[3] = {8, (cuuint64_t)rows, 32};
-  const cuuint64_t strides[2] = {16, (cuuint64_t)rows * 16};
-  const cuuint32_t box[3] = {8, 16, 32};
+  const cuuint64_t dims[3] = {64, (cuuint64_t)rows, 4};
+  const cuuint64_t strides[2] = {128, (cuuint64_t)rows * 128};
+  const cuuint32_t box[3] = {64, 16, 4};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, base, dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return set_error(HMVM_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   return HMVM_OK;
@@ -921,7 +923,7 @@ int tcw_prepare(const hmvm_plan* p) {
 // into Y.
 int launch_tcw_pass(hmvm_plan* p, const void* X, int64_t ldx, void* Y, int64_t ldy, int nr, cudaStream_t st) {
   const bool f32 = p->precision == HMVM_FP32;
-  const int gx = p->num_sms * 4;
+  const int gx = (int)std::min<int64_t>(((int64_t)p->nd + 31) / 32, (int64_t)p->num_sms * 16);
   if (!p->tcw_bf) {
     HMVM_CUDA_TRY(cudaMemsetAsync(p->d_amax128, 0, kTcwRhs * sizeof(unsigned), st), "scale reset");
     const dim3 g((unsigned)std::max(1, std::min(p->num_sms, (p->nd + 255) / 256)), (unsigned)nr);

@@ -7,9 +7,13 @@
 //   M = 128 right-hand sides (TMEM lanes),
 //   N = the item's rows rounded up to 16 (<= 32 row-stage, <= 128 V-stage),
 //   K = 16 matrix columns,
-//   A = the inputs: 16 planes of x_hi (or t_hi) and 16 of x_lo, 8 right-hand
-//       sides x 16 rows each, MN-major without swizzle, one TMA tensor copy per
-//       K step (a 3-D box {8, 16, 32} of the planes tensor [32][rows][8]);
+//   A = the inputs, 16-bit hi and lo parts of 128 right-hand sides, held in
+//       four "chunk" arrays [4][rows][64] (chunk 0/1: hi of right-hand sides
+//       0..63 / 64..127, chunk 2/3: their lo parts); one TMA tensor copy per K
+//       step (a 3-D box {64, 16, 4}, 128-byte rows, SWIZZLE_128B) lands as the
+//       canonical 128-byte-swizzled MN-major layout: per chunk 16 K rows of
+//       128 bytes, 8-row atoms 1 KiB apart, the next 64 right-hand sides 2 KiB
+//       on;
 //   B = the matrix, K-major without swizzle, read by the MMA straight from the
 //       ring the bulk copies fill (8-row core matrices 128 B apart, the second
 //       8 columns R*16 B on; the missing half of an odd last step points at a
@@ -44,7 +48,7 @@ namespace hmvm {
 
 constexpr int kTcwSlotM = 8192;   // matrix ring slot (a K step of a 128-row pair panel is 8 KiB)
 constexpr int kTcwSlotsM = 8;
-constexpr int kTcwSlotA = 8192;   // one K step of inputs: 32 planes x 16 rows x 16 B
+constexpr int kTcwSlotA = 8192;   // one K step of inputs: 4 chunks x 16 rows x 128 B
 constexpr int kTcwSlotsA = 10;
 constexpr int kTcwAccBufs = 4;
 constexpr int kTcwAccCols = 128;  // TMEM columns of an accumulator buffer
@@ -57,7 +61,7 @@ constexpr int kTcwOffZero = kTcwOffStage + 4 * kTcwStageBytes;
 constexpr int kTcwOffBar = kTcwOffZero + kTcwZeroBytes;
 constexpr int kTcwNumBars = 2 * kTcwSlotsM + 2 * kTcwSlotsA + 2 * kTcwAccBufs + 1;
 constexpr int kTcwOffMisc = kTcwOffBar + kTcwNumBars * 8;
-constexpr int kTcwSmem = kTcwOffMisc + 32;
+constexpr int kTcwSmem = kTcwOffMisc + 32 + 1024;  // + room to align the base to 1 KiB
 static_assert(kTcwSmem <= 227 * 1024, "shared memory");
 static_assert(kTcwAccBufs * kTcwAccCols == 512, "the CTA owns the SM's 512 TMEM columns");
 
@@ -70,7 +74,7 @@ struct TcwArgs {
   const int32_t* out_idx;     // V stage: t slot per panel row
   const float* tscale;        // V stage: 2^-c per panel row; row stage: s_i per row (tile _pad indexes it)
   const float* xscale;        // sigma_x per right-hand side [128]
-  uint16_t* tplanes;          // V stage output: 32 planes x trows x 8
+  uint16_t* tplanes;          // V stage output: 4 chunks x trows x 64
   int64_t trows;
   float* part;                // V-stage split panels: FP32 partial sums [row][128]
   void* y;                    // row-stage output, column-major, leading dimension ldy
@@ -85,6 +89,12 @@ struct TcwArgs {
 __host__ __device__ constexpr uint32_t tcw_idesc(int bf, int n) {
   return (1u << 4) | ((uint32_t)bf << 7) | ((uint32_t)bf << 10) | (1u << 15) | ((uint32_t)(n >> 3) << 17) |
          ((uint32_t)(128 >> 4) << 24);
+}
+
+// Shared-memory matrix descriptor of a 128-byte-swizzled layout (tcgen05
+// layout type 2): start address, leading- and stride-dimension byte offsets.
+__device__ __forceinline__ uint64_t tc_desc_sw128(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return tc_desc(saddr, lbo, sbo) | ((uint64_t)2 << 61);
 }
 
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
@@ -147,7 +157,9 @@ template <bool VST, bool BF>
 __global__ void __launch_bounds__(kTcwThreads, 1)
     hmvm_tcw_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap tmap,
                     const TcwArgs a) {
-  extern __shared__ __align__(1024) unsigned char tcw_smem[];
+  extern __shared__ __align__(1024) unsigned char tcw_smem_raw[];
+  // the swizzled input slots need 1 KiB alignment
+  unsigned char* tcw_smem = tcw_smem_raw + ((1024u - (smem_u32(tcw_smem_raw) & 1023u)) & 1023u);
   unsigned char* ringM = tcw_smem;
   unsigned char* ringA = tcw_smem + kTcwOffA;
   unsigned char* zero = tcw_smem + kTcwOffZero;
@@ -245,6 +257,8 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
       uint32_t mC = 0, aC = 0, ic = 0;
       bool ok = true;
       const uint32_t zaddr = smem_u32(zero);
+      // descriptor of input slot 0's hi part; slot s is (8 KiB * s) >> 4 further on, its lo part 4 KiB on
+      const uint64_t adesc0 = tc_desc_sw128(smem_u32(ringA), 2048, 1024);
       for (int it = tb; it < te && ok; it++, ic++) {
         const hmvm_tile_desc d = a.tiles[it];
         const int R = d.nrows;
@@ -257,6 +271,8 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
         tc_fence_after();
         const uint32_t dcol = tmem_base + (uint32_t)(buf * kTcwAccCols);
         int accum = 0;
+        // B descriptor with start address 0: a K step's start is added as (address >> 4)
+        const uint64_t bdesc0 = tc_desc(0, (uint32_t)R * 16u, 128);
         for (int s = 0; s < d.nseg && ok; s++) {
           const TcwSeg sg = tcw_seg(a.segs[d.seg_begin + s], R);
           for (int j = 0; j < sg.nks && ok;) {
@@ -276,19 +292,21 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
               }
               aC++;
               tc_fence_after();
-              const uint32_t abase = smem_u32(ringA + as * kTcwSlotA);
-              const int nvj = min(2, sg.nv - 2 * jj);
+              // A: chunks 0, 1 (hi) and 2, 3 (lo) of the slot; 64-rhs atoms 2 KiB apart, 8-row groups 1 KiB apart
+              const uint64_t ah = adesc0 + (uint64_t)(as * (kTcwSlotA >> 4)), al = ah + (4096 >> 4);
               const uint32_t bhi = cbase + (uint32_t)(jj - j) * 2u * sg.vb;
-              const uint32_t blo = bhi + (uint32_t)nvj * (uint32_t)R * 16u;
-              // A: planes 0..15 (hi) and 16..31 (lo); K 8-row groups 128 B apart, planes 256 B apart
-              const uint64_t ah = tc_desc(abase, 128, 256), al = tc_desc(abase + 4096, 128, 256);
-              const uint64_t bh = tc_desc(bhi, nvj == 2 ? (uint32_t)R * 16u : zaddr - bhi, 128);
+              uint64_t bh, bl;
+              if (jj + 1 < sg.nks || !(sg.nv & 1)) {  // two 8-column vectors
+                bh = bdesc0 + (bhi >> 4);
+                bl = bh + (uint64_t)(2 * R);  // (2 R 16 bytes) >> 4
+              } else {  // an odd last step: the second 8 columns read the zero block
+                const uint32_t blo = bhi + (uint32_t)R * 16u;
+                bh = tc_desc(bhi, zaddr - bhi, 128);
+                bl = tc_desc(blo, zaddr - blo, 128);
+              }
               tc_mma(dcol, ah, bh, idesc, accum);
               tc_mma(dcol, al, bh, idesc, 1);
-              if (sg.fmt) {
-                const uint64_t bl = tc_desc(blo, nvj == 2 ? (uint32_t)R * 16u : zaddr - blo, 128);
-                tc_mma(dcol, ah, bl, idesc, 1);
-              }
+              if (sg.fmt) tc_mma(dcol, ah, bl, idesc, 1);
               accum = 1;
               tc_commit(&aempty[as]);
             }
@@ -341,8 +359,8 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
                 const int64_t slot = a.out_idx[d.out_base + c0 + i];
                 uint16_t hi, lo;
                 tcw_split<BF>(tv, hi, lo);
-                a.tplanes[((int64_t)(r >> 3) * a.trows + slot) * 8 + (r & 7)] = hi;
-                a.tplanes[((int64_t)(16 + (r >> 3)) * a.trows + slot) * 8 + (r & 7)] = lo;
+                a.tplanes[((int64_t)(r >> 6) * a.trows + slot) * 64 + (r & 63)] = hi;
+                a.tplanes[((int64_t)(2 + (r >> 6)) * a.trows + slot) * 64 + (r & 63)] = lo;
               } else {
                 a.part[(int64_t)(d.out_base + c0 + i) * 128 + r] = tv;
               }
@@ -410,38 +428,43 @@ __device__ __forceinline__ float tcw_sigma(unsigned amax_bits) {
   return ldexpf(1.f, (f == 0.5f ? e - 1 : e) - 15);
 }
 
-// X (column-major, nr <= 128 columns) -> planes[32][n][8]: plane p < 16 holds
-// the hi parts of right-hand sides 8p..8p+7 (scaled by 1 / sigma_r), plane
-// 16 + p their lo parts; columns nr..127 are zero.  xscale[r] = sigma_r.
+// X (column-major, nr <= 128 columns) -> chunks[4][n][64]: chunk c < 2 holds
+// the hi parts of right-hand sides 64c..64c+63 (scaled by 1 / sigma_r), chunk
+// 2 + c their lo parts; columns nr..127 are zero.  xscale[r] = sigma_r.  A
+// block of 256 threads takes 32 rows: each warp reads whole columns of them
+// (coalesced), the hi/lo values meet in shared memory, and the block writes
+// the 4 x 32 chunk rows of 128 bytes.
 template <typename TX, bool BF>
-__global__ void hmvm_tcw_xplanes_kernel(const TX* __restrict__ X, int64_t ldx, int n, int nr,
-                                        const unsigned* __restrict__ amax, float* __restrict__ xscale,
-                                        uint16_t* __restrict__ planes) {
-  if (blockIdx.x == 0 && threadIdx.x < 128)
-    xscale[threadIdx.x] = threadIdx.x < nr ? tcw_sigma<BF>(amax[threadIdx.x]) : 1.f;
-  const int64_t total = (int64_t)n * 16;
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
-    const int p = (int)(k / n);
-    const int64_t i = k - (int64_t)p * n;
-    uint16_t hi[8], lo[8];
-#pragma unroll
-    for (int e = 0; e < 8; e++) {
-      const int r = 8 * p + e;
-      float v = 0.f;
-      if (r < nr) v = (float)X[i + r * ldx] / tcw_sigma<BF>(amax[r]);
-      tcw_split<BF>(v, hi[e], lo[e]);
+__global__ void __launch_bounds__(256) hmvm_tcw_xplanes_kernel(const TX* __restrict__ X, int64_t ldx, int n, int nr,
+                                                               const unsigned* __restrict__ amax,
+                                                               float* __restrict__ xscale,
+                                                               uint16_t* __restrict__ planes) {
+  __shared__ float inv[128];
+  __shared__ __align__(16) uint16_t sh[4][32][72];  // chunk, row, right-hand side (+8 to spread the banks)
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid < 128) {
+    const float sg = tid < nr ? tcw_sigma<BF>(amax[tid]) : 1.f;
+    inv[tid] = 1.f / sg;  // a power of two: exact
+    if (blockIdx.x == 0) xscale[tid] = sg;
+  }
+  __syncthreads();
+  for (int64_t i0 = (int64_t)blockIdx.x * 32; i0 < n; i0 += (int64_t)gridDim.x * 32) {
+    const int64_t i = i0 + lane;
+    for (int c = warp; c < 128; c += 8) {
+      const float v = (c < nr && i < n) ? (float)X[i + c * ldx] * inv[c] : 0.f;
+      uint16_t hi, lo;
+      tcw_split<BF>(v, hi, lo);
+      sh[c >> 6][lane][c & 63] = hi;
+      sh[2 + (c >> 6)][lane][c & 63] = lo;
     }
-    uint4 h, l;
-    h.x = hi[0] | ((uint32_t)hi[1] << 16);
-    h.y = hi[2] | ((uint32_t)hi[3] << 16);
-    h.z = hi[4] | ((uint32_t)hi[5] << 16);
-    h.w = hi[6] | ((uint32_t)hi[7] << 16);
-    l.x = lo[0] | ((uint32_t)lo[1] << 16);
-    l.y = lo[2] | ((uint32_t)lo[3] << 16);
-    l.z = lo[4] | ((uint32_t)lo[5] << 16);
-    l.w = lo[6] | ((uint32_t)lo[7] << 16);
-    reinterpret_cast<uint4*>(planes)[(int64_t)p * n + i] = h;
-    reinterpret_cast<uint4*>(planes)[(int64_t)(16 + p) * n + i] = l;
+    __syncthreads();
+    for (int u = tid; u < 4 * 32 * 8; u += 256) {
+      const int ch = u >> 8, row = (u >> 3) & 31, part = u & 7;
+      if (i0 + row < n)
+        reinterpret_cast<uint4*>(planes)[((int64_t)ch * n + i0 + row) * 8 + part] =
+            *reinterpret_cast<const uint4*>(&sh[ch][row][part * 8]);
+    }
+    __syncthreads();
   }
 }
 
@@ -458,8 +481,8 @@ __global__ void hmvm_tcw_reduce_kernel(const int4* __restrict__ red, int n, cons
     for (int q = 0; q < rd.z; q++) s += part[(int64_t)(rd.y + q * rd.w) * 128 + r];
     uint16_t hi, lo;
     tcw_split<BF>(s, hi, lo);
-    tplanes[((int64_t)(r >> 3) * trows + rd.x) * 8 + (r & 7)] = hi;
-    tplanes[((int64_t)(16 + (r >> 3)) * trows + rd.x) * 8 + (r & 7)] = lo;
+    tplanes[((int64_t)(r >> 6) * trows + rd.x) * 64 + (r & 63)] = hi;
+    tplanes[((int64_t)(2 + (r >> 6)) * trows + rd.x) * 64 + (r & 63)] = lo;
   }
 }
 
