@@ -142,7 +142,8 @@ class LayoutView(C.Structure):
                 ("red1", C.POINTER(C.c_int32)), ("red2", C.POINTER(C.c_int32)), ("data", C.c_void_p),
                 ("rowscale", C.POINTER(C.c_double)), ("n_rowscale", C.c_int64),
                 ("tcw", C.c_int32), ("tcw_bf16", C.c_int32), ("tscale", C.POINTER(C.c_float)),
-                ("n_tscale", C.c_int64), ("tscale_rows0", C.c_int32), ("_pad_view", C.c_int32)]
+                ("n_tscale", C.c_int64), ("tscale_rows0", C.c_int32), ("_pad_view", C.c_int32),
+                ("tblocks", C.POINTER(C.c_int32))]
 
 
 class HgenParams(C.Structure):

@@ -18,21 +18,33 @@
 //       ring the bulk copies fill (8-row core matrices 128 B apart, the second
 //       8 columns R*16 B on; the missing half of an odd last step points at a
 //       zero block);
-//   D = FP32 in one of four 128-column accumulator buffers.
-// Per K step: hi x x_hi and hi x x_lo, plus lo x x_hi for pair-stored segments.
+//   D = FP32 in TMEM: V stage 2 accumulator buffers of 256 columns (row block b
+//       at column 128 b), row stage 4 buffers of 128 columns (block b at 32 b).
+// An item is up to 4 row blocks; a segment multiplies the blocks in its mask
+// by one input range, and consecutive segments with the same range form an
+// input group: per K step of a group one TMA copy of the inputs, then for each
+// segment and each of its blocks hi x x_hi and hi x x_lo, plus lo x x_hi for
+// pair-stored segments (the stream holds, per K step, per segment, per block,
+// the hi vectors and then the lo vectors).
 //
 // One CTA of 6 warps per SM, warp-specialised:
-//   warp 0 (one thread)  producer: bulk copies of the matrix stream into an
-//                        8 x 8 KiB ring (chunks never split a K step) and TMA
-//                        tensor copies of each K step's inputs into a
-//                        10 x 8 KiB ring;
+//   warp 0 (one thread)  producer: per K step a bulk copy of its matrix bytes
+//                        into the current 8 KiB slot of a 12-slot ring (a slot
+//                        -- "chunk" -- takes whole K steps, at most 8, across
+//                        segments and items; each copy adds its bytes with
+//                        mbarrier.expect_tx and the chunk is closed by one
+//                        arrive), and a TMA tensor copy of the K step's inputs
+//                        into a 14 x 8 KiB ring;
 //   warp 1 (one thread)  allocates TMEM, issues the MMAs, commits each input
-//                        slot, matrix slot and finished accumulator to its
+//                        slot, matrix chunk and finished accumulator to its
 //                        mbarrier;
-//   warps 2..5           epilogue: tcgen05.ld the accumulator (warp w reads
-//                        lanes 32 (w % 4) ..), scale, and write t (as 16-bit
-//                        hi/lo planes) or y (through a shared-memory transpose
-//                        so each store covers 32 consecutive rows).
+//   warps 2..5           epilogue: tcgen05.ld the accumulators (warp w reads
+//                        lanes 32 (w % 4) ..), scale, and store t (16-bit
+//                        hi/lo chunks) or y (each thread 32 consecutive rows of
+//                        its right-hand side).
+// A chunk holds fewer K steps than the input ring has slots, so the producer
+// always reaches the K step that closes a chunk before it needs an input slot
+// the MMAs of that chunk would free: no wait can close a cycle.
 // Every mbarrier wait is bounded (kWaitLimitNs); a role that gives up records
 // the error and stops; before the CTA exits, the copies still in flight and
 // the MMAs issued are waited for (bounded) and the TMEM is freed.
@@ -46,28 +58,34 @@
 
 namespace hmvm {
 
-constexpr int kTcwSlotM = 8192;   // matrix ring slot (a K step of a 128-row pair panel is 8 KiB)
-constexpr int kTcwSlotsM = 8;
+constexpr int kTcwSlotM = 8192;   // matrix ring chunk: whole K steps (one K step of an item is <= 8 KiB)
+constexpr int kTcwSlotsM = 12;
+constexpr int kTcwChunkSteps = 8; // K steps per chunk at most (< kTcwSlotsA)
 constexpr int kTcwSlotA = 8192;   // one K step of inputs: 4 chunks x 16 rows x 128 B
-constexpr int kTcwSlotsA = 10;
-constexpr int kTcwAccBufs = 4;
-constexpr int kTcwAccCols = 128;  // TMEM columns of an accumulator buffer
+constexpr int kTcwSlotsA = 14;
+static_assert(kTcwChunkSteps < kTcwSlotsA, "a chunk must hold fewer K steps than the input ring has slots");
 constexpr int kTcwThreads = 192;
-constexpr int kTcwStageBytes = 32 * 33 * 8;  // per epilogue warp: 32 rhs x 32 rows of FP64 (+1 column)
-constexpr int kTcwZeroBytes = 2048;          // 128 rows x 16 B of zeros
+constexpr int kTcwZeroBytes = 2048;  // 128 rows x 16 B of zeros
 constexpr int kTcwOffA = kTcwSlotsM * kTcwSlotM;
-constexpr int kTcwOffStage = kTcwOffA + kTcwSlotsA * kTcwSlotA;
-constexpr int kTcwOffZero = kTcwOffStage + 4 * kTcwStageBytes;
+constexpr int kTcwOffZero = kTcwOffA + kTcwSlotsA * kTcwSlotA;
 constexpr int kTcwOffBar = kTcwOffZero + kTcwZeroBytes;
-constexpr int kTcwNumBars = 2 * kTcwSlotsM + 2 * kTcwSlotsA + 2 * kTcwAccBufs + 1;
+constexpr int kTcwNumBars = 2 * kTcwSlotsM + 2 * kTcwSlotsA + 2 * 4 + 1;
 constexpr int kTcwOffMisc = kTcwOffBar + kTcwNumBars * 8;
 constexpr int kTcwSmem = kTcwOffMisc + 32 + 1024;  // + room to align the base to 1 KiB
 static_assert(kTcwSmem <= 227 * 1024, "shared memory");
-static_assert(kTcwAccBufs * kTcwAccCols == 512, "the CTA owns the SM's 512 TMEM columns");
+// TMEM geometry per stage: accumulator buffers x columns, and the column stride of a row block
+template <bool VST>
+struct TcwGeom {
+  static constexpr int bufs = VST ? 2 : 4;
+  static constexpr int cols = VST ? 256 : 128;
+  static constexpr int bstride = VST ? 128 : 32;
+  static_assert(bufs * cols == 512, "the CTA owns the SM's 512 TMEM columns");
+};
 
 struct TcwArgs {
   const hmvm_tile_desc* tiles;
   const hmvm_seg_desc* segs;
+  const int32_t* blocks;      // per item: rows of its row blocks 0..3, 8 bits each
   const int32_t* team_begin;  // [nteams + 1]
   int nteams;
   const char* data;           // the 16-byte vectors of the stream
@@ -105,6 +123,10 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
       : "memory");
 }
+// Adds `bytes` to the transaction count of the current phase without arriving.
+__device__ __forceinline__ void mbar_expect_tx_only(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -132,24 +154,37 @@ __device__ __forceinline__ void tcw_split(float v, uint16_t& hi, uint16_t& lo) {
   }
 }
 
-// A segment's K-step geometry: format, columns, bytes per 8-column vector
-// (hi, or hi + lo), vectors, K steps and K steps per ring chunk.
-struct TcwSeg {
-  int fmt, ncols, nv, nks, per;
-  uint32_t vb;
-  int row0;
+// An input group of an item: segments [s0, s1) with one input range; per K
+// step, the bytes of every (segment, block) pair are (vectors of the step) x 16
+// x hrows, hrows = sum over the group's segments of (1 or 2) x (rows of the
+// blocks in its mask).
+struct TcwGroup {
+  int s1, ncols, nv, nks, row0, hrows;
   bool tsrc;
 };
-__device__ __forceinline__ TcwSeg tcw_seg(const hmvm_seg_desc& s, int R) {
-  TcwSeg g;
-  g.fmt = (s.ncols >> 28) & 1;
-  g.ncols = s.ncols & 0x0fffffff;
-  g.vb = (uint32_t)R * 16u * (g.fmt ? 2u : 1u);
+__device__ __forceinline__ int tcw_mask_rows(int mask, uint32_t R4) {
+  int n = 0;
+#pragma unroll
+  for (int b = 0; b < 4; b++)
+    if (mask >> b & 1) n += (R4 >> (8 * b)) & 0xff;
+  return n;
+}
+__device__ __forceinline__ TcwGroup tcw_group(const hmvm_seg_desc* segs, int s0, int se, uint32_t R4) {
+  TcwGroup g;
+  const hmvm_seg_desc f = segs[s0];
+  g.ncols = f.ncols & 0xffffff;
   g.nv = (g.ncols + 7) >> 3;
   g.nks = (g.nv + 1) >> 1;
-  g.per = max(1, kTcwSlotM / (int)(2 * g.vb));
-  g.tsrc = s.src < 0;
-  g.row0 = s.src & 0x7fffffff;
+  g.tsrc = f.src < 0;
+  g.row0 = f.src & 0x7fffffff;
+  g.hrows = 0;
+  int s = s0;
+  for (; s < se; s++) {
+    const hmvm_seg_desc z = segs[s];
+    if (s > s0 && (z.src != f.src || (z.ncols & 0xffffff) != g.ncols)) break;
+    g.hrows += ((z.ncols >> 28) & 1 ? 2 : 1) * tcw_mask_rows((z.ncols >> 24) & 15, R4);
+  }
+  g.s1 = s;
   return g;
 }
 
@@ -157,6 +192,7 @@ template <bool VST, bool BF>
 __global__ void __launch_bounds__(kTcwThreads, 1)
     hmvm_tcw_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap tmap,
                     const TcwArgs a) {
+  using G = TcwGeom<VST>;
   extern __shared__ __align__(1024) unsigned char tcw_smem_raw[];
   // the swizzled input slots need 1 KiB alignment
   unsigned char* tcw_smem = tcw_smem_raw + ((1024u - (smem_u32(tcw_smem_raw) & 1023u)) & 1023u);
@@ -169,10 +205,10 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
   uint64_t* afull = mempty + kTcwSlotsM;
   uint64_t* aempty = afull + kTcwSlotsA;
   uint64_t* accfull = aempty + kTcwSlotsA;
-  uint64_t* accempty = accfull + kTcwAccBufs;
-  uint64_t* done = accempty + kTcwAccBufs;
+  uint64_t* accempty = accfull + 4;
+  uint64_t* done = accempty + 4;
   uint32_t* misc = reinterpret_cast<uint32_t*>(tcw_smem + kTcwOffMisc);
-  // misc: [0] TMEM base, [1] matrix chunks issued, [2] input steps issued,
+  // misc: [0] TMEM base, [1] matrix chunks opened, [2] input steps issued,
   //       [3] matrix chunks consumed, [4] input steps consumed
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -185,7 +221,7 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
       mbar_init(&afull[s], 1);
       mbar_init(&aempty[s], 1);
     }
-    for (int s = 0; s < kTcwAccBufs; s++) {
+    for (int s = 0; s < G::bufs; s++) {
       mbar_init(&accfull[s], 1);
       mbar_init(&accempty[s], 4);
     }
@@ -211,42 +247,50 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
 
   if (warp == 0) {
     // ---- producer ----
-    if (lane == 0) {
-      uint32_t mI = 0, aI = 0;
-      bool ok = true;
+    if (lane == 0 && tb < te) {
+      uint32_t mI = 0, aI = 0, used = 0, cnt = 0;
+      int ms = 0;
+      bool ok = true, open = false;
+      const char* g = a.data + a.tiles[tb].data_off * 16;  // the team's items are contiguous in the stream
       for (int it = tb; it < te && ok; it++) {
         const hmvm_tile_desc d = a.tiles[it];
-        const int R = d.nrows;
-        const char* g = a.data + d.data_off * 16;
-        for (int s = 0; s < d.nseg && ok; s++) {
-          const TcwSeg sg = tcw_seg(a.segs[d.seg_begin + s], R);
-          const CUtensorMap* map = sg.tsrc ? &tmap : &xmap;
-          for (int j = 0; j < sg.nks && ok;) {
-            const int j2 = min(sg.nks, j + sg.per);
-            const uint32_t bytes = (uint32_t)(j2 == sg.nks ? sg.nv - 2 * j : 2 * (j2 - j)) * sg.vb;
-            const int ms = mI % kTcwSlotsM;
-            if (mI >= kTcwSlotsM && !thread_wait(&mempty[ms], ((mI / kTcwSlotsM) - 1) & 1)) {
+        const uint32_t R4 = (uint32_t)a.blocks[it];
+        const int se = d.seg_begin + d.nseg;
+        for (int s = d.seg_begin; s < se && ok;) {
+          const TcwGroup gr = tcw_group(a.segs, s, se, R4);
+          const CUtensorMap* map = gr.tsrc ? &tmap : &xmap;
+          for (int j = 0; j < gr.nks; j++) {
+            const uint32_t kb = (uint32_t)min(2, gr.nv - 2 * j) * 16u * (uint32_t)gr.hrows;
+            if (!open || used + kb > (uint32_t)kTcwSlotM || cnt == kTcwChunkSteps) {
+              if (open) mbar_arrive(&mfull[ms]);  // close the chunk
+              ms = mI % kTcwSlotsM;
+              if (mI >= kTcwSlotsM && !thread_wait(&mempty[ms], ((mI / kTcwSlotsM) - 1) & 1)) {
+                ok = false;
+                open = false;
+                break;
+              }
+              mI++;
+              open = true;
+              used = cnt = 0;
+            }
+            mbar_expect_tx_only(&mfull[ms], kb);
+            bulk_g2s(ringM + ms * kTcwSlotM + used, g, kb, &mfull[ms]);
+            g += kb;
+            used += kb;
+            cnt++;
+            const int as = aI % kTcwSlotsA;
+            if (aI >= kTcwSlotsA && !thread_wait(&aempty[as], ((aI / kTcwSlotsA) - 1) & 1)) {
               ok = false;
               break;
             }
-            mbar_expect_tx(&mfull[ms], bytes);
-            bulk_g2s(ringM + ms * kTcwSlotM, g, bytes, &mfull[ms]);
-            g += bytes;
-            mI++;
-            for (int jj = j; jj < j2; jj++) {
-              const int as = aI % kTcwSlotsA;
-              if (aI >= kTcwSlotsA && !thread_wait(&aempty[as], ((aI / kTcwSlotsA) - 1) & 1)) {
-                ok = false;
-                break;
-              }
-              mbar_expect_tx(&afull[as], kTcwSlotA);
-              tma_load_3d(ringA + as * kTcwSlotA, map, 0, sg.row0 + 16 * jj, 0, &afull[as]);
-              aI++;
-            }
-            j = j2;
+            mbar_expect_tx(&afull[as], kTcwSlotA);
+            tma_load_3d(ringA + as * kTcwSlotA, map, 0, gr.row0 + 16 * j, 0, &afull[as]);
+            aI++;
           }
+          s = gr.s1;
         }
       }
+      if (open) mbar_arrive(&mfull[ms]);  // close the last chunk (also after a failure, so it can drain)
       misc[1] = mI;
       misc[2] = aI;
       if (!ok) atomicExch(a.err, 1);
@@ -254,69 +298,86 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
   } else if (warp == 1) {
     // ---- MMA issue ----
     if (lane == 0) {
-      uint32_t mC = 0, aC = 0, ic = 0;
-      bool ok = true;
+      uint32_t mC = 0, aC = 0, ic = 0, used = 0, cnt = 0, cbase = 0;
+      int ms = 0;
+      bool ok = true, open = false;
       const uint32_t zaddr = smem_u32(zero);
       // descriptor of input slot 0's hi part; slot s is (8 KiB * s) >> 4 further on, its lo part 4 KiB on
       const uint64_t adesc0 = tc_desc_sw128(smem_u32(ringA), 2048, 1024);
       for (int it = tb; it < te && ok; it++, ic++) {
         const hmvm_tile_desc d = a.tiles[it];
-        const int R = d.nrows;
-        const uint32_t idesc = tcw_idesc(BF ? 1 : 0, max(16, (R + 15) & ~15));
-        const int buf = ic % kTcwAccBufs;
-        if (ic >= kTcwAccBufs && !thread_wait(&accempty[buf], ((ic / kTcwAccBufs) - 1) & 1)) {
+        const uint32_t R4 = (uint32_t)a.blocks[it];
+        const int buf = ic % G::bufs;
+        if (ic >= G::bufs && !thread_wait(&accempty[buf], ((ic / G::bufs) - 1) & 1)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        const uint32_t dcol = tmem_base + (uint32_t)(buf * kTcwAccCols);
-        int accum = 0;
-        // B descriptor with start address 0: a K step's start is added as (address >> 4)
-        const uint64_t bdesc0 = tc_desc(0, (uint32_t)R * 16u, 128);
-        for (int s = 0; s < d.nseg && ok; s++) {
-          const TcwSeg sg = tcw_seg(a.segs[d.seg_begin + s], R);
-          for (int j = 0; j < sg.nks && ok;) {
-            const int j2 = min(sg.nks, j + sg.per);
-            const int ms = mC % kTcwSlotsM;
-            if (!thread_wait(&mfull[ms], (mC / kTcwSlotsM) & 1)) {
+        const uint32_t dcol = tmem_base + (uint32_t)(buf * G::cols);
+        uint32_t started = 0;  // blocks whose accumulator holds a first product
+        const int se = d.seg_begin + d.nseg;
+        for (int s = d.seg_begin; s < se && ok;) {
+          const TcwGroup gr = tcw_group(a.segs, s, se, R4);
+          for (int j = 0; j < gr.nks; j++) {
+            const int nvj = min(2, gr.nv - 2 * j);
+            const uint32_t kb = (uint32_t)nvj * 16u * (uint32_t)gr.hrows;
+            if (!open || used + kb > (uint32_t)kTcwSlotM || cnt == kTcwChunkSteps) {
+              if (open) tc_commit(&mempty[ms]);  // its MMAs done, the chunk can be refilled
+              ms = mC % kTcwSlotsM;
+              if (!thread_wait(&mfull[ms], (mC / kTcwSlotsM) & 1)) {
+                ok = false;
+                open = false;
+                break;
+              }
+              mC++;
+              open = true;
+              used = cnt = 0;
+              cbase = smem_u32(ringM + ms * kTcwSlotM);
+            }
+            const int as = aC % kTcwSlotsA;
+            if (!thread_wait(&afull[as], (aC / kTcwSlotsA) & 1)) {
               ok = false;
               break;
             }
-            mC++;
-            const uint32_t cbase = smem_u32(ringM + ms * kTcwSlotM);
-            for (int jj = j; jj < j2; jj++) {
-              const int as = aC % kTcwSlotsA;
-              if (!thread_wait(&afull[as], (aC / kTcwSlotsA) & 1)) {
-                ok = false;
-                break;
+            aC++;
+            tc_fence_after();
+            // A: chunks 0, 1 (hi) and 2, 3 (lo) of the slot; 64-rhs atoms 2 KiB apart, 8-row groups 1 KiB apart
+            const uint64_t ah = adesc0 + (uint64_t)(as * (kTcwSlotA >> 4)), al = ah + (4096 >> 4);
+            uint32_t off = cbase + used;
+            for (int z = s; z < gr.s1; z++) {
+              const int enc = a.segs[z].ncols;
+              const int mask = (enc >> 24) & 15, pair = (enc >> 28) & 1;
+#pragma unroll
+              for (int b = 0; b < 4; b++) {
+                if (!(mask >> b & 1)) continue;
+                const uint32_t Rb = (R4 >> (8 * b)) & 0xffu;
+                const uint32_t idesc = tcw_idesc(BF ? 1 : 0, max(16, (int)((Rb + 15) & ~15u)));
+                const uint32_t dblk = dcol + (uint32_t)(b * G::bstride);
+                uint64_t bh, bl;
+                const uint32_t blo = off + (uint32_t)nvj * Rb * 16u;
+                if (nvj == 2) {
+                  bh = tc_desc(off, Rb * 16u, 128);
+                  bl = tc_desc(blo, Rb * 16u, 128);
+                } else {  // an odd last step: the second 8 columns read the zero block
+                  bh = tc_desc(off, zaddr - off, 128);
+                  bl = tc_desc(blo, zaddr - blo, 128);
+                }
+                tc_mma(dblk, ah, bh, idesc, (int)(started >> b & 1));
+                tc_mma(dblk, al, bh, idesc, 1);
+                if (pair) tc_mma(dblk, ah, bl, idesc, 1);
+                started |= 1u << b;
+                off += (uint32_t)nvj * Rb * 16u * (pair ? 2u : 1u);
               }
-              aC++;
-              tc_fence_after();
-              // A: chunks 0, 1 (hi) and 2, 3 (lo) of the slot; 64-rhs atoms 2 KiB apart, 8-row groups 1 KiB apart
-              const uint64_t ah = adesc0 + (uint64_t)(as * (kTcwSlotA >> 4)), al = ah + (4096 >> 4);
-              const uint32_t bhi = cbase + (uint32_t)(jj - j) * 2u * sg.vb;
-              uint64_t bh, bl;
-              if (jj + 1 < sg.nks || !(sg.nv & 1)) {  // two 8-column vectors
-                bh = bdesc0 + (bhi >> 4);
-                bl = bh + (uint64_t)(2 * R);  // (2 R 16 bytes) >> 4
-              } else {  // an odd last step: the second 8 columns read the zero block
-                const uint32_t blo = bhi + (uint32_t)R * 16u;
-                bh = tc_desc(bhi, zaddr - bhi, 128);
-                bl = tc_desc(blo, zaddr - blo, 128);
-              }
-              tc_mma(dcol, ah, bh, idesc, accum);
-              tc_mma(dcol, al, bh, idesc, 1);
-              if (sg.fmt) tc_mma(dcol, ah, bl, idesc, 1);
-              accum = 1;
-              tc_commit(&aempty[as]);
             }
-            if (!ok) break;
-            tc_commit(&mempty[ms]);
-            j = j2;
+            tc_commit(&aempty[as]);
+            used += kb;
+            cnt++;
           }
+          s = gr.s1;
         }
         if (ok) tc_commit(&accfull[buf]);
       }
+      if (open) tc_commit(&mempty[ms]);
       misc[3] = mC;
       misc[4] = aC;
       // every MMA issued has completed before the CTA goes on (bounded)
@@ -326,62 +387,64 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
     }
   } else {
     // ---- epilogue ----
-    const int e = warp - 2, q = warp & 3;
+    const int q = warp & 3;
     const int r = 32 * q + lane;  // this thread's right-hand side
-    double* stg = reinterpret_cast<double*>(tcw_smem + kTcwOffStage + e * kTcwStageBytes);
-    const float sx = a.xscale[r];
+    const double sx = a.xscale[r];
     uint32_t ic = 0;
     for (int it = tb; it < te; it++, ic++) {
       const hmvm_tile_desc d = a.tiles[it];
-      const int buf = ic % kTcwAccBufs;
-      if (!warp_wait(&accfull[buf], (ic / kTcwAccBufs) & 1)) {
+      const uint32_t R4 = (uint32_t)a.blocks[it];
+      const int buf = ic % G::bufs;
+      if (!warp_wait(&accfull[buf], (ic / G::bufs) & 1)) {
         if (lane == 0) atomicExch(a.err, 1);
         break;
       }
       tc_fence_after();
-      const int R = d.nrows;
-      const uint32_t tbase = tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * kTcwAccCols);
-      for (int c0 = 0; c0 < R; c0 += 32) {
-        float v[32];
-        if (d.nseg > 0) {
-          tc_ld32(tbase + (uint32_t)c0, v);
-        } else {
+      const int mode = d.mode & 3, has = (d.mode >> 4) & 15;
+      int rb = 0;  // the block's first item row
+      for (int b = 0; b < 4; b++) {
+        const int Rb = (R4 >> (8 * b)) & 0xff;
+        if (!Rb) continue;
+        const uint32_t tbase =
+            tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * G::cols + b * G::bstride);
+        for (int c0 = 0; c0 < Rb; c0 += 32) {
+          float v[32];
+          if (has >> b & 1) {
+            tc_ld32(tbase + (uint32_t)c0, v);
+          } else {
 #pragma unroll
-          for (int i = 0; i < 32; i++) v[i] = 0.f;
-        }
-        const int nrow = min(32, R - c0);
-        if constexpr (VST) {
+            for (int i = 0; i < 32; i++) v[i] = 0.f;
+          }
+          const int nrow = min(32, Rb - c0), row = rb + c0;
+          if constexpr (VST) {
 #pragma unroll
-          for (int i = 0; i < 32; i++) {
-            if (i < nrow) {
-              const float tv = v[i] * a.tscale[d._pad + c0 + i];
-              if (d.mode == 1) {
-                const int64_t slot = a.out_idx[d.out_base + c0 + i];
-                uint16_t hi, lo;
-                tcw_split<BF>(tv, hi, lo);
-                a.tplanes[((int64_t)(r >> 6) * a.trows + slot) * 64 + (r & 63)] = hi;
-                a.tplanes[((int64_t)(2 + (r >> 6)) * a.trows + slot) * 64 + (r & 63)] = lo;
-              } else {
-                a.part[(int64_t)(d.out_base + c0 + i) * 128 + r] = tv;
+            for (int i = 0; i < 32; i++) {
+              if (i < nrow) {
+                const float tv = v[i] * a.tscale[d._pad + row + i];
+                if (mode == 1) {
+                  const int64_t slot = a.out_idx[d.out_base + row + i];
+                  uint16_t hi, lo;
+                  tcw_split<BF>(tv, hi, lo);
+                  a.tplanes[((int64_t)(r >> 6) * a.trows + slot) * 64 + (r & 63)] = hi;
+                  a.tplanes[((int64_t)(2 + (r >> 6)) * a.trows + slot) * 64 + (r & 63)] = lo;
+                } else {
+                  a.part[(int64_t)(d.out_base + row + i) * 128 + r] = tv;
+                }
+              }
+            }
+          } else if (r < a.nr) {
+            const int64_t o = (int64_t)d.out_base + row + (int64_t)r * a.ldy;
+#pragma unroll
+            for (int i = 0; i < 32; i++) {
+              if (i < nrow) {
+                const double val = (double)v[i] * (double)a.tscale[d._pad + row + i] * sx;
+                if (a.y32) static_cast<float*>(a.y)[o + i] = (float)val;
+                else static_cast<double*>(a.y)[o + i] = val;
               }
             }
           }
-        } else {
-#pragma unroll
-          for (int i = 0; i < 32; i++)
-            stg[lane * 33 + i] = i < nrow ? (double)v[i] * (double)a.tscale[d._pad + c0 + i] * (double)sx : 0.0;
-          __syncwarp();
-          for (int c = 0; c < 32; c++) {
-            const int rr = 32 * q + c;
-            if (rr < a.nr && lane < nrow) {
-              const double val = stg[c * 33 + lane];
-              const int64_t o = (int64_t)d.out_base + c0 + lane + (int64_t)rr * a.ldy;
-              if (a.y32) static_cast<float*>(a.y)[o] = (float)val;
-              else static_cast<double*>(a.y)[o] = val;
-            }
-          }
-          __syncwarp();
         }
+        rb += Rb;
       }
       tc_fence_before();
       __syncwarp();

@@ -180,8 +180,9 @@ constexpr int kMultiWarpsPerSm = 8;  // resident warps (teams) per SM of the mul
 // storage): 128 right-hand sides per pass, every product on tcgen05.
 constexpr int kTcwRhs = 128;        // right-hand sides per pass: the MMA's M
 constexpr int kTcwMinNrhs = 32;     // nrhs_max from which a plan takes this form
-constexpr int kTcwPanelRows = 128;  // V-stage panel rows: the MMA's N, at most
 constexpr int kTcwTileRows = 32;    // row-stage tile rows
+constexpr int kTcwTilesPerItem = 4; // row-stage tiles per item (blocks sharing their inputs)
+constexpr int kTcwMaskShift = 24;   // segment ncols: bits 0..23 columns, 24..27 block mask, 28 format
 // Segment formats of the wide tensor-core layout (top bits of ncols).
 enum TcwFmt : int32_t { TF_HI = 0, TF_HILO = 1 };
 
@@ -216,6 +217,7 @@ struct HostLayout {
   bool tcw = false;
   bool tcw_bf16 = false;          // 16-bit format of the stored pairs and the input planes
   std::vector<float> tscale;      // per V-stage panel row 2^-c, then per y row the row scale s_i
+  std::vector<int32_t> tblocks;   // per item: rows of blocks 0..3, 8 bits each
   int32_t tscale_rows0 = 0;       // index of y row 0 in tscale
 };
 

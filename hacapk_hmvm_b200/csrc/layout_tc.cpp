@@ -38,7 +38,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <queue>
+#include <tuple>
 #include <unordered_map>
 #include <utility>
 
@@ -67,39 +69,22 @@ inline double pow2_for_max(double m) {
   return std::ldexp(1.0, ceil_log2(m) - 15);
 }
 
-struct TcPart {  // one part of a row-stage segment's columns
-  int32_t leaf;   // dense leaf, or -1 for a low-rank row group
-  int32_t group;  // row group when leaf < 0
-  int32_t fmt;    // its columns' format (low-rank)
-  int32_t ncols;
+// A segment of an item: an input range (x columns, or t slots) multiplied by
+// the blocks in its mask.  kind 0: V rows (V stage); 1: a dense leaf per block
+// (row stage); 2: the low-rank columns of one format of a row group (row stage).
+struct TcSeg2 {
+  int32_t src = 0, ncols = 0, fmt = 0, mask = 0, kind = 0, group = -1;
+  int32_t leaf[4] = {-1, -1, -1, -1};
 };
 
-struct TcSeg {
-  int32_t src, ncols, fmt;
-  int32_t part_first, nparts;  // row stage
-};
-
-struct TcTile {
+struct TcItem {
   int32_t stage = 2;
-  int32_t row0 = 0, nrows = 0;  // row stage: rows; V stage: panel rows
-  int32_t panel_row0 = 0;       // V stage: first entry in panel_rows
-  int32_t seg_first = 0, nseg = 0;
-  int64_t nvec = 0;
+  int32_t nblk = 0;
+  int32_t R[4] = {0, 0, 0, 0};  // rows per block
+  int32_t row0 = 0;             // row stage: first y row (blocks are consecutive rows)
+  int32_t panel_row0 = 0;       // V stage: first entry in panel_rows (blocks consecutive)
+  std::vector<TcSeg2> segs;
 };
-
-inline int64_t seg_vectors(int32_t ncols, int fmt) { return (int64_t)((ncols + 7) / 8) * (fmt == TF_HILO ? 2 : 1); }
-
-// Byte offset, within a segment of `ncols` columns stored K-step-major for R
-// rows, of element (row r, column c), hi (lo = false) or lo part.
-inline int64_t tc_elem_off(int32_t ncols, int fmt, int32_t R, int32_t r, int32_t c, bool lo) {
-  const int h = fmt == TF_HILO ? 2 : 1;
-  const int32_t nv = (ncols + 7) / 8;
-  const int32_t j = c >> 4, u = (c >> 3) & 1, e = c & 7;
-  const int32_t nvj = std::min(2, nv - 2 * j);
-  int64_t off = (int64_t)j * 2 * h * R * 16 + (int64_t)u * R * 16 + (int64_t)r * 16 + e * 2;
-  if (lo) off += (int64_t)nvj * R * 16;
-  return off;
-}
 
 }  // namespace
 
@@ -267,46 +252,64 @@ int build_tc_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms
     }
     L.t_len = t_len;
 
-    // ---- V stage: panels of <= 128 rows per (column group, format) -------------------
-    std::vector<TcTile> tb;
-    std::vector<TcSeg> sb;
-    std::vector<TcPart> parts;
-    std::vector<std::pair<int32_t, int32_t>> panel_rows;  // (leaf, k)
+    // ---- items: row blocks sharing their input loads --------------------------------
+    // An item is up to 4 row blocks (V stage: panels of one column group, the
+    // pair-stored rows in a block of <= 64, the others in blocks of <= 128;
+    // row stage: up to 4 consecutive row tiles of <= 32 rows).  Its segments
+    // carry a block mask: a segment's K-step streams its input once and
+    // multiplies every block in the mask by it (one MMA group per block), and
+    // consecutive segments with the same input range share the input too.
+    std::vector<TcItem> titems;
+    std::vector<std::pair<int32_t, int32_t>> panel_rows;  // (leaf, k) per V-stage output row
     for (int32_t c = 0; c < (int32_t)cg_members.size(); c++) {
       const auto &mem = cg_members[c];
       const int32_t ndt = lt.ndt[mem[0]], st = lt.nstrtt[mem[0]];
-      for (int fm = TF_HILO; fm >= TF_HI; fm--) {
-        std::vector<std::pair<int32_t, int32_t>> rows;
-        for (int32_t i : mem)
-          for (int32_t k = 0; k < lt.kt[i]; k++)
-            if (col_fmt[colbase[i] + k] == fm) rows.emplace_back(i, k);
-        const int32_t npanels = (int32_t)((rows.size() + kTcwPanelRows - 1) / kTcwPanelRows);
-        for (int32_t p = 0; p < npanels; p++) {
-          // even split so no panel is a sliver
-          const size_t a = rows.size() * p / npanels, e = rows.size() * (p + 1) / npanels;
-          TcTile t;
-          t.stage = 1;
-          t.nrows = (int32_t)(e - a);
-          t.panel_row0 = (int32_t)panel_rows.size();
-          for (size_t r = a; r < e; r++) {
-            const auto lk = rows[r];
+      std::vector<std::pair<int32_t, int32_t>> rows[2];  // by format
+      for (int32_t i : mem)
+        for (int32_t k = 0; k < lt.kt[i]; k++) rows[col_fmt[colbase[i] + k]].emplace_back(i, k);
+      // blocks: pair rows in blocks of <= 64 (a K step of 64 pair rows is 4 KiB), the others <= 128
+      std::vector<std::pair<int, std::vector<std::pair<int32_t, int32_t>>>> blocks[2];
+      for (int fm = 0; fm < 2; fm++) {
+        const size_t cap = fm == TF_HILO ? 64 : 128;
+        const size_t nb = (rows[fm].size() + cap - 1) / cap;
+        for (size_t q = 0; q < nb; q++) {
+          const size_t b0 = rows[fm].size() * q / nb, b1 = rows[fm].size() * (q + 1) / nb;
+          blocks[fm].emplace_back(fm, std::vector<std::pair<int32_t, int32_t>>(rows[fm].begin() + b0,
+                                                                               rows[fm].begin() + b1));
+        }
+      }
+      // pair one block of each format per item (a K step: <= 4 + 4 KiB); the rest alone
+      const size_t nit = std::max(blocks[0].size(), blocks[1].size());
+      for (size_t q = 0; q < nit; q++) {
+        TcItem t;
+        t.stage = 1;
+        t.panel_row0 = (int32_t)panel_rows.size();
+        for (int fm = TF_HILO; fm >= TF_HI; fm--) {
+          if (q >= blocks[fm].size()) continue;
+          const auto &blk = blocks[fm][q].second;
+          const int b = t.nblk++;
+          t.R[b] = (int32_t)blk.size();
+          for (const auto &lk : blk) {
             const int64_t f = colbase[lk.first] + lk.second;
             L.out_idx.push_back((int32_t)slot_of_col[f]);
             L.tscale.push_back((float)(1.0 / csc[f]));
             panel_rows.push_back(lk);
           }
-          t.seg_first = (int32_t)sb.size();
-          t.nseg = 1;
-          sb.push_back(TcSeg{st - 1, ndt, fm, -1, 0});
-          t.nvec = seg_vectors(ndt, fm);
-          tb.push_back(t);
+          TcSeg2 sg;
+          sg.src = st - 1;
+          sg.ncols = ndt;
+          sg.fmt = fm;
+          sg.mask = 1 << b;
+          sg.kind = 0;
+          t.segs.push_back(sg);
         }
+        titems.push_back(std::move(t));
       }
     }
-    const int32_t n1 = (int32_t)tb.size();
+    const int32_t n1 = (int32_t)titems.size();
     L.tscale_rows0 = (int32_t)L.tscale.size();
 
-    // ---- row stage: tiles with their dense and low-rank segments ---------------------
+    // ---- row stage: items of up to 4 consecutive row tiles -------------------------------
     std::vector<int32_t> dcount(nrt + 1, 0), gcount(nrt + 1, 0);
     for (int32_t i = 0; i < nlf; i++) {
       if (lt.ltmtx[i] != 2 || lt.ndl[i] <= 0 || lt.ndt[i] <= 0) continue;
@@ -336,73 +339,73 @@ int build_tc_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms
         for (int32_t ti = row_tile[r0]; ti < nrt && trow0[ti] < r1; ti++) glist[gpos[ti]++] = g;
       }
     }
-    for (int32_t ti = 0; ti < nrt; ti++) {
-      TcTile t;
+    for (int32_t t0 = 0; t0 < nrt; t0 += kTcwTilesPerItem) {
+      TcItem t;
       t.stage = 2;
-      t.row0 = trow0[ti];
-      t.nrows = tnrows[ti];
-      t.seg_first = (int32_t)sb.size();
-      for (int32_t d = dcount[ti]; d < dcount[ti + 1]; d++) {
-        const int32_t i = dlist[d];
-        const int32_t src = lt.nstrtt[i] - 1;
-        if (t.nseg > 0) {
-          TcSeg &last = sb.back();
-          if (last.src >= 0 && last.src + last.ncols == src) {  // column-adjacent dense leaves merge
-            last.ncols += lt.ndt[i];
-            last.nparts++;
-            parts.push_back(TcPart{i, -1, TF_HILO, lt.ndt[i]});
-            continue;
+      t.row0 = trow0[t0];
+      std::map<std::tuple<int32_t, int32_t, int32_t>, size_t> index;  // (src, ncols, fmt) -> segment
+      for (int32_t ti = t0; ti < std::min(nrt, t0 + kTcwTilesPerItem); ti++) {
+        const int b = t.nblk++;
+        t.R[b] = tnrows[ti];
+        auto add = [&](int32_t src, int32_t nc, int32_t fm, int kind, int32_t leaf, int32_t group) {
+          const auto key = std::make_tuple(src, nc, fm);
+          auto it = index.find(key);
+          if (it == index.end()) {
+            TcSeg2 sg;
+            sg.src = src;
+            sg.ncols = nc;
+            sg.fmt = fm;
+            sg.mask = 0;
+            sg.kind = kind;
+            sg.group = group;
+            it = index.emplace(key, t.segs.size()).first;
+            t.segs.push_back(sg);
+          }
+          TcSeg2 &sg = t.segs[it->second];
+          sg.mask |= 1 << b;
+          sg.leaf[b] = leaf;
+        };
+        for (int32_t d = dcount[ti]; d < dcount[ti + 1]; d++) {
+          const int32_t i = dlist[d];
+          add(lt.nstrtt[i] - 1, lt.ndt[i], TF_HILO, 1, i, -1);
+        }
+        for (int32_t gg = gcount[ti]; gg < gcount[ti + 1]; gg++) {
+          const int32_t g = glist[gg];
+          for (int fm = TF_HILO; fm >= TF_HI; fm--) {
+            const int32_t k = rg_k[(size_t)g * 2 + fm];
+            if (k > 0) add(kTFlagTc | rg_slot[(size_t)g * 2 + fm], k, fm, 2, -1, g);
           }
         }
-        sb.push_back(TcSeg{src, lt.ndt[i], TF_HILO, (int32_t)parts.size(), 1});
-        parts.push_back(TcPart{i, -1, TF_HILO, lt.ndt[i]});
-        t.nseg++;
       }
-      for (int32_t gg = gcount[ti]; gg < gcount[ti + 1]; gg++) {
-        const int32_t g = glist[gg];
-        for (int fm = TF_HILO; fm >= TF_HI; fm--) {
-          const int32_t k = rg_k[(size_t)g * 2 + fm];
-          if (k == 0) continue;
-          sb.push_back(TcSeg{kTFlagTc | rg_slot[(size_t)g * 2 + fm], k, fm, (int32_t)parts.size(), 1});
-          parts.push_back(TcPart{-1, g, fm, k});
-          t.nseg++;
-        }
-      }
-      for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) t.nvec += seg_vectors(sb[s].ncols, sb[s].fmt);
-      tb.push_back(t);
+      // input order: x segments by column, then t segments by slot (segments with one input range adjacent)
+      std::stable_sort(t.segs.begin(), t.segs.end(), [](const TcSeg2 &x, const TcSeg2 &y) {
+        const uint32_t ax = (uint32_t)x.src, ay = (uint32_t)y.src;
+        return ax != ay ? ax < ay : x.ncols < y.ncols;
+      });
+      titems.push_back(std::move(t));
     }
-    const int32_t ntb = (int32_t)tb.size();
+    const int32_t ntb = (int32_t)titems.size();
 
-    // ---- row scales s_i: largest stored magnitude of each row -----------------------
+    // ---- row scales s_i: the largest stored magnitude of each row -----------------------
     std::vector<double> rowmax(nd > 0 ? nd : 1, 0.0);
-#pragma omp parallel for schedule(dynamic, 16)
-    for (int32_t k = n1; k < ntb; k++) {
-      const TcTile &t = tb[k];
-      for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++)
-        for (int32_t p = sb[s].part_first; p < sb[s].part_first + sb[s].nparts; p++) {
-          const TcPart &pt = parts[p];
-          if (pt.leaf >= 0) {
-            const int32_t i = pt.leaf, ndt = lt.ndt[i], rs = lt.nstrtl[i] - 1;
-            for (int32_t r = 0; r < t.nrows; r++) {
-              const int64_t src0 = lt.a1(i) + (int64_t)(t.row0 + r - rs) * ndt;
-              double m = rowmax[t.row0 + r];
-              for (int32_t c = 0; c < ndt; c++) m = std::max(m, std::fabs(get(src0 + c)));
-              rowmax[t.row0 + r] = m;
-            }
-          } else {
-            for (int32_t i : rg_members[pt.group]) {
-              const int32_t ndl = lt.ndl[i], rs = lt.nstrtl[i] - 1;
-              for (int32_t kk = 0; kk < lt.kt[i]; kk++) {
-                const int64_t f = colbase[i] + kk;
-                if (col_fmt[f] != pt.fmt) continue;
-                const double w = vsc[f] * csc[f];
-                const int64_t src0 = lt.a2(i) + (int64_t)kk * ndl + (t.row0 - rs);
-                for (int32_t r = 0; r < t.nrows; r++)
-                  rowmax[t.row0 + r] = std::max(rowmax[t.row0 + r], std::fabs(get(src0 + r) * w));
-              }
-            }
-          }
-        }
+    for (int32_t i = 0; i < nlf; i++) {
+      if (lt.ltmtx[i] != 2 || lt.ndl[i] <= 0 || lt.ndt[i] <= 0) continue;
+      const int32_t rs = lt.nstrtl[i] - 1, ndt = lt.ndt[i];
+      for (int32_t r = 0; r < lt.ndl[i]; r++) {
+        double m = rowmax[rs + r];
+        for (int32_t c = 0; c < ndt; c++) m = std::max(m, std::fabs(get(lt.a1(i) + (int64_t)r * ndt + c)));
+        rowmax[rs + r] = m;
+      }
+    }
+    for (int32_t i = 0; i < nlf; i++) {
+      if (!live_lr[i]) continue;
+      const int32_t rs = lt.nstrtl[i] - 1, ndl = lt.ndl[i];
+      for (int32_t kk = 0; kk < lt.kt[i]; kk++) {
+        const int64_t f = colbase[i] + kk;
+        const double w = vsc[f] * csc[f];
+        for (int32_t r = 0; r < ndl; r++)
+          rowmax[rs + r] = std::max(rowmax[rs + r], std::fabs(get(lt.a2(i) + (int64_t)kk * ndl + r) * w));
+      }
     }
     std::vector<double> rowsc(nd > 0 ? nd : 1, 1.0);
     for (int32_t r = 0; r < nd; r++) {
@@ -410,43 +413,60 @@ int build_tc_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms
       L.tscale.push_back((float)rowsc[r]);
     }
 
-    // ---- items ------------------------------------------------------------------------
-    int64_t stage_bytes[2] = {0, 0};
-    for (int32_t k = 0; k < ntb; k++) stage_bytes[k < n1 ? 0 : 1] += tb[k].nvec * tb[k].nrows * 16;
-    const int64_t cap1 = std::max<int64_t>(64 * 1024, stage_bytes[0] / std::max<int64_t>(1, (int64_t)L.num_sms * 4));
+    // ---- items cut into parts (V stage, large), costs ------------------------------------
+    auto item_records = [&](const TcItem &t, int32_t j0, int32_t j1) {  // 16-byte records of K steps [j0, j1)
+      int64_t n = 0;
+      for (const TcSeg2 &sg : t.segs) {
+        const int32_t c0 = 16 * j0, nc = std::min(sg.ncols - c0, 16 * (j1 - j0));
+        if (nc <= 0) continue;
+        const int64_t vec = (int64_t)((nc + 7) / 8) * (sg.fmt == TF_HILO ? 2 : 1);
+        for (int b = 0; b < 4; b++)
+          if (sg.mask >> b & 1) n += vec * t.R[b];
+      }
+      return n;
+    };
+    auto item_nks = [&](const TcItem &t) {
+      int32_t m = 0;
+      for (const TcSeg2 &sg : t.segs) m = std::max(m, (sg.ncols + 15) / 16);
+      return m;
+    };
+    int64_t stage_bytes = 0;
+    for (int32_t k = 0; k < n1; k++) stage_bytes += item_records(titems[k], 0, item_nks(titems[k])) * 16;
+    const int64_t cap1 = std::max<int64_t>(64 * 1024, stage_bytes / std::max<int64_t>(1, (int64_t)L.num_sms * 4));
     struct Item {
-      int32_t tile, j0, j1, mode, out_base;  // V stage: K steps [j0, j1) of the panel
+      int32_t tile, j0, j1, mode, out_base;
       int64_t cost;
     };
     std::vector<Item> items;
     std::vector<int32_t> tile_item0(ntb + 1);
     int64_t p_len = 0;
     for (int32_t k = 0; k < ntb; k++) {
-      const TcTile &t = tb[k];
+      const TcItem &t = titems[k];
       tile_item0[k] = (int32_t)items.size();
-      const int64_t bytes = t.nvec * t.nrows * 16;
+      const int32_t nks = item_nks(t);
+      const int64_t bytes = item_records(t, 0, nks) * 16;
       if (t.stage == 2) {
-        items.push_back(Item{k, 0, 0, 0, t.row0, bytes + 2048});
+        items.push_back(Item{k, 0, nks, 0, t.row0, bytes + 4096});
         continue;
       }
-      const TcSeg &sg = sb[t.seg_first];
-      const int32_t nks = (sg.ncols + 15) / 16;
       const int32_t nparts = (int32_t)std::min<int64_t>(nks, (bytes + cap1 - 1) / cap1);
       if (nparts <= 1) {
-        items.push_back(Item{k, 0, nks, 1, t.panel_row0, bytes + 2048});
+        items.push_back(Item{k, 0, nks, 1, t.panel_row0, bytes + 4096});
         continue;
       }
+      int32_t rows = 0;
+      for (int b = 0; b < t.nblk; b++) rows += t.R[b];
       const int64_t pb = p_len;
-      p_len += (int64_t)nparts * t.nrows;
-      for (int32_t r = 0; r < t.nrows; r++) {
+      p_len += (int64_t)nparts * rows;
+      for (int32_t r = 0; r < rows; r++) {
         L.red1.push_back(L.out_idx[t.panel_row0 + r]);
         L.red1.push_back((int32_t)(pb + r));
         L.red1.push_back(nparts);
-        L.red1.push_back(t.nrows);
+        L.red1.push_back(rows);
       }
       for (int32_t q = 0; q < nparts; q++) {
         const int32_t j0 = (int32_t)((int64_t)nks * q / nparts), j1 = (int32_t)((int64_t)nks * (q + 1) / nparts);
-        items.push_back(Item{k, j0, j1, 2, (int32_t)(pb + (int64_t)q * t.nrows), bytes * (j1 - j0) / nks + 2048});
+        items.push_back(Item{k, j0, j1, 2, (int32_t)(pb + (int64_t)q * rows), item_records(t, j0, j1) * 16 + 4096});
       }
     }
     tile_item0[ntb] = (int32_t)items.size();
@@ -493,114 +513,140 @@ int build_tc_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms
     L.stage1_tiles = ni1;
     L.stage2_tiles = ni2;
 
-    // ---- descriptors --------------------------------------------------------------------
+    // ---- descriptors ---------------------------------------------------------------------
     const int32_t nitems = (int32_t)items.size();
     L.tiles.resize(nitems);
+    L.tblocks.resize(nitems);
     L.segs.clear();
-    // by item index: data offset and vectors, and the item's first vector within its tile's packing
-    std::vector<int64_t> item_off(nitems), item_nvec(nitems), item_src_off(nitems);
+    std::vector<int64_t> item_off(nitems);  // by item index: first 16-byte record
     int64_t off = 0;
     for (int32_t k = 0; k < nitems; k++) {
       const Item &it = items[order[k]];
-      const TcTile &t = tb[it.tile];
+      const TcItem &t = titems[it.tile];
       hmvm_tile_desc &d = L.tiles[k];
       d.data_off = off;
       d.seg_begin = (int32_t)L.segs.size();
       d.out_base = it.out_base;
-      d.nrows = (int16_t)t.nrows;
-      d.mode = (int16_t)it.mode;
-      int64_t nvec = 0, src_off = 0;
-      if (t.stage == 1) {
-        const TcSeg &sg = sb[t.seg_first];
-        const int h = sg.fmt == TF_HILO ? 2 : 1;
-        const int32_t c0 = 16 * it.j0, nc = std::min(sg.ncols - c0, 16 * (it.j1 - it.j0));
-        L.segs.push_back(hmvm_seg_desc{sg.src + c0, nc | (sg.fmt << kSegTypeShift)});
-        d.nseg = 1;
-        nvec = (int64_t)((nc + 7) / 8) * h;
-        src_off = (int64_t)it.j0 * 2 * h;  // vectors before step j0
-        d._pad = t.panel_row0;             // tscale index of panel row 0
-      } else {
-        for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++)
-          L.segs.push_back(hmvm_seg_desc{sb[s].src, sb[s].ncols | (sb[s].fmt << kSegTypeShift)});
-        d.nseg = t.nseg;
-        nvec = t.nvec;
-        d._pad = L.tscale_rows0 + t.row0;  // tscale index of the tile's row 0
+      int32_t rows = 0, used = 0, packed = 0;
+      for (int b = 0; b < t.nblk; b++) {
+        rows += t.R[b];
+        packed |= t.R[b] << (8 * b);
       }
-      d.nvec = (int32_t)nvec;
+      int32_t nseg = 0;
+      for (const TcSeg2 &sg : t.segs) {
+        const int32_t c0 = 16 * it.j0, nc = std::min(sg.ncols - c0, 16 * (it.j1 - it.j0));
+        if (nc <= 0) continue;
+        if (nc >= (1 << kTcwMaskShift)) {
+          msg = "a segment of 2^24 or more columns";
+          return HMVM_ERANGE;
+        }
+        const int32_t src = sg.src < 0 ? (kTFlagTc | ((sg.src & 0x7fffffff) + c0)) : sg.src + c0;
+        L.segs.push_back(hmvm_seg_desc{src, nc | (sg.mask << kTcwMaskShift) | (sg.fmt << kSegTypeShift)});
+        used |= sg.mask;
+        nseg++;
+      }
+      d.nseg = nseg;
+      d.nrows = (int16_t)rows;
+      d.mode = (int16_t)(it.mode | (used << 4));
+      d._pad = t.stage == 1 ? t.panel_row0 : L.tscale_rows0 + t.row0;
+      const int64_t nrec = item_records(t, it.j0, it.j1);
+      d.nvec = (int32_t)nrec;
+      L.tblocks[k] = packed;
       item_off[order[k]] = off;
-      item_nvec[order[k]] = nvec;
-      item_src_off[order[k]] = src_off;
-      off += nvec * t.nrows;
+      off += nrec;
     }
     L.data.resize((size_t)off);
 
-    // ---- pack ---------------------------------------------------------------------------------
+    // ---- pack -------------------------------------------------------------------------------
+    // Per item part: per input group (consecutive segments with one input range),
+    // per K step, per segment, per block in its mask: the hi vectors of the step
+    // (R rows x 16 bytes each), then the lo vectors of a pair segment.
     int64_t stored_bytes = 0, stored_bytes1 = 0;
-#pragma omp parallel reduction(+ : stored_bytes, stored_bytes1)
-    {
-      std::vector<Vec16> buf;
-#pragma omp for schedule(dynamic, 4)
-      for (int32_t k = 0; k < ntb; k++) {
-        const TcTile &t = tb[k];
-        const int32_t R = t.nrows;
-        buf.assign((size_t)t.nvec * R, Vec16{{0, 0, 0, 0}});
-        char *base = reinterpret_cast<char *>(buf.data());
-        int64_t sbase = 0;  // byte offset of the current segment
-        for (int32_t s = t.seg_first; s < t.seg_first + t.nseg; s++) {
-          const TcSeg &sg = sb[s];
-          auto put = [&](int32_t r, int32_t c, double v) {
-            const uint16_t hi = enc(v);
-            std::memcpy(base + sbase + tc_elem_off(sg.ncols, sg.fmt, R, r, c, false), &hi, 2);
-            if (sg.fmt == TF_HILO) {
-              const uint16_t lo = enc(v - dec(hi));
-              std::memcpy(base + sbase + tc_elem_off(sg.ncols, sg.fmt, R, r, c, true), &lo, 2);
-            }
-          };
-          if (t.stage == 1) {
-            for (int32_t r = 0; r < R; r++) {
-              const auto lk = panel_rows[t.panel_row0 + r];
-              const int32_t i = lk.first, kk = lk.second;
-              const double inv = 1.0 / vsc[colbase[i] + kk];
-              const int64_t src0 = lt.a1(i) + (int64_t)kk * lt.ndt[i];
-              for (int32_t c = 0; c < sg.ncols; c++) put(r, c, get(src0 + c) * inv);
-            }
-          } else {
-            int32_t pc = 0;
-            for (int32_t p = sg.part_first; p < sg.part_first + sg.nparts; p++) {
-              const TcPart &pt = parts[p];
-              if (pt.leaf >= 0) {
-                const int32_t i = pt.leaf, ndt = lt.ndt[i], rs = lt.nstrtl[i] - 1;
-                for (int32_t r = 0; r < R; r++) {
-                  const double inv = 1.0 / rowsc[t.row0 + r];
-                  const int64_t src0 = lt.a1(i) + (int64_t)(t.row0 + r - rs) * ndt;
-                  for (int32_t c = 0; c < ndt; c++) put(r, pc + c, get(src0 + c) * inv);
-                }
-                pc += ndt;
-              } else {
-                int32_t kc = 0;
-                for (int32_t i : rg_members[pt.group]) {
-                  const int32_t ndl = lt.ndl[i], rs = lt.nstrtl[i] - 1;
-                  for (int32_t kk = 0; kk < lt.kt[i]; kk++) {
-                    const int64_t f = colbase[i] + kk;
-                    if (col_fmt[f] != pt.fmt) continue;
-                    const double w = vsc[f] * csc[f];
-                    const int64_t src0 = lt.a2(i) + (int64_t)kk * ndl + (t.row0 - rs);
-                    for (int32_t r = 0; r < R; r++) put(r, pc + kc, get(src0 + r) * w / rowsc[t.row0 + r]);
-                    kc++;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : stored_bytes, stored_bytes1)
+    for (int32_t q = 0; q < nitems; q++) {
+      const Item &it = items[q];
+      const TcItem &t = titems[it.tile];
+      char *base = reinterpret_cast<char *>(L.data.data() + item_off[q]);
+      int32_t brow[4] = {0, 0, 0, 0};  // first item row of each block
+      for (int b = 1; b < t.nblk; b++) brow[b] = brow[b - 1] + t.R[b - 1];
+      // the item's segments, trimmed to the part's K steps
+      struct PSeg {
+        const TcSeg2 *sg;
+        int32_t c0, nc;
+      };
+      std::vector<PSeg> ps;
+      for (const TcSeg2 &sg : t.segs) {
+        const int32_t c0 = 16 * it.j0, nc = std::min(sg.ncols - c0, 16 * (it.j1 - it.j0));
+        if (nc > 0) ps.push_back(PSeg{&sg, c0, nc});
+      }
+      // value of segment z, block b, block row r, (absolute) column c, scaled for 16-bit storage
+      // U segments: the (leaf, k) of each of its columns, looked up once
+      std::vector<std::vector<std::pair<int32_t, int32_t>>> ucols(ps.size());
+      for (size_t z = 0; z < ps.size(); z++) {
+        const TcSeg2 &sg = *ps[z].sg;
+        if (sg.kind != 2) continue;
+        for (int32_t i : rg_members[sg.group])
+          for (int32_t kk = 0; kk < lt.kt[i]; kk++)
+            if (col_fmt[colbase[i] + kk] == sg.fmt) ucols[z].emplace_back(i, kk);
+      }
+      auto val = [&](size_t z, int b, int32_t r, int32_t c) -> double {
+        const TcSeg2 &sg = *ps[z].sg;
+        if (sg.kind == 0) {  // V row (leaf, k) of the panel
+          const auto lk = panel_rows[t.panel_row0 + brow[b] + r];
+          const int64_t f = colbase[lk.first] + lk.second;
+          return get(lt.a1(lk.first) + (int64_t)lk.second * lt.ndt[lk.first] + c) / vsc[f];
+        }
+        if (sg.kind == 1) {  // dense leaf of block b
+          const int32_t i = sg.leaf[b], row = t.row0 + brow[b] + r;
+          return get(lt.a1(i) + (int64_t)(row - (lt.nstrtl[i] - 1)) * lt.ndt[i] + c) / rowsc[row];
+        }
+        const auto lk = ucols[z][c];
+        const int64_t f = colbase[lk.first] + lk.second;
+        const int32_t row = t.row0 + brow[b] + r, rs = lt.nstrtl[lk.first] - 1;
+        return get(lt.a2(lk.first) + (int64_t)lk.second * lt.ndl[lk.first] + (row - rs)) * vsc[f] * csc[f] /
+               rowsc[row];
+      };
+      int64_t pos = 0;
+      for (size_t g0 = 0; g0 < ps.size();) {
+        // the input group [g0, g1): consecutive segments with one (trimmed) input range, as the kernel groups them
+        auto same_input = [&](size_t u, size_t v) {
+          return ps[u].sg->src == ps[v].sg->src && ps[u].c0 == ps[v].c0 &&
+                 ps[u].nc == ps[v].nc;
+        };
+        size_t g1 = g0 + 1;
+        while (g1 < ps.size() && same_input(g1, g0)) g1++;
+        const int32_t nc = ps[g0].nc, nv = (nc + 7) / 8, nks = (nv + 1) / 2;
+        for (int32_t j = 0; j < nks; j++) {
+          const int32_t nvj = std::min(2, nv - 2 * j);
+          for (size_t z = g0; z < g1; z++) {
+            const TcSeg2 &sg = *ps[z].sg;
+            for (int b = 0; b < t.nblk; b++) {
+              if (!(sg.mask >> b & 1)) continue;
+              const int32_t R = t.R[b];
+              const int parts = sg.fmt == TF_HILO ? 2 : 1;
+              std::memset(base + pos, 0, (size_t)nvj * R * 16 * parts);
+              for (int32_t u = 0; u < nvj; u++)
+                for (int32_t e = 0; e < 8; e++) {
+                  const int32_t c = 16 * j + 8 * u + e;  // column within the part
+                  if (c >= nc) continue;
+                  for (int32_t r = 0; r < R; r++) {
+                    const double v = val(z, b, r, ps[z].c0 + c);
+                    const uint16_t hi = enc(v);
+                    std::memcpy(base + pos + ((int64_t)u * R + r) * 16 + e * 2, &hi, 2);
+                    if (parts == 2) {
+                      const uint16_t lo = enc(v - dec(hi));
+                      std::memcpy(base + pos + ((int64_t)(nvj + u) * R + r) * 16 + e * 2, &lo, 2);
+                    }
                   }
                 }
-                pc += kc;
-              }
+              pos += (int64_t)nvj * R * 16 * parts;
+              const int64_t sb = (int64_t)std::min(16, nc - 16 * j) * R * 2 * parts;
+              stored_bytes += sb;
+              if (t.stage == 1) stored_bytes1 += sb;
             }
           }
-          const int64_t sb_bytes = (int64_t)sg.ncols * R * 2 * (sg.fmt == TF_HILO ? 2 : 1);
-          stored_bytes += sb_bytes;
-          if (t.stage == 1) stored_bytes1 += sb_bytes;
-          sbase += seg_vectors(sg.ncols, sg.fmt) * R * 16;
         }
-        for (int32_t q = tile_item0[k]; q < tile_item0[k + 1]; q++)
-          std::memcpy(L.data.data() + item_off[q], buf.data() + (size_t)item_src_off[q] * R,
-                      (size_t)item_nvec[q] * R * sizeof(Vec16));
+        g0 = g1;
       }
     }
     L.stored_bytes = stored_bytes;

@@ -424,6 +424,9 @@ typedef struct hmvm_layout_view {
                                         tile), from tscale_rows0 on the row scale s_i of every y row */
   int64_t n_tscale;
   int32_t tscale_rows0, _pad_view;
+  const int32_t *tblocks;            /* [n_tiles]: rows of the item's row blocks 0..3, 8 bits each (block b's
+                                        rows follow block b-1's); segment ncols bits 24..27 select the blocks a
+                                        segment multiplies, and consecutive segments with one input range share it */
 } hmvm_layout_view;
 
 /* Tile and segment records as stored in the data structures above. */

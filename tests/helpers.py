@@ -351,45 +351,29 @@ def _split16(v, bf16: bool):
     return hi, lo
 
 
-def _tcw_decode(raw16, nc, fmt, R):
-    """The stored matrix of one K-step-major segment: (hi, lo) as float64
-    [R, nc] (lo is None for one-value segments)."""
-    nv = -(-nc // 8)
-    h = 2 if fmt else 1
-    hi_idx, lo_idx = [], []
-    for j in range(-(-nv // 2)):
-        nvj = min(2, nv - 2 * j)
-        base = j * 2 * h
-        hi_idx += [base + u for u in range(nvj)]
-        lo_idx += [base + nvj + u for u in range(nvj)]
-    vec = raw16.reshape(-1, R, 8)
-
-    def mat(idx):
-        m = vec[idx].transpose(1, 0, 2).reshape(R, len(idx) * 8)[:, :nc]
-        return m
-
-    return mat(hi_idx), (mat(lo_idx) if fmt else None)
-
-
 def emulate_tcw(view, X: np.ndarray) -> np.ndarray:
     """Y = H X (X: [nrhs, N], nrhs <= 128) for a wide tensor-core layout,
-    walking it as hmvm_tcw_kernel does: the inputs as scaled 16-bit hi/lo
-    planes, per K step hi*x_hi + hi*x_lo (+ lo*x_hi for pair segments), the
-    V-stage output scaled by 2^-c and split into planes, the row stage scaled
-    by s_i and sigma_x.  Products are summed in FP64 here (FP32 on the GPU)."""
+    walking its stream as hmvm_tcw_kernel does: per item, per input group
+    (consecutive segments with one input range), per K step of 16 columns, per
+    segment, per row block in the segment's mask, the block's hi vectors and
+    (pair segments) lo vectors; the inputs as scaled 16-bit hi/lo planes; per
+    K step hi*x_hi + hi*x_lo (+ lo*x_hi); the V-stage output scaled by 2^-c and
+    split into planes, the row stage scaled by s_i and sigma_x.  Products are
+    summed in FP64 here (FP32 on the GPU)."""
     from hacapk_hmvm_b200 import _lib
 
     bf = bool(view.tcw_bf16)
     tiles = np.ctypeslib.as_array((_lib.TileDesc * view.n_tiles).from_address(view.tiles)) if view.n_tiles else []
     segs = np.ctypeslib.as_array((_lib.SegDesc * view.n_segs).from_address(view.segs)) if view.n_segs else []
+    blocks = np.ctypeslib.as_array(view.tblocks, (view.n_tiles,)) if view.n_tiles else []
     raw = (np.ctypeslib.as_array((C.c_uint8 * (16 * view.data_vectors)).from_address(view.data))
            if view.data_vectors else np.zeros(0, np.uint8))
     vals = raw.view("<f2").astype(np.float64) if not bf else \
         (raw.view("<u2").astype(np.uint32) << 16).view("<f4").astype(np.float64)
+    vals = vals.reshape(-1, 8)  # one 16-byte record per row
     tscale = np.ctypeslib.as_array(view.tscale, (view.n_tscale,)).astype(np.float64) if view.n_tscale else np.zeros(0)
-    n_out = max([int(tiles[k]["out_base"]) + int(tiles[k]["nrows"]) for k in range(view.stage1_tiles)
-                 if tiles[k]["mode"] == 1] or [0])
-    out_idx = np.ctypeslib.as_array(view.out_idx, (n_out,)) if n_out else np.zeros(0, np.int32)
+    n1 = view.tscale_rows0
+    out_idx = np.ctypeslib.as_array(view.out_idx, (n1,)) if n1 else np.zeros(0, np.int32)
     X = np.asarray(X, dtype=np.float64)
     nr, nd = X.shape
     if bf:
@@ -404,31 +388,54 @@ def emulate_tcw(view, X: np.ndarray) -> np.ndarray:
     part = np.zeros((view.p_len + 1, nr))
     Y = np.full((nr, nd), np.nan)
 
-    def run_item(td):
-        R = int(td["nrows"])
-        v0 = int(td["data_off"]) * 8
-        acc = np.zeros((R, nr))
-        for s in range(int(td["seg_begin"]), int(td["seg_begin"]) + int(td["nseg"])):
-            src, enc = int(segs[s]["src"]), int(segs[s]["ncols"])
-            fmt, nc = (enc >> 28) & 1, enc & 0x0FFFFFFF
-            nvec = -(-nc // 8) * (2 if fmt else 1)
-            bh, bl = _tcw_decode(vals[v0:v0 + nvec * R * 8], nc, fmt, R)
-            v0 += nvec * R * 8
+    def run_item(k):
+        td = tiles[k]
+        R = [(int(blocks[k]) >> (8 * b)) & 0xFF for b in range(4)]
+        brow = np.cumsum([0] + R[:3])
+        acc = np.zeros((int(td["nrows"]), nr))
+        rec = int(td["data_off"])
+        s0, s1 = int(td["seg_begin"]), int(td["seg_begin"]) + int(td["nseg"])
+        s = s0
+        while s < s1:
+            g1 = s + 1
+            while g1 < s1 and segs[g1]["src"] == segs[s]["src"] and \
+                    (int(segs[g1]["ncols"]) & 0xFFFFFF) == (int(segs[s]["ncols"]) & 0xFFFFFF):
+                g1 += 1
+            src, nc = int(segs[s]["src"]), int(segs[s]["ncols"]) & 0xFFFFFF
             if src < 0:
                 r0 = src & 0x7FFFFFFF
                 ah, al = th[r0:r0 + nc], tl[r0:r0 + nc]
             else:
                 ah, al = xh[src:src + nc], xl[src:src + nc]
-            acc += bh @ ah + bh @ al
-            if fmt:
-                acc += bl @ ah
+            nv = -(-nc // 8)
+            for j in range(-(-nv // 2)):
+                nvj = min(2, nv - 2 * j)
+                c0, c1 = 16 * j, min(nc, 16 * j + 16)
+                for z in range(s, g1):
+                    enc = int(segs[z]["ncols"])
+                    mask, fmt = (enc >> 24) & 0xF, (enc >> 28) & 1
+                    for b in range(4):
+                        if not mask >> b & 1:
+                            continue
+                        Rb = R[b]
+                        h = vals[rec:rec + nvj * Rb].reshape(nvj, Rb, 8).transpose(1, 0, 2).reshape(Rb, 8 * nvj)
+                        rec += nvj * Rb
+                        bh = h[:, :c1 - c0]
+                        blk = acc[brow[b]:brow[b] + Rb]
+                        blk += bh @ ah[c0:c1] + bh @ al[c0:c1]
+                        if fmt:
+                            lo = vals[rec:rec + nvj * Rb].reshape(nvj, Rb, 8).transpose(1, 0, 2).reshape(Rb, 8 * nvj)
+                            rec += nvj * Rb
+                            blk += lo[:, :c1 - c0] @ ah[c0:c1]
+            s = g1
+        assert rec == int(td["data_off"]) + int(td["nvec"]), (k, rec)
         return acc
 
     for k in range(view.stage1_tiles):
         td = tiles[k]
         R, ob, sb = int(td["nrows"]), int(td["out_base"]), int(td["_pad"])
-        tv = (run_item(td) * tscale[sb:sb + R, None]).astype(np.float32)
-        if td["mode"] == 1:
+        tv = (run_item(k) * tscale[sb:sb + R, None]).astype(np.float32)
+        if int(td["mode"]) & 3 == 1:
             h, l = _split16(tv, bf)
             th[out_idx[ob:ob + R]] = h
             tl[out_idx[ob:ob + R]] = l
@@ -442,7 +449,7 @@ def emulate_tcw(view, X: np.ndarray) -> np.ndarray:
     for k in range(view.stage1_tiles, view.n_tiles):
         td = tiles[k]
         R, ob, sb = int(td["nrows"]), int(td["out_base"]), int(td["_pad"])
-        acc = run_item(td)
+        acc = run_item(k)
         Y[:, ob:ob + R] = (acc * tscale[sb:sb + R, None] * sig[None, :]).T
     return Y
 

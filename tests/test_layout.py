@@ -145,42 +145,59 @@ def test_invalid_leaf_tables_rejected():
 
 # ---- the wide tensor-core layout (FP32 / mixed plans with nrhs_max >= 32) -------------
 def _tcw_bounds(view):
-    """Every address hmvm_tcw_kernel and its helpers form stays inside its buffer."""
+    """Every address hmvm_tcw_kernel and its helpers form stays inside its
+    buffer, and every K step of an input group fits one 8 KiB ring chunk."""
     from hacapk_hmvm_b200 import _lib
 
     tiles = np.ctypeslib.as_array((_lib.TileDesc * view.n_tiles).from_address(view.tiles))
     segs = np.ctypeslib.as_array((_lib.SegDesc * view.n_segs).from_address(view.segs))
+    blocks = np.ctypeslib.as_array(view.tblocks, (view.n_tiles,))
     covered = np.zeros(view.data_vectors, np.int32)
     for k in range(view.n_tiles):
         td = tiles[k]
-        R, nv = int(td["nrows"]), int(td["nvec"])
-        assert 1 <= R <= (128 if k < view.stage1_tiles else 32)
-        off = int(td["data_off"])
-        assert 0 <= off and off + nv * R <= view.data_vectors
-        covered[off:off + nv * R] += 1
-        tot = 0
-        for s in range(int(td["seg_begin"]), int(td["seg_begin"]) + int(td["nseg"])):
-            src, enc = int(segs[s]["src"]), int(segs[s]["ncols"])
-            fmt, nc = (enc >> 28) & 1, enc & 0x0FFFFFFF
-            assert nc >= 1 and (enc >> 28) in (0, 1)
-            # a K step (<= 4 vectors of R rows) fits one 8 KiB ring chunk
-            assert 2 * R * 16 * (2 if fmt else 1) <= 8192
-            tot += -(-nc // 8) * (2 if fmt else 1)
-            if src < 0:
-                assert k >= view.stage1_tiles and (src & 0x7FFFFFFF) + nc <= view.t_len
-            else:
-                assert src + nc <= view.nd
-        assert tot == nv
-        pad = int(td["_pad"])
-        if k < view.stage1_tiles:
-            assert td["mode"] in (1, 2) and pad + R <= view.tscale_rows0
-            if td["mode"] == 1:
-                assert int(td["out_base"]) + R <= view.tscale_rows0
-            else:
-                assert int(td["out_base"]) + R <= view.p_len
+        stage1 = k < view.stage1_tiles
+        R = [(int(blocks[k]) >> (8 * b)) & 0xFF for b in range(4)]
+        nblk = sum(1 for r in R if r)
+        assert R[:nblk] == [r for r in R if r] and all(r <= (128 if stage1 else 32) for r in R)
+        assert nblk <= (2 if stage1 else 4)  # the kernel's TMEM geometry per stage
+        assert int(td["nrows"]) == sum(R) >= 1
+        off, nrec = int(td["data_off"]), int(td["nvec"])
+        assert 0 <= off and off + nrec <= view.data_vectors
+        covered[off:off + nrec] += 1
+        tot, used = 0, 0
+        s0, s1 = int(td["seg_begin"]), int(td["seg_begin"]) + int(td["nseg"])
+        s = s0
+        while s < s1:
+            g1 = s + 1
+            while g1 < s1 and segs[g1]["src"] == segs[s]["src"] and \
+                    (int(segs[g1]["ncols"]) & 0xFFFFFF) == (int(segs[s]["ncols"]) & 0xFFFFFF):
+                g1 += 1
+            nc = int(segs[s]["ncols"]) & 0xFFFFFF
+            step = 0  # bytes of a full K step of the group
+            for z in range(s, g1):
+                src, enc = int(segs[z]["src"]), int(segs[z]["ncols"])
+                mask, fmt = (enc >> 24) & 0xF, (enc >> 28) & 1
+                assert enc >> 29 == 0 and mask and all(R[b] for b in range(4) if mask >> b & 1)
+                used |= mask
+                rows = sum(R[b] for b in range(4) if mask >> b & 1)
+                step += 2 * rows * 16 * (2 if fmt else 1)
+                tot += -(-nc // 8) * (2 if fmt else 1) * rows
+                if src < 0:
+                    assert not stage1 and (src & 0x7FFFFFFF) + nc <= view.t_len
+                else:
+                    assert src + nc <= view.nd
+            assert step <= 8192
+            s = g1
+        assert tot == nrec
+        assert (int(td["mode"]) >> 4) == used
+        pad, nrows = int(td["_pad"]), int(td["nrows"])
+        mode = int(td["mode"]) & 3
+        if stage1:
+            assert mode in (1, 2) and pad + nrows <= view.tscale_rows0
+            assert int(td["out_base"]) + nrows <= (view.tscale_rows0 if mode == 1 else view.p_len)
         else:
-            assert td["mode"] == 0 and view.tscale_rows0 <= pad and pad + R <= view.n_tscale
-            assert int(td["out_base"]) + R <= view.nd
+            assert mode == 0 and view.tscale_rows0 <= pad and pad + nrows <= view.n_tscale
+            assert int(td["out_base"]) + nrows <= view.nd
     assert np.all(covered == 1)  # the items partition the stream
     n1 = view.tscale_rows0
     out_idx = np.ctypeslib.as_array(view.out_idx, (n1,)) if n1 else np.zeros(0, np.int32)
