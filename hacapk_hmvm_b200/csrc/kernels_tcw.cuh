@@ -64,6 +64,7 @@ constexpr int kTcwChunkSteps = 8; // K steps per chunk at most (< kTcwSlotsA)
 constexpr int kTcwSlotA = 8192;   // one K step of inputs: 4 chunks x 16 rows x 128 B
 constexpr int kTcwSlotsA = 14;
 static_assert(kTcwChunkSteps < kTcwSlotsA, "a chunk must hold fewer K steps than the input ring has slots");
+constexpr int kTcwGroupSegs = 4;  // segments of one input group, at most (the planner makes 1 or 2)
 constexpr int kTcwThreads = 192;
 constexpr int kTcwZeroBytes = 2048;  // 128 rows x 16 B of zeros
 constexpr int kTcwOffA = kTcwSlotsM * kTcwSlotM;
@@ -313,11 +314,31 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
           break;
         }
         tc_fence_after();
-        const uint32_t dcol = tmem_base + (uint32_t)(buf * G::cols);
+        // per block: instruction descriptor (N = rows rounded up to 16), accumulator columns, and a
+        // B descriptor with start address 0 (LBO = the block's 16-byte column stride)
+        uint32_t idb[4], dblk[4], rb16[4];
+        uint64_t bdb[4];
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+          const uint32_t Rb = (R4 >> (8 * b)) & 0xffu;
+          rb16[b] = Rb * 16u;
+          idb[b] = tcw_idesc(BF ? 1 : 0, max(16, (int)((Rb + 15) & ~15u)));
+          dblk[b] = tmem_base + (uint32_t)(buf * G::cols + b * G::bstride);
+          bdb[b] = tc_desc(0, Rb * 16u, 128);
+        }
         uint32_t started = 0;  // blocks whose accumulator holds a first product
         const int se = d.seg_begin + d.nseg;
         for (int s = d.seg_begin; s < se && ok;) {
           const TcwGroup gr = tcw_group(a.segs, s, se, R4);
+          // the group's segments (at most kTcwGroupSegs): block mask and pair flag each
+          const int nz = gr.s1 - s;
+          int zm[kTcwGroupSegs], zp[kTcwGroupSegs];
+#pragma unroll
+          for (int zz = 0; zz < kTcwGroupSegs; zz++) {
+            const int enc = zz < nz ? a.segs[s + zz].ncols : 0;
+            zm[zz] = (enc >> 24) & 15;
+            zp[zz] = (enc >> 28) & 1;
+          }
           for (int j = 0; j < gr.nks; j++) {
             const int nvj = min(2, gr.nv - 2 * j);
             const uint32_t kb = (uint32_t)nvj * 16u * (uint32_t)gr.hrows;
@@ -344,29 +365,28 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
             // A: chunks 0, 1 (hi) and 2, 3 (lo) of the slot; 64-rhs atoms 2 KiB apart, 8-row groups 1 KiB apart
             const uint64_t ah = adesc0 + (uint64_t)(as * (kTcwSlotA >> 4)), al = ah + (4096 >> 4);
             uint32_t off = cbase + used;
-            for (int z = s; z < gr.s1; z++) {
-              const int enc = a.segs[z].ncols;
-              const int mask = (enc >> 24) & 15, pair = (enc >> 28) & 1;
+            const bool two = nvj == 2;
+#pragma unroll
+            for (int zz = 0; zz < kTcwGroupSegs; zz++) {
 #pragma unroll
               for (int b = 0; b < 4; b++) {
-                if (!(mask >> b & 1)) continue;
-                const uint32_t Rb = (R4 >> (8 * b)) & 0xffu;
-                const uint32_t idesc = tcw_idesc(BF ? 1 : 0, max(16, (int)((Rb + 15) & ~15u)));
-                const uint32_t dblk = dcol + (uint32_t)(b * G::bstride);
+                if (!(zm[zz] >> b & 1)) continue;
+                // B: hi vectors at off, lo vectors nvj vectors on; an odd last step's second
+                // 8 columns read the zero block
                 uint64_t bh, bl;
-                const uint32_t blo = off + (uint32_t)nvj * Rb * 16u;
-                if (nvj == 2) {
-                  bh = tc_desc(off, Rb * 16u, 128);
-                  bl = tc_desc(blo, Rb * 16u, 128);
-                } else {  // an odd last step: the second 8 columns read the zero block
+                if (two) {
+                  bh = bdb[b] + (off >> 4);
+                  bl = bh + (rb16[b] >> 3);
+                } else {
                   bh = tc_desc(off, zaddr - off, 128);
-                  bl = tc_desc(blo, zaddr - blo, 128);
+                  bl = tc_desc(off + rb16[b], zaddr - off - rb16[b], 128);
                 }
-                tc_mma(dblk, ah, bh, idesc, (int)(started >> b & 1));
-                tc_mma(dblk, al, bh, idesc, 1);
-                if (pair) tc_mma(dblk, ah, bl, idesc, 1);
+                const int acc = (int)(started >> b & 1);
+                tc_mma(dblk[b], ah, bh, idb[b], acc);
+                tc_mma(dblk[b], al, bh, idb[b], 1);
+                if (zp[zz]) tc_mma(dblk[b], ah, bl, idb[b], 1);
                 started |= 1u << b;
-                off += (uint32_t)nvj * Rb * 16u * (pair ? 2u : 1u);
+                off += rb16[b] * (uint32_t)nvj * (zp[zz] ? 2u : 1u);
               }
             }
             tc_commit(&aempty[as]);

@@ -186,7 +186,7 @@ def _tcw_bounds(view):
                     assert not stage1 and (src & 0x7FFFFFFF) + nc <= view.t_len
                 else:
                     assert src + nc <= view.nd
-            assert step <= 8192
+            assert step <= 8192 and g1 - s <= 4  # a chunk and the kernel's kTcwGroupSegs
             s = g1
         assert tot == nrec
         assert (int(td["mode"]) >> 4) == used
