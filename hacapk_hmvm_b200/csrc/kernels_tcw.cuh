@@ -35,9 +35,10 @@
 //                        mbarrier.expect_tx and the chunk is closed by one
 //                        arrive), and a TMA tensor copy of the K step's inputs
 //                        into a 14 x 8 KiB ring;
-//   warp 1 (one thread)  allocates TMEM, issues the MMAs, commits each input
-//                        slot, matrix chunk and finished accumulator to its
-//                        mbarrier;
+//   warp 1               allocates TMEM; lanes 0..3 issue the MMAs, lane b those
+//                        of row block b (each block's products in a fixed
+//                        order), and each commits its MMAs to the input slot,
+//                        matrix chunk and accumulator mbarriers (4 arrivals);
 //   warps 2..5           epilogue: tcgen05.ld the accumulators (warp w reads
 //                        lanes 32 (w % 4) ..), scale, and store t (16-bit
 //                        hi/lo chunks) or y (each thread 32 consecutive rows of
@@ -214,19 +215,20 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
+    // the MMA role is lanes 0..3 of warp 1, each committing its own MMAs: 4 arrivals
     for (int s = 0; s < kTcwSlotsM; s++) {
       mbar_init(&mfull[s], 1);
-      mbar_init(&mempty[s], 1);
+      mbar_init(&mempty[s], 4);
     }
     for (int s = 0; s < kTcwSlotsA; s++) {
       mbar_init(&afull[s], 1);
-      mbar_init(&aempty[s], 1);
+      mbar_init(&aempty[s], 4);
     }
     for (int s = 0; s < G::bufs; s++) {
-      mbar_init(&accfull[s], 1);
+      mbar_init(&accfull[s], 4);
       mbar_init(&accempty[s], 4);
     }
-    mbar_init(done, 1);
+    mbar_init(done, 4);
     for (int k = 1; k < 5; k++) misc[k] = 0;
     fence_mbar_init();
   }
@@ -297,8 +299,9 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
       if (!ok) atomicExch(a.err, 1);
     }
   } else if (warp == 1) {
-    // ---- MMA issue ----
-    if (lane == 0) {
+    // ---- MMA issue: lane b < 4 issues the MMAs of row block b ----
+    if (lane < 4) {
+      const uint32_t bl4 = (uint32_t)lane;
       uint32_t mC = 0, aC = 0, ic = 0, used = 0, cnt = 0, cbase = 0;
       int ms = 0;
       bool ok = true, open = false;
@@ -309,43 +312,46 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
         const hmvm_tile_desc d = a.tiles[it];
         const uint32_t R4 = (uint32_t)a.blocks[it];
         const int buf = ic % G::bufs;
-        if (ic >= G::bufs && !thread_wait(&accempty[buf], ((ic / G::bufs) - 1) & 1)) {
+        if (ic >= G::bufs && !thread_wait(&accempty[buf], ((ic / G::bufs) - 1) & 1)) ok = false;
+        if (!__all_sync(0xfu, ok)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        // per block: instruction descriptor (N = rows rounded up to 16), accumulator columns, and a
-        // B descriptor with start address 0 (LBO = the block's 16-byte column stride)
-        uint32_t idb[4], dblk[4], rb16[4];
-        uint64_t bdb[4];
-#pragma unroll
-        for (int b = 0; b < 4; b++) {
-          const uint32_t Rb = (R4 >> (8 * b)) & 0xffu;
-          rb16[b] = Rb * 16u;
-          idb[b] = tcw_idesc(BF ? 1 : 0, max(16, (int)((Rb + 15) & ~15u)));
-          dblk[b] = tmem_base + (uint32_t)(buf * G::cols + b * G::bstride);
-          bdb[b] = tc_desc(0, Rb * 16u, 128);
-        }
-        uint32_t started = 0;  // blocks whose accumulator holds a first product
+        // this lane's block: rows, instruction descriptor (N = rows rounded up to 16), accumulator
+        // columns, and its B descriptor with start address 0 (LBO = its 16-byte column stride)
+        const uint32_t Rb = (R4 >> (8 * bl4)) & 0xffu, rb16 = Rb * 16u;
+        const uint32_t idb = tcw_idesc(BF ? 1 : 0, max(16, (int)((Rb + 15) & ~15u)));
+        const uint32_t dblk = tmem_base + (uint32_t)(buf * G::cols) + bl4 * (uint32_t)G::bstride;
+        const uint64_t bdb = tc_desc(0, rb16, 128);
+        int started = 0;  // this block's accumulator holds a first product
         const int se = d.seg_begin + d.nseg;
         for (int s = d.seg_begin; s < se && ok;) {
           const TcwGroup gr = tcw_group(a.segs, s, se, R4);
-          // the group's segments (at most kTcwGroupSegs): block mask and pair flag each
+          // per segment of the group (at most kTcwGroupSegs): whether it multiplies this block,
+          // pair-stored or not, and where this block's vectors start within a K step (in units
+          // of nvj x 16 bytes: the rows before it in stream order, pair rows counted twice)
           const int nz = gr.s1 - s;
-          int zm[kTcwGroupSegs], zp[kTcwGroupSegs];
+          int zact[kTcwGroupSegs], zpair[kTcwGroupSegs];
+          uint32_t zpre[kTcwGroupSegs];
+          uint32_t pre = 0;
 #pragma unroll
           for (int zz = 0; zz < kTcwGroupSegs; zz++) {
             const int enc = zz < nz ? a.segs[s + zz].ncols : 0;
-            zm[zz] = (enc >> 24) & 15;
-            zp[zz] = (enc >> 28) & 1;
+            const uint32_t mask = (uint32_t)(enc >> 24) & 15u, h = (enc >> 28) & 1 ? 2u : 1u;
+            zact[zz] = (int)(mask >> bl4 & 1u);
+            zpair[zz] = (enc >> 28) & 1;
+            zpre[zz] = pre + h * (uint32_t)tcw_mask_rows((int)(mask & ((1u << bl4) - 1u)), R4);
+            pre += h * (uint32_t)tcw_mask_rows((int)mask, R4);
           }
           for (int j = 0; j < gr.nks; j++) {
-            const int nvj = min(2, gr.nv - 2 * j);
-            const uint32_t kb = (uint32_t)nvj * 16u * (uint32_t)gr.hrows;
+            const uint32_t nvj = (uint32_t)min(2, gr.nv - 2 * j);
+            const uint32_t kb = nvj * 16u * (uint32_t)gr.hrows;
             if (!open || used + kb > (uint32_t)kTcwSlotM || cnt == kTcwChunkSteps) {
               if (open) tc_commit(&mempty[ms]);  // its MMAs done, the chunk can be refilled
               ms = mC % kTcwSlotsM;
-              if (!thread_wait(&mfull[ms], (mC / kTcwSlotsM) & 1)) {
+              if (!thread_wait(&mfull[ms], (mC / kTcwSlotsM) & 1)) ok = false;
+              if (!__all_sync(0xfu, ok)) {
                 ok = false;
                 open = false;
                 break;
@@ -356,38 +362,32 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
               cbase = smem_u32(ringM + ms * kTcwSlotM);
             }
             const int as = aC % kTcwSlotsA;
-            if (!thread_wait(&afull[as], (aC / kTcwSlotsA) & 1)) {
+            if (!thread_wait(&afull[as], (aC / kTcwSlotsA) & 1)) ok = false;
+            if (!__all_sync(0xfu, ok)) {
               ok = false;
               break;
             }
             aC++;
-            tc_fence_after();
             // A: chunks 0, 1 (hi) and 2, 3 (lo) of the slot; 64-rhs atoms 2 KiB apart, 8-row groups 1 KiB apart
             const uint64_t ah = adesc0 + (uint64_t)(as * (kTcwSlotA >> 4)), al = ah + (4096 >> 4);
-            uint32_t off = cbase + used;
-            const bool two = nvj == 2;
 #pragma unroll
             for (int zz = 0; zz < kTcwGroupSegs; zz++) {
-#pragma unroll
-              for (int b = 0; b < 4; b++) {
-                if (!(zm[zz] >> b & 1)) continue;
-                // B: hi vectors at off, lo vectors nvj vectors on; an odd last step's second
-                // 8 columns read the zero block
-                uint64_t bh, bl;
-                if (two) {
-                  bh = bdb[b] + (off >> 4);
-                  bl = bh + (rb16[b] >> 3);
-                } else {
-                  bh = tc_desc(off, zaddr - off, 128);
-                  bl = tc_desc(off + rb16[b], zaddr - off - rb16[b], 128);
-                }
-                const int acc = (int)(started >> b & 1);
-                tc_mma(dblk[b], ah, bh, idb[b], acc);
-                tc_mma(dblk[b], al, bh, idb[b], 1);
-                if (zp[zz]) tc_mma(dblk[b], ah, bl, idb[b], 1);
-                started |= 1u << b;
-                off += rb16[b] * (uint32_t)nvj * (zp[zz] ? 2u : 1u);
+              if (!zact[zz]) continue;
+              // B: this block's hi vectors, then (pair segments) its lo vectors nvj vectors on; an odd
+              // last step's second 8 columns read the zero block
+              const uint32_t off = cbase + used + nvj * 16u * zpre[zz];
+              uint64_t bh, bl;
+              if (nvj == 2) {
+                bh = bdb + (off >> 4);
+                bl = bh + (rb16 >> 3);
+              } else {
+                bh = tc_desc(off, zaddr - off, 128);
+                bl = tc_desc(off + rb16, zaddr - off - rb16, 128);
               }
+              tc_mma(dblk, ah, bh, idb, started);
+              tc_mma(dblk, al, bh, idb, 1);
+              if (zpair[zz]) tc_mma(dblk, ah, bl, idb, 1);
+              started = 1;
             }
             tc_commit(&aempty[as]);
             used += kb;
@@ -398,8 +398,10 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
         if (ok) tc_commit(&accfull[buf]);
       }
       if (open) tc_commit(&mempty[ms]);
-      misc[3] = mC;
-      misc[4] = aC;
+      if (lane == 0) {
+        misc[3] = mC;
+        misc[4] = aC;
+      }
       // every MMA issued has completed before the CTA goes on (bounded)
       tc_commit(done);
       if (!thread_wait(done, 0)) ok = false;
