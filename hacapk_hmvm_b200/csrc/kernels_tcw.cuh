@@ -35,10 +35,10 @@
 //                        mbarrier.expect_tx and the chunk is closed by one
 //                        arrive), and a TMA tensor copy of the K step's inputs
 //                        into a 14 x 8 KiB ring;
-//   warp 1               allocates TMEM; lanes 0..3 issue the MMAs, lane b those
-//                        of row block b (each block's products in a fixed
-//                        order), and each commits its MMAs to the input slot,
-//                        matrix chunk and accumulator mbarriers (4 arrivals);
+//   warp 1 (one thread)  allocates TMEM, issues the MMAs (per input group a
+//                        packed list of at most 4 block jobs), commits each
+//                        input slot, matrix chunk and finished accumulator to
+//                        its mbarrier;
 //   warps 2..5           epilogue: tcgen05.ld the accumulators (warp w reads
 //                        lanes 32 (w % 4) ..), scale, and store t (16-bit
 //                        hi/lo chunks) or y (each thread 32 consecutive rows of
@@ -65,12 +65,12 @@ constexpr int kTcwChunkSteps = 8; // K steps per chunk at most (< kTcwSlotsA)
 constexpr int kTcwSlotA = 8192;   // one K step of inputs: 4 chunks x 16 rows x 128 B
 constexpr int kTcwSlotsA = 14;
 static_assert(kTcwChunkSteps < kTcwSlotsA, "a chunk must hold fewer K steps than the input ring has slots");
-constexpr int kTcwGroupSegs = 4;  // segments of one input group, at most (the planner makes 1 or 2)
 constexpr int kTcwThreads = 192;
 constexpr int kTcwZeroBytes = 2048;  // 128 rows x 16 B of zeros
 constexpr int kTcwOffA = kTcwSlotsM * kTcwSlotM;
 constexpr int kTcwOffZero = kTcwOffA + kTcwSlotsA * kTcwSlotA;
-constexpr int kTcwOffBar = kTcwOffZero + kTcwZeroBytes;
+constexpr int kTcwOffRec = kTcwOffZero + kTcwZeroBytes;  // one 16-byte K-step record per input slot
+constexpr int kTcwOffBar = kTcwOffRec + kTcwSlotsA * 16;
 constexpr int kTcwNumBars = 2 * kTcwSlotsM + 2 * kTcwSlotsA + 2 * 4 + 1;
 constexpr int kTcwOffMisc = kTcwOffBar + kTcwNumBars * 8;
 constexpr int kTcwSmem = kTcwOffMisc + 32 + 1024;  // + room to align the base to 1 KiB
@@ -215,20 +215,19 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
-    // the MMA role is lanes 0..3 of warp 1, each committing its own MMAs: 4 arrivals
     for (int s = 0; s < kTcwSlotsM; s++) {
       mbar_init(&mfull[s], 1);
-      mbar_init(&mempty[s], 4);
+      mbar_init(&mempty[s], 1);
     }
     for (int s = 0; s < kTcwSlotsA; s++) {
       mbar_init(&afull[s], 1);
-      mbar_init(&aempty[s], 4);
+      mbar_init(&aempty[s], 1);
     }
     for (int s = 0; s < G::bufs; s++) {
-      mbar_init(&accfull[s], 4);
+      mbar_init(&accfull[s], 1);
       mbar_init(&accempty[s], 4);
     }
-    mbar_init(done, 4);
+    mbar_init(done, 1);
     for (int k = 1; k < 5; k++) misc[k] = 0;
     fence_mbar_init();
   }
@@ -250,7 +249,14 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
 
   if (warp == 0) {
     // ---- producer ----
+    // Per K step: the matrix bytes into the current chunk, the inputs into an
+    // input slot, and beside that slot a 16-byte record for the MMA thread (written
+    // before the slot's arrive, which publishes it): the step's MMA jobs (up to 4
+    // x 14 bits: block, pair-stored, the block's first vector in units of
+    // nvj x 16 bytes), its offset in its chunk, flags (starts a chunk, the item's
+    // last step, two 8-column vectors), the job count and the item's block rows.
     if (lane == 0 && tb < te) {
+      uint4* rec = reinterpret_cast<uint4*>(tcw_smem + kTcwOffRec);
       uint32_t mI = 0, aI = 0, used = 0, cnt = 0;
       int ms = 0;
       bool ok = true, open = false;
@@ -262,8 +268,23 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
         for (int s = d.seg_begin; s < se && ok;) {
           const TcwGroup gr = tcw_group(a.segs, s, se, R4);
           const CUtensorMap* map = gr.tsrc ? &tmap : &xmap;
+          uint64_t jobs = 0;
+          uint32_t njob = 0, pre = 0;
+          for (int z = s; z < gr.s1; z++) {
+            const int enc = a.segs[z].ncols;
+            const uint32_t mask = (uint32_t)(enc >> 24) & 15u, pair = (uint32_t)(enc >> 28) & 1u;
+            for (int b = 0; b < 4; b++) {
+              if (!(mask >> b & 1u)) continue;
+              if (njob < 4) jobs |= (uint64_t)((uint32_t)b | (pair << 2) | (pre << 3)) << (14 * njob);
+              njob++;
+              pre += ((R4 >> (8 * b)) & 0xffu) * (pair ? 2u : 1u);
+            }
+          }
+          const bool last_group = gr.s1 == se;
           for (int j = 0; j < gr.nks; j++) {
-            const uint32_t kb = (uint32_t)min(2, gr.nv - 2 * j) * 16u * (uint32_t)gr.hrows;
+            const uint32_t nvj = (uint32_t)min(2, gr.nv - 2 * j);
+            const uint32_t kb = nvj * 16u * (uint32_t)gr.hrows;
+            uint32_t flags = 0;
             if (!open || used + kb > (uint32_t)kTcwSlotM || cnt == kTcwChunkSteps) {
               if (open) mbar_arrive(&mfull[ms]);  // close the chunk
               ms = mI % kTcwSlotsM;
@@ -275,20 +296,24 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
               mI++;
               open = true;
               used = cnt = 0;
+              flags |= 1u << 16;
             }
             mbar_expect_tx_only(&mfull[ms], kb);
             bulk_g2s(ringM + ms * kTcwSlotM + used, g, kb, &mfull[ms]);
-            g += kb;
-            used += kb;
-            cnt++;
             const int as = aI % kTcwSlotsA;
             if (aI >= kTcwSlotsA && !thread_wait(&aempty[as], ((aI / kTcwSlotsA) - 1) & 1)) {
               ok = false;
               break;
             }
+            if (last_group && j + 1 == gr.nks) flags |= 1u << 17;
+            if (nvj == 2) flags |= 1u << 18;
+            rec[as] = make_uint4((uint32_t)jobs, (uint32_t)(jobs >> 32), used | flags | (njob << 19), R4);
             mbar_expect_tx(&afull[as], kTcwSlotA);
             tma_load_3d(ringA + as * kTcwSlotA, map, 0, gr.row0 + 16 * j, 0, &afull[as]);
             aI++;
+            g += kb;
+            used += kb;
+            cnt++;
           }
           s = gr.s1;
         }
@@ -299,109 +324,93 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
       if (!ok) atomicExch(a.err, 1);
     }
   } else if (warp == 1) {
-    // ---- MMA issue: lane b < 4 issues the MMAs of row block b ----
-    if (lane < 4) {
-      const uint32_t bl4 = (uint32_t)lane;
-      uint32_t mC = 0, aC = 0, ic = 0, used = 0, cnt = 0, cbase = 0;
+    // ---- MMA issue (one thread), driven by the producer's K-step records ----
+    if (lane == 0) {
+      const uint4* rec = reinterpret_cast<const uint4*>(tcw_smem + kTcwOffRec);
+      uint32_t mC = 0, aC = 0, ic = 0, cbase = 0;
       int ms = 0;
       bool ok = true, open = false;
       const uint32_t zaddr = smem_u32(zero);
       // descriptor of input slot 0's hi part; slot s is (8 KiB * s) >> 4 further on, its lo part 4 KiB on
       const uint64_t adesc0 = tc_desc_sw128(smem_u32(ringA), 2048, 1024);
       for (int it = tb; it < te && ok; it++, ic++) {
-        const hmvm_tile_desc d = a.tiles[it];
+        const int nseg = a.tiles[it].nseg;
         const uint32_t R4 = (uint32_t)a.blocks[it];
         const int buf = ic % G::bufs;
-        if (ic >= G::bufs && !thread_wait(&accempty[buf], ((ic / G::bufs) - 1) & 1)) ok = false;
-        if (!__all_sync(0xfu, ok)) {
+        if (ic >= G::bufs && !thread_wait(&accempty[buf], ((ic / G::bufs) - 1) & 1)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        // this lane's block: rows, instruction descriptor (N = rows rounded up to 16), accumulator
-        // columns, and its B descriptor with start address 0 (LBO = its 16-byte column stride)
-        const uint32_t Rb = (R4 >> (8 * bl4)) & 0xffu, rb16 = Rb * 16u;
-        const uint32_t idb = tcw_idesc(BF ? 1 : 0, max(16, (int)((Rb + 15) & ~15u)));
-        const uint32_t dblk = tmem_base + (uint32_t)(buf * G::cols) + bl4 * (uint32_t)G::bstride;
-        const uint64_t bdb = tc_desc(0, rb16, 128);
-        int started = 0;  // this block's accumulator holds a first product
-        const int se = d.seg_begin + d.nseg;
-        for (int s = d.seg_begin; s < se && ok;) {
-          const TcwGroup gr = tcw_group(a.segs, s, se, R4);
-          // per segment of the group (at most kTcwGroupSegs): whether it multiplies this block,
-          // pair-stored or not, and where this block's vectors start within a K step (in units
-          // of nvj x 16 bytes: the rows before it in stream order, pair rows counted twice)
-          const int nz = gr.s1 - s;
-          int zact[kTcwGroupSegs], zpair[kTcwGroupSegs];
-          uint32_t zpre[kTcwGroupSegs];
-          uint32_t pre = 0;
+        // per block (scalars, picked by block index): 16-byte column stride and instruction
+        // descriptor (N = rows rounded up to 16)
+        uint32_t rbs[4], ids[4];
 #pragma unroll
-          for (int zz = 0; zz < kTcwGroupSegs; zz++) {
-            const int enc = zz < nz ? a.segs[s + zz].ncols : 0;
-            const uint32_t mask = (uint32_t)(enc >> 24) & 15u, h = (enc >> 28) & 1 ? 2u : 1u;
-            zact[zz] = (int)(mask >> bl4 & 1u);
-            zpair[zz] = (enc >> 28) & 1;
-            zpre[zz] = pre + h * (uint32_t)tcw_mask_rows((int)(mask & ((1u << bl4) - 1u)), R4);
-            pre += h * (uint32_t)tcw_mask_rows((int)mask, R4);
+        for (int b = 0; b < 4; b++) {
+          const uint32_t Rb = (R4 >> (8 * b)) & 0xffu;
+          rbs[b] = Rb * 16u;
+          ids[b] = tcw_idesc(BF ? 1 : 0, max(16, (int)((Rb + 15) & ~15u)));
+        }
+        const uint32_t dbase = tmem_base + (uint32_t)(buf * G::cols);
+        uint32_t started = 0;  // blocks whose accumulator holds a first product
+        bool last = nseg == 0;
+        while (!last) {
+          const int as = aC % kTcwSlotsA;
+          if (!thread_wait(&afull[as], (aC / kTcwSlotsA) & 1)) {
+            ok = false;
+            break;
           }
-          for (int j = 0; j < gr.nks; j++) {
-            const uint32_t nvj = (uint32_t)min(2, gr.nv - 2 * j);
-            const uint32_t kb = nvj * 16u * (uint32_t)gr.hrows;
-            if (!open || used + kb > (uint32_t)kTcwSlotM || cnt == kTcwChunkSteps) {
-              if (open) tc_commit(&mempty[ms]);  // its MMAs done, the chunk can be refilled
-              ms = mC % kTcwSlotsM;
-              if (!thread_wait(&mfull[ms], (mC / kTcwSlotsM) & 1)) ok = false;
-              if (!__all_sync(0xfu, ok)) {
-                ok = false;
-                open = false;
-                break;
-              }
-              mC++;
-              open = true;
-              used = cnt = 0;
-              cbase = smem_u32(ringM + ms * kTcwSlotM);
-            }
-            const int as = aC % kTcwSlotsA;
-            if (!thread_wait(&afull[as], (aC / kTcwSlotsA) & 1)) ok = false;
-            if (!__all_sync(0xfu, ok)) {
+          aC++;
+          const uint4 r = rec[as];
+          const uint32_t fl = r.z;
+          last = (fl >> 17) & 1u;
+          if ((fl >> 16) & 1u) {  // the step starts a chunk
+            if (open) tc_commit(&mempty[ms]);  // the previous chunk's MMAs done: it can be refilled
+            ms = mC % kTcwSlotsM;
+            if (!thread_wait(&mfull[ms], (mC / kTcwSlotsM) & 1)) {
               ok = false;
+              open = false;
               break;
             }
-            aC++;
-            // A: chunks 0, 1 (hi) and 2, 3 (lo) of the slot; 64-rhs atoms 2 KiB apart, 8-row groups 1 KiB apart
-            const uint64_t ah = adesc0 + (uint64_t)(as * (kTcwSlotA >> 4)), al = ah + (4096 >> 4);
-#pragma unroll
-            for (int zz = 0; zz < kTcwGroupSegs; zz++) {
-              if (!zact[zz]) continue;
-              // B: this block's hi vectors, then (pair segments) its lo vectors nvj vectors on; an odd
-              // last step's second 8 columns read the zero block
-              const uint32_t off = cbase + used + nvj * 16u * zpre[zz];
-              uint64_t bh, bl;
-              if (nvj == 2) {
-                bh = bdb + (off >> 4);
-                bl = bh + (rb16 >> 3);
-              } else {
-                bh = tc_desc(off, zaddr - off, 128);
-                bl = tc_desc(off + rb16, zaddr - off - rb16, 128);
-              }
-              tc_mma(dblk, ah, bh, idb, started);
-              tc_mma(dblk, al, bh, idb, 1);
-              if (zpair[zz]) tc_mma(dblk, ah, bl, idb, 1);
-              started = 1;
-            }
-            tc_commit(&aempty[as]);
-            used += kb;
-            cnt++;
+            mC++;
+            open = true;
+            cbase = smem_u32(ringM + ms * kTcwSlotM);
           }
-          s = gr.s1;
+          tc_fence_after();  // the MMAs below are ordered after the waits that saw their operands land
+          // A: chunks 0, 1 (hi) and 2, 3 (lo) of the slot; 64-rhs atoms 2 KiB apart, 8-row groups 1 KiB apart
+          const uint64_t ah = adesc0 + (uint64_t)(as * (kTcwSlotA >> 4)), al = ah + (4096 >> 4);
+          const uint32_t kbase = cbase + (fl & 0xffffu), two = (fl >> 18) & 1u, nvj16 = two ? 32u : 16u;
+          const uint32_t njob = (fl >> 19) & 7u;
+          const uint64_t jobs = (uint64_t)r.x | ((uint64_t)r.y << 32);
+          for (uint32_t q = 0; q < njob; q++) {
+            const uint32_t f = (uint32_t)(jobs >> (14 * q)) & 0x3fffu;
+            const uint32_t b = f & 3u, pair = (f >> 2) & 1u;
+            const uint32_t rb16 = b == 0 ? rbs[0] : b == 1 ? rbs[1] : b == 2 ? rbs[2] : rbs[3];
+            const uint32_t idb = b == 0 ? ids[0] : b == 1 ? ids[1] : b == 2 ? ids[2] : ids[3];
+            const uint32_t dblk = dbase + b * (uint32_t)G::bstride;
+            // B: the block's hi vectors, then (pair segments) its lo vectors nvj vectors on; an
+            // odd last step's second 8 columns read the zero block
+            const uint32_t off = kbase + nvj16 * (f >> 3);
+            uint64_t bh, bl;
+            if (two) {
+              bh = tc_desc(off, rb16, 128);
+              bl = bh + (rb16 >> 3);
+            } else {
+              bh = tc_desc(off, zaddr - off, 128);
+              bl = tc_desc(off + rb16, zaddr - off - rb16, 128);
+            }
+            tc_mma(dblk, ah, bh, idb, (int)(started >> b & 1u));
+            tc_mma(dblk, al, bh, idb, 1);
+            if (pair) tc_mma(dblk, ah, bl, idb, 1);
+            started |= 1u << b;
+          }
+          tc_commit(&aempty[as]);
         }
         if (ok) tc_commit(&accfull[buf]);
       }
       if (open) tc_commit(&mempty[ms]);
-      if (lane == 0) {
-        misc[3] = mC;
-        misc[4] = aC;
-      }
+      misc[3] = mC;
+      misc[4] = aC;
       // every MMA issued has completed before the CTA goes on (bounded)
       tc_commit(done);
       if (!thread_wait(done, 0)) ok = false;

@@ -186,7 +186,8 @@ def _tcw_bounds(view):
                     assert not stage1 and (src & 0x7FFFFFFF) + nc <= view.t_len
                 else:
                     assert src + nc <= view.nd
-            assert step <= 8192 and g1 - s <= 4  # a chunk and the kernel's kTcwGroupSegs
+            jobs = sum(bin((int(segs[z]["ncols"]) >> 24) & 0xF).count("1") for z in range(s, g1))
+            assert step <= 8192 and jobs <= 4  # a chunk, and the kernel's 4 MMA jobs per input group
             s = g1
         assert tot == nrec
         assert (int(td["mode"]) >> 4) == used
