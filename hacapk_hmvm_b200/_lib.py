@@ -143,7 +143,9 @@ class LayoutView(C.Structure):
                 ("rowscale", C.POINTER(C.c_double)), ("n_rowscale", C.c_int64),
                 ("tcw", C.c_int32), ("tcw_bf16", C.c_int32), ("tscale", C.POINTER(C.c_float)),
                 ("n_tscale", C.c_int64), ("tscale_rows0", C.c_int32), ("_pad_view", C.c_int32),
-                ("tblocks", C.POINTER(C.c_int32))]
+                ("tblocks", C.POINTER(C.c_int32)), ("tgroups", C.POINTER(C.c_uint32)),
+                ("tops", C.POINTER(C.c_uint32)), ("tgfirst", C.POINTER(C.c_int32)), ("n_tgroups", C.c_int64),
+                ("n_tops", C.c_int64)]
 
 
 class HgenParams(C.Structure):

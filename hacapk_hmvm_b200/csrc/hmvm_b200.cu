@@ -223,6 +223,10 @@ struct hmvm_plan {
   unsigned* d_amax128 = nullptr;
   float* d_part = nullptr;    // split V-stage panels' partial sums [p_len][128]
   int32_t* d_tblocks = nullptr;  // per item: rows of its row blocks, 8 bits each
+  uint32_t* d_tgroups = nullptr;  // the step program: input group headers, MMA templates
+  uint32_t* d_tops = nullptr;
+  int32_t* d_tgfirst = nullptr;
+  int tcw_ngops = 0;            // templates in d_tops, the zero ones included
   CUtensorMap xmap, tmap;     // the planes as 3-D tensors {8, rows, 32}
   void* d_xh = nullptr;  // staging for apply_multi_host
   void* d_yh = nullptr;
@@ -262,7 +266,8 @@ void free_plan_buffers(hmvm_plan* p) {
                   p->d_red2, p->d_t,     p->d_p,    p->d_err, p->d_x,    p->d_y,       p->d_x32,
                   p->d_scale, p->d_xm64, p->d_xm32, p->d_tm,  p->d_pm,   p->d_xh,      p->d_yh,
                   p->d_xplanes, p->d_tplanes, p->d_scal, p->d_amax, p->d_xpl, p->d_tpl,
-                  p->d_tscale, p->d_xscale, p->d_amax128, p->d_part, p->d_tblocks};
+                  p->d_tscale, p->d_xscale, p->d_amax128, p->d_part, p->d_tblocks, p->d_tgroups,
+                  p->d_tops, p->d_tgfirst};
   for (void* b : bufs)
     if (b) cudaFree(b);
 }
@@ -402,6 +407,10 @@ int tcw_buffers(hmvm_plan* p, const HostLayout& L) {
   HMVM_CUDA_TRY(cudaMalloc(&p->d_part, (size_t)(L.p_len + 1) * kTcwRhs * sizeof(float)), "partial sums");
   int rc = upload(&p->d_tscale, L.tscale.data(), L.tscale.size() * sizeof(float), nullptr);
   if (!rc) rc = upload(&p->d_tblocks, L.tblocks.data(), L.tblocks.size() * sizeof(int32_t), nullptr);
+  if (!rc) rc = upload(&p->d_tgroups, L.tgroups.data(), L.tgroups.size() * sizeof(uint32_t), nullptr);
+  if (!rc) rc = upload(&p->d_tops, L.tops.data(), L.tops.size() * sizeof(uint32_t), nullptr);
+  p->tcw_ngops = (int)(L.tops.size() / 2);
+  if (!rc) rc = upload(&p->d_tgfirst, L.tgfirst.data(), L.tgfirst.size() * sizeof(int32_t), nullptr);
   if (!rc) rc = encode_planes_map(&p->xmap, p->d_xpl, xrows);
   if (!rc) rc = encode_planes_map(&p->tmap, p->d_tpl, p->tpl_rows);
   return rc;
@@ -944,6 +953,10 @@ int launch_tcw_pass(hmvm_plan* p, const void* X, int64_t ldx, void* Y, int64_t l
   a.tiles = p->d_tiles;
   a.segs = p->d_segs;
   a.blocks = p->d_tblocks;
+  a.groups = reinterpret_cast<const uint4*>(p->d_tgroups);
+  a.gops = reinterpret_cast<const uint2*>(p->d_tops);
+  a.gfirst = p->d_tgfirst;
+  a.n_gops = p->tcw_ngops;
   a.data = static_cast<const char*>(p->d_data);
   a.out_idx = p->d_out_idx;
   a.tscale = p->d_tscale;
@@ -1625,6 +1638,11 @@ int hmvm_b200_layout_view(const hmvm_layout* h, hmvm_layout_view* v) {
   v->n_tscale = (int64_t)L.tscale.size();
   v->tscale_rows0 = L.tscale_rows0;
   v->tblocks = L.tblocks.empty() ? nullptr : L.tblocks.data();
+  v->tgroups = L.tgroups.empty() ? nullptr : L.tgroups.data();
+  v->tops = L.tops.empty() ? nullptr : L.tops.data();
+  v->tgfirst = L.tgfirst.empty() ? nullptr : L.tgfirst.data();
+  v->n_tgroups = (int64_t)(L.tgroups.size() / 4);
+  v->n_tops = L.tops.empty() ? 0 : (int64_t)(L.tops.size() / 2) - kTcwMaxOps;
   return HMVM_OK;
 }
 

@@ -33,12 +33,14 @@
 //                        -- "chunk" -- takes whole K steps, at most 8, across
 //                        segments and items; each copy adds its bytes with
 //                        mbarrier.expect_tx and the chunk is closed by one
-//                        arrive), and a TMA tensor copy of the K step's inputs
-//                        into a 14 x 8 KiB ring;
-//   warp 1 (one thread)  allocates TMEM, issues the MMAs (per input group a
-//                        packed list of at most 4 block jobs), commits each
-//                        input slot, matrix chunk and finished accumulator to
-//                        its mbarrier;
+//                        arrive), a TMA tensor copy of the K step's inputs
+//                        into a 14 x 8 KiB ring, and beside the input slot the
+//                        step's MMAs fully formed (16 bytes each);
+//   warp 1 (one thread)  allocates TMEM, issues the listed MMAs (a load and an
+//                        issue each: a lone issuing thread with any more
+//                        arithmetic per MMA falls behind the tensor core),
+//                        commits each input slot, matrix chunk and finished
+//                        accumulator to its mbarrier;
 //   warps 2..5           epilogue: tcgen05.ld the accumulators (warp w reads
 //                        lanes 32 (w % 4) ..), scale, and store t (16-bit
 //                        hi/lo chunks) or y (each thread 32 consecutive rows of
@@ -56,6 +58,7 @@
 #include <cuda_fp16.h>
 
 #include "kernels_tc.cuh"
+#include "layout.hpp"
 
 namespace hmvm {
 
@@ -66,11 +69,18 @@ constexpr int kTcwSlotA = 8192;   // one K step of inputs: 4 chunks x 16 rows x 
 constexpr int kTcwSlotsA = 14;
 static_assert(kTcwChunkSteps < kTcwSlotsA, "a chunk must hold fewer K steps than the input ring has slots");
 constexpr int kTcwThreads = 192;
-constexpr int kTcwZeroBytes = 2048;  // 128 rows x 16 B of zeros
+// Zeros: the B operand of the per-item MMA that clears the accumulators (256
+// rows x 16 columns, the second 8 columns 4 KiB on; its first 4 KiB also serve
+// as that MMA's A operand) and of an odd last K step's missing 8 columns.
+constexpr int kTcwZeroBytes = 8192;
 constexpr int kTcwOffA = kTcwSlotsM * kTcwSlotM;
 constexpr int kTcwOffZero = kTcwOffA + kTcwSlotsA * kTcwSlotA;
-constexpr int kTcwOffRec = kTcwOffZero + kTcwZeroBytes;  // one 16-byte K-step record per input slot
-constexpr int kTcwOffBar = kTcwOffRec + kTcwSlotsA * 16;
+// Per input slot, the MMAs of its K step as the producer formed them (at most
+// kTcwMaxOps), 16 bytes each, and a header word (count, flags).
+constexpr uint32_t kTcwNewChunk = 1u << 16, kTcwLastStep = 1u << 17;  // header flags
+constexpr int kTcwOffOps = kTcwOffZero + kTcwZeroBytes;
+constexpr int kTcwOffHdr = kTcwOffOps + kTcwSlotsA * kTcwMaxOps * 16;
+constexpr int kTcwOffBar = kTcwOffHdr + ((kTcwSlotsA * 4 + 15) & ~15);
 constexpr int kTcwNumBars = 2 * kTcwSlotsM + 2 * kTcwSlotsA + 2 * 4 + 1;
 constexpr int kTcwOffMisc = kTcwOffBar + kTcwNumBars * 8;
 constexpr int kTcwSmem = kTcwOffMisc + 32 + 1024;  // + room to align the base to 1 KiB
@@ -88,6 +98,10 @@ struct TcwArgs {
   const hmvm_tile_desc* tiles;
   const hmvm_seg_desc* segs;
   const int32_t* blocks;      // per item: rows of its row blocks 0..3, 8 bits each
+  const uint4* groups;        // the step program: per input group its header ...
+  const uint2* gops;          // ... and its MMA templates (kTcwMaxOps zero templates after the last)
+  const int32_t* gfirst;      // [items + 1]: first input group of each item
+  int n_gops;                 // templates in gops, the zero ones included
   const int32_t* team_begin;  // [nteams + 1]
   int nteams;
   const char* data;           // the 16-byte vectors of the stream
@@ -103,13 +117,6 @@ struct TcwArgs {
   int y32;                    // y is FP32 (FP32 plans), else FP64
   int* err;
 };
-
-// Instruction descriptor, kind::f16: D FP32, A and B FP16 (bf = 0) or BF16
-// (bf = 1), A MN-major, B K-major, M = 128, N = n.
-__host__ __device__ constexpr uint32_t tcw_idesc(int bf, int n) {
-  return (1u << 4) | ((uint32_t)bf << 7) | ((uint32_t)bf << 10) | (1u << 15) | ((uint32_t)(n >> 3) << 17) |
-         ((uint32_t)(128 >> 4) << 24);
-}
 
 // Shared-memory matrix descriptor of a 128-byte-swizzled layout (tcgen05
 // layout type 2): start address, leading- and stride-dimension byte offsets.
@@ -154,40 +161,6 @@ __device__ __forceinline__ void tcw_split(float v, uint16_t& hi, uint16_t& lo) {
     hi = __half_as_ushort(h);
     lo = __half_as_ushort(l);
   }
-}
-
-// An input group of an item: segments [s0, s1) with one input range; per K
-// step, the bytes of every (segment, block) pair are (vectors of the step) x 16
-// x hrows, hrows = sum over the group's segments of (1 or 2) x (rows of the
-// blocks in its mask).
-struct TcwGroup {
-  int s1, ncols, nv, nks, row0, hrows;
-  bool tsrc;
-};
-__device__ __forceinline__ int tcw_mask_rows(int mask, uint32_t R4) {
-  int n = 0;
-#pragma unroll
-  for (int b = 0; b < 4; b++)
-    if (mask >> b & 1) n += (R4 >> (8 * b)) & 0xff;
-  return n;
-}
-__device__ __forceinline__ TcwGroup tcw_group(const hmvm_seg_desc* segs, int s0, int se, uint32_t R4) {
-  TcwGroup g;
-  const hmvm_seg_desc f = segs[s0];
-  g.ncols = f.ncols & 0xffffff;
-  g.nv = (g.ncols + 7) >> 3;
-  g.nks = (g.nv + 1) >> 1;
-  g.tsrc = f.src < 0;
-  g.row0 = f.src & 0x7fffffff;
-  g.hrows = 0;
-  int s = s0;
-  for (; s < se; s++) {
-    const hmvm_seg_desc z = segs[s];
-    if (s > s0 && (z.src != f.src || (z.ncols & 0xffffff) != g.ncols)) break;
-    g.hrows += ((z.ncols >> 28) & 1 ? 2 : 1) * tcw_mask_rows((z.ncols >> 24) & 15, R4);
-  }
-  g.s1 = s;
-  return g;
 }
 
 template <bool VST, bool BF>
@@ -248,111 +221,154 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
   const int te = team < a.nteams ? a.team_begin[team + 1] : 0;
 
   if (warp == 0) {
-    // ---- producer ----
-    // Per K step: the matrix bytes into the current chunk, the inputs into an
-    // input slot, and beside that slot a 16-byte record for the MMA thread (written
-    // before the slot's arrive, which publishes it): the step's MMA jobs (up to 4
-    // x 14 bits: block, pair-stored, the block's first vector in units of
-    // nvj x 16 bytes), its offset in its chunk, flags (starts a chunk, the item's
-    // last step, two 8-column vectors), the job count and the item's block rows.
-    if (lane == 0 && tb < te) {
-      uint4* rec = reinterpret_cast<uint4*>(tcw_smem + kTcwOffRec);
-      uint32_t mI = 0, aI = 0, used = 0, cnt = 0;
+    // ---- producer (the whole warp) ----
+    // Walks the team's step program: per input group its header and MMA
+    // templates (lane q gets template q), read by shuffles from two 32-entry
+    // windows of headers and two of templates that the warp loads coalesced one
+    // window ahead, so no global load latency lands on a K step; per K step the
+    // matrix bytes into the current chunk (lane 0),
+    // the step's MMAs formed from the templates (lane q writes MMA q: low words
+    // of the A and B descriptors, block, instruction descriptor), a header word
+    // (count, starts a chunk, the item's last step) and the input slot's TMA copy
+    // (lane 0), whose arrive publishes the MMAs.  Every lane keeps the same
+    // counters; lane 0's waits decide for all.
+    if (tb < te) {
+      uint4* ops = reinterpret_cast<uint4*>(tcw_smem + kTcwOffOps);
+      uint32_t* hdr = reinterpret_cast<uint32_t*>(tcw_smem + kTcwOffHdr);
+      const uint32_t zaddr = smem_u32(zero);
+      // A: input slot 0's hi part; slot s is (8 KiB * s) >> 4 further on, its lo part 4 KiB on
+      const uint32_t alo0 = (uint32_t)tc_desc_sw128(smem_u32(ringA), 2048, 1024);
+      const int g0 = a.gfirst[tb], gend = a.gfirst[te];
+      const int glast = max(gend - 1, 0);  // window loads past the team's groups read its last one
+      const int tlast = a.n_gops - 1;
+      int hb = g0;  // group of lane 0 of the header window H0; H1 holds the next 32
+      uint4 H0 = a.groups[min(hb + lane, glast)], H1 = a.groups[min(hb + 32 + lane, glast)];
+      uint32_t tc = __shfl_sync(0xffffffffu, H0.w, 0);  // this group's first template
+      uint32_t tw = tc;                                  // template of lane 0 of window T0; T1 the next 32
+      uint2 T0 = a.gops[min((int)tw + lane, tlast)], T1 = a.gops[min((int)tw + 32 + lane, tlast)];
+      uint32_t mI = 0, aI = 0, used = 0, cnt = 0, cbase = 0;
       int ms = 0;
       bool ok = true, open = false;
       const char* g = a.data + a.tiles[tb].data_off * 16;  // the team's items are contiguous in the stream
-      for (int it = tb; it < te && ok; it++) {
-        const hmvm_tile_desc d = a.tiles[it];
-        const uint32_t R4 = (uint32_t)a.blocks[it];
-        const int se = d.seg_begin + d.nseg;
-        for (int s = d.seg_begin; s < se && ok;) {
-          const TcwGroup gr = tcw_group(a.segs, s, se, R4);
-          const CUtensorMap* map = gr.tsrc ? &tmap : &xmap;
-          uint64_t jobs = 0;
-          uint32_t njob = 0, pre = 0;
-          for (int z = s; z < gr.s1; z++) {
-            const int enc = a.segs[z].ncols;
-            const uint32_t mask = (uint32_t)(enc >> 24) & 15u, pair = (uint32_t)(enc >> 28) & 1u;
-            for (int b = 0; b < 4; b++) {
-              if (!(mask >> b & 1u)) continue;
-              if (njob < 4) jobs |= (uint64_t)((uint32_t)b | (pair << 2) | (pre << 3)) << (14 * njob);
-              njob++;
-              pre += ((R4 >> (8 * b)) & 0xffu) * (pair ? 2u : 1u);
+      for (int gi = g0; gi < gend && ok; gi++) {
+        if (gi - hb == 32) {
+          hb += 32;
+          H0 = H1;
+          H1 = a.groups[min(hb + 32 + lane, glast)];
+        }
+        const int hl = gi - hb;
+        uint4 gh;
+        gh.x = __shfl_sync(0xffffffffu, H0.x, hl);
+        gh.y = __shfl_sync(0xffffffffu, H0.y, hl);
+        gh.z = __shfl_sync(0xffffffffu, H0.z, hl);
+        const uint32_t nops = (gh.z >> 16) & 15u, hrows = gh.z & 0xffffu;
+        if (tc - tw >= 32u) {  // a group's templates (<= kTcwMaxOps) span at most the two windows
+          tw += 32;
+          T0 = T1;
+          T1 = a.gops[min((int)tw + 32 + lane, tlast)];
+        }
+        const uint32_t ti = tc - tw + (uint32_t)min(lane, kTcwMaxOps - 1);
+        const uint32_t t0x = __shfl_sync(0xffffffffu, T0.x, (int)(ti & 31u));
+        const uint32_t t0y = __shfl_sync(0xffffffffu, T0.y, (int)(ti & 31u));
+        const uint32_t t1x = __shfl_sync(0xffffffffu, T1.x, (int)(ti & 31u));
+        const uint32_t t1y = __shfl_sync(0xffffffffu, T1.y, (int)(ti & 31u));
+        const uint2 tp = ti < 32u ? make_uint2(t0x, t0y) : make_uint2(t1x, t1y);
+        tc += nops;
+        const CUtensorMap* map = (gh.x >> 31) ? &tmap : &xmap;
+        const int row0 = (int)(gh.x & 0x7fffffffu), nv = (int)gh.y, nks = (nv + 1) >> 1;
+        const uint32_t prow = tp.x & 0xfffu, alo = (tp.x >> 12) & 1u, blk = (tp.x >> 13) & 3u, rb16 = tp.x >> 16;
+        for (int j = 0; j < nks; j++) {
+          const uint32_t nvj = (uint32_t)min(2, nv - 2 * j);
+          const uint32_t kb = nvj * 16u * hrows;
+          uint32_t flags = 0;
+          if (!open || used + kb > (uint32_t)kTcwSlotM || cnt == kTcwChunkSteps) {
+            ms = mI % kTcwSlotsM;
+            bool okw = true;
+            if (lane == 0) {
+              if (open) mbar_arrive(&mfull[(mI + kTcwSlotsM - 1) % kTcwSlotsM]);  // close the chunk
+              okw = mI < kTcwSlotsM || thread_wait(&mempty[ms], ((mI / kTcwSlotsM) - 1) & 1);
             }
-          }
-          const bool last_group = gr.s1 == se;
-          for (int j = 0; j < gr.nks; j++) {
-            const uint32_t nvj = (uint32_t)min(2, gr.nv - 2 * j);
-            const uint32_t kb = nvj * 16u * (uint32_t)gr.hrows;
-            uint32_t flags = 0;
-            if (!open || used + kb > (uint32_t)kTcwSlotM || cnt == kTcwChunkSteps) {
-              if (open) mbar_arrive(&mfull[ms]);  // close the chunk
-              ms = mI % kTcwSlotsM;
-              if (mI >= kTcwSlotsM && !thread_wait(&mempty[ms], ((mI / kTcwSlotsM) - 1) & 1)) {
-                ok = false;
-                open = false;
-                break;
-              }
-              mI++;
-              open = true;
-              used = cnt = 0;
-              flags |= 1u << 16;
-            }
-            mbar_expect_tx_only(&mfull[ms], kb);
-            bulk_g2s(ringM + ms * kTcwSlotM + used, g, kb, &mfull[ms]);
-            const int as = aI % kTcwSlotsA;
-            if (aI >= kTcwSlotsA && !thread_wait(&aempty[as], ((aI / kTcwSlotsA) - 1) & 1)) {
+            if (!__shfl_sync(0xffffffffu, okw, 0)) {
               ok = false;
+              open = false;
               break;
             }
-            if (last_group && j + 1 == gr.nks) flags |= 1u << 17;
-            if (nvj == 2) flags |= 1u << 18;
-            rec[as] = make_uint4((uint32_t)jobs, (uint32_t)(jobs >> 32), used | flags | (njob << 19), R4);
-            mbar_expect_tx(&afull[as], kTcwSlotA);
-            tma_load_3d(ringA + as * kTcwSlotA, map, 0, gr.row0 + 16 * j, 0, &afull[as]);
-            aI++;
-            g += kb;
-            used += kb;
-            cnt++;
+            mI++;
+            open = true;
+            used = cnt = 0;
+            cbase = smem_u32(ringM + ms * kTcwSlotM);
+            flags |= kTcwNewChunk;
           }
-          s = gr.s1;
+          const int as = aI % kTcwSlotsA;
+          bool okw = true;
+          if (lane == 0) {
+            mbar_expect_tx_only(&mfull[ms], kb);
+            bulk_g2s(ringM + ms * kTcwSlotM + used, g, kb, &mfull[ms]);
+            okw = aI < kTcwSlotsA || thread_wait(&aempty[as], ((aI / kTcwSlotsA) - 1) & 1);
+          }
+          if (!__shfl_sync(0xffffffffu, okw, 0)) {
+            ok = false;
+            break;
+          }
+          if ((gh.z & kTcwGroupLast) && j + 1 == nks) flags |= kTcwLastStep;
+          if ((uint32_t)lane < nops) {
+            // B: the block's rows from prow on, K-major core matrices; an odd last step's
+            // second 8 columns read the zero block
+            const uint32_t start = cbase + used + nvj * 16u * prow;
+            const uint32_t lbo = nvj == 2 ? rb16 : zaddr - start;
+            ops[as * kTcwMaxOps + lane] =
+                make_uint4(alo0 + (uint32_t)as * (uint32_t)(kTcwSlotA >> 4) + alo * (4096u >> 4),
+                           ((start >> 4) & 0x3fffu) | (((lbo >> 4) & 0x3fffu) << 16), blk * (uint32_t)G::bstride,
+                           tp.y);
+          }
+          __syncwarp();
+          if (lane == 0) {
+            hdr[as] = nops | flags;
+            mbar_expect_tx(&afull[as], kTcwSlotA);
+            tma_load_3d(ringA + as * kTcwSlotA, map, 0, row0 + 16 * j, 0, &afull[as]);
+          }
+          aI++;
+          g += kb;
+          used += kb;
+          cnt++;
         }
       }
-      if (open) mbar_arrive(&mfull[ms]);  // close the last chunk (also after a failure, so it can drain)
-      misc[1] = mI;
-      misc[2] = aI;
-      if (!ok) atomicExch(a.err, 1);
+      if (lane == 0) {
+        if (open) mbar_arrive(&mfull[ms]);  // close the last chunk (also after a failure, so it can drain)
+        misc[1] = mI;
+        misc[2] = aI;
+        if (!ok) atomicExch(a.err, 1);
+      }
     }
   } else if (warp == 1) {
-    // ---- MMA issue (one thread), driven by the producer's K-step records ----
+    // ---- MMA issue (one thread): per item one MMA that clears its accumulators,
+    // then the producer's per-step MMA lists ----
     if (lane == 0) {
-      const uint4* rec = reinterpret_cast<const uint4*>(tcw_smem + kTcwOffRec);
-      uint32_t mC = 0, aC = 0, ic = 0, cbase = 0;
+      const uint4* ops = reinterpret_cast<const uint4*>(tcw_smem + kTcwOffOps);
+      const uint32_t* hdr = reinterpret_cast<const uint32_t*>(tcw_smem + kTcwOffHdr);
+      // descriptor high words: stride byte offset, version, layout (128-byte swizzle for A)
+      const uint64_t ahi = tc_desc_sw128(0, 0, 1024) & 0xffffffff00000000ull;
+      const uint64_t bhi = tc_desc(0, 0, 128) & 0xffffffff00000000ull;
+      // the clearing MMA: zeros x zeros over all the buffer's columns
+      const uint32_t zaddr = smem_u32(zero);
+      const uint64_t zadesc = tc_desc_sw128(zaddr, 2048, 1024);
+      const uint64_t zbdesc = tc_desc(zaddr, 4096, 128);
+      const uint32_t zidesc = tcw_idesc(BF ? 1 : 0, G::cols);
+      uint32_t mC = 0, aC = 0, ic = 0;
       int ms = 0;
       bool ok = true, open = false;
-      const uint32_t zaddr = smem_u32(zero);
-      // descriptor of input slot 0's hi part; slot s is (8 KiB * s) >> 4 further on, its lo part 4 KiB on
-      const uint64_t adesc0 = tc_desc_sw128(smem_u32(ringA), 2048, 1024);
+      int nseg_next = tb < te ? a.tiles[tb].nseg : 0;
       for (int it = tb; it < te && ok; it++, ic++) {
-        const int nseg = a.tiles[it].nseg;
-        const uint32_t R4 = (uint32_t)a.blocks[it];
+        const int nseg = nseg_next;
+        nseg_next = it + 1 < te ? a.tiles[it + 1].nseg : 0;
         const int buf = ic % G::bufs;
         if (ic >= G::bufs && !thread_wait(&accempty[buf], ((ic / G::bufs) - 1) & 1)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        // per block (scalars, picked by block index): 16-byte column stride and instruction
-        // descriptor (N = rows rounded up to 16)
-        uint32_t rbs[4], ids[4];
-#pragma unroll
-        for (int b = 0; b < 4; b++) {
-          const uint32_t Rb = (R4 >> (8 * b)) & 0xffu;
-          rbs[b] = Rb * 16u;
-          ids[b] = tcw_idesc(BF ? 1 : 0, max(16, (int)((Rb + 15) & ~15u)));
-        }
         const uint32_t dbase = tmem_base + (uint32_t)(buf * G::cols);
-        uint32_t started = 0;  // blocks whose accumulator holds a first product
+        if (nseg > 0) tc_mma(dbase, zadesc, zbdesc, zidesc, 0);
         bool last = nseg == 0;
         while (!last) {
           const int as = aC % kTcwSlotsA;
@@ -361,10 +377,9 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
             break;
           }
           aC++;
-          const uint4 r = rec[as];
-          const uint32_t fl = r.z;
-          last = (fl >> 17) & 1u;
-          if ((fl >> 16) & 1u) {  // the step starts a chunk
+          const uint32_t h = hdr[as];
+          last = (h & kTcwLastStep) != 0;
+          if (h & kTcwNewChunk) {
             if (open) tc_commit(&mempty[ms]);  // the previous chunk's MMAs done: it can be refilled
             ms = mC % kTcwSlotsM;
             if (!thread_wait(&mfull[ms], (mC / kTcwSlotsM) & 1)) {
@@ -374,35 +389,18 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
             }
             mC++;
             open = true;
-            cbase = smem_u32(ringM + ms * kTcwSlotM);
           }
           tc_fence_after();  // the MMAs below are ordered after the waits that saw their operands land
-          // A: chunks 0, 1 (hi) and 2, 3 (lo) of the slot; 64-rhs atoms 2 KiB apart, 8-row groups 1 KiB apart
-          const uint64_t ah = adesc0 + (uint64_t)(as * (kTcwSlotA >> 4)), al = ah + (4096 >> 4);
-          const uint32_t kbase = cbase + (fl & 0xffffu), two = (fl >> 18) & 1u, nvj16 = two ? 32u : 16u;
-          const uint32_t njob = (fl >> 19) & 7u;
-          const uint64_t jobs = (uint64_t)r.x | ((uint64_t)r.y << 32);
-          for (uint32_t q = 0; q < njob; q++) {
-            const uint32_t f = (uint32_t)(jobs >> (14 * q)) & 0x3fffu;
-            const uint32_t b = f & 3u, pair = (f >> 2) & 1u;
-            const uint32_t rb16 = b == 0 ? rbs[0] : b == 1 ? rbs[1] : b == 2 ? rbs[2] : rbs[3];
-            const uint32_t idb = b == 0 ? ids[0] : b == 1 ? ids[1] : b == 2 ? ids[2] : ids[3];
-            const uint32_t dblk = dbase + b * (uint32_t)G::bstride;
-            // B: the block's hi vectors, then (pair segments) its lo vectors nvj vectors on; an
-            // odd last step's second 8 columns read the zero block
-            const uint32_t off = kbase + nvj16 * (f >> 3);
-            uint64_t bh, bl;
-            if (two) {
-              bh = tc_desc(off, rb16, 128);
-              bl = bh + (rb16 >> 3);
-            } else {
-              bh = tc_desc(off, zaddr - off, 128);
-              bl = tc_desc(off + rb16, zaddr - off - rb16, 128);
-            }
-            tc_mma(dblk, ah, bh, idb, (int)(started >> b & 1u));
-            tc_mma(dblk, al, bh, idb, 1);
-            if (pair) tc_mma(dblk, ah, bl, idb, 1);
-            started |= 1u << b;
+          const uint4* o = ops + as * kTcwMaxOps;
+          const uint32_t n = h & 0xffu;
+          // a compact loop (an unrolled one measured slower), the next MMA's record loaded ahead
+          // (past the last it reads the next slot's, or the header words: inside shared memory)
+          uint4 r = o[0];
+#pragma unroll 1
+          for (uint32_t k = 0; k < n; k++) {
+            const uint4 nx = o[k + 1];
+            tc_mma(dbase + r.z, ahi | r.x, bhi | r.y, r.w, 1);
+            r = nx;
           }
           tc_commit(&aempty[as]);
         }
@@ -447,13 +445,17 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
             for (int i = 0; i < 32; i++) v[i] = 0.f;
           }
           const int nrow = min(32, Rb - c0), row = rb + c0;
+          // row i's scale (and t slot) from lane i, taken by shuffles
+          const float ts_l = lane < nrow ? a.tscale[d._pad + row + lane] : 0.f;
           if constexpr (VST) {
+            const int32_t slot_l = (mode == 1 && lane < nrow) ? a.out_idx[d.out_base + row + lane] : 0;
 #pragma unroll
             for (int i = 0; i < 32; i++) {
+              const float ts = __shfl_sync(0xffffffffu, ts_l, i);
+              const int32_t slot = __shfl_sync(0xffffffffu, slot_l, i);
               if (i < nrow) {
-                const float tv = v[i] * a.tscale[d._pad + row + i];
+                const float tv = v[i] * ts;
                 if (mode == 1) {
-                  const int64_t slot = a.out_idx[d.out_base + row + i];
                   uint16_t hi, lo;
                   tcw_split<BF>(tv, hi, lo);
                   a.tplanes[((int64_t)(r >> 6) * a.trows + slot) * 64 + (r & 63)] = hi;
@@ -463,12 +465,13 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
                 }
               }
             }
-          } else if (r < a.nr) {
+          } else {
             const int64_t o = (int64_t)d.out_base + row + (int64_t)r * a.ldy;
 #pragma unroll
             for (int i = 0; i < 32; i++) {
-              if (i < nrow) {
-                const double val = (double)v[i] * (double)a.tscale[d._pad + row + i] * sx;
+              const float ts = __shfl_sync(0xffffffffu, ts_l, i);
+              if (i < nrow && r < a.nr) {
+                const double val = (double)v[i] * (double)ts * sx;
                 if (a.y32) static_cast<float*>(a.y)[o + i] = (float)val;
                 else static_cast<double*>(a.y)[o + i] = val;
               }

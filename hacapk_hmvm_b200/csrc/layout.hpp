@@ -185,6 +185,29 @@ constexpr int kTcwTilesPerItem = 4; // row-stage tiles per item (blocks sharing 
 constexpr int kTcwMaskShift = 24;   // segment ncols: bits 0..23 columns, 24..27 block mask, 28 format
 // Segment formats of the wide tensor-core layout (top bits of ncols).
 enum TcwFmt : int32_t { TF_HI = 0, TF_HILO = 1 };
+// The step program of the wide form, per input group (consecutive segments of
+// an item with one input range) a 4-word header:
+//   [0] the segments' src word (bit 31: t planes, bits 0..30: first input row)
+//   [1] 8-column vectors of the range
+//   [2] rows streamed per K step (pairs count twice) | MMAs << 16 | item's last group << 20
+//   [3] index of its first MMA template
+// and per MMA of a K step a 2-word template:
+//   [0] first B row (in 16-byte units of the step's vectors) | A lo part << 12 | block << 13 |
+//       the block's rows * 16 << 16
+//   [1] instruction descriptor
+constexpr int kTcwMaxOps = 12;         // MMAs of one K step at most (4 block jobs x 3 products)
+constexpr uint32_t kTcwGroupLast = 1u << 20;
+#if defined(__CUDACC__)
+#define HMVM_TCW_HD __host__ __device__
+#else
+#define HMVM_TCW_HD
+#endif
+// tcgen05 instruction descriptor, kind::f16: D FP32, A and B FP16 (bf = 0) or
+// BF16 (bf = 1), A MN-major, B K-major, M = 128, N = n.
+HMVM_TCW_HD constexpr uint32_t tcw_idesc(int bf, int n) {
+  return (1u << 4) | ((uint32_t)bf << 7) | ((uint32_t)bf << 10) | (1u << 15) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(128 >> 4) << 24);
+}
 
 struct HostLayout {
   int precision = HMVM_FP64;
@@ -218,6 +241,9 @@ struct HostLayout {
   bool tcw_bf16 = false;          // 16-bit format of the stored pairs and the input planes
   std::vector<float> tscale;      // per V-stage panel row 2^-c, then per y row the row scale s_i
   std::vector<int32_t> tblocks;   // per item: rows of blocks 0..3, 8 bits each
+  std::vector<uint32_t> tgroups;  // the step program: 4 words per input group
+  std::vector<uint32_t> tops;     // ... 2 words per MMA template, then kTcwMaxOps zero templates
+  std::vector<int32_t> tgfirst;   // [items + 1]: first input group of each item
   int32_t tscale_rows0 = 0;       // index of y row 0 in tscale
 };
 

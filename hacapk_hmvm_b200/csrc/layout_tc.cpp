@@ -557,6 +557,55 @@ int build_tc_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms
     }
     L.data.resize((size_t)off);
 
+    // ---- step program -----------------------------------------------------------------------
+    // Per item, its input groups (consecutive segments with one input range) in
+    // stream order; per group the MMAs of each of its K steps: per segment, per
+    // block of its mask, hi x x_hi, hi x x_lo and (pairs) lo x x_hi, B at the
+    // block's hi vectors (then lo vectors) of the step.
+    L.tgroups.clear();
+    L.tops.clear();
+    L.tgfirst.assign((size_t)nitems + 1, 0);
+    for (int32_t k = 0; k < nitems; k++) {
+      const hmvm_tile_desc &d = L.tiles[k];
+      const uint32_t R4 = (uint32_t)L.tblocks[k];
+      L.tgfirst[k] = (int32_t)(L.tgroups.size() / 4);
+      const int32_t se = d.seg_begin + d.nseg;
+      for (int32_t s = d.seg_begin; s < se;) {
+        const hmvm_seg_desc &f = L.segs[s];
+        const int32_t nc = f.ncols & ((1 << kTcwMaskShift) - 1);
+        int32_t s1 = s + 1;
+        while (s1 < se && L.segs[s1].src == f.src && (L.segs[s1].ncols & ((1 << kTcwMaskShift) - 1)) == nc) s1++;
+        const uint32_t op0 = (uint32_t)(L.tops.size() / 2);
+        uint32_t pre = 0, nops = 0;
+        for (int32_t z = s; z < s1; z++) {
+          const uint32_t enc = (uint32_t)L.segs[z].ncols, mask = (enc >> kTcwMaskShift) & 15u;
+          const bool pair = ((enc >> kSegTypeShift) & 1u) == (uint32_t)TF_HILO;
+          for (int b = 0; b < 4; b++) {
+            if (!(mask >> b & 1u)) continue;
+            const uint32_t R = (R4 >> (8 * b)) & 0xffu;
+            const uint32_t id = tcw_idesc(L.tcw_bf16 ? 1 : 0, std::max(16, (int)((R + 15) & ~15u)));
+            const uint32_t blk = ((uint32_t)b << 13) | ((R * 16u) << 16);
+            L.tops.insert(L.tops.end(), {pre | blk, id, pre | (1u << 12) | blk, id});
+            nops += 2;
+            if (pair) {
+              L.tops.insert(L.tops.end(), {(pre + R) | blk, id});
+              nops++;
+            }
+            pre += pair ? 2 * R : R;
+          }
+        }
+        if (nops > (uint32_t)kTcwMaxOps || pre >= 4096u) {
+          msg = "an input group of more than 4 block jobs";
+          return HMVM_ERANGE;
+        }
+        L.tgroups.insert(L.tgroups.end(), {(uint32_t)f.src, (uint32_t)((nc + 7) / 8),
+                                           pre | (nops << 16) | (s1 == se ? kTcwGroupLast : 0u), op0});
+        s = s1;
+      }
+    }
+    L.tgfirst[nitems] = (int32_t)(L.tgroups.size() / 4);
+    L.tops.insert(L.tops.end(), 2 * (size_t)kTcwMaxOps, 0u);
+
     // ---- pack -------------------------------------------------------------------------------
     // Per item part: per input group (consecutive segments with one input range),
     // per K step, per segment, per block in its mask: the hi vectors of the step

@@ -427,6 +427,13 @@ typedef struct hmvm_layout_view {
   const int32_t *tblocks;            /* [n_tiles]: rows of the item's row blocks 0..3, 8 bits each (block b's
                                         rows follow block b-1's); segment ncols bits 24..27 select the blocks a
                                         segment multiplies, and consecutive segments with one input range share it */
+  /* the step program the kernel's producer walks: per input group 4 words (src word, 8-column vectors,
+     rows per K step | MMAs << 16 | item's last group << 20, first MMA template), per MMA 2 words (first B row
+     | A lo part << 12 | block << 13 | block rows * 16 << 16, tcgen05 instruction descriptor) */
+  const uint32_t *tgroups;           /* [n_tgroups][4] */
+  const uint32_t *tops;              /* [n_tops][2] (+ 12 zero templates) */
+  const int32_t *tgfirst;            /* [n_tiles + 1]: first input group of each item */
+  int64_t n_tgroups, n_tops;
 } hmvm_layout_view;
 
 /* Tile and segment records as stored in the data structures above. */

@@ -144,6 +144,60 @@ def test_invalid_leaf_tables_rejected():
 
 
 # ---- the wide tensor-core layout (FP32 / mixed plans with nrhs_max >= 32) -------------
+def _tcw_idesc(bf, n):
+    """tcgen05 instruction descriptor, kind::f16, D FP32, A MN-major, B K-major, M 128."""
+    return (1 << 4) | (bf << 7) | (bf << 10) | (1 << 15) | ((n >> 3) << 17) | ((128 >> 4) << 24)
+
+
+def _tcw_program(view, tiles, segs, blocks):
+    """The step program the kernel's producer walks is the segments' own
+    grouping: per input group its src word, vector count, rows per K step, MMA
+    count and last-group flag; per MMA (per segment, per block of its mask: hi x
+    x_hi, hi x x_lo, and lo x x_hi for pairs) its first B row, A part, block,
+    block rows and instruction descriptor; every B read stays inside its step."""
+    ng, nops = view.n_tgroups, view.n_tops
+    grp = np.ctypeslib.as_array(view.tgroups, (ng * 4,)).reshape(-1, 4).astype(np.int64)
+    ops = np.ctypeslib.as_array(view.tops, ((nops + 12) * 2,)).reshape(-1, 2).astype(np.int64)
+    first = np.ctypeslib.as_array(view.tgfirst, (view.n_tiles + 1,))
+    assert np.all(ops[nops:] == 0)  # the zero templates the producer may read ahead
+    gi, oi = 0, 0
+    for k in range(view.n_tiles):
+        assert first[k] == gi
+        td = tiles[k]
+        R = [(int(blocks[k]) >> (8 * b)) & 0xFF for b in range(4)]
+        s, s1 = int(td["seg_begin"]), int(td["seg_begin"]) + int(td["nseg"])
+        while s < s1:
+            g1 = s + 1
+            while g1 < s1 and segs[g1]["src"] == segs[s]["src"] and \
+                    (int(segs[g1]["ncols"]) & 0xFFFFFF) == (int(segs[s]["ncols"]) & 0xFFFFFF):
+                g1 += 1
+            nc = int(segs[s]["ncols"]) & 0xFFFFFF
+            want, pre = [], 0
+            for z in range(s, g1):
+                enc = int(segs[z]["ncols"])
+                mask, pair = (enc >> 24) & 0xF, (enc >> 28) & 1
+                for b in range(4):
+                    if not mask >> b & 1:
+                        continue
+                    idesc = _tcw_idesc(view.tcw_bf16, max(16, (R[b] + 15) & ~15))
+                    blk = (b << 13) | ((R[b] * 16) << 16)
+                    want += [(pre | blk, idesc), (pre | (1 << 12) | blk, idesc)]
+                    if pair:
+                        want.append(((pre + R[b]) | blk, idesc))
+                    pre += 2 * R[b] if pair else R[b]
+            h = grp[gi]
+            assert h[0] == int(segs[s]["src"]) & 0xFFFFFFFF and h[1] == (nc + 7) // 8
+            assert h[2] == pre | (len(want) << 16) | ((1 << 20) if g1 == s1 else 0) and h[3] == oi
+            assert len(want) <= 12
+            got = [tuple(int(v) for v in ops[oi + q]) for q in range(len(want))]
+            assert got == want, (k, s, got, want)
+            for t0, _ in want:  # the B rows of the MMA stay inside the group's rows of the step
+                assert (t0 & 0xFFF) + ((t0 >> 16) // 16) <= pre
+            gi, oi = gi + 1, oi + len(want)
+            s = g1
+    assert first[view.n_tiles] == gi == ng and oi == nops
+
+
 def _tcw_bounds(view):
     """Every address hmvm_tcw_kernel and its helpers form stays inside its
     buffer, and every K step of an input group fits one 8 KiB ring chunk."""
@@ -200,6 +254,7 @@ def _tcw_bounds(view):
             assert mode == 0 and view.tscale_rows0 <= pad and pad + nrows <= view.n_tscale
             assert int(td["out_base"]) + nrows <= view.nd
     assert np.all(covered == 1)  # the items partition the stream
+    _tcw_program(view, tiles, segs, blocks)
     n1 = view.tscale_rows0
     out_idx = np.ctypeslib.as_array(view.out_idx, (n1,)) if n1 else np.zeros(0, np.int32)
     assert np.all((out_idx >= 0) & (out_idx < max(view.t_len, 1)))
