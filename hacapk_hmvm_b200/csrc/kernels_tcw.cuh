@@ -27,21 +27,26 @@
 // pair-stored segments (the stream holds, per K step, per segment, per block,
 // the hi vectors and then the lo vectors).
 //
-// One CTA of 6 warps per SM, warp-specialised:
-//   warp 0 (one thread)  producer: per K step a bulk copy of its matrix bytes
-//                        into the current 8 KiB slot of a 12-slot ring (a slot
-//                        -- "chunk" -- takes whole K steps, at most 8, across
+// One CTA of 9 warps per SM, warp-specialised:
+//   warp 0               producer (the whole warp; lane 0 issues the copies):
+//                        per K step a bulk copy of its matrix bytes into the
+//                        current 8 KiB slot of a 12-slot ring (a slot --
+//                        "chunk" -- takes whole K steps, at most 8, across
 //                        segments and items; each copy adds its bytes with
 //                        mbarrier.expect_tx and the chunk is closed by one
 //                        arrive), a TMA tensor copy of the K step's inputs
 //                        into a 14 x 8 KiB ring, and beside the input slot the
-//                        step's MMAs fully formed (16 bytes each);
-//   warp 1 (one thread)  allocates TMEM, issues the listed MMAs (a load and an
-//                        issue each: a lone issuing thread with any more
-//                        arithmetic per MMA falls behind the tensor core),
-//                        commits each input slot, matrix chunk and finished
-//                        accumulator to its mbarrier;
-//   warps 2..5           epilogue: tcgen05.ld the accumulators (warp w reads
+//                        step's MMAs fully formed (16 bytes each, lane q the
+//                        q-th) from the host-built step program;
+//   warps 1..4           MMA issue, one thread each: warp 1 + b issues row
+//                        block b's MMAs into its own TMEM columns (a thread
+//                        that issues MMAs whose operands it loads sustains
+//                        about one per 100 cycles; four of them keep the
+//                        tensor core busy), and commits each input slot,
+//                        matrix chunk and finished accumulator to its
+//                        mbarrier, which counts the issuing warps (warp 1 also
+//                        allocates the TMEM);
+//   warps 5..8           epilogue: tcgen05.ld the accumulators (warp w reads
 //                        lanes 32 (w % 4) ..), scale, and store t (16-bit
 //                        hi/lo chunks) or y (each thread 32 consecutive rows of
 //                        its right-hand side).
@@ -68,7 +73,7 @@ constexpr int kTcwChunkSteps = 8; // K steps per chunk at most (< kTcwSlotsA)
 constexpr int kTcwSlotA = 8192;   // one K step of inputs: 4 chunks x 16 rows x 128 B
 constexpr int kTcwSlotsA = 14;
 static_assert(kTcwChunkSteps < kTcwSlotsA, "a chunk must hold fewer K steps than the input ring has slots");
-constexpr int kTcwThreads = 192;
+constexpr int kTcwThreads = 288;  // producer, 4 MMA-issue warps, 4 epilogue warps
 // Zeros: the B operand of the per-item MMA that clears the accumulators (256
 // rows x 16 columns, the second 8 columns 4 KiB on; its first 4 KiB also serve
 // as that MMA's A operand) and of an odd last K step's missing 8 columns.
@@ -76,7 +81,8 @@ constexpr int kTcwZeroBytes = 8192;
 constexpr int kTcwOffA = kTcwSlotsM * kTcwSlotM;
 constexpr int kTcwOffZero = kTcwOffA + kTcwSlotsA * kTcwSlotA;
 // Per input slot, the MMAs of its K step as the producer formed them (at most
-// kTcwMaxOps), 16 bytes each, and a header word (count, flags).
+// kTcwMaxOps, ordered by row block), 16 bytes each, and a header word (per row
+// block its MMA count in 4 bits, flags).
 constexpr uint32_t kTcwNewChunk = 1u << 16, kTcwLastStep = 1u << 17;  // header flags
 constexpr int kTcwOffOps = kTcwOffZero + kTcwZeroBytes;
 constexpr int kTcwOffHdr = kTcwOffOps + kTcwSlotsA * kTcwMaxOps * 16;
@@ -91,6 +97,7 @@ struct TcwGeom {
   static constexpr int bufs = VST ? 2 : 4;
   static constexpr int cols = VST ? 256 : 128;
   static constexpr int bstride = VST ? 128 : 32;
+  static constexpr int issuers = VST ? 2 : 4;  // row blocks: one MMA-issue warp each
   static_assert(bufs * cols == 512, "the CTA owns the SM's 512 TMEM columns");
 };
 
@@ -184,24 +191,25 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
   uint64_t* done = accempty + 4;
   uint32_t* misc = reinterpret_cast<uint32_t*>(tcw_smem + kTcwOffMisc);
   // misc: [0] TMEM base, [1] matrix chunks opened, [2] input steps issued,
-  //       [3] matrix chunks consumed, [4] input steps consumed
+  //       [3] matrix chunks consumed, [4] input steps consumed (least over the issuers)
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
     for (int s = 0; s < kTcwSlotsM; s++) {
       mbar_init(&mfull[s], 1);
-      mbar_init(&mempty[s], 1);
+      mbar_init(&mempty[s], G::issuers);
     }
     for (int s = 0; s < kTcwSlotsA; s++) {
       mbar_init(&afull[s], 1);
-      mbar_init(&aempty[s], 1);
+      mbar_init(&aempty[s], G::issuers);
     }
     for (int s = 0; s < G::bufs; s++) {
-      mbar_init(&accfull[s], 1);
+      mbar_init(&accfull[s], G::issuers);
       mbar_init(&accempty[s], 4);
     }
-    mbar_init(done, 1);
-    for (int k = 1; k < 5; k++) misc[k] = 0;
+    mbar_init(done, G::issuers);
+    misc[1] = misc[2] = 0;
+    misc[3] = misc[4] = 0xffffffffu;  // the issuers' least progress
     fence_mbar_init();
   }
   for (int k = tid; k < kTcwZeroBytes / 16; k += kTcwThreads)
@@ -261,7 +269,8 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
         gh.x = __shfl_sync(0xffffffffu, H0.x, hl);
         gh.y = __shfl_sync(0xffffffffu, H0.y, hl);
         gh.z = __shfl_sync(0xffffffffu, H0.z, hl);
-        const uint32_t nops = (gh.z >> 16) & 15u, hrows = gh.z & 0xffffu;
+        const uint32_t counts = gh.z >> 16, hrows = gh.z & 0xfffu;
+        const uint32_t nops = (counts & 15u) + ((counts >> 4) & 15u) + ((counts >> 8) & 15u) + (counts >> 12);
         if (tc - tw >= 32u) {  // a group's templates (<= kTcwMaxOps) span at most the two windows
           tw += 32;
           T0 = T1;
@@ -323,7 +332,7 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
           }
           __syncwarp();
           if (lane == 0) {
-            hdr[as] = nops | flags;
+            hdr[as] = counts | flags;
             mbar_expect_tx(&afull[as], kTcwSlotA);
             tma_load_3d(ringA + as * kTcwSlotA, map, 0, row0 + 16 * j, 0, &afull[as]);
           }
@@ -340,20 +349,23 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
         if (!ok) atomicExch(a.err, 1);
       }
     }
-  } else if (warp == 1) {
-    // ---- MMA issue (one thread): per item one MMA that clears its accumulators,
-    // then the producer's per-step MMA lists ----
-    if (lane == 0) {
+  } else if (warp <= 4) {
+    // ---- MMA issue: warp 1 + b, one thread, row block b ----
+    // Per item one MMA that clears the block's accumulator, then per K step
+    // the block's part of the producer's MMA list.  Every issuer waits for and
+    // commits every step, chunk and item (the barriers count the issuers).
+    const int b = warp - 1;
+    if (b < G::issuers && lane == 0) {
       const uint4* ops = reinterpret_cast<const uint4*>(tcw_smem + kTcwOffOps);
       const uint32_t* hdr = reinterpret_cast<const uint32_t*>(tcw_smem + kTcwOffHdr);
       // descriptor high words: stride byte offset, version, layout (128-byte swizzle for A)
       const uint64_t ahi = tc_desc_sw128(0, 0, 1024) & 0xffffffff00000000ull;
       const uint64_t bhi = tc_desc(0, 0, 128) & 0xffffffff00000000ull;
-      // the clearing MMA: zeros x zeros over all the buffer's columns
+      // the clearing MMA: zeros x zeros over the block's columns
       const uint32_t zaddr = smem_u32(zero);
       const uint64_t zadesc = tc_desc_sw128(zaddr, 2048, 1024);
       const uint64_t zbdesc = tc_desc(zaddr, 4096, 128);
-      const uint32_t zidesc = tcw_idesc(BF ? 1 : 0, G::cols);
+      const uint32_t zidesc = tcw_idesc(BF ? 1 : 0, G::bstride);
       uint32_t mC = 0, aC = 0, ic = 0;
       int ms = 0;
       bool ok = true, open = false;
@@ -368,7 +380,7 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
         }
         tc_fence_after();
         const uint32_t dbase = tmem_base + (uint32_t)(buf * G::cols);
-        if (nseg > 0) tc_mma(dbase, zadesc, zbdesc, zidesc, 0);
+        if (nseg > 0) tc_mma(dbase + (uint32_t)(b * G::bstride), zadesc, zbdesc, zidesc, 0);
         bool last = nseg == 0;
         while (!last) {
           const int as = aC % kTcwSlotsA;
@@ -391,8 +403,12 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
             open = true;
           }
           tc_fence_after();  // the MMAs below are ordered after the waits that saw their operands land
-          const uint4* o = ops + as * kTcwMaxOps;
-          const uint32_t n = h & 0xffu;
+          uint32_t off = 0;  // this block's first MMA in the list: the counts of the blocks before it
+#pragma unroll
+          for (int c = 0; c < 3; c++)
+            if (c < b) off += (h >> (4 * c)) & 15u;
+          const uint32_t n = (h >> (4 * b)) & 15u;
+          const uint4* o = ops + as * kTcwMaxOps + off;
           // a compact loop (an unrolled one measured slower), the next MMA's record loaded ahead
           // (past the last it reads the next slot's, or the header words: inside shared memory)
           uint4 r = o[0];
@@ -407,8 +423,8 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
         if (ok) tc_commit(&accfull[buf]);
       }
       if (open) tc_commit(&mempty[ms]);
-      misc[3] = mC;
-      misc[4] = aC;
+      atomicMin(&misc[3], mC);
+      atomicMin(&misc[4], aC);
       // every MMA issued has completed before the CTA goes on (bounded)
       tc_commit(done);
       if (!thread_wait(done, 0)) ok = false;

@@ -189,14 +189,16 @@ enum TcwFmt : int32_t { TF_HI = 0, TF_HILO = 1 };
 // an item with one input range) a 4-word header:
 //   [0] the segments' src word (bit 31: t planes, bits 0..30: first input row)
 //   [1] 8-column vectors of the range
-//   [2] rows streamed per K step (pairs count twice) | MMAs << 16 | item's last group << 20
+//   [2] rows streamed per K step (pairs count twice) | item's last group << 12 |
+//       MMAs on row block b << (16 + 4 b)
 //   [3] index of its first MMA template
-// and per MMA of a K step a 2-word template:
+// and per MMA of a K step (ordered by row block: block b's MMAs are issued by
+// their own warp) a 2-word template:
 //   [0] first B row (in 16-byte units of the step's vectors) | A lo part << 12 | block << 13 |
 //       the block's rows * 16 << 16
 //   [1] instruction descriptor
 constexpr int kTcwMaxOps = 12;         // MMAs of one K step at most (4 block jobs x 3 products)
-constexpr uint32_t kTcwGroupLast = 1u << 20;
+constexpr uint32_t kTcwGroupLast = 1u << 12;
 #if defined(__CUDACC__)
 #define HMVM_TCW_HD __host__ __device__
 #else

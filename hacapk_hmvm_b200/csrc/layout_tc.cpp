@@ -576,7 +576,8 @@ int build_tc_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms
         int32_t s1 = s + 1;
         while (s1 < se && L.segs[s1].src == f.src && (L.segs[s1].ncols & ((1 << kTcwMaskShift) - 1)) == nc) s1++;
         const uint32_t op0 = (uint32_t)(L.tops.size() / 2);
-        uint32_t pre = 0, nops = 0;
+        uint32_t pre = 0, nops = 0, counts = 0;
+        std::vector<uint32_t> by_block[4];  // template words, per row block in stream order
         for (int32_t z = s; z < s1; z++) {
           const uint32_t enc = (uint32_t)L.segs[z].ncols, mask = (enc >> kTcwMaskShift) & 15u;
           const bool pair = ((enc >> kSegTypeShift) & 1u) == (uint32_t)TF_HILO;
@@ -585,10 +586,10 @@ int build_tc_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms
             const uint32_t R = (R4 >> (8 * b)) & 0xffu;
             const uint32_t id = tcw_idesc(L.tcw_bf16 ? 1 : 0, std::max(16, (int)((R + 15) & ~15u)));
             const uint32_t blk = ((uint32_t)b << 13) | ((R * 16u) << 16);
-            L.tops.insert(L.tops.end(), {pre | blk, id, pre | (1u << 12) | blk, id});
+            by_block[b].insert(by_block[b].end(), {pre | blk, id, pre | (1u << 12) | blk, id});
             nops += 2;
             if (pair) {
-              L.tops.insert(L.tops.end(), {(pre + R) | blk, id});
+              by_block[b].insert(by_block[b].end(), {(pre + R) | blk, id});
               nops++;
             }
             pre += pair ? 2 * R : R;
@@ -598,8 +599,12 @@ int build_tc_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms
           msg = "an input group of more than 4 block jobs";
           return HMVM_ERANGE;
         }
+        for (int b = 0; b < 4; b++) {
+          L.tops.insert(L.tops.end(), by_block[b].begin(), by_block[b].end());
+          counts |= (uint32_t)(by_block[b].size() / 2) << (16 + 4 * b);
+        }
         L.tgroups.insert(L.tgroups.end(), {(uint32_t)f.src, (uint32_t)((nc + 7) / 8),
-                                           pre | (nops << 16) | (s1 == se ? kTcwGroupLast : 0u), op0});
+                                           pre | (s1 == se ? kTcwGroupLast : 0u) | counts, op0});
         s = s1;
       }
     }

@@ -152,9 +152,10 @@ def _tcw_idesc(bf, n):
 def _tcw_program(view, tiles, segs, blocks):
     """The step program the kernel's producer walks is the segments' own
     grouping: per input group its src word, vector count, rows per K step, MMA
-    count and last-group flag; per MMA (per segment, per block of its mask: hi x
-    x_hi, hi x x_lo, and lo x x_hi for pairs) its first B row, A part, block,
-    block rows and instruction descriptor; every B read stays inside its step."""
+    counts per row block and last-group flag; per MMA (per segment, per block of
+    its mask: hi x x_hi, hi x x_lo, and lo x x_hi for pairs; ordered by block)
+    its first B row, A part, block, block rows and instruction descriptor; every
+    B read stays inside its step."""
     ng, nops = view.n_tgroups, view.n_tops
     grp = np.ctypeslib.as_array(view.tgroups, (ng * 4,)).reshape(-1, 4).astype(np.int64)
     ops = np.ctypeslib.as_array(view.tops, ((nops + 12) * 2,)).reshape(-1, 2).astype(np.int64)
@@ -172,7 +173,7 @@ def _tcw_program(view, tiles, segs, blocks):
                     (int(segs[g1]["ncols"]) & 0xFFFFFF) == (int(segs[s]["ncols"]) & 0xFFFFFF):
                 g1 += 1
             nc = int(segs[s]["ncols"]) & 0xFFFFFF
-            want, pre = [], 0
+            per_block, pre = [[], [], [], []], 0
             for z in range(s, g1):
                 enc = int(segs[z]["ncols"])
                 mask, pair = (enc >> 24) & 0xF, (enc >> 28) & 1
@@ -181,13 +182,15 @@ def _tcw_program(view, tiles, segs, blocks):
                         continue
                     idesc = _tcw_idesc(view.tcw_bf16, max(16, (R[b] + 15) & ~15))
                     blk = (b << 13) | ((R[b] * 16) << 16)
-                    want += [(pre | blk, idesc), (pre | (1 << 12) | blk, idesc)]
+                    per_block[b] += [(pre | blk, idesc), (pre | (1 << 12) | blk, idesc)]
                     if pair:
-                        want.append(((pre + R[b]) | blk, idesc))
+                        per_block[b].append(((pre + R[b]) | blk, idesc))
                     pre += 2 * R[b] if pair else R[b]
+            want = [t for b in range(4) for t in per_block[b]]  # each block's MMAs together
+            counts = sum(len(per_block[b]) << (16 + 4 * b) for b in range(4))
             h = grp[gi]
             assert h[0] == int(segs[s]["src"]) & 0xFFFFFFFF and h[1] == (nc + 7) // 8
-            assert h[2] == pre | (len(want) << 16) | ((1 << 20) if g1 == s1 else 0) and h[3] == oi
+            assert h[2] == pre | ((1 << 12) if g1 == s1 else 0) | counts and h[3] == oi
             assert len(want) <= 12
             got = [tuple(int(v) for v in ops[oi + q]) for q in range(len(want))]
             assert got == want, (k, s, got, want)
