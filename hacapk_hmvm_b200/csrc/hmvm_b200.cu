@@ -386,7 +386,7 @@ int encode_planes_map(CUtensorMap* map, void* base, int64_t rows) {
   if (!fn) return set_error(HMVM_ECUDA, "cuTensorMapEncodeTiled is not available");
   const cuuint64_t dims[3] = {64, (cuuint64_t)rows, 4};
   const cuuint64_t strides[2] = {128, (cuuint64_t)rows * 128};
-  const cuuint32_t box[3] = {64, 16, 4};
+  const cuuint32_t box[3] = {64, (cuuint32_t)kTcwStepCols, 4};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, base, dims, strides, box, estr,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,

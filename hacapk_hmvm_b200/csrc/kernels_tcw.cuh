@@ -6,14 +6,14 @@
 // GEMM orientation: Y^T = X^T H^T, so the MMA (kind::f16, cta_group::1) has
 //   M = 128 right-hand sides (TMEM lanes),
 //   N = the item's rows rounded up to 16 (<= 32 row-stage, <= 128 V-stage),
-//   K = 16 matrix columns,
+//   K = 16 matrix columns (a K step of the pipeline is 32: two MMA "halves"),
 //   A = the inputs, 16-bit hi and lo parts of 128 right-hand sides, held in
 //       four "chunk" arrays [4][rows][64] (chunk 0/1: hi of right-hand sides
 //       0..63 / 64..127, chunk 2/3: their lo parts); one TMA tensor copy per K
-//       step (a 3-D box {64, 16, 4}, 128-byte rows, SWIZZLE_128B) lands as the
-//       canonical 128-byte-swizzled MN-major layout: per chunk 16 K rows of
-//       128 bytes, 8-row atoms 1 KiB apart, the next 64 right-hand sides 2 KiB
-//       on;
+//       step (a 3-D box {64, 32, 4}, 128-byte rows, SWIZZLE_128B) lands as the
+//       canonical 128-byte-swizzled MN-major layout: per chunk 32 K rows of
+//       128 bytes, 8-row atoms 1 KiB apart, the second half 2 KiB on, the next
+//       64 right-hand sides 4 KiB on;
 //   B = the matrix, K-major without swizzle, read by the MMA straight from the
 //       ring the bulk copies fill (8-row core matrices 128 B apart, the second
 //       8 columns R*16 B on; the missing half of an odd last step points at a
@@ -30,12 +30,12 @@
 // One CTA of 9 warps per SM, warp-specialised:
 //   warp 0               producer (the whole warp; lane 0 issues the copies):
 //                        per K step a bulk copy of its matrix bytes into the
-//                        current 8 KiB slot of a 12-slot ring (a slot --
-//                        "chunk" -- takes whole K steps, at most 8, across
+//                        current 16 KiB slot of a 6-slot ring (a slot --
+//                        "chunk" -- takes whole K steps, at most 6, across
 //                        segments and items; each copy adds its bytes with
 //                        mbarrier.expect_tx and the chunk is closed by one
 //                        arrive), a TMA tensor copy of the K step's inputs
-//                        into a 14 x 8 KiB ring, and beside the input slot the
+//                        into a 7 x 16 KiB ring, and beside the input slot the
 //                        step's MMAs fully formed (16 bytes each, lane q the
 //                        q-th) from the host-built step program;
 //   warps 1..4           MMA issue, one thread each: warp 1 + b issues row
@@ -67,11 +67,13 @@
 
 namespace hmvm {
 
-constexpr int kTcwSlotM = 8192;   // matrix ring chunk: whole K steps (one K step of an item is <= 8 KiB)
-constexpr int kTcwSlotsM = 12;
-constexpr int kTcwChunkSteps = 8; // K steps per chunk at most (< kTcwSlotsA)
-constexpr int kTcwSlotA = 8192;   // one K step of inputs: 4 chunks x 16 rows x 128 B
-constexpr int kTcwSlotsA = 14;
+// A K step covers 32 matrix columns: two 16-column MMA steps ("halves").
+constexpr int kTcwStepCols = 32;
+constexpr int kTcwSlotM = 16384;  // matrix ring chunk: whole K steps (one K step of an item is <= 16 KiB)
+constexpr int kTcwSlotsM = 6;
+constexpr int kTcwChunkSteps = 6; // K steps per chunk at most (< kTcwSlotsA)
+constexpr int kTcwSlotA = 16384;  // one K step of inputs: 4 chunks x 32 rows x 128 B
+constexpr int kTcwSlotsA = 7;
 static_assert(kTcwChunkSteps < kTcwSlotsA, "a chunk must hold fewer K steps than the input ring has slots");
 constexpr int kTcwThreads = 288;  // producer, 4 MMA-issue warps, 4 epilogue warps
 // Zeros: the B operand of the per-item MMA that clears the accumulators (256
@@ -80,12 +82,13 @@ constexpr int kTcwThreads = 288;  // producer, 4 MMA-issue warps, 4 epilogue war
 constexpr int kTcwZeroBytes = 8192;
 constexpr int kTcwOffA = kTcwSlotsM * kTcwSlotM;
 constexpr int kTcwOffZero = kTcwOffA + kTcwSlotsA * kTcwSlotA;
-// Per input slot, the MMAs of its K step as the producer formed them (at most
-// kTcwMaxOps, ordered by row block), 16 bytes each, and a header word (per row
-// block its MMA count in 4 bits, flags).
-constexpr uint32_t kTcwNewChunk = 1u << 16, kTcwLastStep = 1u << 17;  // header flags
+// Per input slot, the MMAs of its K step as the producer formed them, per half
+// at most kTcwMaxOps ordered by row block, 16 bytes each, and a header word
+// (per row block its MMA count per half in 4 bits, flags).
+constexpr uint32_t kTcwNewChunk = 1u << 16, kTcwLastStep = 1u << 17, kTcwTwoHalves = 1u << 18;  // header flags
+constexpr int kTcwOpsPerSlot = 2 * kTcwMaxOps;
 constexpr int kTcwOffOps = kTcwOffZero + kTcwZeroBytes;
-constexpr int kTcwOffHdr = kTcwOffOps + kTcwSlotsA * kTcwMaxOps * 16;
+constexpr int kTcwOffHdr = kTcwOffOps + kTcwSlotsA * kTcwOpsPerSlot * 16;
 constexpr int kTcwOffBar = kTcwOffHdr + ((kTcwSlotsA * 4 + 15) & ~15);
 constexpr int kTcwNumBars = 2 * kTcwSlotsM + 2 * kTcwSlotsA + 2 * 4 + 1;
 constexpr int kTcwOffMisc = kTcwOffBar + kTcwNumBars * 8;
@@ -244,8 +247,9 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
       uint4* ops = reinterpret_cast<uint4*>(tcw_smem + kTcwOffOps);
       uint32_t* hdr = reinterpret_cast<uint32_t*>(tcw_smem + kTcwOffHdr);
       const uint32_t zaddr = smem_u32(zero);
-      // A: input slot 0's hi part; slot s is (8 KiB * s) >> 4 further on, its lo part 4 KiB on
-      const uint32_t alo0 = (uint32_t)tc_desc_sw128(smem_u32(ringA), 2048, 1024);
+      // A: input slot 0's first half, hi part (the two 64-rhs chunks 4 KiB apart); slot s is
+      // (16 KiB * s) >> 4 further on, the second half 2 KiB on, the lo part 8 KiB on
+      const uint32_t alo0 = (uint32_t)tc_desc_sw128(smem_u32(ringA), 4096, 1024);
       const int g0 = a.gfirst[tb], gend = a.gfirst[te];
       const int glast = max(gend - 1, 0);  // window loads past the team's groups read its last one
       const int tlast = a.n_gops - 1;
@@ -276,7 +280,8 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
           T0 = T1;
           T1 = a.gops[min((int)tw + 32 + lane, tlast)];
         }
-        const uint32_t ti = tc - tw + (uint32_t)min(lane, kTcwMaxOps - 1);
+        const int hq = lane >= kTcwMaxOps ? 1 : 0, q = lane - hq * kTcwMaxOps;  // lane: half hq, MMA q
+        const uint32_t ti = tc - tw + (uint32_t)min(q, kTcwMaxOps - 1);
         const uint32_t t0x = __shfl_sync(0xffffffffu, T0.x, (int)(ti & 31u));
         const uint32_t t0y = __shfl_sync(0xffffffffu, T0.y, (int)(ti & 31u));
         const uint32_t t1x = __shfl_sync(0xffffffffu, T1.x, (int)(ti & 31u));
@@ -284,11 +289,12 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
         const uint2 tp = ti < 32u ? make_uint2(t0x, t0y) : make_uint2(t1x, t1y);
         tc += nops;
         const CUtensorMap* map = (gh.x >> 31) ? &tmap : &xmap;
-        const int row0 = (int)(gh.x & 0x7fffffffu), nv = (int)gh.y, nks = (nv + 1) >> 1;
+        const int row0 = (int)(gh.x & 0x7fffffffu), nv = (int)gh.y, nks = (nv + 3) >> 2;
         const uint32_t prow = tp.x & 0xfffu, alo = (tp.x >> 12) & 1u, blk = (tp.x >> 13) & 3u, rb16 = tp.x >> 16;
         for (int j = 0; j < nks; j++) {
-          const uint32_t nvj = (uint32_t)min(2, nv - 2 * j);
-          const uint32_t kb = nvj * 16u * hrows;
+          // 8-column vectors of the two halves (an odd last one: 1; a missing second half: 0)
+          const uint32_t nvj0 = (uint32_t)min(2, nv - 4 * j), nvj1 = (uint32_t)max(0, min(2, nv - 4 * j - 2));
+          const uint32_t kb0 = nvj0 * 16u * hrows, kb = kb0 + nvj1 * 16u * hrows;
           uint32_t flags = 0;
           if (!open || used + kb > (uint32_t)kTcwSlotM || cnt == kTcwChunkSteps) {
             ms = mI % kTcwSlotsM;
@@ -320,21 +326,23 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
             break;
           }
           if ((gh.z & kTcwGroupLast) && j + 1 == nks) flags |= kTcwLastStep;
-          if ((uint32_t)lane < nops) {
-            // B: the block's rows from prow on, K-major core matrices; an odd last step's
-            // second 8 columns read the zero block
-            const uint32_t start = cbase + used + nvj * 16u * prow;
-            const uint32_t lbo = nvj == 2 ? rb16 : zaddr - start;
-            ops[as * kTcwMaxOps + lane] =
-                make_uint4(alo0 + (uint32_t)as * (uint32_t)(kTcwSlotA >> 4) + alo * (4096u >> 4),
+          const uint32_t nvjh = hq ? nvj1 : nvj0;
+          if ((uint32_t)q < nops && nvjh > 0) {
+            // B: the block's rows from prow on in the half's vectors, K-major core matrices; an odd
+            // last half's second 8 columns read the zero block
+            const uint32_t start = cbase + used + (hq ? kb0 : 0u) + nvjh * 16u * prow;
+            const uint32_t lbo = nvjh == 2 ? rb16 : zaddr - start;
+            ops[as * kTcwOpsPerSlot + hq * (int)nops + q] =
+                make_uint4(alo0 + (uint32_t)as * (uint32_t)(kTcwSlotA >> 4) + (uint32_t)hq * (2048u >> 4) +
+                               alo * (8192u >> 4),
                            ((start >> 4) & 0x3fffu) | (((lbo >> 4) & 0x3fffu) << 16), blk * (uint32_t)G::bstride,
                            tp.y);
           }
           __syncwarp();
           if (lane == 0) {
-            hdr[as] = counts | flags;
+            hdr[as] = counts | flags | (nvj1 > 0 ? kTcwTwoHalves : 0u);
             mbar_expect_tx(&afull[as], kTcwSlotA);
-            tma_load_3d(ringA + as * kTcwSlotA, map, 0, row0 + 16 * j, 0, &afull[as]);
+            tma_load_3d(ringA + as * kTcwSlotA, map, 0, row0 + kTcwStepCols * j, 0, &afull[as]);
           }
           aI++;
           g += kb;
@@ -403,20 +411,24 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
             open = true;
           }
           tc_fence_after();  // the MMAs below are ordered after the waits that saw their operands land
-          uint32_t off = 0;  // this block's first MMA in the list: the counts of the blocks before it
+          uint32_t off = 0;  // this block's first MMA in a half's list: the counts of the blocks before it
 #pragma unroll
           for (int c = 0; c < 3; c++)
             if (c < b) off += (h >> (4 * c)) & 15u;
           const uint32_t n = (h >> (4 * b)) & 15u;
-          const uint4* o = ops + as * kTcwMaxOps + off;
-          // a compact loop (an unrolled one measured slower), the next MMA's record loaded ahead
-          // (past the last it reads the next slot's, or the header words: inside shared memory)
-          uint4 r = o[0];
+          const uint32_t nall = (h & 15u) + ((h >> 4) & 15u) + ((h >> 8) & 15u) + ((h >> 12) & 15u);
+          const uint4* o = ops + as * kTcwOpsPerSlot + off;
+          // this block's MMAs of each half: the half's list holds nall; the loop is compact (an
+          // unrolled one measured slower), the next record loaded ahead (past the last it reads a
+          // later record or the header words: inside shared memory)
+          for (int half = 0; half < ((h & kTcwTwoHalves) ? 2 : 1); half++, o += nall) {
+            uint4 r = o[0];
 #pragma unroll 1
-          for (uint32_t k = 0; k < n; k++) {
-            const uint4 nx = o[k + 1];
-            tc_mma(dbase + r.z, ahi | r.x, bhi | r.y, r.w, 1);
-            r = nx;
+            for (uint32_t k = 0; k < n; k++) {
+              const uint4 nx = o[k + 1];
+              tc_mma(dbase + r.z, ahi | r.x, bhi | r.y, r.w, 1);
+              r = nx;
+            }
           }
           tc_commit(&aempty[as]);
         }
