@@ -101,6 +101,8 @@ struct TcwGeom {
   static constexpr int cols = VST ? 256 : 128;
   static constexpr int bstride = VST ? 128 : 32;
   static constexpr int issuers = VST ? 2 : 4;  // row blocks: one MMA-issue warp each
+  static constexpr int cpb = VST ? 4 : 1;      // 32-row chunks of a row block at most
+  static constexpr int chunks = issuers * cpb; // 32-row chunks of an item at most
   static_assert(bufs * cols == 512, "the CTA owns the SM's 512 TMEM columns");
 };
 
@@ -447,36 +449,80 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
     const int q = warp & 3;
     const int r = 32 * q + lane;  // this thread's right-hand side
     const double sx = a.xscale[r];
+    // The scale (and t slot) of row 32 k + lane of an item's chunk k (chunk k = 32-row
+    // piece k % cpb of row block k / cpb), loaded a whole item ahead; the descriptors
+    // two items ahead; a chunk's values are then taken by shuffles.
+    struct Rows {
+      float ts[G::chunks];
+      int32_t sl[G::chunks];
+    };
+    auto load_rows = [&](const hmvm_tile_desc& d, uint32_t R4, Rows& rw) {
+      const int mode = d.mode & 3;
+      int rb = 0;
+#pragma unroll
+      for (int b = 0; b < G::issuers; b++) {
+        const int Rb = (int)((R4 >> (8 * b)) & 0xffu);
+#pragma unroll
+        for (int c = 0; c < G::cpb; c++) {
+          const bool in = lane < Rb - 32 * c;
+          const int row = rb + 32 * c + lane;
+          rw.ts[b * G::cpb + c] = in ? a.tscale[d._pad + row] : 0.f;
+          rw.sl[b * G::cpb + c] = (VST && in && mode == 1) ? a.out_idx[d.out_base + row] : 0;
+        }
+        rb += Rb;
+      }
+    };
+    hmvm_tile_desc dc, dn;
+    uint32_t Rc = 0, Rn = 0;
+    Rows rc, rn;
+    if (tb < te) {
+      dc = a.tiles[tb];
+      Rc = (uint32_t)a.blocks[tb];
+      load_rows(dc, Rc, rc);
+    }
+    if (tb + 1 < te) {
+      dn = a.tiles[tb + 1];
+      Rn = (uint32_t)a.blocks[tb + 1];
+    }
     uint32_t ic = 0;
     for (int it = tb; it < te; it++, ic++) {
-      const hmvm_tile_desc d = a.tiles[it];
-      const uint32_t R4 = (uint32_t)a.blocks[it];
+      const hmvm_tile_desc d = dc;
+      const uint32_t R4 = Rc;
+      if (it + 1 < te) load_rows(dn, Rn, rn);  // the next item's rows, in flight during this one
+      hmvm_tile_desc dnn = dn;
+      uint32_t Rnn = 0;
+      if (it + 2 < te) {
+        dnn = a.tiles[it + 2];
+        Rnn = (uint32_t)a.blocks[it + 2];
+      }
       const int buf = ic % G::bufs;
+      const int mode = d.mode & 3, has = (d.mode >> 4) & 15;
       if (!warp_wait(&accfull[buf], (ic / G::bufs) & 1)) {
         if (lane == 0) atomicExch(a.err, 1);
         break;
       }
       tc_fence_after();
-      const int mode = d.mode & 3, has = (d.mode >> 4) & 15;
       int rb = 0;  // the block's first item row
-      for (int b = 0; b < 4; b++) {
-        const int Rb = (R4 >> (8 * b)) & 0xff;
-        if (!Rb) continue;
-        const uint32_t tbase =
-            tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * G::cols + b * G::bstride);
+      for (int b = 0; b < G::issuers; b++) {
+        const int Rb = (int)((R4 >> (8 * b)) & 0xffu);
+        if (!Rb) break;  // blocks after the last are empty
         for (int c0 = 0; c0 < Rb; c0 += 32) {
+          const int k = b * G::cpb + (c0 >> 5), nrow = min(32, Rb - c0), row = rb + c0;
+          float ts_l = rc.ts[0];
+          int32_t slot_l = rc.sl[0];
+#pragma unroll
+          for (int j = 1; j < G::chunks; j++) {
+            ts_l = k == j ? rc.ts[j] : ts_l;
+            slot_l = k == j ? rc.sl[j] : slot_l;
+          }
           float v[32];
           if (has >> b & 1) {
-            tc_ld32(tbase + (uint32_t)c0, v);
+            tc_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * G::cols + b * G::bstride + c0), v);
           } else {
 #pragma unroll
             for (int i = 0; i < 32; i++) v[i] = 0.f;
           }
-          const int nrow = min(32, Rb - c0), row = rb + c0;
-          // row i's scale (and t slot) from lane i, taken by shuffles
-          const float ts_l = lane < nrow ? a.tscale[d._pad + row + lane] : 0.f;
           if constexpr (VST) {
-            const int32_t slot_l = (mode == 1 && lane < nrow) ? a.out_idx[d.out_base + row + lane] : 0;
 #pragma unroll
             for (int i = 0; i < 32; i++) {
               const float ts = __shfl_sync(0xffffffffu, ts_l, i);
@@ -508,6 +554,11 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
         }
         rb += Rb;
       }
+      dc = dn;
+      Rc = Rn;
+      rc = rn;
+      dn = dnn;
+      Rn = Rnn;
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&accempty[buf]);
