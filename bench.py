@@ -337,23 +337,30 @@ def run_reference(a, rank):
 
 
 # Right-hand sides from which FP32 and mixed workloads run on the wide tensor-core form.
-TC_WIDE_MIN = 16
+TC_WIDE_MIN = 32  # from here the wide tensor-core form (128 right-hand sides per pass)
+TC16_MIN = 16     # mixed plans from here: the 16-wide tensor-core pass
+
+
+def plan_width(precision, nrhs):
+    """nrhs_max of the plan a workload of nrhs right-hand sides runs on."""
+    if precision in ("fp32", "mixed") and nrhs >= TC_WIDE_MIN:
+        return 128
+    if precision == "mixed" and nrhs >= TC16_MIN:
+        return 16
+    return min(nrhs, 8)
 
 
 def make_plan(hm, precision, nrhs, lr_format, device, a=None):
     """The plan a workload runs on: single-vector plans for nrhs 1, multi-RHS
-    plans sized for the pass width otherwise (tensor-core passes for mixed
-    plans from 16 right-hand sides)."""
+    plans sized for the pass width otherwise: the wide tensor-core form (128
+    right-hand sides per pass) from 32 right-hand sides, the 16-wide
+    tensor-core pass for mixed plans from 16."""
     from hacapk_hmvm_b200 import Plan
 
     kw = {}
     if a is not None:
         kw = dict(stage1_cfg=a.stage1_cfg, stage2_cfg=a.stage2_cfg, ctas_per_sm=a.ctas_per_sm, kernel=a.kernel)
-    if precision in ("fp32", "mixed") and nrhs >= TC_WIDE_MIN:
-        nrhs_max = 128  # the wide tensor-core form: 128 right-hand sides per pass on tcgen05
-    else:
-        nrhs_max = min(nrhs, 8)
-    return Plan(hm, precision, device=device, nrhs_max=nrhs_max,
+    return Plan(hm, precision, device=device, nrhs_max=plan_width(precision, nrhs),
                 mixed_lr_format=lr_format if precision == "mixed" else None, **kw)
 
 
@@ -567,8 +574,7 @@ def run_secondary(a, hm, X, cpucols, fp64_rate, local_rank, stream, dev):
     import torch
 
     legs = []
-    key_of = lambda prec, nrhs, fmt: (prec, fmt, "single" if nrhs == 1 else
-                                      ("tc" if prec in ("fp32", "mixed") and nrhs >= TC_WIDE_MIN else "multi"))
+    key_of = lambda prec, nrhs, fmt: (prec, fmt, plan_width(prec, nrhs))
     plans = {}
     for i, (label, prec, nrhs, fmt) in enumerate(SECONDARY):
         key = key_of(prec, nrhs, fmt)
