@@ -221,10 +221,12 @@ def max_over_ranks(value: float, dist, device) -> float:
 DTYPES = {"fp64": "f64", "fp32": "f32",
           "mixed": "mixed: f32/f16/e4m3 low-rank, f32/f64 dense storage; f32 segment sums, f64 rows and x, y"}
 
-# ncu summaries that carry traffic_per_algorithmic_byte lines, by the single-vector
-# kernel they captured: FP64 stream kernel, mixed kernel (FP16 factors)
+# ncu summaries that carry traffic_per_algorithmic_byte lines, by the kernel they
+# captured: FP64 stream kernel, mixed kernel (FP16 factors), wide tensor-core
+# kernel (mixed, FP16 factors, 128 right-hand sides)
 TRAFFIC_PROFILES = {"fp64": os.path.join(ROOT, "profiles", "stream_kernel_fp64_sphere65536.md"),
-                    "mixed": os.path.join(ROOT, "profiles", "mixed_kernel_fp16_sphere65536.md")}
+                    "mixed": os.path.join(ROOT, "profiles", "mixed_kernel_fp16_sphere65536.md"),
+                    "tcw": os.path.join(ROOT, "profiles", "tcw_kernel_mixed_sphere65536_nrhs128.md")}
 
 
 def traffic_ratio(stage: int, precision: str = "fp64"):
@@ -394,10 +396,14 @@ def roofline_of(plan, info, nrhs, stage_ms, napplies, ms_step, precision, lr_for
     # a multi-RHS step streams the matrix once per pass and reads/writes every column once
     alg_bytes = info["algorithmic_bytes"] * passes + 2 * plan.nd * elem_xy * (nrhs - passes)
     kname = kernel_name(plan, info, nrhs)
-    ratio = None
+    ratio, tkey = None, None
     if dom in (0, 2) and nrhs == 1 and lr_format == "fp16" and (
             (info["kernel"] == 1 and precision == "fp64") or precision == "mixed"):
-        ratio = traffic_ratio(1 if dom == 0 else 2, precision)
+        tkey = precision
+    elif dom in (0, 2) and info["kernel"] == 4 and precision == "mixed" and lr_format == "fp16":
+        tkey = "tcw"
+    if tkey:
+        ratio = traffic_ratio(1 if dom == 0 else 2, tkey)
     roof = {
         "bound": "hbm",
         "kernel": [f"{kname} (V stage)", "hmvm_reduce_kernel (V stage)", f"{kname} (row stage)",
@@ -413,7 +419,7 @@ def roofline_of(plan, info, nrhs, stage_ms, napplies, ms_step, precision, lr_for
     }
     if ratio:
         roof["traffic_source"] = ("ncu capture of the same kernel at N=65536, scaled by algorithmic bytes ("
-                                  + os.path.relpath(TRAFFIC_PROFILES[precision], ROOT) + ")")
+                                  + os.path.relpath(TRAFFIC_PROFILES[tkey], ROOT) + ")")
     return roof, alg_bytes
 
 
