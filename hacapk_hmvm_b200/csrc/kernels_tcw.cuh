@@ -18,8 +18,12 @@
 //       ring the bulk copies fill (8-row core matrices 128 B apart, the second
 //       8 columns R*16 B on; the missing half of an odd last step points at a
 //       zero block);
-//   D = FP32 in TMEM: V stage 2 accumulator buffers of 256 columns (row block b
-//       at column 128 b), row stage 4 buffers of 128 columns (block b at 32 b).
+//   D = FP32 in TMEM, 2 accumulator buffers of 256 columns: V stage row block b
+//       at column 128 b, row stage at 32 b; the correction products (hi x x_lo,
+//       lo x x_hi) in a second accumulator where the block has room (row stage
+//       at 128 + 32 b, V-stage blocks of <= 64 rows at 128 b + 64), added to
+//       the main one in the epilogue: each addition into a TMEM accumulator
+//       rounds, and the main one then takes one per 16 columns, not three.
 // An item is up to 4 row blocks; a segment multiplies the blocks in its mask
 // by one input range, and consecutive segments with the same range form an
 // input group: per K step of a group one TMA copy of the inputs, then for each
@@ -95,11 +99,14 @@ constexpr int kTcwOffMisc = kTcwOffBar + kTcwNumBars * 8;
 constexpr int kTcwSmem = kTcwOffMisc + 32 + 1024;  // + room to align the base to 1 KiB
 static_assert(kTcwSmem <= 227 * 1024, "shared memory");
 // TMEM geometry per stage: accumulator buffers x columns, and the column stride of a row block
+// (a block's correction accumulator is corr columns after its main one: row
+// stage at 128 + 32 b, V stage at 128 b + 64 for blocks of <= 64 rows)
 template <bool VST>
 struct TcwGeom {
-  static constexpr int bufs = VST ? 2 : 4;
-  static constexpr int cols = VST ? 256 : 128;
+  static constexpr int bufs = 2;
+  static constexpr int cols = 256;
   static constexpr int bstride = VST ? 128 : 32;
+  static constexpr int corr = VST ? 64 : 128;
   static constexpr int issuers = VST ? 2 : 4;  // row blocks: one MMA-issue warp each
   static constexpr int cpb = VST ? 4 : 1;      // 32-row chunks of a row block at most
   static constexpr int chunks = issuers * cpb; // 32-row chunks of an item at most
@@ -293,6 +300,7 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
         const CUtensorMap* map = (gh.x >> 31) ? &tmap : &xmap;
         const int row0 = (int)(gh.x & 0x7fffffffu), nv = (int)gh.y, nks = (nv + 3) >> 2;
         const uint32_t prow = tp.x & 0xfffu, alo = (tp.x >> 12) & 1u, blk = (tp.x >> 13) & 3u, rb16 = tp.x >> 16;
+        const uint32_t dcol = blk * (uint32_t)G::bstride + ((tp.x & kTcwCorrBit) ? (uint32_t)G::corr : 0u);
         for (int j = 0; j < nks; j++) {
           // 8-column vectors of the two halves (an odd last one: 1; a missing second half: 0)
           const uint32_t nvj0 = (uint32_t)min(2, nv - 4 * j), nvj1 = (uint32_t)max(0, min(2, nv - 4 * j - 2));
@@ -337,8 +345,7 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
             ops[as * kTcwOpsPerSlot + hq * (int)nops + q] =
                 make_uint4(alo0 + (uint32_t)as * (uint32_t)(kTcwSlotA >> 4) + (uint32_t)hq * (2048u >> 4) +
                                alo * (8192u >> 4),
-                           ((start >> 4) & 0x3fffu) | (((lbo >> 4) & 0x3fffu) << 16), blk * (uint32_t)G::bstride,
-                           tp.y);
+                           ((start >> 4) & 0x3fffu) | (((lbo >> 4) & 0x3fffu) << 16), dcol, tp.y);
           }
           __syncwarp();
           if (lane == 0) {
@@ -371,7 +378,8 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
       // descriptor high words: stride byte offset, version, layout (128-byte swizzle for A)
       const uint64_t ahi = tc_desc_sw128(0, 0, 1024) & 0xffffffff00000000ull;
       const uint64_t bhi = tc_desc(0, 0, 128) & 0xffffffff00000000ull;
-      // the clearing MMA: zeros x zeros over the block's columns
+      // the clearing MMA: zeros x zeros over the block's columns (V stage: its main and
+      // correction accumulators; row stage: the main one, and a second for the correction one)
       const uint32_t zaddr = smem_u32(zero);
       const uint64_t zadesc = tc_desc_sw128(zaddr, 2048, 1024);
       const uint64_t zbdesc = tc_desc(zaddr, 4096, 128);
@@ -390,7 +398,10 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
         }
         tc_fence_after();
         const uint32_t dbase = tmem_base + (uint32_t)(buf * G::cols);
-        if (nseg > 0) tc_mma(dbase + (uint32_t)(b * G::bstride), zadesc, zbdesc, zidesc, 0);
+        if (nseg > 0) {
+          tc_mma(dbase + (uint32_t)(b * G::bstride), zadesc, zbdesc, zidesc, 0);
+          if (!VST) tc_mma(dbase + (uint32_t)(b * G::bstride + G::corr), zadesc, zbdesc, zidesc, 0);
+        }
         bool last = nseg == 0;
         while (!last) {
           const int as = aC % kTcwSlotsA;
@@ -517,7 +528,14 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
           }
           float v[32];
           if (has >> b & 1) {
-            tc_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * G::cols + b * G::bstride + c0), v);
+            const uint32_t ta = tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(buf * G::cols + b * G::bstride + c0);
+            tc_ld32(ta, v);
+            if (!VST || Rb <= 64) {  // plus the correction accumulator
+              float w[32];
+              tc_ld32(ta + (uint32_t)G::corr, w);
+#pragma unroll
+              for (int i = 0; i < 32; i++) v[i] += w[i];
+            }
           } else {
 #pragma unroll
             for (int i = 0; i < 32; i++) v[i] = 0.f;

@@ -195,10 +195,14 @@ enum TcwFmt : int32_t { TF_HI = 0, TF_HILO = 1 };
 // and per MMA of a K step (ordered by row block: block b's MMAs are issued by
 // their own warp) a 2-word template:
 //   [0] first B row (in 16-byte units of the step's vectors) | A lo part << 12 | block << 13 |
-//       the block's rows * 16 << 16
+//       into the block's correction accumulator << 15 | the block's rows * 16 << 16
 //   [1] instruction descriptor
+// The correction products (hi x x_lo, lo x x_hi, about 2^-11 of the main ones)
+// go to a second accumulator where the block has room for one, so the main
+// accumulator takes one rounding per 16 columns instead of three.
 constexpr int kTcwMaxOps = 12;         // MMAs of one K step at most (4 block jobs x 3 products)
 constexpr uint32_t kTcwGroupLast = 1u << 12;
+constexpr uint32_t kTcwCorrBit = 1u << 15;
 #if defined(__CUDACC__)
 #define HMVM_TCW_HD __host__ __device__
 #else

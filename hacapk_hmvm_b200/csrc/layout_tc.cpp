@@ -586,10 +586,13 @@ int build_tc_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms
             const uint32_t R = (R4 >> (8 * b)) & 0xffu;
             const uint32_t id = tcw_idesc(L.tcw_bf16 ? 1 : 0, std::max(16, (int)((R + 15) & ~15u)));
             const uint32_t blk = ((uint32_t)b << 13) | ((R * 16u) << 16);
-            by_block[b].insert(by_block[b].end(), {pre | blk, id, pre | (1u << 12) | blk, id});
+            // the correction products (hi x x_lo, lo x x_hi) into their own accumulator where
+            // the block has room for one (every row-stage block; V-stage blocks of <= 64 rows)
+            const uint32_t corr = (k >= L.stage1_tiles || R <= 64u) ? kTcwCorrBit : 0u;
+            by_block[b].insert(by_block[b].end(), {pre | blk, id, pre | (1u << 12) | blk | corr, id});
             nops += 2;
             if (pair) {
-              by_block[b].insert(by_block[b].end(), {(pre + R) | blk, id});
+              by_block[b].insert(by_block[b].end(), {(pre + R) | blk | corr, id});
               nops++;
             }
             pre += pair ? 2 * R : R;

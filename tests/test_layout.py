@@ -154,8 +154,9 @@ def _tcw_program(view, tiles, segs, blocks):
     grouping: per input group its src word, vector count, rows per K step, MMA
     counts per row block and last-group flag; per MMA (per segment, per block of
     its mask: hi x x_hi, hi x x_lo, and lo x x_hi for pairs; ordered by block)
-    its first B row, A part, block, block rows and instruction descriptor; every
-    B read stays inside its step."""
+    its first B row, A part, block, correction-accumulator flag (the correction
+    products of row-stage blocks and of V-stage blocks of <= 64 rows), block rows
+    and instruction descriptor; every B read stays inside its step."""
     ng, nops = view.n_tgroups, view.n_tops
     grp = np.ctypeslib.as_array(view.tgroups, (ng * 4,)).reshape(-1, 4).astype(np.int64)
     ops = np.ctypeslib.as_array(view.tops, ((nops + 12) * 2,)).reshape(-1, 2).astype(np.int64)
@@ -182,9 +183,10 @@ def _tcw_program(view, tiles, segs, blocks):
                         continue
                     idesc = _tcw_idesc(view.tcw_bf16, max(16, (R[b] + 15) & ~15))
                     blk = (b << 13) | ((R[b] * 16) << 16)
-                    per_block[b] += [(pre | blk, idesc), (pre | (1 << 12) | blk, idesc)]
+                    corr = (1 << 15) if (k >= view.stage1_tiles or R[b] <= 64) else 0  # own accumulator
+                    per_block[b] += [(pre | blk, idesc), (pre | (1 << 12) | blk | corr, idesc)]
                     if pair:
-                        per_block[b].append(((pre + R[b]) | blk, idesc))
+                        per_block[b].append(((pre + R[b]) | blk | corr, idesc))
                     pre += 2 * R[b] if pair else R[b]
             want = [t for b in range(4) for t in per_block[b]]  # each block's MMAs together
             counts = sum(len(per_block[b]) << (16 + 4 * b) for b in range(4))
