@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the secondary workloads (FP32, mixed, multi-RHS) timed after the headline")
     ap.add_argument("--secondary-steps", type=int, default=40, help="timed steps of each single-vector secondary leg")
+    ap.add_argument("--no-batch-leg", action="store_true",
+                    help="default run: skip the batch workload (config C4) among the secondary legs")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own hybrid2 CUDA kernels on this GPU")
     ap.add_argument("--reference-gpu-runs", type=int, default=20, help="timed runs of the reference's GPU kernel")
@@ -754,6 +756,11 @@ def run_b200(a, rank, world, local_rank):
             cpu_line.update(cpu_bench_variants(cpu, x, a.cpu_seconds))
         if secondary:
             legs = run_secondary(a, hm, X, cpucols, 1e3 / ms_step, local_rank, stream, dev)
+            if not a.no_batch_leg:
+                try:
+                    legs.append(batch_leg(a, local_rank))
+                except Exception as e:  # reported in its place
+                    legs.append({"workload": batch_workload_text(a), "error": f"{type(e).__name__}: {e}"})
         if secondary and not a.no_reference_gpu:
             ours = {"fp64": 1e3 / ms_step}
             for leg in legs or []:
@@ -815,9 +822,11 @@ def batch_specs(a):
     return specs
 
 
-def run_batch(a, rank, world, local_rank):
-    """Many independent FP32 H-matrices: one block-diagonal batch plan replayed
-    as a CUDA graph, against a loop of per-matrix multi-RHS applies."""
+def measure_batch(a, local_rank, oracle=True):
+    """Many independent FP32 H-matrices: the batch (every class and pass in one
+    launch per stage) replayed as a CUDA graph, against a loop of per-matrix
+    applies.  With oracle, the graph's first column of every instance is checked
+    against the reference CPU HMVM in FP64 on the stored elements."""
     import torch
 
     from hacapk_hmvm_b200 import Batch, HMatrix, Plan
@@ -840,6 +849,7 @@ def run_batch(a, rank, world, local_rank):
     batch = Batch(mats, "fp32", device=local_rank, nrhs=nrhs)
     setup_s = time.perf_counter() - t0
     batch.capture(Xs, Yb)
+    kc = batch.kernel_count()
     plans = [Plan(m, "fp32", device=local_rank, nrhs_max=min(k, 8)) for m, k in zip(mats, nrhs)]
 
     def seq_step():
@@ -850,7 +860,7 @@ def run_batch(a, rank, world, local_rank):
                 pl.apply_multi(x, y, stream)
 
     def timed(fn, steps):
-        for _ in range(a.warmup):
+        for _ in range(max(a.warmup, 3)):
             fn()
         torch.cuda.synchronize(dev)
         e0 = torch.cuda.Event(enable_timing=True)
@@ -862,67 +872,110 @@ def run_batch(a, rank, world, local_rank):
         torch.cuda.synchronize(dev)
         return e0.elapsed_time(e1) / steps
 
+    steps = min(a.steps, 50)
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
     clocks = ClockSampler(vis.split(",")[local_rank].strip() if vis else str(local_rank))
     clocks.start()
     time.sleep(0.3)
-    ms_graph = timed(lambda: batch.launch(stream), a.steps)
+    ms_graph = timed(lambda: batch.launch(stream), steps)
     clk = clocks.stop()
-    ms_seq = timed(seq_step, max(3, a.steps // 4))
+    ms_seq = timed(seq_step, max(3, steps // 4))
     batch.status()
-    # parity: the graph's Y against the per-matrix plans' Y, and a few columns against the oracle port
     rel_seq = max(float(torch.linalg.norm((yb - ys).double()) / torch.linalg.norm(ys.double())) for yb, ys in zip(Yb, Ys))
-    rel_or = None
-    if rank == 0 and not a.no_cpu_baseline:
-        # the CPU HMVM (reference build, else the port) in FP64 on the FP32-stored elements of a sample
-        rel_or = 0.0
-        for i in range(0, len(mats), max(1, len(mats) // 6)):
-            m = mats[i]
+    rel_inst = None
+    kind = None
+    if oracle:
+        # every instance: its first column against the CPU HMVM (reference build, else the
+        # port) in FP64 on the FP32-stored elements, one instance converted at a time
+        rel_inst = []
+        for i, m in enumerate(mats):
             m64 = HMatrix.from_arrays(m.nd, m.ktmax, m.ltmtx, m.kt, m.ndl, m.ndt, m.nstrtl, m.nstrtt, m.a1, m.a2,
                                       m.rowmat.astype(np.float64))
             x0 = Xs[i][0].cpu().numpy().astype(np.float64)
             yo = np.empty(m.nd)
-            CpuReference(m64).run(x0, yo)
-            rel_or = max(rel_or, float(np.linalg.norm(Yb[i][0].cpu().numpy() - yo) / np.linalg.norm(yo)))
+            cpu = CpuReference(m64)
+            kind = cpu.kind
+            cpu.run(x0, yo)
+            rel_inst.append(float(np.linalg.norm(Yb[i][0].cpu().numpy() - yo) / np.linalg.norm(yo)))
+            del m64, cpu
     vecs = sum(nrhs)
     info = batch.info()
     peak, peak_kind = measured_peak_gbs()
-    kc = batch.kernel_count()
-    # each class streams its matrices once per pass (width 1, 2, 4 or 8 columns per pass)
+    # each class streams its matrices once per pass (2, 4 or 8 columns per pass)
     alg = 0
     for m, k in zip(mats, nrhs):
-        w = 1 if k <= 1 else 2 if k <= 2 else 4 if k <= 4 else 8
+        w = 2 if k <= 2 else 4 if k <= 4 else 8
         alg += m.stored_elements() * 4 * -(-k // w) + 8 * m.nd * k
     alg = int(alg)
-    if rank == 0:
-        line = {
-            "metric": "vectors/s", "value": vecs / (ms_graph * 1e-3), "unit": "vectors/s", "n_gpus": world,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_graph, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded HACApK-rule H-matrices; X uniform[-1,1])",
-            "config": {"workload": f"batch of {len(mats)} H-matrices, N log-uniform in [{a.batch_nmin}, "
-                                   f"{a.batch_nmax}], sphere/cube/plate, eta 1|2, ACA eps 1e-3|1e-4|1e-6, "
-                                   f"1..{a.batch_rhs_max} RHS each, FP32 storage, one CUDA-graph replay",
-                       "instances": [{"n": sp[0], "geometry": sp[1], "eta": sp[2], "eps": sp[3], "nrhs": sp[4]}
-                                     for sp in specs],
-                       "total_rows": int(sum(m.nd for m in mats)), "total_vectors": vecs,
-                       "classes": batch.class_count(),
-                       "device_bytes": info["device_bytes"], "batch_setup_s": setup_s, "generate_s": gen_s,
-                       "l2": "inputs larger than L2 (the batch's matrix bytes far exceed 126 MB)"},
-            "sequential_baseline": {"value": vecs / (ms_seq * 1e-3), "unit": "vectors/s", "ms_per_step": ms_seq,
-                                    "what": "per-matrix plans, one apply/apply_multi per matrix in a loop"},
-            "speedup_vs_sequential": ms_seq / ms_graph,
-            "relerr_graph_vs_sequential": rel_seq,
-            "relerr_vs_fp64_cpu_on_stored_elements_sampled": rel_or,
-            "roofline": {"bound": "hbm", "achieved": alg / (ms_graph * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
-                         "frac": alg / (ms_graph * 1e-3) / 1e9 / peak, "peak_source": peak_kind,
-                         "traffic": None, "scope": "whole graph replay (all kernels), algorithmic bytes"},
-            "clocks": clk, "gpu_launches": a.steps * kc,
-        }
-        print(json.dumps(line), flush=True)
+    out = {
+        "value": vecs / (ms_graph * 1e-3), "unit": "vectors/s", "ms_per_step": ms_graph, "steps": steps,
+        "specs": specs, "total_rows": int(sum(m.nd for m in mats)), "total_vectors": vecs,
+        "classes": batch.class_count(), "device_bytes": info["device_bytes"], "batch_setup_s": setup_s,
+        "generate_s": gen_s, "kernels_per_replay": kc,
+        "sequential_baseline": {"value": vecs / (ms_seq * 1e-3), "unit": "vectors/s", "ms_per_step": ms_seq,
+                                "what": "per-matrix plans, one apply/apply_multi per matrix in a loop"},
+        "speedup_vs_sequential": ms_seq / ms_graph,
+        "relerr_graph_vs_sequential": rel_seq,
+        "relerr_vs_fp64_cpu_reference": max(rel_inst) if rel_inst else None,
+        "relerr_instances_checked": len(rel_inst) if rel_inst else 0,
+        "relerr_per_instance": rel_inst,
+        "relerr_kind": kind,
+        "roofline": {"bound": "hbm", "achieved": alg / (ms_graph * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (ms_graph * 1e-3) / 1e9 / peak, "peak_source": peak_kind,
+                     "traffic": None, "scope": "whole graph replay (all kernels), algorithmic bytes"},
+        "clocks": clk,
+    }
     for pl in plans:
         pl.close()
     batch.close()
+    return out
+
+
+def batch_workload_text(a):
+    return (f"batch of {a.batch_count} H-matrices, N log-uniform in [{a.batch_nmin}, {a.batch_nmax}], "
+            f"sphere/cube/plate, eta 1|2, ACA eps 1e-3|1e-4|1e-6, 1..{a.batch_rhs_max} RHS each, FP32 storage, "
+            f"one CUDA-graph replay")
+
+
+def run_batch(a, rank, world, local_rank):
+    """The batch workload's own JSON line."""
+    r = measure_batch(a, local_rank, oracle=rank == 0 and not a.no_cpu_baseline)
+    if rank == 0:
+        line = {
+            "metric": "vectors/s", "value": r["value"], "unit": "vectors/s", "n_gpus": world,
+            "steps": r["steps"], "warmup": a.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded HACApK-rule H-matrices; X uniform[-1,1])",
+            "config": {"workload": batch_workload_text(a),
+                       "instances": [{"n": sp[0], "geometry": sp[1], "eta": sp[2], "eps": sp[3], "nrhs": sp[4]}
+                                     for sp in r["specs"]],
+                       "total_rows": r["total_rows"], "total_vectors": r["total_vectors"],
+                       "classes": r["classes"], "device_bytes": r["device_bytes"],
+                       "batch_setup_s": r["batch_setup_s"], "generate_s": r["generate_s"],
+                       "l2": "inputs larger than L2 (the batch's matrix bytes far exceed 126 MB)"},
+            "sequential_baseline": r["sequential_baseline"],
+            "speedup_vs_sequential": r["speedup_vs_sequential"],
+            "relerr_graph_vs_sequential": r["relerr_graph_vs_sequential"],
+            "relerr_vs_fp64_cpu_reference": r["relerr_vs_fp64_cpu_reference"],
+            "relerr_instances_checked": r["relerr_instances_checked"],
+            "roofline": r["roofline"],
+            "clocks": r["clocks"], "gpu_launches": r["steps"] * r["kernels_per_replay"],
+            "kernels_per_replay": r["kernels_per_replay"],
+        }
+        print(json.dumps(line), flush=True)
+
+
+def batch_leg(a, local_rank):
+    """The batch workload as a secondary leg of the default run."""
+    r = measure_batch(a, local_rank, oracle=True)
+    return {"workload": batch_workload_text(a), "precision": "fp32", "unit": r["unit"], "value": r["value"],
+            "ms_per_step": r["ms_per_step"], "steps": r["steps"], "classes": r["classes"],
+            "kernels_per_replay": r["kernels_per_replay"], "total_vectors": r["total_vectors"],
+            "sequential_baseline": r["sequential_baseline"], "speedup_vs_sequential": r["speedup_vs_sequential"],
+            "relerr_vs_fp64_cpu_reference": r["relerr_vs_fp64_cpu_reference"],
+            "relerr_instances_checked": r["relerr_instances_checked"], "relerr_kind": r["relerr_kind"],
+            "relerr_graph_vs_sequential": r["relerr_graph_vs_sequential"], "roofline": r["roofline"],
+            "gpu_launches": r["steps"] * r["kernels_per_replay"]}
 
 
 def main():

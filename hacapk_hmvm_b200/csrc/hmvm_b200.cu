@@ -416,7 +416,9 @@ int tcw_buffers(hmvm_plan* p, const HostLayout& L) {
   return rc;
 }
 
-int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** out) {
+// sms_cap > 0: plan the layout's teams for that many SMs (a batch class shares the GPU
+// with the other classes of its batch, which run in the same launches).
+int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** out, int sms_cap = 0) {
   if (!out) return set_error(HMVM_EINVAL, "plan output pointer is NULL");
   *out = nullptr;
   hmvm_plan_opts opts;
@@ -439,7 +441,8 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   HostLayout* L = new (std::nothrow) HostLayout();
   if (!L) return set_error(HMVM_ENOMEM, "host allocation failed");
   std::string msg;
-  rc = want_tcw ? build_tc_layout(lt, opts, sms, *L, msg) : build_layout(lt, opts, sms, *L, msg, ctas2);
+  const int lsms = sms_cap > 0 ? std::min(sms, sms_cap) : sms;
+  rc = want_tcw ? build_tc_layout(lt, opts, lsms, *L, msg) : build_layout(lt, opts, lsms, *L, msg, ctas2);
   if (rc) {
     delete L;
     return set_error(rc, msg);
@@ -456,7 +459,7 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   p->nlf = L->nlf;
   p->n_lowrank = L->n_lowrank;
   p->n_dense = L->n_dense;
-  p->num_sms = sms;
+  p->num_sms = lsms;  // the SMs its layout's teams were planned for
   p->kernel = L->kernel;
   p->ctas_per_sm = L->ctas_per_sm;
   p->ctas2_per_sm = L->ctas2_per_sm;
@@ -1670,26 +1673,38 @@ int hmvm_b200_version(void) { return 2; }
 }  // extern "C"
 
 // ---- batches of independent H-matrices ----------------------------------------
-// Instances are grouped into classes by the number of right-hand sides they
-// will be applied with (width 1, 2, 4 or 8 per pass, and the number of 8-wide
-// passes above 8).  Each class is planned as ONE block-diagonal H-matrix:
-// instance m's leaves are shifted by its offset in rows and columns, so each
-// stage of a class is one persistent launch over all its instances' items,
-// load-balanced together.  One apply (or one graph replay) runs the classes
-// one after the other.
+// Instances are grouped into classes by the pass width their right-hand sides
+// need (2, 4 or 8 columns; a single column runs in a 2-wide pass) and by their
+// number of passes (above 8 columns: ceil(k / 8) passes of 8).  Each class is
+// planned as ONE block-diagonal H-matrix: instance m's leaves are shifted by
+// its offset in rows and columns, and the class's layout is planned for its
+// share of the SMs: every pass of every class runs at once, so a class gets
+// the SMs in proportion to its stored elements among all passes' elements.  An apply runs every
+// (class, pass) -- a part, with its own packed inputs, t, partial sums and
+// concatenated outputs -- at once: one packing launch, one launch per stage
+// (hmvm_batch_multi_kernel, each block running its part's body), one per
+// reduction, one unpacking launch.
+
+struct PassBufs {  // a class's buffers for one pass (pass 0: its plan's own)
+  double* xm64 = nullptr;
+  float* xm32 = nullptr;
+  void* tm = nullptr;
+  void* pm = nullptr;
+  void* ycat = nullptr;
+  bool owned = false;  // allocated by the batch (passes >= 1)
+};
 
 struct BatchClass {
   hmvm_plan* plan = nullptr;
-  int width = 1;                 // rhs per pass (the plan's nrhs_max)
+  int width = 2;                 // rhs per pass (the plan's nrhs_max)
+  int npass = 1;                 // passes it was grouped by (the columns given may differ)
   std::vector<int32_t> members;  // instance ids
   std::vector<int32_t> n;
   std::vector<int64_t> off;
   int64_t ntot = 0;
   int32_t nmax = 0;
-  std::vector<BatchIO> io;
-  BatchIO* d_io = nullptr;
-  void* d_xcat = nullptr;  // width 1: concatenated x (ntot + 16)
-  void* d_ycat = nullptr;  // concatenated Y, column r at d_ycat + r * ntot
+  int passes = 0;                // passes of the columns last given
+  std::vector<PassBufs> pass;    // buffers per pass (grown on demand, kept)
 };
 
 struct hmvm_batch {
@@ -1697,6 +1712,20 @@ struct hmvm_batch {
   std::vector<int32_t> cls_of;  // class of each instance
   std::vector<int32_t> pos_of;  // position within its class
   std::vector<BatchClass> cls;
+  // the part tables of the columns last given
+  std::vector<BatchIO> io;      // per instance
+  std::vector<BatchPack> pack;  // per (instance, pass)
+  std::vector<BatchPart> parts;        // the V-stage parts, then the row-stage parts
+  int n1 = 0;                          // V-stage parts
+  std::vector<BatchRedPart> reds;      // the V-stage reductions, then the row-stage ones
+  int nr1 = 0;
+  int64_t red_total[2] = {0, 0};       // work items of each reduction launch
+  BatchIO* d_io = nullptr;
+  BatchPack* d_pack = nullptr;
+  BatchPart* d_parts = nullptr;
+  BatchRedPart* d_reds = nullptr;
+  size_t cap_io = 0, cap_pack = 0, cap_parts = 0, cap_reds = 0;
+  int64_t nmax_rows = 0;        // the largest instance (pack / unpack grids)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int device = 0;
@@ -1704,10 +1733,9 @@ struct hmvm_batch {
 
 namespace {
 
-// Class key of an instance applied with k right-hand sides: the pass width
-// (1, 2, 4 or 8; a pass of width w runs ceil(k / 8) times when k > 8).
+// Pass width of an instance applied with k right-hand sides (k > 8: ceil(k / 8)
+// passes of 8).
 int batch_width(int32_t k) {
-  if (k <= 1) return 1;
   if (k <= 2) return 2;
   if (k <= 4) return 4;
   return 8;
@@ -1718,17 +1746,62 @@ void free_batch(hmvm_batch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
   b->graph = nullptr;
+  for (void* q : {(void*)b->d_io, (void*)b->d_pack, (void*)b->d_parts, (void*)b->d_reds})
+    if (q) cudaFree(q);
+  b->d_io = nullptr;
+  b->d_pack = nullptr;
+  b->d_parts = nullptr;
+  b->d_reds = nullptr;
   for (BatchClass& c : b->cls) {
-    for (void* q : {(void*)c.d_io, c.d_xcat, c.d_ycat})
-      if (q) cudaFree(q);
-    c.d_io = nullptr;
-    c.d_xcat = c.d_ycat = nullptr;
+    for (PassBufs& q : c.pass) {
+      if (q.owned)
+        for (void* v : {(void*)q.xm64, (void*)q.xm32, q.tm, q.pm})
+          if (v) cudaFree(v);
+      if (q.ycat) cudaFree(q.ycat);
+    }
+    c.pass.clear();
     if (c.plan) hmvm_b200_plan_destroy(c.plan);
     c.plan = nullptr;
   }
 }
 
-int class_create(BatchClass& c, const std::vector<LeafTable>& tabs, bool is_float, hmvm_plan_opts o) {
+// Buffers of pass q of class c (pass 0 uses the plan's packed inputs, t and partials).
+int class_pass_buffers(BatchClass& c, int q) {
+  hmvm_plan* p = c.plan;
+  while ((int)c.pass.size() <= q) {
+    const int k = (int)c.pass.size();
+    const size_t nr = (size_t)c.width;
+    PassBufs b;
+    cudaError_t e = cudaSuccess;
+    if (k == 0) {
+      b.xm64 = p->d_xm64;
+      b.xm32 = p->d_xm32;
+      b.tm = p->d_tm;
+      b.pm = p->d_pm;
+    } else {
+      b.owned = true;
+      if (p->d_xm64) e = cudaMalloc(&b.xm64, (size_t)(c.ntot + 16) * nr * sizeof(double));
+      if (e == cudaSuccess && b.xm64) e = cudaMemset(b.xm64, 0, (size_t)(c.ntot + 16) * nr * sizeof(double));
+      if (e == cudaSuccess && p->d_xm32) e = cudaMalloc(&b.xm32, (size_t)(c.ntot + 16) * nr * sizeof(float));
+      if (e == cudaSuccess && b.xm32) e = cudaMemset(b.xm32, 0, (size_t)(c.ntot + 16) * nr * sizeof(float));
+      if (e == cudaSuccess) e = cudaMalloc(&b.tm, (size_t)(p->t_len + 16) * nr * p->t_elem);
+      if (e == cudaSuccess) e = cudaMemset(b.tm, 0, (size_t)(p->t_len + 16) * nr * p->t_elem);
+      if (e == cudaSuccess) e = cudaMalloc(&b.pm, (size_t)(p->p_len + 16) * nr * p->p_elem);
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&b.ycat, (size_t)(c.ntot + 16) * nr * p->elem);
+    if (e != cudaSuccess) {
+      if (b.owned)
+        for (void* v : {(void*)b.xm64, (void*)b.xm32, b.tm, b.pm})
+          if (v) cudaFree(v);
+      if (b.ycat) cudaFree(b.ycat);
+      return cuda_fail(e, "batch pass buffers");
+    }
+    c.pass.push_back(b);
+  }
+  return HMVM_OK;
+}
+
+int class_create(BatchClass& c, const std::vector<LeafTable>& tabs, bool is_float, hmvm_plan_opts o, int sms) {
   int64_t ntot = 0, nlf = 0, len = 0;
   int32_t ktmax = 0, nmax = 0;
   for (int32_t m : c.members) {
@@ -1789,23 +1862,36 @@ int class_create(BatchClass& c, const std::vector<LeafTable>& tabs, bool is_floa
   mt.rowmat = rowmat.data();
   mt.rowmat_is_float = is_float;
   o.nrhs_max = c.width;
-  int rc = create_plan(mt, &o, &c.plan);
+  int rc = create_plan(mt, &o, &c.plan, sms);
   if (rc) return rc;
+  DeviceGuard g(c.plan->device);
+  // the packed inputs' pad rows are never written: zero them once
   hmvm_plan* p = c.plan;
-  DeviceGuard g(p->device);
-  const size_t ncols = (size_t)c.width;
-  cudaError_t e = cudaMalloc(&c.d_io, sizeof(BatchIO) * c.members.size());
-  if (e == cudaSuccess) e = cudaMalloc(&c.d_ycat, (size_t)(ntot + 16) * ncols * p->elem);
-  if (e == cudaSuccess && c.width == 1) {
-    e = cudaMalloc(&c.d_xcat, (size_t)(ntot + 16) * p->elem);
-    if (e == cudaSuccess) e = cudaMemset(c.d_xcat, 0, (size_t)(ntot + 16) * p->elem);
-  }
-  // the packed multi-RHS inputs: the batch packing kernels never write the pad rows
-  if (e == cudaSuccess && p->d_xm64) e = cudaMemset(p->d_xm64, 0, (size_t)(ntot + 16) * ncols * sizeof(double));
-  if (e == cudaSuccess && p->d_xm32) e = cudaMemset(p->d_xm32, 0, (size_t)(ntot + 16) * ncols * sizeof(float));
-  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaError_t e = cudaSuccess;
+  if (p->d_xm64) e = cudaMemset(p->d_xm64, 0, (size_t)(ntot + 16) * c.width * sizeof(double));
+  if (e == cudaSuccess && p->d_xm32) e = cudaMemset(p->d_xm32, 0, (size_t)(ntot + 16) * c.width * sizeof(float));
+  if (e != cudaSuccess) return cuda_fail(e, "batch buffers");
+  rc = class_pass_buffers(c, 0);
+  if (rc) return rc;
+  e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return cuda_fail(e, "batch buffers");
   return HMVM_OK;
+}
+
+int batch_mode(const hmvm_batch* b) { return plan_mode(b->cls.front().plan); }
+
+template <int MODE, bool VST>
+const void* batch_stage_kernel() {
+  constexpr MultiCfg c = kMultiCfgs[kDefaultMultiCfg];
+  return (const void*)hmvm_batch_multi_kernel<c.wpb, c.slots, c.chunk, MODE, VST>;
+}
+const void* batch_stage_kernel_for(int mode, bool vst) {
+  switch (mode) {
+    case kModePlain64: return vst ? batch_stage_kernel<kModePlain64, true>() : batch_stage_kernel<kModePlain64, false>();
+    case kModePlain32: return vst ? batch_stage_kernel<kModePlain32, true>() : batch_stage_kernel<kModePlain32, false>();
+    case kModeMixed16: return vst ? batch_stage_kernel<kModeMixed16, true>() : batch_stage_kernel<kModeMixed16, false>();
+    default: return vst ? batch_stage_kernel<kModeMixedBF16, true>() : batch_stage_kernel<kModeMixedBF16, false>();
+  }
 }
 
 int batch_create(const std::vector<LeafTable>& tabs, bool is_float, const hmvm_plan_opts* opts,
@@ -1823,31 +1909,52 @@ int batch_create(const std::vector<LeafTable>& tabs, bool is_float, const hmvm_p
     if (rc) return set_error(rc, "batch instance " + std::to_string(m) + ": " + msg);
     if (nrhs && nrhs[m] < 0) return set_error(HMVM_EINVAL, "nrhs < 0");
   }
+  int dev = 0, sms = 0;
+  {
+    int rc = check_device(o.device, &dev, &sms);
+    if (rc) return rc;
+  }
   hmvm_batch* b = new (std::nothrow) hmvm_batch();
   if (!b) return set_error(HMVM_ENOMEM, "host allocation failed");
   b->count = count;
   b->cls_of.assign(count, -1);
   b->pos_of.assign(count, -1);
-  // classes in the order of their widths: 1, 2, 4, 8
-  const int default_w = batch_width(std::min(std::max(o.nrhs_max, 1), kMaxNrhsPass));
-  for (int w : {1, 2, 4, 8}) {
-    BatchClass c;
-    c.width = w;
-    for (int32_t m = 0; m < count; m++) {
-      const int wm = nrhs ? batch_width(nrhs[m]) : default_w;
-      if (wm == w) {
-        b->cls_of[m] = (int32_t)b->cls.size();
-        b->pos_of[m] = (int32_t)c.members.size();
-        c.members.push_back(m);
-      }
-    }
-    if (!c.members.empty()) b->cls.push_back(std::move(c));
+  // classes in the order of their widths (2, 4, 8) and passes; each planned for its
+  // share of the SMs: its stored elements among the elements of all passes
+  const int32_t kdef = std::min(std::max(o.nrhs_max, 1), kMaxNrhsPass);
+  std::vector<int> keys;  // width * 1024 + passes
+  for (int32_t m = 0; m < count; m++) {
+    const int32_t k = nrhs ? nrhs[m] : kdef;
+    const int w = batch_width(k), np = std::max(1, (k + w - 1) / w);
+    keys.push_back(w * 1024 + np);
   }
-  for (BatchClass& c : b->cls) {
-    int rc = class_create(c, tabs, is_float, o);
+  std::vector<int> order(keys);
+  std::sort(order.begin(), order.end());
+  order.erase(std::unique(order.begin(), order.end()), order.end());
+  std::vector<double> elems;
+  double wsum = 0;
+  for (int key : order) {
+    BatchClass c;
+    c.width = key / 1024;
+    c.npass = key % 1024;
+    double el = 0;
+    for (int32_t m = 0; m < count; m++) {
+      if (keys[m] != key) continue;
+      b->cls_of[m] = (int32_t)b->cls.size();
+      b->pos_of[m] = (int32_t)c.members.size();
+      c.members.push_back(m);
+      el += (double)std::max<int64_t>(tabs[m].len, 1);
+    }
+    wsum += el * c.npass;
+    b->cls.push_back(std::move(c));
+    elems.push_back(el);
+  }
+  for (size_t k = 0; k < b->cls.size(); k++) {
+    const int share = std::max(1, (int)std::lround(sms * elems[k] / std::max(wsum, 1.0)));
+    int rc = class_create(b->cls[k], tabs, is_float, o, std::min(share, sms));
     if (rc) {
       {
-        DeviceGuard g(b->cls.front().plan ? b->cls.front().plan->device : 0);
+        DeviceGuard g(dev);
         free_batch(b);
       }
       delete b;
@@ -1855,19 +1962,59 @@ int batch_create(const std::vector<LeafTable>& tabs, bool is_float, const hmvm_p
     }
   }
   b->device = b->cls.front().plan->device;
+  {
+    DeviceGuard g(b->device);
+    const int smem = multi_smem_bytes(kMultiCfgs[kDefaultMultiCfg]);
+    for (bool vst : {true, false}) {
+      cudaError_t e = cudaFuncSetAttribute(batch_stage_kernel_for(batch_mode(b), vst),
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) {
+        free_batch(b);
+        delete b;
+        return cuda_fail(e, "cudaFuncSetAttribute");
+      }
+    }
+  }
   *out = b;
   return HMVM_OK;
 }
 
+MultiArgs part_args(const hmvm_plan* p, const PassBufs& q, bool vst, int64_t ldy) {
+  MultiArgs a;
+  const int64_t w = p->nrhs_max;
+  a.xcap = (int64_t)(p->nd + 16) * w;
+  a.tcap = (int64_t)(p->t_len + 16) * w;
+  a.pcap = (int64_t)(p->p_len + 16) * w;
+  a.ycap = (int64_t)(p->nd + 16) * w;
+  a.err = p->d_err;
+  a.tiles = p->d_tiles;
+  a.segs = p->d_segs;
+  a.team_begin = vst ? p->d_tb1 : p->d_tb2;
+  a.nteams = vst ? p->stage1_teams : p->stage2_teams;
+  a.data = p->d_data;
+  a.x64 = q.xm64;
+  a.x32 = q.xm32;
+  a.t = q.tm;
+  a.y = q.ycat;
+  a.ldy = ldy;
+  a.nr = p->nrhs_max;
+  a.p = q.pm;
+  a.out_idx = p->d_out_idx;
+  a.scale = p->d_scale;
+  return a;
+}
+
+// The part tables for these columns: per class its passes (the widest instance
+// sets them), per (class, pass) a part of each stage and reduction, per
+// (instance, pass) a row of the pack / unpack grids.
 int batch_set_io(hmvm_batch* b, const void* const* X, const int64_t* ldx, void* const* Y, const int64_t* ldy,
                  const int32_t* nrhs) {
   if (!b) return set_error(HMVM_EINVAL, "batch is NULL");
   if (!X || !ldx || !Y || !ldy || !nrhs) return set_error(HMVM_EINVAL, "NULL argument array");
-  std::vector<std::vector<BatchIO>> io(b->cls.size());
-  for (size_t k = 0; k < b->cls.size(); k++) io[k].resize(b->cls[k].members.size());
+  std::vector<BatchIO> io(b->count);
   for (int32_t m = 0; m < b->count; m++) {
     const BatchClass& c = b->cls[b->cls_of[m]];
-    BatchIO& q = io[b->cls_of[m]][b->pos_of[m]];
+    BatchIO& q = io[m];
     q.X = X[m];
     q.ldx = ldx[m];
     q.Y = Y[m];
@@ -1880,62 +2027,172 @@ int batch_set_io(hmvm_batch* b, const void* const* X, const int64_t* ldx, void* 
     if (!q.X || !q.Y) return set_error(HMVM_EINVAL, "instance " + std::to_string(m) + ": X or Y is NULL");
     if (q.ldx < q.n || q.ldy < q.n) return set_error(HMVM_EINVAL, "instance " + std::to_string(m) + ": ld < N");
   }
-  for (size_t k = 0; k < b->cls.size(); k++) b->cls[k].io.swap(io[k]);
+  DeviceGuard g(b->device);
+  if (!g.ok) return set_error(HMVM_ECUDA, "cannot select the batch's device");
+  std::vector<BatchPack> pack;
+  std::vector<BatchPart> p1, p2;
+  std::vector<BatchRedPart> r1, r2;
+  int64_t nmax_rows = 0;
+  auto stage_add = [](std::vector<BatchPart>& v, const MultiArgs& a, int nr) {
+    const int ctas = (a.nteams + kMultiCfgs[kDefaultMultiCfg].wpb - 1) / kMultiCfgs[kDefaultMultiCfg].wpb;
+    if (ctas <= 0) return;
+    BatchPart q;
+    q.a = a;
+    q.cta0 = v.empty() ? 0 : v.back().cta0 + (v.back().a.nteams + kMultiCfgs[kDefaultMultiCfg].wpb - 1) /
+                                                  kMultiCfgs[kDefaultMultiCfg].wpb;
+    q.nr = nr;
+    v.push_back(q);
+  };
+  auto red_add = [](std::vector<BatchRedPart>& v, const int4* red, int n, const void* pp, int64_t pcap, void* dst,
+                    int64_t dcap, int64_t ld, int nr) {
+    if (n <= 0) return;
+    BatchRedPart q;
+    q.red = red;
+    q.p = pp;
+    q.dst = dst;
+    q.ldy = ld;
+    q.w0 = v.empty() ? 0 : v.back().w0 + (int64_t)v.back().n * v.back().nr;
+    q.pcap = pcap;
+    q.dcap = dcap;
+    q.n = n;
+    q.nr = nr;
+    v.push_back(q);
+  };
+  for (BatchClass& c : b->cls) {
+    int mx = 0;
+    for (size_t i = 0; i < c.members.size(); i++) mx = std::max(mx, (int)io[c.members[i]].nrhs);
+    c.passes = (mx + c.width - 1) / c.width;
+    if (c.passes > 0) {
+      int rc = class_pass_buffers(c, c.passes - 1);
+      if (rc) return rc;
+    }
+    const hmvm_plan* p = c.plan;
+    const int64_t w = c.width;
+    const int64_t xcap = (c.ntot + 16) * w, tcap = (p->t_len + 16) * w, pcap = (p->p_len + 16) * w;
+    for (int q = 0; q < c.passes; q++) {
+      const PassBufs& pb = c.pass[q];
+      if (p->stage1_tiles > 0) stage_add(p1, part_args(p, pb, true, c.ntot), c.width);
+      stage_add(p2, part_args(p, pb, false, c.ntot), c.width);
+      red_add(r1, (const int4*)p->d_red1, p->n_red1, pb.pm, pcap, pb.tm, tcap, 0, c.width);
+      red_add(r2, (const int4*)p->d_red2, p->n_red2, pb.pm, pcap, pb.ycat, xcap, c.ntot, c.width);
+      for (size_t i = 0; i < c.members.size(); i++) {
+        const int32_t m = c.members[i];
+        if (io[m].n == 0 || io[m].nrhs <= q * c.width) continue;  // no columns in this pass
+        BatchPack e;
+        e.io = m;
+        e.c0 = q * c.width;
+        e.nr = c.width;
+        e._pad = 0;
+        e.x64 = pb.xm64;
+        e.x32 = pb.xm32;
+        e.ycat = pb.ycat;
+        e.ldc = c.ntot;
+        e.xcap = xcap;
+        e.ycap = xcap;
+        pack.push_back(e);
+        nmax_rows = std::max<int64_t>(nmax_rows, io[m].n);
+      }
+    }
+  }
+  const int n1 = (int)p1.size(), nr1 = (int)r1.size();
+  const int64_t tot1 = r1.empty() ? 0 : r1.back().w0 + (int64_t)r1.back().n * r1.back().nr;
+  const int64_t tot2 = r2.empty() ? 0 : r2.back().w0 + (int64_t)r2.back().n * r2.back().nr;
+  p1.insert(p1.end(), p2.begin(), p2.end());
+  r1.insert(r1.end(), r2.begin(), r2.end());
+  // device copies of the tables (grown on demand)
+  auto grow = [](auto*& d, size_t& cap, size_t need, const char* what) -> int {
+    if (need <= cap) return HMVM_OK;
+    if (d) cudaFree(d);
+    d = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc((void**)&d, need * sizeof(*d));
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    cap = need;
+    return HMVM_OK;
+  };
+  int rc = grow(b->d_io, b->cap_io, io.size(), "batch table");
+  if (!rc) rc = grow(b->d_pack, b->cap_pack, std::max<size_t>(pack.size(), 1), "batch table");
+  if (!rc) rc = grow(b->d_parts, b->cap_parts, std::max<size_t>(p1.size(), 1), "batch table");
+  if (!rc) rc = grow(b->d_reds, b->cap_reds, std::max<size_t>(r1.size(), 1), "batch table");
+  if (rc) return rc;
+  b->io.swap(io);
+  b->pack.swap(pack);
+  b->parts.swap(p1);
+  b->n1 = n1;
+  b->reds.swap(r1);
+  b->nr1 = nr1;
+  b->red_total[0] = tot1;
+  b->red_total[1] = tot2;
+  b->nmax_rows = nmax_rows;
   return HMVM_OK;
 }
 
-int class_max_nrhs(const BatchClass& c) {
-  int mx = 0;
-  for (const BatchIO& q : c.io) mx = std::max(mx, (int)q.nrhs);
-  return mx;
-}
-
 template <typename T>
-int class_run_t(BatchClass& c, cudaStream_t st) {
-  hmvm_plan* p = c.plan;
-  const int mx = class_max_nrhs(c);
-  const unsigned cnt = (unsigned)c.members.size();
-  auto blocks = [&](int64_t work) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 64)); };
-  if (p->nrhs_max <= 1) {
-    for (int col = 0; col < mx; col++) {
-      hmvm_batch_pack1_kernel<T><<<dim3(blocks(c.nmax), cnt), 256, 0, st>>>(c.d_io, col, static_cast<T*>(c.d_xcat));
-      HMVM_CUDA_TRY(cudaGetLastError(), "batch packing launch");
-      int rc = apply_impl(p, c.d_xcat, c.d_ycat, st);
-      if (rc) return rc;
-      hmvm_batch_unpack_kernel<T><<<dim3(blocks(c.nmax), cnt), 256, 0, st>>>(
-          c.d_io, col, 1, static_cast<const T*>(c.d_ycat), c.ntot);
-      HMVM_CUDA_TRY(cudaGetLastError(), "batch unpacking launch");
+int batch_run_t(hmvm_batch* b, cudaStream_t st) {
+  if (b->pack.empty()) return HMVM_OK;
+  const int mode = batch_mode(b);
+  int* err = b->cls.front().plan->d_err;
+  const MultiCfg& mc = kMultiCfgs[kDefaultMultiCfg];
+  const int threads = 32 * mc.wpb, smem = multi_smem_bytes(mc);
+  const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((b->nmax_rows * 8 + 255) / 256, 64));
+  const dim3 pgrid(gx, (unsigned)b->pack.size());
+  const int nio = (int)b->io.size();
+  hmvm_batch_pack_kernel<T><<<pgrid, 256, 0, st>>>(b->d_io, nio, b->d_pack, err);
+  HMVM_CUDA_TRY(cudaGetLastError(), "batch packing launch");
+  const bool f32 = b->cls.front().plan->precision == HMVM_FP32;  // partial sums in FP32
+  auto run_reduce = [&](const BatchRedPart* parts, int n, int64_t total, bool vst) -> int {
+    if (n == 0 || total == 0) return HMVM_OK;
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 65535);
+    if (vst) {
+      if (mode == kModePlain64) hmvm_batch_reduce_kernel<double, double, true><<<blocks, 256, 0, st>>>(parts, n, total, err);
+      else if (f32) hmvm_batch_reduce_kernel<float, float, true><<<blocks, 256, 0, st>>>(parts, n, total, err);
+      else hmvm_batch_reduce_kernel<double, float, true><<<blocks, 256, 0, st>>>(parts, n, total, err);
+    } else {
+      if (f32) hmvm_batch_reduce_kernel<float, float, false><<<blocks, 256, 0, st>>>(parts, n, total, err);
+      else hmvm_batch_reduce_kernel<double, double, false><<<blocks, 256, 0, st>>>(parts, n, total, err);
     }
+    HMVM_CUDA_TRY(cudaGetLastError(), "batch reduction launch");
     return HMVM_OK;
-  }
-  const int w = c.width;  // every pass of a class has the class width
-  for (int c0 = 0; c0 < mx; c0 += w) {
-    const dim3 grid(blocks((int64_t)c.nmax * w), cnt);
-    double* x64 = p->d_xm64;
-    float* x32 = p->d_xm32;
-    switch (w) {
-      case 2: hmvm_batch_packm_kernel<T, 2><<<grid, 256, 0, st>>>(c.d_io, c0, x64, x32); break;
-      case 4: hmvm_batch_packm_kernel<T, 4><<<grid, 256, 0, st>>>(c.d_io, c0, x64, x32); break;
-      default: hmvm_batch_packm_kernel<T, 8><<<grid, 256, 0, st>>>(c.d_io, c0, x64, x32); break;
-    }
-    HMVM_CUDA_TRY(cudaGetLastError(), "batch packing launch");
-    int rc = launch_multi_stages(p, c.d_ycat, c.ntot, w, w, st);
-    if (rc) return rc;
-    hmvm_batch_unpack_kernel<T><<<grid, 256, 0, st>>>(c.d_io, c0, w, static_cast<const T*>(c.d_ycat), c.ntot);
-    HMVM_CUDA_TRY(cudaGetLastError(), "batch unpacking launch");
-  }
+  };
+  auto run_stage = [&](int k0, int n, bool vst) -> int {
+    if (n == 0) return HMVM_OK;
+    const BatchPart& last = b->parts[k0 + n - 1];
+    const unsigned grid = (unsigned)(last.cta0 + (last.a.nteams + mc.wpb - 1) / mc.wpb);
+    const BatchPart* dp = b->d_parts + k0;
+    void* args[] = {(void*)&dp, (void*)&n};
+    HMVM_CUDA_TRY(cudaLaunchKernel(batch_stage_kernel_for(mode, vst), dim3(grid), dim3((unsigned)threads), args,
+                                   (size_t)smem, st),
+                  vst ? "batch V-stage launch" : "batch row-stage launch");
+    return HMVM_OK;
+  };
+  const int np = (int)b->parts.size(), nrd = (int)b->reds.size();
+  int rc = run_stage(0, b->n1, true);
+  if (!rc) rc = run_reduce(b->d_reds, b->nr1, b->red_total[0], true);
+  if (!rc) rc = run_stage(b->n1, np - b->n1, false);
+  if (!rc) rc = run_reduce(b->d_reds + b->nr1, nrd - b->nr1, b->red_total[1], false);
+  if (rc) return rc;
+  hmvm_batch_unpack_parts_kernel<T><<<pgrid, 256, 0, st>>>(b->d_io, nio, b->d_pack, err);
+  HMVM_CUDA_TRY(cudaGetLastError(), "batch unpacking launch");
   return HMVM_OK;
 }
 
 int batch_run(hmvm_batch* b, cudaStream_t st) {
-  for (BatchClass& c : b->cls) {
-    if (class_max_nrhs(c) == 0) continue;
-    HMVM_CUDA_TRY(cudaMemcpyAsync(c.d_io, c.io.data(), sizeof(BatchIO) * c.io.size(), cudaMemcpyHostToDevice, st),
+  HMVM_CUDA_TRY(cudaMemcpyAsync(b->d_io, b->io.data(), sizeof(BatchIO) * b->io.size(), cudaMemcpyHostToDevice, st),
+                "batch table upload");
+  if (!b->pack.empty())
+    HMVM_CUDA_TRY(cudaMemcpyAsync(b->d_pack, b->pack.data(), sizeof(BatchPack) * b->pack.size(),
+                                  cudaMemcpyHostToDevice, st),
                   "batch table upload");
-    int rc = c.plan->precision == HMVM_FP32 ? class_run_t<float>(c, st) : class_run_t<double>(c, st);
-    if (rc) return rc;
-  }
-  return HMVM_OK;
+  if (!b->parts.empty())
+    HMVM_CUDA_TRY(cudaMemcpyAsync(b->d_parts, b->parts.data(), sizeof(BatchPart) * b->parts.size(),
+                                  cudaMemcpyHostToDevice, st),
+                  "batch table upload");
+  if (!b->reds.empty())
+    HMVM_CUDA_TRY(cudaMemcpyAsync(b->d_reds, b->reds.data(), sizeof(BatchRedPart) * b->reds.size(),
+                                  cudaMemcpyHostToDevice, st),
+                  "batch table upload");
+  // X and Y: FP32 for FP32 plans, FP64 otherwise (whatever the stored elements were)
+  return b->cls.front().plan->precision == HMVM_FP32 ? batch_run_t<float>(b, st) : batch_run_t<double>(b, st);
 }
 
 int batch_create_tables(std::vector<LeafTable>& t, bool is_float, const hmvm_plan_opts* opts, const int32_t* nrhs,
@@ -2094,20 +2351,10 @@ int hmvm_b200_batch_status(hmvm_batch* b) {
 }
 
 int hmvm_b200_batch_kernel_count(const hmvm_batch* b) {
-  if (!b) return 0;
-  int total = 0;
-  for (const BatchClass& c : b->cls) {
-    const int mx = class_max_nrhs(c);
-    if (mx == 0) continue;
-    const hmvm_plan* p = c.plan;
-    if (p->nrhs_max <= 1) {
-      total += mx * (2 + hmvm_b200_plan_kernel_count(p));  // pack, stages, unpack
-    } else {
-      const int passes = (mx + c.width - 1) / c.width;
-      total += passes * (2 + (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1 + (p->n_red2 > 0));
-    }
-  }
-  return total;
+  if (!b || b->pack.empty()) return 0;
+  // pack, one launch per stage and per reduction that has work, unpack
+  const int np = (int)b->parts.size(), nrd = (int)b->reds.size();
+  return 2 + (b->n1 > 0) + (np > b->n1) + (b->nr1 > 0 && b->red_total[0] > 0) + (nrd > b->nr1 && b->red_total[1] > 0);
 }
 
 }  // extern "C"

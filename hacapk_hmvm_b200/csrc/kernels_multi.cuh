@@ -47,6 +47,8 @@ struct MultiArgs {
   void* p;                 // partial sums [(p_len) * NR]: double, or float for FP32 plans
   const int32_t* out_idx;  // V-stage output slots
   const double* scale;     // mixed, V stage: per panel-row column scale
+  // elements of x64 / x32, t, p and y (checked by the batch instances only)
+  int64_t xcap = 0, tcap = 0, pcap = 0, ycap = 0;
 };
 
 // X[i + r * ldx] -> xpk[i * NR + r] for i < n, r < nr; zeros for r >= nr and
@@ -93,7 +95,7 @@ struct MultiMode {
 // Copy the inputs item `d` reads into zb: for each segment, ncp columns of
 // NR values (ncp = columns rounded up to whole vectors; the padding is zero).
 // FP64 segments take 8-byte values, the others 4-byte values.
-template <int MODE, int NR>
+template <int MODE, int NR, bool CHECK = false>
 __device__ __forceinline__ void gather_multi(const hmvm_tile_desc& d, const hmvm_seg_desc& sreg, const MultiArgs& a,
                                              unsigned char* zb, int lane) {
   using TT = typename MultiMode<MODE>::TT;
@@ -107,6 +109,14 @@ __device__ __forceinline__ void gather_multi(const hmvm_tile_desc& d, const hmvm
     const int ncp = ((nc + (1 << lg) - 1) >> lg) << lg;
     const bool from_t = src < 0;
     const int64_t base = (int64_t)(from_t ? (src & 0x7fffffff) : src) * NR;
+    if constexpr (CHECK) {  // a range outside its buffer: record it and read nothing
+      if (base + (int64_t)ncp * NR > (from_t ? a.tcap : a.xcap)) {
+        if (lane == 0) atomicExch(a.err, 3);
+        for (int c = lane; c < ncp * NR * (type == kF64 ? 2 : 1); c += 32) reinterpret_cast<float*>(zb + zoff)[c] = 0.f;
+        zoff += ncp * NR * (type == kF64 ? 8 : 4);
+        continue;
+      }
+    }
     if (type == kF64) {
       const double* s = from_t ? reinterpret_cast<const double*>(static_cast<const TT*>(a.t)) + base : a.x64 + base;
       double* z = reinterpret_cast<double*>(zb + zoff);
@@ -225,9 +235,10 @@ constexpr int multi_min_blocks() {
   return m > 0 ? m : 1;
 }
 
-template <int WPB, int S, int CHUNK, int NR, int MODE, bool VST>
-__global__ void __launch_bounds__(32 * WPB, (multi_min_blocks<WPB, S, CHUNK>()))
-    hmvm_multi_kernel(MultiArgs a) {
+// The body of hmvm_multi_kernel for block bid of the launch (a batch launch
+// runs several plans' bodies, each over its own range of blocks).
+template <int WPB, int S, int CHUNK, int NR, int MODE, bool VST, bool CHECK = false>
+__device__ __forceinline__ void multi_body(const MultiArgs& a, int bid) {
   using MM = MultiMode<MODE>;
   using TT = typename MM::TT;
   using TYO = typename MM::TY;
@@ -240,7 +251,7 @@ __global__ void __launch_bounds__(32 * WPB, (multi_min_blocks<WPB, S, CHUNK>()))
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const int team = blockIdx.x * WPB + warp;
+  const int team = bid * WPB + warp;
   if (team >= a.nteams) return;
   const int tb = a.team_begin[team], te = a.team_begin[team + 1];
   if (tb >= te) return;
@@ -289,7 +300,7 @@ __global__ void __launch_bounds__(32 * WPB, (multi_min_blocks<WPB, S, CHUNK>()))
     else return 0;
   };
   hmvm_seg_desc cur_seg = lane < cur.nseg ? segs[cur.seg_begin + lane] : szero;
-  gather_multi<MODE, NR>(cur, cur_seg, a, zbase, lane);
+  gather_multi<MODE, NR, CHECK>(cur, cur_seg, a, zbase, lane);
   cp_async_commit();
   int cur_oidx = out_slot(cur);
   double cur_scale = row_scale(cur);
@@ -301,7 +312,7 @@ __global__ void __launch_bounds__(32 * WPB, (multi_min_blocks<WPB, S, CHUNK>()))
   for (int ti = tb, k = 0; ti < te; ++ti, ++k) {
     unsigned char* zcur = zbase + (k & 1) * kMultiZBytes;
     __syncwarp();
-    if (ti + 1 < te) gather_multi<MODE, NR>(nxt, nxt_seg, a, zbase + ((k + 1) & 1) * kMultiZBytes, lane);
+    if (ti + 1 < te) gather_multi<MODE, NR, CHECK>(nxt, nxt_seg, a, zbase + ((k + 1) & 1) * kMultiZBytes, lane);
     cp_async_commit();
     const bool has_nn = ti + 2 < te;
     const hmvm_tile_desc nn = has_nn ? tiles[ti + 2] : dzero;
@@ -400,7 +411,16 @@ __global__ void __launch_bounds__(32 * WPB, (multi_min_blocks<WPB, S, CHUNK>()))
       }
     }
     if (failed) break;
-    if (lane < R) {
+    bool store_ok = true;
+    if constexpr (CHECK) {  // an output outside its buffer: record it and write nothing
+      const int64_t hi = VST ? (cur.mode == 1 ? ((int64_t)cur_oidx + 1) * NR : ((int64_t)cur.out_base + R) * NR)
+                             : (cur.mode == 0 ? (int64_t)cur.out_base + R + (int64_t)(NR - 1) * a.ldy
+                                              : ((int64_t)cur.out_base + R) * NR);
+      const int64_t cap = VST ? (cur.mode == 1 ? a.tcap : a.pcap) : (cur.mode == 0 ? a.ycap : a.pcap);
+      store_ok = cur_oidx >= 0 && cur.out_base >= 0 && hi <= cap;
+      if (!store_ok && lane == 0) atomicExch(a.err, 3);
+    }
+    if (lane < R && store_ok) {
       if constexpr (VST) {
         if (cur.mode == 1) {
 #pragma unroll
@@ -436,6 +456,12 @@ __global__ void __launch_bounds__(32 * WPB, (multi_min_blocks<WPB, S, CHUNK>()))
     for (uint32_t q = q_ready; q < issued; q++) warp_wait(&bars[q % S], (q / S) & 1);
     if (lane == 0) atomicExch(a.err, 1);
   }
+}
+
+template <int WPB, int S, int CHUNK, int NR, int MODE, bool VST>
+__global__ void __launch_bounds__(32 * WPB, (multi_min_blocks<WPB, S, CHUNK>()))
+    hmvm_multi_kernel(MultiArgs a) {
+  multi_body<WPB, S, CHUNK, NR, MODE, VST>(a, (int)blockIdx.x);
 }
 
 // ---- batches of independent H-matrices ----------------------------------------
@@ -487,6 +513,129 @@ __global__ void hmvm_batch_unpack_kernel(const BatchIO* __restrict__ io, int c0,
     const int r = (int)(k / b.n);
     const int64_t i = k % b.n;
     if (c0 + r < b.nrhs) Y[i + (int64_t)(c0 + r) * b.ldy] = ycat[b.off + i + r * ldc];
+  }
+}
+
+// ---- a whole batch in one launch per stage --------------------------------------
+// A batch is planned as block-diagonal classes (one plan per pass width), and an
+// apply runs each class's passes; every (class, pass) -- a "part" -- has its own
+// packed inputs, t, partial sums and concatenated outputs, so all parts run at
+// once: each of these kernels reads the batch's part table (global memory) and
+// cuts its blocks (or work items) into per-part ranges.  Every buffer access of
+// a part is checked against the part's capacities (a miss records error 3 and
+// is skipped).
+struct BatchPart {
+  MultiArgs a;
+  int32_t cta0;  // first block of the part in its stage launch
+  int32_t nr;    // pass width: 2, 4 or 8
+};
+template <int WPB, int S, int CHUNK, int MODE, bool VST>
+__global__ void __launch_bounds__(32 * WPB, (multi_min_blocks<WPB, S, CHUNK>()))
+    hmvm_batch_multi_kernel(const BatchPart* __restrict__ parts, int nparts) {
+  int k = 0;
+  while (k + 1 < nparts && (int)blockIdx.x >= parts[k + 1].cta0) k++;
+  const MultiArgs a = parts[k].a;
+  const int bid = (int)blockIdx.x - parts[k].cta0;
+  switch (parts[k].nr) {
+    case 2: multi_body<WPB, S, CHUNK, 2, MODE, VST, true>(a, bid); break;
+    case 4: multi_body<WPB, S, CHUNK, 4, MODE, VST, true>(a, bid); break;
+    default: multi_body<WPB, S, CHUNK, 8, MODE, VST, true>(a, bid); break;
+  }
+}
+
+// The split-tile reductions of every part (hmvm_reduce_multi_kernel's sums, with
+// each part's width): work items [w0, w0 + n * nr) are the part's.
+struct BatchRedPart {
+  const int4* red;
+  const void* p;
+  void* dst;
+  int64_t ldy;
+  int64_t w0;
+  int64_t pcap, dcap;  // elements of p and dst
+  int32_t n, nr;
+};
+template <typename TP, typename TD, bool VST>
+__global__ void hmvm_batch_reduce_kernel(const BatchRedPart* __restrict__ parts, int nparts, int64_t total,
+                                         int* err) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+    int q = 0;
+    while (q + 1 < nparts && k >= parts[q + 1].w0) q++;
+    const BatchRedPart& P = parts[q];
+    const int NR = P.nr;
+    const int64_t l = k - P.w0;
+    const int i = (int)(l / NR), r = (int)(l % NR);
+    const int4 e = P.red[i];
+    const int64_t last = (int64_t)(e.y + (e.z - 1) * e.w) * NR + r;
+    const int64_t d = VST ? (int64_t)e.x * NR + r : (int64_t)e.x + (int64_t)r * P.ldy;
+    if (e.y < 0 || e.z < 0 || last >= P.pcap || d < 0 || d >= P.dcap) {
+      atomicExch(err, 3);
+      continue;
+    }
+    const TP* p = static_cast<const TP*>(P.p);
+    TP sum = TP(0);
+    for (int u = 0; u < e.z; u++) sum += p[(int64_t)(e.y + u * e.w) * NR + r];
+    static_cast<TD*>(P.dst)[d] = (TD)sum;
+  }
+}
+
+// One row of the pack / unpack grids (blockIdx.y): an instance in one part.
+struct BatchPack {
+  int32_t io;       // the instance (index into the batch's BatchIO table)
+  int32_t c0;       // first column of the part's pass
+  int32_t nr;       // pass width
+  int32_t _pad;
+  double* x64;      // the part's packed inputs (row-interleaved, nr per row)
+  float* x32;
+  void* ycat;       // the part's concatenated outputs, column r at ycat + r * ldc
+  int64_t ldc;
+  int64_t xcap, ycap;  // elements of the packed inputs and of ycat
+};
+// Columns [c0, c0 + nr) of each instance -> its part's packed inputs (zero past nrhs).
+template <typename TI>
+__global__ void hmvm_batch_pack_kernel(const BatchIO* __restrict__ io, int nio, const BatchPack* __restrict__ e,
+                                       int* err) {
+  const BatchPack q = e[blockIdx.y];
+  if (q.io < 0 || q.io >= nio) {
+    if (threadIdx.x == 0) atomicExch(err, 3);
+    return;
+  }
+  const BatchIO b = io[q.io];
+  if (b.off < 0 || (b.off + b.n) * q.nr > q.xcap) {
+    if (threadIdx.x == 0) atomicExch(err, 3);
+    return;
+  }
+  const TI* X = static_cast<const TI*>(b.X);
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)b.n * q.nr;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = k / q.nr;
+    const int r = (int)(k % q.nr);
+    const double v = q.c0 + r < b.nrhs ? (double)X[i + (int64_t)(q.c0 + r) * b.ldx] : 0.0;
+    const int64_t dst = (b.off + i) * q.nr + r;
+    if (q.x64) q.x64[dst] = v;
+    if (q.x32) q.x32[dst] = (float)v;
+  }
+}
+// Each instance's columns of its part's concatenated outputs -> its own Y.
+template <typename T>
+__global__ void hmvm_batch_unpack_parts_kernel(const BatchIO* __restrict__ io, int nio,
+                                               const BatchPack* __restrict__ e, int* err) {
+  const BatchPack q = e[blockIdx.y];
+  if (q.io < 0 || q.io >= nio) {
+    if (threadIdx.x == 0) atomicExch(err, 3);
+    return;
+  }
+  const BatchIO b = io[q.io];
+  if (b.off < 0 || b.off + b.n + (int64_t)(q.nr - 1) * q.ldc > q.ycap) {
+    if (threadIdx.x == 0) atomicExch(err, 3);
+    return;
+  }
+  T* Y = static_cast<T*>(b.Y);
+  const T* yc = static_cast<const T*>(q.ycat);
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)b.n * q.nr;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(k / b.n);
+    const int64_t i = k % b.n;
+    if (q.c0 + r < b.nrhs) Y[i + (int64_t)(q.c0 + r) * b.ldy] = yc[b.off + i + r * q.ldc];
   }
 }
 

@@ -1,7 +1,8 @@
 """Batches of independent H-matrices (hmvm_b200_batch_*) on the GPU.
 
-Instances of uneven N, geometry, eta and ACA tolerance run as one
-block-diagonal plan; every instance's Y columns are checked against the FP64
+Instances of uneven N, geometry, eta and ACA tolerance run as block-diagonal
+plans (one per pass width) whose passes all run in the same launches, one per
+stage; every instance's Y columns are checked against the FP64
 oracle on that instance alone (FP32 <= 1e-5, FP64 <= 1e-12, mixed <= 1e-4
 relative error per column).  The CUDA-graph replay must give the same bits as
 the direct apply.
@@ -70,7 +71,11 @@ def test_batch_graph_replay_matches_apply(gpu):
     Xh, Xs, Ys = _blocks(mats, nrhs, np.float32, seed=3)
     _, _, Y2 = _blocks(mats, nrhs, np.float32, seed=3)
     with Batch(mats, "fp32", nrhs=nrhs) as b:
-        assert b.class_count() == 4  # pass widths 1, 2, 4 and 8
+        assert b.class_count() == 4  # (width, passes): (2, 1), (4, 1), (8, 1), (8, 2)
+        b.apply(Xs, Ys)
+        # one launch for packing, one per stage and reduction, one for unpacking, over all
+        # classes and passes (5 parts here: 16 columns take two 8-wide passes)
+        assert b.kernel_count() <= 6
         b.apply(Xs, Ys)
         b.capture(Xs, Y2)
         s = torch.cuda.Stream()
