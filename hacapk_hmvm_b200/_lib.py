@@ -107,6 +107,9 @@ class PlanInfo(C.Structure):
 TUNE_MAX_ENTRIES = 64
 
 
+HMVM_SHAPE_BINS = 128  # include/hmvm_b200.h
+
+
 class TuneEntry(C.Structure):
     _fields_ = [("kernel", C.c_int32), ("stage1_cfg", C.c_int32), ("stage2_cfg", C.c_int32),
                 ("max_tile_rows", C.c_int32), ("ctas_per_sm", C.c_int32), ("_pad0", C.c_int32),
@@ -224,6 +227,9 @@ HMVM_SIGNATURES = {
                                  C.c_void_p, C.c_void_p]),
     "hmvm_b200_autotune64": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "hmvm_b200_autotune_d": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "hmvm_b200_shape_histogram64": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "hmvm_b200_autotune_cached64": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_char_p, C.c_double,
+                                              C.c_void_p, C.c_void_p, C.c_void_p]),
     "hmvm_b200_batch_create64_d": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hmvm_b200_batch_create64_f": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hmvm_b200_batch_create_d": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),

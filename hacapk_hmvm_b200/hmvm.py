@@ -285,3 +285,40 @@ def autotune(hm: HMatrix, precision: str = "fp64", reps: int = 5, device: int = 
     for i, e in enumerate(entries):
         e["best"] = i == rep.best_entry
     return chosen, entries
+
+
+def shape_histogram(hm: HMatrix) -> np.ndarray:
+    """The fraction of hm's stored elements in each (kind, rows, width) shape
+    class (hmvm_b200_shape_histogram64): 128 bins, dense leaves then low-rank."""
+    h = np.zeros(_lib.HMVM_SHAPE_BINS, dtype=np.float32)
+    lv = hm.as_leaves64()
+    _lib.check(_lib.hmvm_lib().hmvm_b200_shape_histogram64(C.byref(lv), h.ctypes.data_as(C.c_void_p)),
+               "shape histogram")
+    return h
+
+
+def autotune_cached(hm: HMatrix, precision: str, cache: str, reps: int = 5, max_distance: float = 0.45,
+                    device: int = -1, **base) -> tuple[dict, list, bool]:
+    """autotune() through a tuning cache file (hmvm_b200_autotune_cached64): a
+    choice stored for this device, precision and factor format whose shape-class
+    histogram lies within max_distance of hm's is returned without timing
+    anything; otherwise the sweep runs and its choice is appended to the file.
+    Returns (plan options, entries, whether the choice came from the cache)."""
+    lib = _lib.hmvm_lib()
+    o = default_opts(precision=PRECISIONS[precision], device=device, **base)
+    best = _lib.PlanOpts()
+    rep = _lib.TuneReport()
+    hit = C.c_int32(0)
+    lv = hm.as_leaves64()
+    _lib.check(lib.hmvm_b200_autotune_cached64(C.byref(lv), 1 if hm.rowmat.dtype == np.float32 else 0, C.byref(o),
+                                               reps, str(cache).encode(), max_distance, C.byref(best),
+                                               C.byref(rep), C.byref(hit)), "autotune")
+    keys = ("kernel", "stage1_cfg", "stage2_cfg", "max_tile_rows")
+    chosen = {k: getattr(best, k) for k in keys}
+    if precision == "mixed":
+        chosen.pop("kernel")
+    entries = [{f: getattr(rep.entries[i], f) for f, _ in _lib.TuneEntry._fields_ if not f.startswith("_")}
+               for i in range(rep.n_entries)]
+    for i, e in enumerate(entries):
+        e["best"] = i == rep.best_entry
+    return chosen, entries, bool(hit.value)

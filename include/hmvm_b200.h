@@ -338,6 +338,26 @@ int hmvm_b200_autotune64(const hmvm_leaves64 *lv, int32_t rowmat_is_float, const
                          hmvm_plan_opts *best, hmvm_tune_report *report);
 int hmvm_b200_autotune_d(const hmvm_matrix2_d *mat2, const hmvm_plan_opts *base, int32_t reps,
                          hmvm_plan_opts *best, hmvm_tune_report *report);
+/* Shape classes and a persistent choice (no counterpart in the reference, which
+ * re-runs its offline sweeps per matrix, src_hmvm/src_cpp/hmvm1.cpp:82-89).
+ * hmvm_b200_shape_histogram64 fills hist[HMVM_SHAPE_BINS] with the fraction of
+ * the matrix's stored elements in each (kind, rows, width) class: bins 0..63
+ * dense leaves, 64..127 low-rank leaves; within a kind 8 row buckets (<= 8, 16,
+ * ..., 512, above) times 8 width buckets (dense: columns <= 8 .. above 512;
+ * low-rank: rank <= 2 .. above 128).
+ * hmvm_b200_autotune_cached64 looks in the text file cache_path for a choice
+ * stored for this device (name and SM count), precision and factor format
+ * whose histogram lies within max_distance of this matrix's (L1 distance, in
+ * [0, 2]; a negative value means 0.45, which joins generated matrices of one
+ * family within 2x in size and keeps other geometries apart), and returns the
+ * closest one without timing anything (*from_cache = 1; report holds that one
+ * entry).  Otherwise it runs hmvm_b200_autotune64 and appends the fastest
+ * measured choice, with the histogram, to the file (created if missing). */
+#define HMVM_SHAPE_BINS 128
+int hmvm_b200_shape_histogram64(const hmvm_leaves64 *lv, float *hist);
+int hmvm_b200_autotune_cached64(const hmvm_leaves64 *lv, int32_t rowmat_is_float, const hmvm_plan_opts *base,
+                                int32_t reps, const char *cache_path, double max_distance, hmvm_plan_opts *best,
+                                hmvm_tune_report *report, int32_t *from_cache);
 
 /* Capacity of the scratch array used by hmvm_b200_apply_noalloc: 16 MiB. */
 #define HMVM_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
