@@ -770,13 +770,22 @@ __global__ void __launch_bounds__(32 * WPB, (mixed_min_blocks<WPB, S, CHUNK, ZBY
         // the last batch of a stretch is predicated (vectors past nb are
         // neither loaded nor used)
         uint4 m[B];
+        if (nb == B) {  // a full batch: no predicates
 #pragma unroll
-        for (int u = 0; u < B; u++)
-          if (u < nb) m[u] = *reinterpret_cast<const uint4*>(ring + ((ol + (uint32_t)u * rstride) & (RING - 1)));
+          for (int u = 0; u < B; u++)
+            m[u] = *reinterpret_cast<const uint4*>(ring + ((ol + (uint32_t)u * rstride) & (RING - 1)));
 #pragma unroll
-        for (int u = 0; u < B; u++) {
-          if (u < nb)
+          for (int u = 0; u < B; u++)
             mixed_fma<TY>(m[u], zv + u * MixedZ<TY>::bytes, acc + (TY == kF32 ? (u & 1) * 4 : 0), e + (u & 1) * 2);
+        } else {
+#pragma unroll
+          for (int u = 0; u < B; u++)
+            if (u < nb) m[u] = *reinterpret_cast<const uint4*>(ring + ((ol + (uint32_t)u * rstride) & (RING - 1)));
+#pragma unroll
+          for (int u = 0; u < B; u++) {
+            if (u < nb)
+              mixed_fma<TY>(m[u], zv + u * MixedZ<TY>::bytes, acc + (TY == kF32 ? (u & 1) * 4 : 0), e + (u & 1) * 2);
+          }
         }
         o = o_end;
       }

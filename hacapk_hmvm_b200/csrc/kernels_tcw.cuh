@@ -31,17 +31,21 @@
 // pair-stored segments (the stream holds, per K step, per segment, per block,
 // the hi vectors and then the lo vectors).
 //
-// One CTA of 9 warps per SM, warp-specialised:
-//   warp 0               producer (the whole warp; lane 0 issues the copies):
-//                        per K step a bulk copy of its matrix bytes into the
-//                        current 16 KiB slot of a 6-slot ring (a slot --
-//                        "chunk" -- takes whole K steps, at most 6, across
+// One CTA of 10 warps per SM, warp-specialised:
+//   warp 9               matrix producer of the row stage (the whole warp; lane 0 issues the
+//                        copies): per K step a bulk copy of its matrix bytes
+//                        into the current 16 KiB slot of a 6-slot ring (a slot
+//                        -- "chunk" -- takes whole K steps, at most 6, across
 //                        segments and items; each copy adds its bytes with
 //                        mbarrier.expect_tx and the chunk is closed by one
-//                        arrive), a TMA tensor copy of the K step's inputs
-//                        into a 7 x 16 KiB ring, and beside the input slot the
-//                        step's MMAs fully formed (16 bytes each, lane q the
-//                        q-th) from the host-built step program;
+//                        arrive);
+//   warp 0               input producer (the whole warp; in the V stage also
+//                        the matrix producer, warp 9 idle): per K step a TMA
+//                        tensor copy of its inputs into a 7 x 16 KiB ring and,
+//                        beside the input slot, the step's MMAs fully formed
+//                        (16 bytes each, lane q the q-th) from the host-built
+//                        step program; it repeats the matrix producer's chunk
+//                        arithmetic to know where each step's matrix bytes lie;
 //   warps 1..4           MMA issue, one thread each: warp 1 + b issues row
 //                        block b's MMAs into its own TMEM columns (a thread
 //                        that issues MMAs whose operands it loads sustains
@@ -54,9 +58,12 @@
 //                        lanes 32 (w % 4) ..), scale, and store t (16-bit
 //                        hi/lo chunks) or y (each thread 32 consecutive rows of
 //                        its right-hand side).
-// A chunk holds fewer K steps than the input ring has slots, so the producer
-// always reaches the K step that closes a chunk before it needs an input slot
-// the MMAs of that chunk would free: no wait can close a cycle.
+// The matrix producer waits only for the chunk 6 back, the input producer only
+// for the input slot 7 back, and the MMAs of a chunk need only that chunk and
+// its input slots: no wait can close a cycle.  Where one warp holds both roles,
+// a chunk holds fewer K steps than the input ring has slots, so it always
+// reaches the K step that closes a chunk before it needs an input slot the
+// MMAs of that chunk would free.
 // Every mbarrier wait is bounded (kWaitLimitNs); a role that gives up records
 // the error and stops; before the CTA exits, the copies still in flight and
 // the MMAs issued are waited for (bounded) and the TMEM is freed.
@@ -79,7 +86,8 @@ constexpr int kTcwChunkSteps = 6; // K steps per chunk at most (< kTcwSlotsA)
 constexpr int kTcwSlotA = 16384;  // one K step of inputs: 4 chunks x 32 rows x 128 B
 constexpr int kTcwSlotsA = 7;
 static_assert(kTcwChunkSteps < kTcwSlotsA, "a chunk must hold fewer K steps than the input ring has slots");
-constexpr int kTcwThreads = 288;  // producer, 4 MMA-issue warps, 4 epilogue warps
+constexpr int kTcwThreads = 320;  // input producer, 4 MMA-issue warps, 4 epilogue warps, matrix producer
+constexpr int kTcwBoth = 0, kTcwInputs = 1, kTcwMatrix = 2;  // producer roles
 // Zeros: the B operand of the per-item MMA that clears the accumulators (256
 // rows x 16 columns, the second 8 columns 4 KiB on; its first 4 KiB also serve
 // as that MMA's A operand) and of an odd last K step's missing 8 columns.
@@ -240,74 +248,87 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
   const int tb = team < a.nteams ? a.team_begin[team] : 0;
   const int te = team < a.nteams ? a.team_begin[team + 1] : 0;
 
-  if (warp == 0) {
-    // ---- producer (the whole warp) ----
-    // Walks the team's step program: per input group its header and MMA
-    // templates (lane q gets template q), read by shuffles from two 32-entry
-    // windows of headers and two of templates that the warp loads coalesced one
-    // window ahead, so no global load latency lands on a K step; per K step the
-    // matrix bytes into the current chunk (lane 0),
-    // the step's MMAs formed from the templates (lane q writes MMA q: low words
-    // of the A and B descriptors, block, instruction descriptor), a header word
-    // (count, starts a chunk, the item's last step) and the input slot's TMA copy
-    // (lane 0), whose arrive publishes the MMAs.  Every lane keeps the same
-    // counters; lane 0's waits decide for all.
-    if (tb < te) {
-      uint4* ops = reinterpret_cast<uint4*>(tcw_smem + kTcwOffOps);
-      uint32_t* hdr = reinterpret_cast<uint32_t*>(tcw_smem + kTcwOffHdr);
-      const uint32_t zaddr = smem_u32(zero);
-      // A: input slot 0's first half, hi part (the two 64-rhs chunks 4 KiB apart); slot s is
-      // (16 KiB * s) >> 4 further on, the second half 2 KiB on, the lo part 8 KiB on
-      const uint32_t alo0 = (uint32_t)tc_desc_sw128(smem_u32(ringA), 4096, 1024);
-      const int g0 = a.gfirst[tb], gend = a.gfirst[te];
-      const int glast = max(gend - 1, 0);  // window loads past the team's groups read its last one
-      const int tlast = a.n_gops - 1;
-      int hb = g0;  // group of lane 0 of the header window H0; H1 holds the next 32
-      uint4 H0 = a.groups[min(hb + lane, glast)], H1 = a.groups[min(hb + 32 + lane, glast)];
-      uint32_t tc = __shfl_sync(0xffffffffu, H0.w, 0);  // this group's first template
-      uint32_t tw = tc;                                  // template of lane 0 of window T0; T1 the next 32
-      uint2 T0 = a.gops[min((int)tw + lane, tlast)], T1 = a.gops[min((int)tw + 32 + lane, tlast)];
-      uint32_t mI = 0, aI = 0, used = 0, cnt = 0, cbase = 0;
-      int ms = 0;
-      bool ok = true, open = false;
-      const char* g = a.data + a.tiles[tb].data_off * 16;  // the team's items are contiguous in the stream
-      for (int gi = g0; gi < gend && ok; gi++) {
-        if (gi - hb == 32) {
-          hb += 32;
-          H0 = H1;
-          H1 = a.groups[min(hb + 32 + lane, glast)];
-        }
-        const int hl = gi - hb;
-        uint4 gh;
-        gh.x = __shfl_sync(0xffffffffu, H0.x, hl);
-        gh.y = __shfl_sync(0xffffffffu, H0.y, hl);
-        gh.z = __shfl_sync(0xffffffffu, H0.z, hl);
-        const uint32_t counts = gh.z >> 16, hrows = gh.z & 0xfffu;
-        const uint32_t nops = (counts & 15u) + ((counts >> 4) & 15u) + ((counts >> 8) & 15u) + (counts >> 12);
+  // ---- producers (two whole warps, one role each) ----
+  // Each walks the team's step program: per input group its header (and, for
+  // the inputs, its MMA templates: lane q gets template q), read by shuffles
+  // from two 32-entry windows that the warp loads coalesced one window ahead,
+  // so no global load latency lands on a K step.  Both run the same chunk
+  // arithmetic.  The matrix role (warp 9) copies each K step's matrix bytes
+  // into the current chunk (lane 0: the chunk's mbarriers and bulk copies).
+  // The input role (warp 0) forms the step's MMAs from the templates (lane q
+  // writes MMA q: low words of the A and B descriptors, block, instruction
+  // descriptor), a header word (counts, starts a chunk, the item's last step)
+  // and the input slot's TMA copy (lane 0), whose arrive publishes the MMAs.
+  // Every lane keeps the same counters; lane 0's waits decide for all.  The
+  // row stage splits the roles (its producer bounds it); the V stage, bound by
+  // its epilogue, runs both in warp 0 (measured faster there).
+  auto produce = [&](auto role) {
+    constexpr int R = decltype(role)::value;  // kTcwBoth, kTcwInputs or kTcwMatrix
+    constexpr bool MAT = R != kTcwInputs, INP = R != kTcwMatrix;
+    if (tb >= te) return;
+    uint4* ops = reinterpret_cast<uint4*>(tcw_smem + kTcwOffOps);
+    uint32_t* hdr = reinterpret_cast<uint32_t*>(tcw_smem + kTcwOffHdr);
+    const uint32_t zaddr = smem_u32(zero);
+    // A: input slot 0's first half, hi part (the two 64-rhs chunks 4 KiB apart); slot s is
+    // (16 KiB * s) >> 4 further on, the second half 2 KiB on, the lo part 8 KiB on
+    const uint32_t alo0 = (uint32_t)tc_desc_sw128(smem_u32(ringA), 4096, 1024);
+    const int g0 = a.gfirst[tb], gend = a.gfirst[te];
+    const int glast = max(gend - 1, 0);  // window loads past the team's groups read its last one
+    const int tlast = a.n_gops - 1;
+    int hb = g0;  // group of lane 0 of the header window H0; H1 holds the next 32
+    uint4 H0 = a.groups[min(hb + lane, glast)], H1 = a.groups[min(hb + 32 + lane, glast)];
+    uint32_t tc = __shfl_sync(0xffffffffu, H0.w, 0);  // this group's first template
+    uint32_t tw = tc;                                  // template of lane 0 of window T0; T1 the next 32
+    uint2 T0 = make_uint2(0, 0), T1 = make_uint2(0, 0);
+    if constexpr (INP) {
+      T0 = a.gops[min((int)tw + lane, tlast)];
+      T1 = a.gops[min((int)tw + 32 + lane, tlast)];
+    }
+    uint32_t mI = 0, aI = 0, used = 0, cnt = 0, cbase = 0;
+    int ms = 0;
+    bool ok = true, open = false;
+    const char* g = a.data + a.tiles[tb].data_off * 16;  // the team's items are contiguous in the stream
+    for (int gi = g0; gi < gend && ok; gi++) {
+      if (gi - hb == 32) {
+        hb += 32;
+        H0 = H1;
+        H1 = a.groups[min(hb + 32 + lane, glast)];
+      }
+      const int hl = gi - hb;
+      uint4 gh;
+      gh.x = __shfl_sync(0xffffffffu, H0.x, hl);
+      gh.y = __shfl_sync(0xffffffffu, H0.y, hl);
+      gh.z = __shfl_sync(0xffffffffu, H0.z, hl);
+      const uint32_t counts = gh.z >> 16, hrows = gh.z & 0xfffu;
+      const uint32_t nops = (counts & 15u) + ((counts >> 4) & 15u) + ((counts >> 8) & 15u) + (counts >> 12);
+      const int hq = lane >= kTcwMaxOps ? 1 : 0, q = lane - hq * kTcwMaxOps;  // lane: half hq, MMA q
+      uint2 tp = make_uint2(0, 0);
+      if constexpr (INP) {
         if (tc - tw >= 32u) {  // a group's templates (<= kTcwMaxOps) span at most the two windows
           tw += 32;
           T0 = T1;
           T1 = a.gops[min((int)tw + 32 + lane, tlast)];
         }
-        const int hq = lane >= kTcwMaxOps ? 1 : 0, q = lane - hq * kTcwMaxOps;  // lane: half hq, MMA q
         const uint32_t ti = tc - tw + (uint32_t)min(q, kTcwMaxOps - 1);
         const uint32_t t0x = __shfl_sync(0xffffffffu, T0.x, (int)(ti & 31u));
         const uint32_t t0y = __shfl_sync(0xffffffffu, T0.y, (int)(ti & 31u));
         const uint32_t t1x = __shfl_sync(0xffffffffu, T1.x, (int)(ti & 31u));
         const uint32_t t1y = __shfl_sync(0xffffffffu, T1.y, (int)(ti & 31u));
-        const uint2 tp = ti < 32u ? make_uint2(t0x, t0y) : make_uint2(t1x, t1y);
+        tp = ti < 32u ? make_uint2(t0x, t0y) : make_uint2(t1x, t1y);
         tc += nops;
-        const CUtensorMap* map = (gh.x >> 31) ? &tmap : &xmap;
-        const int row0 = (int)(gh.x & 0x7fffffffu), nv = (int)gh.y, nks = (nv + 3) >> 2;
-        const uint32_t prow = tp.x & 0xfffu, alo = (tp.x >> 12) & 1u, blk = (tp.x >> 13) & 3u, rb16 = tp.x >> 16;
-        const uint32_t dcol = blk * (uint32_t)G::bstride + ((tp.x & kTcwCorrBit) ? (uint32_t)G::corr : 0u);
-        for (int j = 0; j < nks; j++) {
-          // 8-column vectors of the two halves (an odd last one: 1; a missing second half: 0)
-          const uint32_t nvj0 = (uint32_t)min(2, nv - 4 * j), nvj1 = (uint32_t)max(0, min(2, nv - 4 * j - 2));
-          const uint32_t kb0 = nvj0 * 16u * hrows, kb = kb0 + nvj1 * 16u * hrows;
-          uint32_t flags = 0;
-          if (!open || used + kb > (uint32_t)kTcwSlotM || cnt == kTcwChunkSteps) {
-            ms = mI % kTcwSlotsM;
+      }
+      const CUtensorMap* map = (gh.x >> 31) ? &tmap : &xmap;
+      const int row0 = (int)(gh.x & 0x7fffffffu), nv = (int)gh.y, nks = (nv + 3) >> 2;
+      const uint32_t prow = tp.x & 0xfffu, alo = (tp.x >> 12) & 1u, blk = (tp.x >> 13) & 3u, rb16 = tp.x >> 16;
+      const uint32_t dcol = blk * (uint32_t)G::bstride + ((tp.x & kTcwCorrBit) ? (uint32_t)G::corr : 0u);
+      for (int j = 0; j < nks; j++) {
+        // 8-column vectors of the two halves (an odd last one: 1; a missing second half: 0)
+        const uint32_t nvj0 = (uint32_t)min(2, nv - 4 * j), nvj1 = (uint32_t)max(0, min(2, nv - 4 * j - 2));
+        const uint32_t kb0 = nvj0 * 16u * hrows, kb = kb0 + nvj1 * 16u * hrows;
+        uint32_t flags = 0;
+        if (!open || used + kb > (uint32_t)kTcwSlotM || cnt == kTcwChunkSteps) {
+          ms = mI % kTcwSlotsM;
+          if constexpr (MAT) {
             bool okw = true;
             if (lane == 0) {
               if (open) mbar_arrive(&mfull[(mI + kTcwSlotsM - 1) % kTcwSlotsM]);  // close the chunk
@@ -318,19 +339,23 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
               open = false;
               break;
             }
-            mI++;
-            open = true;
-            used = cnt = 0;
-            cbase = smem_u32(ringM + ms * kTcwSlotM);
-            flags |= kTcwNewChunk;
           }
-          const int as = aI % kTcwSlotsA;
-          bool okw = true;
+          mI++;
+          open = true;
+          used = cnt = 0;
+          cbase = smem_u32(ringM + ms * kTcwSlotM);
+          flags |= kTcwNewChunk;
+        }
+        if constexpr (MAT) {
           if (lane == 0) {
             mbar_expect_tx_only(&mfull[ms], kb);
             bulk_g2s(ringM + ms * kTcwSlotM + used, g, kb, &mfull[ms]);
-            okw = aI < kTcwSlotsA || thread_wait(&aempty[as], ((aI / kTcwSlotsA) - 1) & 1);
           }
+        }
+        if constexpr (INP) {
+          const int as = aI % kTcwSlotsA;
+          bool okw = true;
+          if (lane == 0) okw = aI < kTcwSlotsA || thread_wait(&aempty[as], ((aI / kTcwSlotsA) - 1) & 1);
           if (!__shfl_sync(0xffffffffu, okw, 0)) {
             ok = false;
             break;
@@ -354,18 +379,26 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
             tma_load_3d(ringA + as * kTcwSlotA, map, 0, row0 + kTcwStepCols * j, 0, &afull[as]);
           }
           aI++;
-          g += kb;
-          used += kb;
-          cnt++;
         }
-      }
-      if (lane == 0) {
-        if (open) mbar_arrive(&mfull[ms]);  // close the last chunk (also after a failure, so it can drain)
-        misc[1] = mI;
-        misc[2] = aI;
-        if (!ok) atomicExch(a.err, 1);
+        g += kb;
+        used += kb;
+        cnt++;
       }
     }
+    if (lane == 0) {
+      if constexpr (MAT) {
+        if (open) mbar_arrive(&mfull[ms]);  // close the last chunk (also after a failure, so it can drain)
+        misc[1] = mI;
+      }
+      if constexpr (INP) misc[2] = aI;
+      if (!ok) atomicExch(a.err, 1);
+    }
+  };
+  if (warp == 0) {
+    if constexpr (VST) produce(std::integral_constant<int, kTcwBoth>{});
+    else produce(std::integral_constant<int, kTcwInputs>{});
+  } else if (warp == kTcwThreads / 32 - 1) {
+    if constexpr (!VST) produce(std::integral_constant<int, kTcwMatrix>{});
   } else if (warp <= 4) {
     // ---- MMA issue: warp 1 + b, one thread, row block b ----
     // Per item one MMA that clears the block's accumulator, then per K step
