@@ -31,8 +31,8 @@
 // pair-stored segments (the stream holds, per K step, per segment, per block,
 // the hi vectors and then the lo vectors).
 //
-// One CTA of 10 warps per SM, warp-specialised:
-//   warp 9               matrix producer of the row stage (the whole warp; lane 0 issues the
+// One CTA of 14 warps per SM, warp-specialised:
+//   warp 13              matrix producer of the row stage (the whole warp; lane 0 issues the
 //                        copies): per K step a bulk copy of its matrix bytes
 //                        into the current 16 KiB slot of a 6-slot ring (a slot
 //                        -- "chunk" -- takes whole K steps, at most 6, across
@@ -40,7 +40,7 @@
 //                        mbarrier.expect_tx and the chunk is closed by one
 //                        arrive);
 //   warp 0               input producer (the whole warp; in the V stage also
-//                        the matrix producer, warp 9 idle): per K step a TMA
+//                        the matrix producer, warp 13 idle): per K step a TMA
 //                        tensor copy of its inputs into a 7 x 16 KiB ring and,
 //                        beside the input slot, the step's MMAs fully formed
 //                        (16 bytes each, lane q the q-th) from the host-built
@@ -54,10 +54,13 @@
 //                        matrix chunk and finished accumulator to its
 //                        mbarrier, which counts the issuing warps (warp 1 also
 //                        allocates the TMEM);
-//   warps 5..8           epilogue: tcgen05.ld the accumulators (warp w reads
+//   warps 5..12          epilogue: tcgen05.ld the accumulators (warp w reads
 //                        lanes 32 (w % 4) ..), scale, and store t (16-bit
 //                        hi/lo chunks) or y (each thread 32 consecutive rows of
-//                        its right-hand side).
+//                        its right-hand side); in the V stage, whose bound is
+//                        converting and storing t, warps 5..8 take an item's
+//                        even 32-row chunks and warps 9..12 its odd ones; in
+//                        the row stage warps 5..8 take all and 9..12 idle.
 // The matrix producer waits only for the chunk 6 back, the input producer only
 // for the input slot 7 back, and the MMAs of a chunk need only that chunk and
 // its input slots: no wait can close a cycle.  Where one warp holds both roles,
@@ -86,7 +89,8 @@ constexpr int kTcwChunkSteps = 6; // K steps per chunk at most (< kTcwSlotsA)
 constexpr int kTcwSlotA = 16384;  // one K step of inputs: 4 chunks x 32 rows x 128 B
 constexpr int kTcwSlotsA = 7;
 static_assert(kTcwChunkSteps < kTcwSlotsA, "a chunk must hold fewer K steps than the input ring has slots");
-constexpr int kTcwThreads = 320;  // input producer, 4 MMA-issue warps, 4 epilogue warps, matrix producer
+constexpr int kTcwEpiWarps = 8;   // two per TMEM lane quadrant
+constexpr int kTcwThreads = 32 * (6 + kTcwEpiWarps);  // input producer, 4 MMA-issue warps, epilogue, matrix producer
 constexpr int kTcwBoth = 0, kTcwInputs = 1, kTcwMatrix = 2;  // producer roles
 // Zeros: the B operand of the per-item MMA that clears the accumulators (256
 // rows x 16 columns, the second 8 columns 4 KiB on; its first 4 KiB also serve
@@ -118,6 +122,9 @@ struct TcwGeom {
   static constexpr int issuers = VST ? 2 : 4;  // row blocks: one MMA-issue warp each
   static constexpr int cpb = VST ? 4 : 1;      // 32-row chunks of a row block at most
   static constexpr int chunks = issuers * cpb; // 32-row chunks of an item at most
+  // epilogue warps: V stage two per TMEM lane quadrant (converting and storing t
+  // bounds it), row stage one (more warps polling beside the producers slow it)
+  static constexpr int epi = VST ? kTcwEpiWarps : 4;
   static_assert(bufs * cols == 512, "the CTA owns the SM's 512 TMEM columns");
 };
 
@@ -225,7 +232,7 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
     }
     for (int s = 0; s < G::bufs; s++) {
       mbar_init(&accfull[s], G::issuers);
-      mbar_init(&accempty[s], 4);
+      mbar_init(&accempty[s], G::epi);
     }
     mbar_init(done, G::issuers);
     misc[1] = misc[2] = 0;
@@ -253,7 +260,7 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
   // the inputs, its MMA templates: lane q gets template q), read by shuffles
   // from two 32-entry windows that the warp loads coalesced one window ahead,
   // so no global load latency lands on a K step.  Both run the same chunk
-  // arithmetic.  The matrix role (warp 9) copies each K step's matrix bytes
+  // arithmetic.  The matrix role (warp 13) copies each K step's matrix bytes
   // into the current chunk (lane 0: the chunk's mbarriers and bulk copies).
   // The input role (warp 0) forms the step's MMAs from the templates (lane q
   // writes MMA q: low words of the A and B descriptors, block, instruction
@@ -488,9 +495,13 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
       if (!thread_wait(done, 0)) ok = false;
       if (!ok) atomicExch(a.err, 1);
     }
-  } else {
+  } else if (warp < 5 + G::epi) {
     // ---- epilogue ----
+    // Warps 5..4+G::epi: warp w reads TMEM lanes 32 (w % 4) .. (the right-hand
+    // sides 32 (w % 4) + lane); with 8 of them, of each item's 32-row chunks in
+    // order the even ones (w <= 8) or the odd ones.
     const int q = warp & 3;
+    const int half = G::epi == 8 ? (warp - 5) >> 2 : 0;
     const int r = 32 * q + lane;  // this thread's right-hand side
     const double sx = a.xscale[r];
     // The scale (and t slot) of row 32 k + lane of an item's chunk k (chunk k = 32-row
@@ -547,10 +558,12 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
       }
       tc_fence_after();
       int rb = 0;  // the block's first item row
+      int seq = 0;  // the item's chunks in order: this warp takes every other one
       for (int b = 0; b < G::issuers; b++) {
         const int Rb = (int)((R4 >> (8 * b)) & 0xffu);
         if (!Rb) break;  // blocks after the last are empty
         for (int c0 = 0; c0 < Rb; c0 += 32) {
+          if (G::epi == 8 && (seq++ & 1) != half) continue;
           const int k = b * G::cpb + (c0 >> 5), nrow = min(32, Rb - c0), row = rb + c0;
           float ts_l = rc.ts[0];
           int32_t slot_l = rc.sl[0];
