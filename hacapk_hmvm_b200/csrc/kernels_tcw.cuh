@@ -108,7 +108,9 @@ constexpr int kTcwOffHdr = kTcwOffOps + kTcwSlotsA * kTcwOpsPerSlot * 16;
 constexpr int kTcwOffBar = kTcwOffHdr + ((kTcwSlotsA * 4 + 15) & ~15);
 constexpr int kTcwNumBars = 2 * kTcwSlotsM + 2 * kTcwSlotsA + 2 * 4 + 1;
 constexpr int kTcwOffMisc = kTcwOffBar + kTcwNumBars * 8;
-constexpr int kTcwSmem = kTcwOffMisc + 32 + 1024;  // + room to align the base to 1 KiB
+// per epilogue warp: the current 32-row chunk's row scales and t slots (V stage)
+constexpr int kTcwOffRows = kTcwOffMisc + 32;
+constexpr int kTcwSmem = kTcwOffRows + kTcwEpiWarps * 32 * 8 + 1024;  // + room to align the base to 1 KiB
 static_assert(kTcwSmem <= 227 * 1024, "shared memory");
 // TMEM geometry per stage: accumulator buffers x columns, and the column stride of a row block
 // (a block's correction accumulator is corr columns after its main one: row
@@ -504,6 +506,12 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
     const int half = G::epi == 8 ? (warp - 5) >> 2 : 0;
     const int r = 32 * q + lane;  // this thread's right-hand side
     const double sx = a.xscale[r];
+    // V stage: this right-hand side's element of t slot 0 in the hi chunk and in
+    // the lo chunk (slot s is s * 64 elements on); per row of a chunk its scale
+    // and slot by one broadcast shared-memory load
+    uint16_t* const thi = VST ? a.tplanes + (int64_t)(r >> 6) * a.trows * 64 + (r & 63) : nullptr;
+    uint16_t* const tlo = VST ? thi + (int64_t)2 * a.trows * 64 : nullptr;
+    uint2* const rows_sm = reinterpret_cast<uint2*>(tcw_smem + kTcwOffRows) + (warp - 5) * 32;
     // The scale (and t slot) of row 32 k + lane of an item's chunk k (chunk k = 32-row
     // piece k % cpb of row block k / cpb), loaded a whole item ahead; the descriptors
     // two items ahead; a chunk's values are then taken by shuffles.
@@ -587,22 +595,29 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
             for (int i = 0; i < 32; i++) v[i] = 0.f;
           }
           if constexpr (VST) {
+            rows_sm[lane] = make_uint2(__float_as_uint(ts_l), (uint32_t)slot_l);
+            __syncwarp();
+            if (mode == 1) {
 #pragma unroll
-            for (int i = 0; i < 32; i++) {
-              const float ts = __shfl_sync(0xffffffffu, ts_l, i);
-              const int32_t slot = __shfl_sync(0xffffffffu, slot_l, i);
-              if (i < nrow) {
-                const float tv = v[i] * ts;
-                if (mode == 1) {
+              for (int i = 0; i < 32; i++) {
+                const uint2 e = rows_sm[i];
+                if (i < nrow) {
                   uint16_t hi, lo;
-                  tcw_split<BF>(tv, hi, lo);
-                  a.tplanes[((int64_t)(r >> 6) * a.trows + slot) * 64 + (r & 63)] = hi;
-                  a.tplanes[((int64_t)(2 + (r >> 6)) * a.trows + slot) * 64 + (r & 63)] = lo;
-                } else {
-                  a.part[(int64_t)(d.out_base + row + i) * 128 + r] = tv;
+                  tcw_split<BF>(v[i] * __uint_as_float(e.x), hi, lo);
+                  const int64_t so = (int64_t)(int32_t)e.y * 64;
+                  thi[so] = hi;
+                  tlo[so] = lo;
                 }
               }
+            } else {
+              float* const pp = a.part + (int64_t)(d.out_base + row) * 128 + r;
+#pragma unroll
+              for (int i = 0; i < 32; i++) {
+                const uint2 e = rows_sm[i];
+                if (i < nrow) pp[(int64_t)i * 128] = v[i] * __uint_as_float(e.x);
+              }
             }
+            __syncwarp();  // the chunk's rows are read before the next chunk writes them
           } else {
             const int64_t o = (int64_t)d.out_base + row + (int64_t)r * a.ldy;
 #pragma unroll
