@@ -940,9 +940,15 @@ int launch_tcw_pass(hmvm_plan* p, const void* X, int64_t ldx, void* Y, int64_t l
   const int gx = (int)std::min<int64_t>(((int64_t)p->nd + 31) / 32, (int64_t)p->num_sms * 16);
   if (!p->tcw_bf) {
     HMVM_CUDA_TRY(cudaMemsetAsync(p->d_amax128, 0, kTcwRhs * sizeof(unsigned), st), "scale reset");
-    const dim3 g((unsigned)std::max(1, std::min(p->num_sms, (p->nd + 255) / 256)), (unsigned)nr);
-    if (f32) hmvm_tcw_absmax_kernel<float><<<g, 256, 0, st>>>(static_cast<const float*>(X), ldx, p->nd, p->d_amax128);
-    else hmvm_tcw_absmax_kernel<double><<<g, 256, 0, st>>>(static_cast<const double*>(X), ldx, p->nd, p->d_amax128);
+    // per column at most 32 blocks of at least 16 elements per thread
+    const int per_col = std::max(1, std::min(32, p->nd / (kTcwAbsmaxThreads * 16)));
+    const dim3 g((unsigned)per_col, (unsigned)nr);
+    if (f32)
+      hmvm_tcw_absmax_kernel<float><<<g, kTcwAbsmaxThreads, 0, st>>>(static_cast<const float*>(X), ldx, p->nd,
+                                                                     p->d_amax128);
+    else
+      hmvm_tcw_absmax_kernel<double><<<g, kTcwAbsmaxThreads, 0, st>>>(static_cast<const double*>(X), ldx, p->nd,
+                                                                      p->d_amax128);
   }
   if (f32) {
     if (p->tcw_bf) hmvm_tcw_xplanes_kernel<float, true><<<gx, 256, 0, st>>>(static_cast<const float*>(X), ldx, p->nd, nr, p->d_amax128, p->d_xscale, p->d_xpl);

@@ -661,15 +661,37 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
 
 // ---- per-pass input planes -------------------------------------------------------
 // amax[r] = max |X[:, r]| as float bits (FP16 plans scale each right-hand side).
+// Grid (blocks per column, columns) with 256 threads: each block reduces its
+// share of column r in shared memory and makes one atomic (same-address
+// atomics from every warp of many small blocks measured slower than reading X).
+constexpr int kTcwAbsmaxThreads = 256;
 template <typename TX>
-__global__ void hmvm_tcw_absmax_kernel(const TX* __restrict__ X, int64_t ldx, int n, unsigned* __restrict__ amax) {
+__global__ void __launch_bounds__(kTcwAbsmaxThreads) hmvm_tcw_absmax_kernel(const TX* __restrict__ X, int64_t ldx,
+                                                                           int n, unsigned* __restrict__ amax) {
+  __shared__ float wm[kTcwAbsmaxThreads / 32];
   const int r = blockIdx.y;
-  float m = 0.f;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    m = fmaxf(m, fabsf((float)X[i + r * ldx]));
+  const TX* __restrict__ col = X + (int64_t)r * ldx;
+  const int64_t step = (int64_t)gridDim.x * kTcwAbsmaxThreads;
+  float m0 = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f;
+  int64_t i = blockIdx.x * (int64_t)kTcwAbsmaxThreads + threadIdx.x;
+  for (; i + 3 * step < n; i += 4 * step) {  // four independent loads in flight
+    m0 = fmaxf(m0, fabsf((float)col[i]));
+    m1 = fmaxf(m1, fabsf((float)col[i + step]));
+    m2 = fmaxf(m2, fabsf((float)col[i + 2 * step]));
+    m3 = fmaxf(m3, fabsf((float)col[i + 3 * step]));
+  }
+  for (; i < n; i += step) m0 = fmaxf(m0, fabsf((float)col[i]));
+  float m = fmaxf(fmaxf(m0, m1), fmaxf(m2, m3));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(amax + r, __float_as_uint(m));
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float b = wm[0];
+#pragma unroll
+    for (int w = 1; w < kTcwAbsmaxThreads / 32; w++) b = fmaxf(b, wm[w]);
+    if (b > 0.f) atomicMax(amax + r, __float_as_uint(b));
+  }
 }
 
 // sigma = 2^(ceil(log2 m) - 15), so |x| / sigma <= 2^15; 1 for m = 0, not finite, or BF16.
