@@ -515,7 +515,8 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
         // greedy: close an item before it exceeds the byte bound, the input
         // buffer or kMixedMaxSegs segments
         const int cfg = st == 0 ? L.stage1_cfg : L.stage2_cfg;
-        const int64_t zcap = std::min<int64_t>(kMixedCfgs[cfg].zbytes, kMultiZBytes / nrhs_max);
+        const int64_t zcap = std::min<int64_t>(kMixedCfgs[cfg].zbytes,
+                                               (nrhs_max == kTcNrhs ? kTcItemZBytes : kMultiZBytes) / nrhs_max);
         const int64_t bcap = std::max<int64_t>(max_item[st], (int64_t)t.nrows * 16);
         const int32_t vsplit = (st == 0 && opts.split_cols > 0) ? std::max(1, opts.split_cols / 4) : INT32_MAX;
         int64_t zb = 0, by = 0;

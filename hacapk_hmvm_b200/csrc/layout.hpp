@@ -164,7 +164,12 @@ constexpr int kDefaultMixedCfg2 = 8;
 constexpr int kMaxNrhsPass = 8;   // CUDA-core multi-RHS passes
 constexpr int kTcNrhs = 16;        // tensor-core passes (mixed plans with nrhs_max = 16)
 constexpr int kTcWarpsPerSm = 7;   // resident warps (teams) per SM of the tensor-core kernel
-constexpr int kMultiZBytes = 8192;
+// Each warp's two input buffers of the multi-RHS kernel (an item's x/t columns
+// for all of a pass's right-hand sides): 4 KiB each lets 3 CTAs of 4 warps
+// share an SM (12 warps; 8 with 8 KiB: 12 % faster at 8 FP32 right-hand sides).
+constexpr int kMultiZBytes = 4096;
+// An item's inputs for the 16-wide tensor-core pass (its kernel's buffer is kTcZBytes).
+constexpr int kTcItemZBytes = 8192;
 struct MultiCfg {
   int wpb, slots, chunk;
 };
@@ -174,7 +179,7 @@ constexpr int kNumMultiCfgs = 1;
 constexpr MultiCfg kMultiCfgs[kNumMultiCfgs] = {{4, 2, 4096}};
 inline int multi_smem_bytes(const MultiCfg& c) { return c.wpb * (c.slots * c.chunk + 2 * kMultiZBytes + c.slots * 8); }
 constexpr int kDefaultMultiCfg = 0;
-constexpr int kMultiWarpsPerSm = 8;  // resident warps (teams) per SM of the multi-RHS kernel
+constexpr int kMultiWarpsPerSm = 12;  // resident warps (teams) per SM of the multi-RHS kernel
 
 // Wide tensor-core passes (plans with nrhs_max >= kTcwMinNrhs, FP32 or mixed
 // storage): 128 right-hand sides per pass, every product on tcgen05.

@@ -98,7 +98,7 @@ def test_multi_rhs_items_fit_input_buffer(nrhs_max):
     for prec in (0, 1, 2):
         h, v = layout_for(hm, precision=prec, nrhs_max=nrhs_max)
         check_layout_bounds(v)
-        assert v.stage1_teams <= 148 * 8 and v.stage2_teams <= 148 * 8
+        assert v.stage1_teams <= 148 * 12 and v.stage2_teams <= 148 * 12  # kMultiWarpsPerSm (layout.hpp)
         tiles = np.ctypeslib.as_array((_lib.TileDesc * v.n_tiles).from_address(v.tiles))
         segs = np.ctypeslib.as_array((_lib.SegDesc * v.n_segs).from_address(v.segs))
         for td in tiles:
@@ -106,7 +106,7 @@ def test_multi_rhs_items_fit_input_buffer(nrhs_max):
             for sidx in range(int(td["seg_begin"]), int(td["seg_begin"]) + int(td["nseg"])):
                 ty, nc = seg_type(v, int(segs[sidx]["ncols"]))
                 zb += -(-nc // SEG_VEC[ty]) * SEG_VEC[ty] * (8 if ty == 0 else 4)
-            assert zb * nrhs_max <= 8192
+            assert zb * nrhs_max <= 4096  # kMultiZBytes (layout.hpp)
         assert relerr(emulate_layout(v, x), yo) < (1e-14 if prec == 0 else 1e-6 if prec == 1 else 1e-4)
         _lib.hmvm_lib().hmvm_b200_layout_destroy(h)
 
