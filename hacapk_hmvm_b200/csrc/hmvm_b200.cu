@@ -319,7 +319,7 @@ int prepare_kernels(const hmvm_plan* p) {
     int rc = tc_prepare(p);
     if (rc) return rc;
   } else if (p->nrhs_max > 1) {
-    const int smem = multi_smem_bytes(kMultiCfgs[kDefaultMultiCfg]);
+    const int smem = multi_smem_bytes(kMultiCfgs[kDefaultMultiCfg], plan_mode(p) == kModePlain64);
     for (int nr : {2, 4, 8})
       for (MultiFn f : {multi_kernel_for<true>(plan_mode(p), nr, kDefaultMultiCfg),
                         multi_kernel_for<false>(plan_mode(p), nr, kDefaultMultiCfg)})
@@ -787,7 +787,7 @@ int launch_multi_stages(hmvm_plan* p, void* Y, int64_t ldy, int nr, int nr_inst,
   a.scale = p->d_scale;
   const int mode = plan_mode(p);
   const MultiCfg& c = kMultiCfgs[kDefaultMultiCfg];
-  const int threads = 32 * c.wpb, smem = multi_smem_bytes(c);
+  const int threads = 32 * c.wpb, smem = multi_smem_bytes(c, mode == kModePlain64);
   cudaEvent_t* ev = nullptr;
   if (p->profiling && p->prof_count < kMaxProfiled) {
     ev = &p->prof_events[kEventsPerApply * (size_t)p->prof_count];
@@ -1970,7 +1970,7 @@ int batch_create(const std::vector<LeafTable>& tabs, bool is_float, const hmvm_p
   b->device = b->cls.front().plan->device;
   {
     DeviceGuard g(b->device);
-    const int smem = multi_smem_bytes(kMultiCfgs[kDefaultMultiCfg]);
+    const int smem = multi_smem_bytes(kMultiCfgs[kDefaultMultiCfg], batch_mode(b) == kModePlain64);
     for (bool vst : {true, false}) {
       cudaError_t e = cudaFuncSetAttribute(batch_stage_kernel_for(batch_mode(b), vst),
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -2139,7 +2139,7 @@ int batch_run_t(hmvm_batch* b, cudaStream_t st) {
   const int mode = batch_mode(b);
   int* err = b->cls.front().plan->d_err;
   const MultiCfg& mc = kMultiCfgs[kDefaultMultiCfg];
-  const int threads = 32 * mc.wpb, smem = multi_smem_bytes(mc);
+  const int threads = 32 * mc.wpb, smem = multi_smem_bytes(mc, mode == kModePlain64);
   const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((b->nmax_rows * 8 + 255) / 256, 64));
   const dim3 pgrid(gx, (unsigned)b->pack.size());
   const int nio = (int)b->io.size();

@@ -226,9 +226,9 @@ __device__ __forceinline__ void multi_vec(const uint4 m, const unsigned char* z,
   }
 }
 
-template <int WPB, int S, int CHUNK>
+template <int WPB, int S, int CHUNK, int ZB>
 constexpr int multi_min_blocks() {
-  constexpr int smem = WPB * (S * CHUNK + 2 * kMultiZBytes + S * 8);
+  constexpr int smem = WPB * (S * CHUNK + 2 * ZB + S * 8);
   constexpr int by_smem = (227 * 1024) / smem;
   constexpr int by_warps = 16 / WPB;
   constexpr int m = by_smem < by_warps ? by_smem : by_warps;
@@ -243,6 +243,7 @@ __device__ __forceinline__ void multi_body(const MultiArgs& a, int bid) {
   using TT = typename MM::TT;
   using TYO = typename MM::TY;
   constexpr uint32_t RING = (uint32_t)S * CHUNK;
+  constexpr int ZB = MODE == kModePlain64 ? kMultiZBytesF64 : kMultiZBytes;  // each of the two input buffers
   constexpr int B = 2;  // vectors per batch: each carries 2..16 columns of NR products
   static_assert((RING & (RING - 1)) == 0, "ring size must be a power of two");
   static_assert(CHUNK % 16 == 0 && CHUNK >= 512, "bulk copies move multiples of 16 bytes");
@@ -256,8 +257,8 @@ __device__ __forceinline__ void multi_body(const MultiArgs& a, int bid) {
   const int tb = a.team_begin[team], te = a.team_begin[team + 1];
   if (tb >= te) return;
   unsigned char* ring = smem + (size_t)warp * RING;
-  unsigned char* zbase = smem + (size_t)WPB * RING + (size_t)warp * 2 * kMultiZBytes;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)WPB * RING + (size_t)WPB * 2 * kMultiZBytes) + warp * S;
+  unsigned char* zbase = smem + (size_t)WPB * RING + (size_t)warp * 2 * ZB;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)WPB * RING + (size_t)WPB * 2 * ZB) + warp * S;
 
   const hmvm_tile_desc* __restrict__ tiles = a.tiles;
   const hmvm_seg_desc* __restrict__ segs = a.segs;
@@ -310,9 +311,9 @@ __device__ __forceinline__ void multi_body(const MultiArgs& a, int bid) {
   uint32_t q_ready = 0, q_rel = 0;
   bool failed = false;
   for (int ti = tb, k = 0; ti < te; ++ti, ++k) {
-    unsigned char* zcur = zbase + (k & 1) * kMultiZBytes;
+    unsigned char* zcur = zbase + (k & 1) * ZB;
     __syncwarp();
-    if (ti + 1 < te) gather_multi<MODE, NR, CHECK>(nxt, nxt_seg, a, zbase + ((k + 1) & 1) * kMultiZBytes, lane);
+    if (ti + 1 < te) gather_multi<MODE, NR, CHECK>(nxt, nxt_seg, a, zbase + ((k + 1) & 1) * ZB, lane);
     cp_async_commit();
     const bool has_nn = ti + 2 < te;
     const hmvm_tile_desc nn = has_nn ? tiles[ti + 2] : dzero;
@@ -459,7 +460,8 @@ __device__ __forceinline__ void multi_body(const MultiArgs& a, int bid) {
 }
 
 template <int WPB, int S, int CHUNK, int NR, int MODE, bool VST>
-__global__ void __launch_bounds__(32 * WPB, (multi_min_blocks<WPB, S, CHUNK>()))
+__global__ void __launch_bounds__(
+    32 * WPB, (multi_min_blocks<WPB, S, CHUNK, (MODE == kModePlain64 ? kMultiZBytesF64 : kMultiZBytes)>()))
     hmvm_multi_kernel(MultiArgs a) {
   multi_body<WPB, S, CHUNK, NR, MODE, VST>(a, (int)blockIdx.x);
 }
@@ -530,7 +532,8 @@ struct BatchPart {
   int32_t nr;    // pass width: 2, 4 or 8
 };
 template <int WPB, int S, int CHUNK, int MODE, bool VST>
-__global__ void __launch_bounds__(32 * WPB, (multi_min_blocks<WPB, S, CHUNK>()))
+__global__ void __launch_bounds__(
+    32 * WPB, (multi_min_blocks<WPB, S, CHUNK, (MODE == kModePlain64 ? kMultiZBytesF64 : kMultiZBytes)>()))
     hmvm_batch_multi_kernel(const BatchPart* __restrict__ parts, int nparts) {
   int k = 0;
   while (k + 1 < nparts && (int)blockIdx.x >= parts[k + 1].cta0) k++;

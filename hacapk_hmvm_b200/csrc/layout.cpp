@@ -468,7 +468,8 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
     if (nrhs_max > 1) {
       // teams for the multi-RHS kernel, all resident at once (and no more than
       // the single-vector kernels launch)
-      const int per_sm = nrhs_max == kTcNrhs ? kTcWarpsPerSm : kMultiWarpsPerSm;
+      const bool f64 = !L.mixed && L.elem_size == 8;
+      const int per_sm = nrhs_max == kTcNrhs ? kTcWarpsPerSm : (f64 ? kMultiWarpsPerSmF64 : kMultiWarpsPerSm);
       L.stage1_teams = std::min(L.stage1_teams, L.num_sms * per_sm);
       L.stage2_teams = std::min(L.stage2_teams, L.num_sms * per_sm);
     }
@@ -506,7 +507,7 @@ int build_layout(const LeafTable &lt, const hmvm_plan_opts &opts, int num_sms, H
           // an item's x/t columns must fit the kernels' input buffers
           const int32_t cfg = st == 0 ? L.stage1_cfg : L.stage2_cfg;
           int32_t zcap = L.kernel == 1 ? kStreamCfgs[cfg].zcap : INT32_MAX;
-          if (nrhs_max > 1) zcap = std::min(zcap, kMultiZBytes / (nrhs_max * L.elem_size));
+          if (nrhs_max > 1) zcap = std::min(zcap, multi_zbytes(L.elem_size == 8) / (nrhs_max * L.elem_size));
           const int32_t vmax = std::max(1, zcap / VEC);
           nparts = std::max(nparts, (t.nvec + vmax - 1) / vmax);
         }

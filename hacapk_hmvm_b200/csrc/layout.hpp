@@ -167,7 +167,11 @@ constexpr int kTcWarpsPerSm = 7;   // resident warps (teams) per SM of the tenso
 // Each warp's two input buffers of the multi-RHS kernel (an item's x/t columns
 // for all of a pass's right-hand sides): 4 KiB each lets 3 CTAs of 4 warps
 // share an SM (12 warps; 8 with 8 KiB: 12 % faster at 8 FP32 right-hand sides).
+// FP64 plans keep 8 KiB and 8 warps: their inputs are twice as wide, and 4 KiB
+// cut their items twice as often (10 % slower at 8 right-hand sides).
 constexpr int kMultiZBytes = 4096;
+constexpr int kMultiZBytesF64 = 8192;
+constexpr int multi_zbytes(bool f64) { return f64 ? kMultiZBytesF64 : kMultiZBytes; }
 // An item's inputs for the 16-wide tensor-core pass (its kernel's buffer is kTcZBytes).
 constexpr int kTcItemZBytes = 8192;
 struct MultiCfg {
@@ -177,9 +181,12 @@ struct MultiCfg {
 // 4 x 2 KiB and 8 x 1 KiB rings it replaced)
 constexpr int kNumMultiCfgs = 1;
 constexpr MultiCfg kMultiCfgs[kNumMultiCfgs] = {{4, 2, 4096}};
-inline int multi_smem_bytes(const MultiCfg& c) { return c.wpb * (c.slots * c.chunk + 2 * kMultiZBytes + c.slots * 8); }
+inline int multi_smem_bytes(const MultiCfg& c, bool f64) {
+  return c.wpb * (c.slots * c.chunk + 2 * multi_zbytes(f64) + c.slots * 8);
+}
 constexpr int kDefaultMultiCfg = 0;
-constexpr int kMultiWarpsPerSm = 12;  // resident warps (teams) per SM of the multi-RHS kernel
+constexpr int kMultiWarpsPerSm = 12;    // resident warps (teams) per SM of the multi-RHS kernel
+constexpr int kMultiWarpsPerSmF64 = 8;  // the same for FP64 plans (8 KiB input buffers)
 
 // Wide tensor-core passes (plans with nrhs_max >= kTcwMinNrhs, FP32 or mixed
 // storage): 128 right-hand sides per pass, every product on tcgen05.

@@ -106,7 +106,7 @@ def test_multi_rhs_items_fit_input_buffer(nrhs_max):
             for sidx in range(int(td["seg_begin"]), int(td["seg_begin"]) + int(td["nseg"])):
                 ty, nc = seg_type(v, int(segs[sidx]["ncols"]))
                 zb += -(-nc // SEG_VEC[ty]) * SEG_VEC[ty] * (8 if ty == 0 else 4)
-            assert zb * nrhs_max <= 4096  # kMultiZBytes (layout.hpp)
+            assert zb * nrhs_max <= (8192 if prec == 0 else 4096)  # kMultiZBytesF64, kMultiZBytes (layout.hpp)
         assert relerr(emulate_layout(v, x), yo) < (1e-14 if prec == 0 else 1e-6 if prec == 1 else 1e-4)
         _lib.hmvm_lib().hmvm_b200_layout_destroy(h)
 
