@@ -199,6 +199,49 @@ __device__ __forceinline__ void tcw_split(float v, uint16_t& hi, uint16_t& lo) {
   }
 }
 
+// Row-stage output: rows 0..31 of a 32-row chunk for this lane's right-hand
+// side, y[o + i] = v[i] * ts_i * sx (ts_i from lane i), rows >= nrow skipped.
+// W consecutive rows go out as one 16-byte store (W = 2 doubles or 4 floats;
+// W = 1: single stores) from row P on, P chosen by the caller so that o + P is
+// a multiple of W (the same on every lane when the leading dimension is);
+// the rows before P and after the last whole group go out singly.
+template <typename T, int W, int P>
+__device__ __forceinline__ void tcw_store_rows(T* __restrict__ y, int64_t o, int nrow, bool act, const float* v,
+                                               float ts_l, double sx) {
+  auto val = [&](int i, float ts) { return (T)((double)v[i] * (double)ts * sx); };
+#pragma unroll
+  for (int i = 0; i < P; i++) {
+    const float ts = __shfl_sync(0xffffffffu, ts_l, i);
+    if (act && i < nrow) y[o + i] = val(i, ts);
+  }
+  constexpr int kEnd = P + ((32 - P) / W) * W;
+#pragma unroll
+  for (int i = P; i < kEnd; i += W) {
+    float ts[W];
+#pragma unroll
+    for (int k = 0; k < W; k++) ts[k] = __shfl_sync(0xffffffffu, ts_l, i + k);
+    if (act) {
+      if (W > 1 && i + W <= nrow) {
+        if constexpr (W == 2) {
+          *reinterpret_cast<double2*>(y + o + i) = make_double2(val(i, ts[0]), val(i + 1, ts[1]));
+        } else if constexpr (W == 4) {
+          *reinterpret_cast<float4*>(y + o + i) =
+              make_float4(val(i, ts[0]), val(i + 1, ts[1]), val(i + 2, ts[2]), val(i + 3, ts[3]));
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < W; k++)
+          if (i + k < nrow) y[o + i + k] = val(i + k, ts[k]);
+      }
+    }
+  }
+#pragma unroll
+  for (int i = kEnd; i < 32; i++) {
+    const float ts = __shfl_sync(0xffffffffu, ts_l, i);
+    if (act && i < nrow) y[o + i] = val(i, ts);
+  }
+}
+
 template <bool VST, bool BF>
 __global__ void __launch_bounds__(kTcwThreads, 1)
     hmvm_tcw_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap tmap,
@@ -512,6 +555,9 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
     uint16_t* const thi = VST ? a.tplanes + (int64_t)(r >> 6) * a.trows * 64 + (r & 63) : nullptr;
     uint16_t* const tlo = VST ? thi + (int64_t)2 * a.trows * 64 : nullptr;
     uint2* const rows_sm = reinterpret_cast<uint2*>(tcw_smem + kTcwOffRows) + (warp - 5) * 32;
+    // row stage: 16-byte stores of consecutive rows where y's base is 16-byte aligned and its
+    // leading dimension a multiple of the rows per store (then every lane's rows align alike)
+    const bool vec_y = !VST && (reinterpret_cast<uintptr_t>(a.y) & 15) == 0 && (a.ldy & (a.y32 ? 3 : 1)) == 0;
     // The scale (and t slot) of row 32 k + lane of an item's chunk k (chunk k = 32-row
     // piece k % cpb of row block k / cpb), loaded a whole item ahead; the descriptors
     // two items ahead; a chunk's values are then taken by shuffles.
@@ -620,14 +666,20 @@ __global__ void __launch_bounds__(kTcwThreads, 1)
             __syncwarp();  // the chunk's rows are read before the next chunk writes them
           } else {
             const int64_t o = (int64_t)d.out_base + row + (int64_t)r * a.ldy;
-#pragma unroll
-            for (int i = 0; i < 32; i++) {
-              const float ts = __shfl_sync(0xffffffffu, ts_l, i);
-              if (i < nrow && r < a.nr) {
-                const double val = (double)v[i] * (double)ts * sx;
-                if (a.y32) static_cast<float*>(a.y)[o + i] = (float)val;
-                else static_cast<double*>(a.y)[o + i] = val;
-              }
+            const bool act = r < a.nr;
+            const int m = (int)(((int64_t)d.out_base + row) & 3);  // o's offset from a 4-element boundary (vec_y)
+            if (a.y32) {
+              float* const y = static_cast<float*>(a.y);
+              if (!vec_y) tcw_store_rows<float, 1, 0>(y, o, nrow, act, v, ts_l, sx);
+              else if (m == 0) tcw_store_rows<float, 4, 0>(y, o, nrow, act, v, ts_l, sx);
+              else if (m == 1) tcw_store_rows<float, 4, 3>(y, o, nrow, act, v, ts_l, sx);
+              else if (m == 2) tcw_store_rows<float, 4, 2>(y, o, nrow, act, v, ts_l, sx);
+              else tcw_store_rows<float, 4, 1>(y, o, nrow, act, v, ts_l, sx);
+            } else {
+              double* const y = static_cast<double*>(a.y);
+              if (!vec_y) tcw_store_rows<double, 1, 0>(y, o, nrow, act, v, ts_l, sx);
+              else if ((m & 1) == 0) tcw_store_rows<double, 2, 0>(y, o, nrow, act, v, ts_l, sx);
+              else tcw_store_rows<double, 2, 1>(y, o, nrow, act, v, ts_l, sx);
             }
           }
         }

@@ -63,7 +63,10 @@ def _check(hm, prec, fmt, X, Y, cols):
 
 
 @pytest.mark.parametrize("prec,fmt", [("mixed", "fp16"), ("mixed", "bf16"), ("fp32", None)])
-@pytest.mark.parametrize("case", [(3000, "cube", 2), (2048, "sphere", 1), (1500, "plate", 3)],
+# N (= the leading dimension of Y) sets the row stage's stores: multiples of 4 take
+# 16-byte stores for FP64 and FP32 outputs, 1202 for FP64 only, 1201 single stores.
+@pytest.mark.parametrize("case", [(3000, "cube", 2), (2048, "sphere", 1), (1500, "plate", 3), (1202, "sphere", 4),
+                                  (1201, "cube", 6)],
                          ids=lambda c: f"{c[1]}{c[0]}")
 def test_tcw_parity(gpu, prec, fmt, case):
     hm = _mat(*case)
