@@ -9,7 +9,10 @@ import ctypes as C
 import os
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_HMVM_PATH = os.path.join(_PKG, "libhmvm_b200.so")
+# HMVM_B200_DEVICE_CHECKS=1 selects the build with device bounds checks
+# (hmvm_b200_layout_validate's checks before every single-vector stage launch)
+DEVICE_CHECKS = os.environ.get("HMVM_B200_DEVICE_CHECKS", "0") == "1"
+LIB_HMVM_PATH = os.path.join(_PKG, "libhmvm_b200_checked.so" if DEVICE_CHECKS else "libhmvm_b200.so")
 LIB_HGEN_PATH = os.path.join(_PKG, "libhgen.so")
 
 # ---- status codes (hmvm_b200.h) ------------------------------------------
@@ -209,6 +212,9 @@ HMVM_SIGNATURES = {
     "hmvm_b200_layout_build64": (C.c_int, [C.POINTER(Leaves64), C.c_int32, C.POINTER(PlanOpts), C.c_int32,
                                            C.POINTER(C.c_void_p)]),
     "hmvm_b200_layout_view": (C.c_int, [C.c_void_p, C.POINTER(LayoutView)]),
+    "hmvm_b200_layout_validate": (C.c_int, [C.c_void_p]),
+    "hmvm_b200_plan_descriptors": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int32),
+                                             C.POINTER(C.c_int32)]),
     "hmvm_b200_layout_destroy": (None, [C.c_void_p]),
     "hmvm_b200_strerror": (C.c_char_p, [C.c_int]),
     "hmvm_b200_last_error": (C.c_char_p, []),

@@ -2,6 +2,10 @@
 
     libhmvm_b200.so  the HMVM library: host planner + sm_100a kernels + C ABI
                      (nvcc -gencode arch=compute_100a,code=sm_100a)
+    libhmvm_b200_checked.so
+                     the same built with HMVM_DEVICE_CHECKS: descriptor bounds
+                     checks on the device before every single-vector stage
+                     (loaded instead when HMVM_B200_DEVICE_CHECKS=1)
     libhgen.so       the H-matrix generator / writer (host C++, OpenMP)
 
 Run ``python -m hacapk_hmvm_b200.build`` (or ``__graft_entry__.build()``).  The
@@ -20,6 +24,7 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 
 LIB_HMVM = os.path.join(PKG, "libhmvm_b200.so")
+LIB_HMVM_CHECKED = os.path.join(PKG, "libhmvm_b200_checked.so")
 LIB_HGEN = os.path.join(PKG, "libhgen.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -56,15 +61,17 @@ def hmvm_sources() -> list[str]:
 
 
 def hmvm_deps() -> list[str]:
-    deps = hmvm_sources() + [os.path.join(CSRC, f) for f in ("kernels.cuh", "kernels_multi.cuh", "kernels_tc.cuh", "kernels_tcw.cuh", "layout.hpp", "numfmt.hpp")]
+    deps = hmvm_sources() + [os.path.join(CSRC, f) for f in ("kernels.cuh", "kernels_multi.cuh", "kernels_tc.cuh", "kernels_tcw.cuh", "layout.hpp", "numfmt.hpp", "validate.hpp")]
     deps += [os.path.join(INCLUDE, "hmvm_b200.h"), os.path.join(INCLUDE, "hacapk_hgen.h")]
     return deps
 
 
-def build_hmvm(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
-    if not force and not _stale(LIB_HMVM, hmvm_deps()):
-        return LIB_HMVM
-    tmp = LIB_HMVM + ".tmp"
+def build_hmvm(force: bool = False, verbose: bool = False, extra: list[str] | None = None,
+               checked: bool = False) -> str:
+    out = LIB_HMVM_CHECKED if checked else LIB_HMVM
+    if not force and not _stale(out, hmvm_deps()):
+        return out
+    tmp = out + ".tmp"
     cmd = [
         _nvcc(), "-O3", "-std=c++17", "-lineinfo", *ARCH,
         "-ccbin", _hostcxx(),
@@ -73,11 +80,13 @@ def build_hmvm(force: bool = False, verbose: bool = False, extra: list[str] | No
         "-I", INCLUDE, "-I", CSRC,
         "-shared", "-o", tmp, *hmvm_sources(), "-lgomp",
     ]
+    if checked:
+        cmd[1:1] = ["-DHMVM_DEVICE_CHECKS"]
     if extra:
         cmd[1:1] = extra
     _run(cmd, verbose)
-    os.replace(tmp, LIB_HMVM)
-    return LIB_HMVM
+    os.replace(tmp, out)
+    return out
 
 
 def build_hgen(force: bool = False, verbose: bool = False) -> str:
@@ -93,8 +102,13 @@ def build_hgen(force: bool = False, verbose: bool = False) -> str:
 
 
 def build_all(force: bool = False, verbose: bool = False) -> None:
+    from concurrent.futures import ThreadPoolExecutor
+
     build_hgen(force, verbose)
-    build_hmvm(force, verbose)
+    with ThreadPoolExecutor(2) as ex:  # the two nvcc runs side by side
+        jobs = [ex.submit(build_hmvm, force, verbose, None, c) for c in (False, True)]
+        for j in jobs:
+            j.result()
 
 
 if __name__ == "__main__":

@@ -199,6 +199,11 @@ struct hmvm_plan {
   double* d_scale = nullptr;
   int64_t cols_fp32 = 0, cols_lr16 = 0, cols_fp8 = 0, stored_bytes = 0;
   int t_elem = 8, p_elem = 8;  // bytes per t slot and per partial sum
+  // device bounds checks (HMVM_DEVICE_CHECKS builds): buffer lengths, elements per
+  // vector of plain layouts, and each stage kernel's input buffer in bytes
+  LayoutCaps caps;
+  int vec = 2;
+  int64_t zcap1 = 0, zcap2 = 0;
   int64_t stage1_bytes = 0, stage2_bytes = 0;
   // multi-RHS (nrhs_max > 1): packed inputs, t and partial sums for up to nrhs_max rhs
   int nrhs_max = 1;
@@ -418,6 +423,87 @@ int tcw_buffers(hmvm_plan* p, const HostLayout& L) {
 
 // sms_cap > 0: plan the layout's teams for that many SMs (a batch class shares the GPU
 // with the other classes of its batch, which run in the same launches).
+// The input buffer of a stage's kernel for a layout's shapes, in bytes, as the
+// planner bounds items by it (0: the kernel has none, or the layout is the
+// wide tensor-core one, whose items these checks do not describe).
+int64_t stage_zcap_bytes(const HostLayout& L, int stage) {
+  if (L.tcw) return 0;
+  const int cfg = stage == 1 ? L.stage1_cfg : L.stage2_cfg;
+  if (L.mixed)
+    return std::min<int64_t>(kMixedCfgs[cfg].zbytes,
+                             (L.nrhs_max == kTcNrhs ? kTcItemZBytes : kMultiZBytes) / L.nrhs_max);
+  int64_t zcap = L.kernel == 1 ? (int64_t)kStreamCfgs[cfg].zcap : -1;
+  if (L.nrhs_max > 1) {
+    const int64_t zm = multi_zbytes(L.elem_size == 8) / ((int64_t)L.nrhs_max * L.elem_size);
+    zcap = zcap < 0 ? zm : std::min(zcap, zm);
+  }
+  return zcap < 0 ? 0 : zcap * L.elem_size;
+}
+
+LayoutCaps caps_of(const HostLayout& L) {
+  LayoutCaps c;
+  c.data_vectors = (int64_t)L.data.size();
+  c.n_segs = (int64_t)L.segs.size();
+  c.n_out_idx = (int64_t)L.out_idx.size();
+  c.t_len = L.t_len;
+  c.p_len = L.p_len;
+  c.nd = L.nd;
+  c.n_rowscale = (int64_t)L.rowscale.size();
+  c.n_tiles = (int32_t)L.tiles.size();
+  c.max_rows = kMaxRows;
+  c.max_segs = L.mixed ? kMixedMaxSegs : 0;
+  c.mixed = L.mixed ? 1 : 0;
+  return c;
+}
+
+const char* check_name(int rc) {
+  switch (rc) {
+    case kCheckData: return "its vectors leave the data stream";
+    case kCheckSegs: return "its segment descriptors leave the segment table";
+    case kCheckRows: return "its rows are outside 1..32 or its vectors negative";
+    case kCheckOut: return "its output rows leave their buffer";
+    case kCheckSlot: return "a t slot it writes is outside t";
+    case kCheckSrc: return "a segment's columns leave x or t";
+    case kCheckInputs: return "its inputs exceed the kernel's input buffer";
+    case kCheckType: return "a segment's storage type is unknown";
+    case kCheckScale: return "its row scales leave the row-scale table";
+    default: return "bounds check failed";
+  }
+}
+
+// Every descriptor of a single-vector layout against the buffers it indexes
+// (validate.hpp); wide tensor-core layouts are not described by these checks.
+int validate_layout(const HostLayout& L, std::string& msg) {
+  if (L.tcw) return HMVM_OK;
+  const LayoutCaps c = caps_of(L);
+  const int64_t z1 = stage_zcap_bytes(L, 1), z2 = stage_zcap_bytes(L, 2);
+  for (int32_t k = 0; k < (int32_t)L.tiles.size(); k++) {
+    const bool st1 = k < L.stage1_tiles;
+    const int rc = check_tile(L.tiles[k], L.segs.data(), L.out_idx.data(), c, L.vec, L.elem_size, st1 ? z1 : z2, st1);
+    if (rc) {
+      msg = "item " + std::to_string(k) + " (stage " + (st1 ? "1" : "2") + "): " + check_name(rc);
+      return HMVM_ERANGE;
+    }
+  }
+  for (int st = 1; st <= 2; st++) {
+    const std::vector<int32_t>& red = st == 1 ? L.red1 : L.red2;
+    for (size_t e = 0; e + 4 <= red.size(); e += 4)
+      if (check_red(&red[e], c, st == 1)) {
+        msg = "reduction entry " + std::to_string(e / 4) + " of stage " + std::to_string(st) +
+              " reads or writes outside its buffers";
+        return HMVM_ERANGE;
+      }
+    const std::vector<int32_t>& tb = st == 1 ? L.team_begin1 : L.team_begin2;
+    const int32_t nt = st == 1 ? L.stage1_teams : L.stage2_teams;
+    const int32_t first = st == 1 ? 0 : L.stage1_tiles, end = st == 1 ? L.stage1_tiles : (int32_t)L.tiles.size();
+    if ((int64_t)tb.size() != (int64_t)nt + 1 || check_teams(tb.data(), nt, first, end)) {
+      msg = "the team ranges of stage " + std::to_string(st) + " do not cover its items in order";
+      return HMVM_ERANGE;
+    }
+  }
+  return HMVM_OK;
+}
+
 int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** out, int sms_cap = 0) {
   if (!out) return set_error(HMVM_EINVAL, "plan output pointer is NULL");
   *out = nullptr;
@@ -485,6 +571,19 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   p->cols_fp8 = L->cols_fp8;
   p->t_elem = L->mixed ? 4 : L->elem_size;
   p->p_elem = L->elem_size;
+  p->caps = caps_of(*L);
+  p->vec = L->vec;
+  p->zcap1 = stage_zcap_bytes(*L, 1);
+  p->zcap2 = stage_zcap_bytes(*L, 2);
+  if (kDeviceChecks) {  // checked builds also check the layout on the host
+    std::string vmsg;
+    rc = validate_layout(*L, vmsg);
+    if (rc) {
+      delete L;
+      delete p;
+      return set_error(rc, "layout check: " + vmsg);
+    }
+  }
   if (L->tcw) {
     // Algorithmic bytes per pass: the stored elements in their storage formats
     // (pairs count 4 bytes) and scales; per stage kernel also the 16-bit planes
@@ -580,6 +679,32 @@ int create_plan(const LeafTable& lt, const hmvm_plan_opts* opts_in, hmvm_plan** 
   return HMVM_OK;
 }
 
+// HMVM_DEVICE_CHECKS builds: the stage's descriptors checked on the device
+// (hmvm_validate_kernel) before it runs; other builds launch nothing.
+int launch_validate(bool& first, hmvm_plan* p, int stage, cudaStream_t st) {
+  if (!kDeviceChecks) return HMVM_OK;
+  ValidateArgs v;
+  v.tiles = p->d_tiles;
+  v.segs = p->d_segs;
+  v.out_idx = p->d_out_idx;
+  v.team_begin = stage == 1 ? p->d_tb1 : p->d_tb2;
+  v.red = stage == 1 ? p->d_red1 : p->d_red2;
+  v.nteams = stage == 1 ? p->stage1_teams : p->stage2_teams;
+  v.first = stage == 1 ? 0 : p->stage1_tiles;
+  v.end = stage == 1 ? p->stage1_tiles : p->stage1_tiles + p->stage2_tiles;
+  v.n_red = stage == 1 ? p->n_red1 : p->n_red2;
+  v.caps = p->caps;
+  v.vec = p->vec;
+  v.elem = p->elem;
+  v.stage1 = stage == 1 ? 1 : 0;
+  v.zcap = stage == 1 ? p->zcap1 : p->zcap2;
+  v.err = p->d_err;
+  const int64_t n = std::max<int64_t>(v.end - v.first, v.n_red);
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)p->num_sms * 4));
+  HMVM_CUDA_TRY(launch_in_apply(first, hmvm_validate_kernel, grid, 256, 0, st, v), "validation launch");
+  return HMVM_OK;
+}
+
 // Mixed plans: x rounded to FP32, V stage (scaled t in FP32), its reduction,
 // row stage, its reduction into y (partials in FP64).
 int launch_stages_mixed(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, float* x32, cudaStream_t st) {
@@ -606,6 +731,8 @@ int launch_stages_mixed(hmvm_plan* p, const void* x, void* y, void* tbuf, void* 
                                 256, 0, st, static_cast<const double*>(x), x32, p->nd),
                 "x rounding launch");
   if (p->stage1_tiles > 0) {
+    int vrc = launch_validate(first, p, 1, st);
+    if (vrc) return vrc;
     const Launch l = stage_launch<double>(p->mixed_kcode, p->stage1_cfg, 1);
     a.team_begin = p->d_tb1;
     a.nteams = p->stage1_teams;
@@ -616,11 +743,13 @@ int launch_stages_mixed(hmvm_plan* p, const void* x, void* y, void* tbuf, void* 
   if (p->n_red1 > 0) {
     HMVM_CUDA_TRY(launch_in_apply(first, hmvm_reduce_kernel<double, float>, (unsigned)((p->n_red1 + 255) / 256), 256,
                                   0, st, (const int4*)p->d_red1, p->n_red1, static_cast<const double*>(pbuf),
-                                  static_cast<float*>(tbuf)),
+                                  static_cast<float*>(tbuf), (const int*)p->d_err),
                   "V-stage reduction launch");
   }
   if (ev) cudaEventRecord(ev[2], st);
   {
+    int vrc = launch_validate(first, p, 2, st);
+    if (vrc) return vrc;
     const Launch l = stage_launch<double>(p->mixed_kcode, p->stage2_cfg, 2);
     a.team_begin = p->d_tb2;
     a.nteams = p->stage2_teams;
@@ -631,7 +760,7 @@ int launch_stages_mixed(hmvm_plan* p, const void* x, void* y, void* tbuf, void* 
   if (p->n_red2 > 0) {
     HMVM_CUDA_TRY(launch_in_apply(first, hmvm_reduce_kernel<double, double>, (unsigned)((p->n_red2 + 255) / 256), 256,
                                   0, st, (const int4*)p->d_red2, p->n_red2, static_cast<const double*>(pbuf),
-                                  static_cast<double*>(y)),
+                                  static_cast<double*>(y), (const int*)p->d_err),
                   "row-stage reduction launch");
   }
   if (ev) cudaEventRecord(ev[4], st);
@@ -663,6 +792,8 @@ int launch_stages(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, 
   bool first = true;
   if (ev) cudaEventRecord(ev[0], st);
   if (p->stage1_tiles > 0) {
+    int vrc = launch_validate(first, p, 1, st);
+    if (vrc) return vrc;
     const Launch l = stage_launch<T>(p->kernel, p->stage1_cfg, 1);
     a.team_begin = p->d_tb1;
     a.nteams = p->stage1_teams;
@@ -672,11 +803,13 @@ int launch_stages(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, 
   if (p->n_red1 > 0) {
     HMVM_CUDA_TRY(launch_in_apply(first, hmvm_reduce_kernel<T, T>, (unsigned)((p->n_red1 + 255) / 256), 256, 0, st,
                                   (const int4*)p->d_red1, p->n_red1, static_cast<const T*>(pbuf),
-                                  static_cast<T*>(tbuf)),
+                                  static_cast<T*>(tbuf), (const int*)p->d_err),
                   "V-stage reduction launch");
   }
   if (ev) cudaEventRecord(ev[2], st);
   {
+    int vrc = launch_validate(first, p, 2, st);
+    if (vrc) return vrc;
     const Launch l = stage_launch<T>(p->kernel, p->stage2_cfg, 2);
     a.team_begin = p->d_tb2;
     a.nteams = p->stage2_teams;
@@ -685,7 +818,8 @@ int launch_stages(hmvm_plan* p, const void* x, void* y, void* tbuf, void* pbuf, 
   if (ev) cudaEventRecord(ev[3], st);
   if (p->n_red2 > 0) {
     HMVM_CUDA_TRY(launch_in_apply(first, hmvm_reduce_kernel<T, T>, (unsigned)((p->n_red2 + 255) / 256), 256, 0, st,
-                                  (const int4*)p->d_red2, p->n_red2, static_cast<const T*>(pbuf), static_cast<T*>(y)),
+                                  (const int4*)p->d_red2, p->n_red2, static_cast<const T*>(pbuf), static_cast<T*>(y),
+                                  (const int*)p->d_err),
                   "row-stage reduction launch");
   }
   if (ev) cudaEventRecord(ev[4], st);
@@ -1264,14 +1398,17 @@ int hmvm_b200_plan_status(hmvm_plan* p) {
   HMVM_CUDA_TRY(cudaMemcpy(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost), "read status word");
   if (h == 0) return HMVM_OK;
   HMVM_CUDA_TRY(cudaMemset(p->d_err, 0, sizeof(int)), "clear status word");
-  return set_error(HMVM_EDEVICE, h == 1 ? "a kernel gave up waiting for its bulk copies"
-                                        : "a kernel found a stream region too large");
+  return set_error(HMVM_EDEVICE, h == 1   ? "a kernel gave up waiting for its bulk copies"
+                                 : h == 2 ? "a kernel found a stream region too large"
+                                 : h == 3 ? "a kernel found an index outside its buffers"
+                                          : "device bounds check: a plan descriptor points outside its buffer");
 }
 
 int hmvm_b200_plan_kernel_count(const hmvm_plan* p) {
   if (!p || p->nd == 0) return 0;
   if (p->tcw) return tcw_kernels_per_pass(p);
-  return (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1 + (p->n_red2 > 0) + (p->mixed ? 1 : 0);
+  return (p->stage1_tiles > 0) + (p->n_red1 > 0) + 1 + (p->n_red2 > 0) + (p->mixed ? 1 : 0) +
+         (kDeviceChecks ? (p->stage1_tiles > 0) + 1 : 0);  // checked builds: a validation per stage
 }
 
 int hmvm_b200_apply(hmvm_plan* p, const void* x, void* y, void* stream) {
@@ -1610,6 +1747,21 @@ int hmvm_b200_layout_build64(const hmvm_leaves64* lv, int32_t rowmat_is_float, c
   }
   *out = h;
   return HMVM_OK;
+}
+
+int hmvm_b200_plan_descriptors(const hmvm_plan* p, void** tiles_dev, int32_t* n_tiles, int32_t* stage1_tiles) {
+  if (!p || !tiles_dev || !n_tiles || !stage1_tiles) return set_error(HMVM_EINVAL, "NULL argument");
+  *tiles_dev = p->d_tiles;
+  *n_tiles = p->stage1_tiles + p->stage2_tiles;
+  *stage1_tiles = p->stage1_tiles;
+  return HMVM_OK;
+}
+
+int hmvm_b200_layout_validate(const hmvm_layout* h) {
+  if (!h) return set_error(HMVM_EINVAL, "NULL argument");
+  std::string msg;
+  const int rc = validate_layout(h->L, msg);
+  return rc ? set_error(rc, "layout check: " + msg) : HMVM_OK;
 }
 
 int hmvm_b200_layout_view(const hmvm_layout* h, hmvm_layout_view* v) {

@@ -39,6 +39,7 @@
 #include <cuda_runtime.h>
 
 #include "hmvm_b200.h"
+#include "validate.hpp"
 
 namespace hmvm {
 
@@ -92,6 +93,26 @@ __device__ __forceinline__ void griddep_launch_dependents() {
 }
 __device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// Device bounds checks (builds compiled with HMVM_DEVICE_CHECKS): before every
+// stage launch hmvm_validate_kernel checks the stage's descriptors against the
+// lengths of the buffers they index and sets the error word to
+// kErrDeviceCheck on a violation; each stage kernel first waits for its
+// predecessors and returns, touching nothing, while the error word is set.
+// Other builds compile none of it.
+#ifdef HMVM_DEVICE_CHECKS
+constexpr bool kDeviceChecks = true;
+#else
+constexpr bool kDeviceChecks = false;
+#endif
+constexpr int kErrDeviceCheck = 4;
+__device__ __forceinline__ bool checks_failed(const int* err) {
+  if constexpr (kDeviceChecks) {
+    griddep_wait();
+    return *reinterpret_cast<const volatile int*>(err) != 0;
+  }
+  return false;
+}
+
 template <typename T>
 __device__ __forceinline__ typename VecT<T>::V zero_vec() {
   typename VecT<T>::V v;
@@ -125,6 +146,7 @@ __global__ void __launch_bounds__(32 * WG * TPC) hmvm_tile_kernel(TileArgs a) {
   __shared__ T red[TPC][2][WG > 1 ? WG : 1][32];
   griddep_launch_dependents();
   griddep_wait();
+  if (checks_failed(a.err)) return;
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -332,6 +354,7 @@ __global__ void __launch_bounds__(32 * WPB, (stream_min_blocks<T, WPB, S, CHUNK,
   static_assert(ZCAP % 4 == 0, "input buffers hold whole vectors");
   extern __shared__ __align__(128) unsigned char smem[];
   griddep_launch_dependents();
+  if (checks_failed(a.err)) return;
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -488,15 +511,46 @@ __global__ void __launch_bounds__(32 * WPB, (stream_min_blocks<T, WPB, S, CHUNK,
 
 template <typename TP, typename TD>
 __global__ void hmvm_reduce_kernel(const int4* __restrict__ red, int n, const TP* __restrict__ p,
-                                   TD* __restrict__ dst) {
+                                   TD* __restrict__ dst, const int* __restrict__ err) {
   griddep_launch_dependents();
   griddep_wait();
+  if (checks_failed(err)) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int4 e = red[i];  // destination, first partial, parts, stride
     TP s = p[e.y];
     for (int c = 1; c < e.z; c++) s += p[e.y + c * e.w];
     dst[e.x] = (TD)s;
   }
+}
+
+// One stage's descriptors (HMVM_DEVICE_CHECKS builds): tiles [first, end)
+// with their segments, output slots and row scales, the stage's reduction
+// entries and its team ranges, checked against the lengths of the buffers they
+// index (validate.hpp).  The kernel waits for its predecessors before it ends,
+// so the stage launched after it stays ordered after them.
+struct ValidateArgs {
+  const hmvm_tile_desc* tiles;
+  const hmvm_seg_desc* segs;
+  const int32_t* out_idx;
+  const int32_t* team_begin;
+  const int4* red;
+  int32_t nteams, first, end, n_red;
+  LayoutCaps caps;
+  int32_t vec, elem, stage1;
+  int64_t zcap;
+  int* err;
+};
+__global__ void hmvm_validate_kernel(ValidateArgs v) {
+  griddep_launch_dependents();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  int rc = kCheckOk;
+  for (int k = v.first + i; k < v.end && rc == kCheckOk; k += stride)
+    rc = check_tile(v.tiles[k], v.segs, v.out_idx, v.caps, v.vec, v.elem, v.zcap, v.stage1 != 0);
+  for (int k = i; k < v.n_red && rc == kCheckOk; k += stride)
+    rc = check_red(reinterpret_cast<const int32_t*>(v.red + k), v.caps, v.stage1 != 0);
+  if (i == 0 && rc == kCheckOk) rc = check_teams(v.team_begin, v.nteams, v.first, v.end);
+  if (rc != kCheckOk) atomicCAS(v.err, 0, kErrDeviceCheck);
+  griddep_wait();
 }
 
 // x rounded to FP32 once per HMVM (the inputs of the FP32 / FP16 / FP8 segments).
@@ -650,6 +704,7 @@ __global__ void __launch_bounds__(32 * WPB, (mixed_min_blocks<WPB, S, CHUNK, ZBY
   static_assert(mixed_batch<kF32, S, CHUNK, VST, WIDE>() * 32 * 16 <= (S - 1) * CHUNK, "ring too small for one batch");
   extern __shared__ __align__(128) unsigned char smem[];
   griddep_launch_dependents();
+  if (checks_failed(a.err)) return;
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;

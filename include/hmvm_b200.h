@@ -473,6 +473,26 @@ int hmvm_b200_layout_build_d(const hmvm_matrix2_d *mat2, const hmvm_plan_opts *o
                              hmvm_layout **layout);
 int hmvm_b200_layout_build64(const hmvm_leaves64 *lv, int32_t rowmat_is_float, const hmvm_plan_opts *opts,
                              int32_t num_sms, hmvm_layout **layout);
+/* Bounds checks of every descriptor of a single-vector layout against the
+ * buffers it indexes: each item's data-stream range, segment range, rows, the
+ * x or t columns of its segments, its padded inputs against the stage kernel's
+ * input buffer, the y / t / partial-sum rows it writes, its t slots and row
+ * scales, every reduction entry, and the team ranges.  HMVM_OK, or HMVM_ERANGE
+ * with a message naming the first failing item.  Wide tensor-core layouts
+ * (view.tcw = 1) are not described by these checks and return HMVM_OK.  The
+ * library built with HMVM_DEVICE_CHECKS (libhmvm_b200_checked.so) runs the same
+ * checks at plan creation and on the device before every single-vector stage
+ * launch: a violation sets the status word (hmvm_b200_plan_status returns
+ * HMVM_EDEVICE) and the stage kernels then touch no memory.  The reference
+ * checks none of its offsets (hmvm_seq.cpp, hmvm_cuda2.cu index the leaf
+ * arrays directly). */
+int hmvm_b200_layout_validate(const hmvm_layout *layout);
+/* The device address of a plan's item descriptors (hmvm_tile_desc[n_tiles],
+ * stage-1 items first), for inspection and for tests of the device checks;
+ * a caller that changes them owns the consequences (the HMVM_DEVICE_CHECKS
+ * build reports descriptors that leave their buffers instead of following
+ * them). */
+int hmvm_b200_plan_descriptors(const hmvm_plan *plan, void **tiles_dev, int32_t *n_tiles, int32_t *stage1_tiles);
 int hmvm_b200_layout_view(const hmvm_layout *layout, hmvm_layout_view *view);
 void hmvm_b200_layout_destroy(hmvm_layout *layout);
 
