@@ -100,7 +100,7 @@ def test_reference_sample_matrix():
     assert np.array_equal(Y["sample/y_seq1_d_sin"], Y["sample/y_seq2_d_sin"])  # AoS == SoA in the reference
     xf = np.sin(np.arange(1, hm.nd + 1, dtype=np.float32))
     assert np.array_equal(oracle_hmvm(hm.to_float(), xf), Y["sample/y_seq2_f_sin"])
-    # structure the survey recorded for the shipped sample
+    # the shipped sample's structure: 210 low-rank and 1216 dense leaves, ranks 10..31
     lr = hm.ltmtx == 1
     assert int(lr.sum()) == 210 and int((~lr).sum()) == 1216
     assert hm.kt[lr].min() == 10 and hm.kt[lr].max() == 31
